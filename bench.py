@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark: Newton-step solves/s (assemble -> factor -> solve to ||b-Hx||/||b|| <= 1e-10).
+
+One "step" = one Newton solve of the configured workload: on-device element
+assembly (K1), numeric factorization (K2-K5) and the multi-RHS solve (K6) with
+FP64 refinement (K7 residuals) for the FP32 form. `value` times that with the
+element Hessians and right-hand sides already resident in HBM; `e2e` times the
+same step through the C ABI with host (pinned) buffers, copies included.
+
+Multi-GPU: the path does not shard (one sparse factorization per step), so
+`--gpus N` runs N independent replicas (one per rank, no collective on the data
+path); value = solves of all ranks / max-over-ranks device time.
+
+`--impl reference` times the CPU restatement of the reference path (the oracle
+port: FP64 supernodal multifrontal factor + solve with OpenBLAS dense kernels,
+all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Newton solves/s at 1e-10 residual: FP32+refine & learned PCG vs FP64 plain"
+UNIT = "solves/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--config", type=int, default=2)
+    p.add_argument("--k", type=int, default=None, help="override the cube side (smaller runs)")
+    p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison arm")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--cpu-budget", type=float, default=2.5e11, help="flops of the CPU factorization sample")
+    return p.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- GPU arm
+def run_b200(args, rank, world, local, dist):
+    import torch
+    from meshfemsparse_b200 import B200Factorizer, _lib, workloads
+
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    t0 = time.time()
+    wl = workloads.build(args.config, k=args.k, device=dev)
+    t_gen = time.time() - t0
+    stream = torch.cuda.current_stream()
+    lib = _lib.load()
+    n_full = wl.n_full
+    nrhs = wl.nrhs
+
+    def make(single):
+        f = B200Factorizer(single, refine=single, stream=stream.cuda_stream, device=local)
+        t = time.time()
+        f.factorizeSymbolic(wl.H, wl.pins)
+        f.setElements(wl.tets)
+        return f, time.time() - t
+
+    f32, t_sym = make(True)
+    Ke_dev = torch.from_numpy(wl.Ke.reshape(-1)).to(dev)
+    B_dev = torch.from_numpy(np.ascontiguousarray(wl.rhs.T)).to(dev)        # column-major n_full x nrhs
+    X_dev = torch.empty_like(B_dev)
+    D = _lib.MFS_DEVICE_POINTERS
+
+    def step(f, Ke_ptr, B_ptr, X_ptr, flags):
+        _lib.check(lib.mfs_assemble(f._h, Ke_ptr, None, flags), f._h, "assemble")
+        _lib.check(lib.mfs_numeric(f._h, None, None, 0.0, 0), f._h, "numeric")
+        _lib.check(lib.mfs_solve(f._h, B_ptr, X_ptr, nrhs, n_full, _lib.MFS_SOLVE_FULL | flags), f._h, "solve")
+
+    def timed(f, K, W, Ke_ptr, B_ptr, X_ptr, flags, sample_clocks=False):
+        for _ in range(W):
+            step(f, Ke_ptr, B_ptr, X_ptr, flags)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        l0 = f.stats()["kernel_launches"]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            step(f, Ke_ptr, B_ptr, X_ptr, flags)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = f.stats()["kernel_launches"] - l0
+        clocks = sampler.stop() if sampler else None
+        total = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([total], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        if dist:
+            dist.barrier()
+        return total, launches, clocks
+
+    pK, pB, pX = C.c_void_p(Ke_dev.data_ptr()), C.c_void_p(B_dev.data_ptr()), C.c_void_p(X_dev.data_ptr())
+    tot32, launches, clocks = timed(f32, args.steps, args.warmup, pK, pB, pX, D, sample_clocks=True)
+    st32 = f32.stats()
+    ms32 = tot32 / args.steps
+
+    # residual of the timed FP32+refine result, checked in FP64 on the device
+    def residual(f, X):
+        Y = torch.empty_like(X)
+        _lib.check(lib.mfs_apply(f._h, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()), nrhs, n_full,
+                                 _lib.MFS_SOLVE_FULL | D), f._h, "apply")
+        keep = torch.ones(n_full, dtype=torch.bool, device=dev)
+        keep[torch.from_numpy(wl.pins).to(dev)] = False
+        R = (B_dev - Y)[:, keep]
+        return float((R.norm(dim=1) / B_dev[:, keep].norm(dim=1)).max().item())
+
+    res32 = residual(f32, X_dev)
+
+    # e2e through host (pinned) buffers
+    Ke_h = torch.from_numpy(wl.Ke.reshape(-1)).pin_memory()
+    B_h = torch.from_numpy(np.ascontiguousarray(wl.rhs.T)).pin_memory()
+    X_h = torch.empty_like(B_h).pin_memory()
+    K_e2e = max(1, min(args.steps, 3))
+    tot_e2e, _, _ = timed(f32, K_e2e, 1, C.c_void_p(Ke_h.data_ptr()), C.c_void_p(B_h.data_ptr()),
+                          C.c_void_p(X_h.data_ptr()), 0)
+    e2e_ms = tot_e2e / K_e2e
+
+    out64 = {}
+    if not args.no_fp64:
+        f64, _ = make(False)
+        X64 = torch.empty_like(B_dev)
+        K64 = max(1, min(args.steps, 3))
+        tot64, _, _ = timed(f64, K64, 1, pK, pB, C.c_void_p(X64.data_ptr()), D)
+        ms64 = tot64 / K64
+        st64 = f64.stats()
+        out64 = {"fp64_plain_solves_per_s": world * 1000.0 / ms64, "fp64_plain_ms_per_step": ms64,
+                 "fp64_factor_ms": st64["factor_ms"], "fp64_solve_ms": st64["solve_ms"],
+                 "fp64_residual": residual(f64, X64),
+                 "speedup_fp32_refine_vs_fp64_plain": ms64 / ms32}
+        del f64
+
+    peaks, peak_kind = measured_peaks()
+    flops = f32.getFlopEstimate()
+    achieved = flops / (st32["factor_ms"] * 1e-3) / 1e12
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops_sustained"], "unit": "TFLOP/s",
+                "frac": achieved / peaks["bf16_tflops_sustained"], "traffic": None,
+                "kernel": "numeric factorization (K2-K5 sequence), FP32 storage",
+                "note": f"symbolic flop count / factorization device time; peak = {peak_kind} sustained bf16 "
+                        "(TF32 dense peak is half of it)"}
+
+    result = {
+        "metric": METRIC, "value": world * 1000.0 * 1.0 / ms32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 factor / f64 refine", "data": "synthetic",
+        "config": {"workload": f"config{args.config}:{wl.name}", "n_free_dofs": f32.n_reduced(),
+                   "tets": int(wl.tets.shape[0]), "nrhs": nrhs, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (element Hessians %.2f GB)" % (wl.Ke.nbytes / 1e9),
+                   **wl.info},
+        "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT,
+                "h2d_bytes_per_step": int(wl.Ke.nbytes + wl.rhs.nbytes), "d2h_bytes_per_step": int(wl.rhs.nbytes)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "roofline": roofline,
+        "residual": res32,
+        "refine_iterations": st32["refine_iterations"],
+        "factor_ms": st32["factor_ms"], "solve_ms": st32["solve_ms"], "assemble_ms": st32["assemble_ms"],
+        "factor_nnz": f32.getFactorNNZ(), "flops": flops, "symbolic_s": t_sym, "input_gen_s": t_gen,
+        **out64,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        result["cpu_baseline"] = cpu_baseline(wl, f32, args)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+# -------------------------------------------------------------- CPU legs
+def cpu_baseline(wl, f, args):
+    """Oracle port (FP64 multifrontal + OpenBLAS, all host threads) on a bounded sample:
+    full CPU assembly and value injection, a postordered subtree of the assembly tree
+    for the factorization and solve, extrapolated to the whole tree by flops / nnz."""
+    from oracle import pyoracle
+    pyoracle.load_blas()
+    threads = int(pyoracle.load().orc_max_threads())
+    sn = f.supernodes()
+    plan = f.conversionPlan()
+    w, d, fr, pan, col0 = pyoracle.panel_layout(sn)
+    t = time.time()
+    Ax = pyoracle.assemble(wl.H.numBlocks, wl.H.Ap, wl.H.Ai, wl.tets, wl.Ke)
+    t_asm = time.time() - t
+    t = time.time()
+    vals = pyoracle.inject(plan["entries"], sn["vb"], 3, Ax, int(pan[-1]))
+    t_inj = time.time() - t
+    flops_sn = w ** 3 / 3 + w * w * d + w * d * d
+    nnz_sn = w * (w + 1) / 2 + w * d
+    nsn = len(w)
+    # subtree sizes / flops in postorder
+    desc = np.ones(nsn, dtype=np.int64)
+    sub_fl = flops_sn.astype(float).copy()
+    sub_nnz = nnz_sn.astype(float).copy()
+    parent = sn["parent"]
+    for s in range(nsn):
+        p = parent[s]
+        if p >= 0:
+            desc[p] += desc[s]
+            sub_fl[p] += sub_fl[s]
+            sub_nnz[p] += sub_nnz[s]
+    total_fl, total_nnz = float(flops_sn.sum()), float(nnz_sn.sum())
+    if total_fl <= args.cpu_budget:
+        root, lo = nsn - 1, 0
+        sample_fl, sample_nnz = total_fl, total_nnz
+        pyoracle.set_range(0, -1)
+        desc_txt = "whole factorization"
+    else:
+        cand = np.nonzero(sub_fl <= args.cpu_budget)[0]
+        root = int(cand[np.argmax(sub_fl[cand])])
+        lo = root - int(desc[root]) + 1
+        sample_fl, sample_nnz = float(sub_fl[root]), float(sub_nnz[root])
+        pyoracle.set_range(lo, root)
+        desc_txt = f"subtree of supernodes [{lo},{root}] ({100 * sample_fl / total_fl:.1f}% of the flops)"
+    t = time.time()
+    fail = pyoracle.mf_factor(sn, vals, threads)
+    t_fac = time.time() - t
+    B = np.zeros((f.n_reduced(), wl.nrhs))
+    B[:] = 1.0
+    t = time.time()
+    pyoracle.mf_solve(sn, vals, B, threads)
+    t_sol = time.time() - t
+    pyoracle.set_range(0, -1)
+    est = t_asm + t_inj + t_fac * total_fl / sample_fl + t_sol * total_nnz / sample_nnz
+    return {"value": 1.0 / est, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"CPU assembly + injection of the full workload, {desc_txt} factored and solved "
+                      f"(nrhs={wl.nrhs}) in FP64 with OpenBLAS, scaled to the full tree by flops/nnz; "
+                      f"measured {t_asm:.2f}s asm, {t_inj:.2f}s inject, {t_fac:.2f}s factor, {t_sol:.2f}s solve",
+            "pivot_failure": int(fail)}
+
+
+def run_reference(args, rank, world, dist):
+    if rank != 0:
+        return
+    from meshfemsparse_b200 import B200Factorizer, workloads
+    wl = workloads.build(args.config, k=args.k, device=None)
+    f = B200Factorizer(False, device=-1)        # host-only analysis (ordering, supernodes, plan)
+    f.factorizeSymbolic(wl.H, wl.pins)
+    samples = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(wl, f, args)
+        if i >= args.warmup:
+            samples.append(r)
+    value = float(np.mean([s["value"] for s in samples]))
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"config{args.config}:{wl.name}", "nrhs": wl.nrhs, **wl.info},
+           "cpu_baseline": {**samples[-1], "value": value},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local, dist = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world, dist)
+        else:
+            run_b200(args, rank, world, local, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

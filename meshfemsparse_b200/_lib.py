@@ -1,0 +1,150 @@
+"""ctypes binding of the in-tree C ABI (include/mfs_b200.h).
+
+The shared library is required: importing a GPU entry point without it raises
+immediately instead of silently falling back to CPU code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libmfs_b200.so"
+
+MFS_OK, MFS_NOT_POSDEF, MFS_INVALID_ARG, MFS_SIZE_MISMATCH, MFS_NO_FACTOR, MFS_OOM, MFS_TIMEOUT, \
+    MFS_CUDA_ERROR, MFS_INTERNAL = range(9)
+MFS_PREC_FP64, MFS_PREC_FP32 = 0, 1
+MFS_ORDER_ND, MFS_ORDER_NATIVE, MFS_ORDER_MD, MFS_ORDER_USER = 0, 1, 2, 3
+MFS_SOLVE_FULL, MFS_SOLVE_REDUCED, MFS_SOLVE_REDUCED_PERMUTED = 0, 1, 2
+MFS_DEVICE_POINTERS = 16
+
+EXPORTED = [
+    "mfs_default_options", "mfs_create", "mfs_destroy", "mfs_last_error", "mfs_build_pattern", "mfs_symbolic",
+    "mfs_numeric", "mfs_solve", "mfs_assembly_setup", "mfs_assemble", "mfs_apply", "mfs_info",
+    "mfs_inverse_permutation", "mfs_nd_ordering", "mfs_supernodes", "mfs_conversion_plan", "mfs_factor_values",
+    "mfs_stash", "mfs_swap_stash", "mfs_clear_stash", "mfs_has_stash", "mfs_clear_factors", "mfs_get_stats",
+    "mfs_set_options",
+]
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("precision", C.c_int32), ("ordering", C.c_int32), ("relax", C.c_int32), ("device", C.c_int32),
+        ("relax_zeros", C.c_int64), ("relax_ratio", C.c_double), ("nd_leaf_size", C.c_int64),
+        ("seed", C.c_uint64), ("stream", C.c_void_p), ("small_front_max", C.c_int32), ("refine", C.c_int32),
+        ("refine_tol", C.c_double), ("refine_maxit", C.c_int32), ("use_graphs", C.c_int32),
+        ("tensor_cores", C.c_int32), ("reserved", C.c_int32 * 7),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("factor_ms", C.c_double), ("solve_ms", C.c_double), ("assemble_ms", C.c_double),
+        ("refine_iterations", C.c_int32), ("failed_column", C.c_int32), ("residual", C.c_double),
+        ("device_bytes", C.c_int64), ("num_levels", C.c_int32), ("num_large", C.c_int32),
+        ("kernel_launches", C.c_int64),
+    ]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libmfs_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m meshfemsparse_b200.build` first")
+    lib = C.CDLL(str(LIB_PATH))
+    P = C.c_void_p
+    i64p = C.POINTER(C.c_int64)
+    lib.mfs_default_options.argtypes = [C.POINTER(Options)]
+    lib.mfs_create.argtypes = [C.POINTER(P), C.POINTER(Options)]
+    lib.mfs_set_options.argtypes = [P, C.POINTER(Options)]
+    lib.mfs_destroy.argtypes = [P]
+    lib.mfs_last_error.argtypes = [P, C.c_char_p, C.c_size_t]
+    lib.mfs_build_pattern.argtypes = [C.c_int64, C.c_int64, C.c_int32, i64p, i64p, i64p, i64p]
+    lib.mfs_symbolic.argtypes = [P, C.c_int64, i64p, i64p, C.c_int32, i64p, C.c_int64, i64p, i64p, C.c_int64]
+    lib.mfs_numeric.argtypes = [P, P, P, C.c_double, C.c_int32]
+    lib.mfs_solve.argtypes = [P, P, P, C.c_int64, C.c_int64, C.c_int32]
+    lib.mfs_assembly_setup.argtypes = [P, C.c_int64, i64p]
+    lib.mfs_assemble.argtypes = [P, P, P, C.c_int32]
+    lib.mfs_apply.argtypes = [P, P, P, C.c_int64, C.c_int64, C.c_int32]
+    lib.mfs_info.argtypes = [P, i64p, i64p, i64p, C.POINTER(C.c_double), i64p, C.POINTER(C.c_int32)]
+    lib.mfs_inverse_permutation.argtypes = [P, i64p]
+    lib.mfs_nd_ordering.argtypes = [P, i64p, i64p, i64p, i64p]
+    lib.mfs_supernodes.argtypes = [P, i64p, i64p, C.POINTER(C.c_int32), i64p, i64p, i64p, i64p, i64p]
+    lib.mfs_conversion_plan.argtypes = [P, i64p, i64p, i64p, i64p]
+    lib.mfs_factor_values.argtypes = [P, i64p, P]
+    for name in ("mfs_stash", "mfs_swap_stash", "mfs_clear_stash", "mfs_clear_factors"):
+        getattr(lib, name).argtypes = [P]
+    lib.mfs_has_stash.argtypes = [P, C.POINTER(C.c_int32)]
+    lib.mfs_get_stats.argtypes = [P, C.POINTER(Stats)]
+    for name in EXPORTED:
+        getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def i64ptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.int64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def dptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float64
+    return C.c_void_p(a.ctypes.data)
+
+
+class MFSError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(msg)
+        self.status = status
+
+
+def check(status: int, handle=None, what: str = ""):
+    """Raise like the reference: invalid_argument -> ValueError, everything else RuntimeError."""
+    if status == MFS_OK:
+        return
+    msg = what
+    if handle is not None:
+        buf = C.create_string_buffer(1024)
+        load().mfs_last_error(handle, buf, 1024)
+        if buf.value:
+            msg = buf.value.decode(errors="replace")
+    if status == MFS_INVALID_ARG:
+        raise ValueError(msg or "invalid argument")
+    raise MFSError(status, msg or f"mfs status {status}")
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    load().mfs_default_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def build_pattern(nvars: int, conn: np.ndarray):
+    """SystemAssembler::blockSparsityPattern through the C ABI: returns (Ap, Ai)."""
+    lib = load()
+    conn = np.ascontiguousarray(conn, dtype=np.int64)
+    nelem, npe = conn.shape
+    Ap = np.zeros(nvars + 1, dtype=np.int64)
+    nnz = C.c_int64(0)
+    check(lib.mfs_build_pattern(nvars, nelem, npe, i64ptr(conn), i64ptr(Ap), None, C.byref(nnz)), what="pattern")
+    Ai = np.zeros(nnz.value, dtype=np.int64)
+    check(lib.mfs_build_pattern(nvars, nelem, npe, i64ptr(conn), i64ptr(Ap), i64ptr(Ai), C.byref(nnz)),
+          what="pattern")
+    return Ap, Ai
+
+
+def library_present() -> bool:
+    return LIB_PATH.exists() and os.access(LIB_PATH, os.R_OK)

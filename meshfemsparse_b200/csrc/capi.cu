@@ -1,0 +1,1121 @@
+// C ABI (include/mfs_b200.h): handle lifetime, symbolic upload, the level
+// schedule of the numeric factorization, solves, FP64 refinement, element
+// assembly and the factor stash. Host logic only; kernels live in
+// kernels_factor.cu / kernels_solve.cu.
+#include "../../include/mfs_b200.h"
+#include "device.h"
+#include "host_symbolic.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace mfs {
+
+long long g_kernel_launches = 0;
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct StatusError : std::runtime_error {
+    mfs_status status;
+    StatusError(mfs_status s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+#define MFS_CUDA(call)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t _e = (call);                                                                         \
+        if (_e != cudaSuccess)                                                                           \
+            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(_e));                         \
+    } while (0)
+
+#define MFS_LAUNCHED() MFS_CUDA(cudaGetLastError())
+
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void ensure(size_t count) {
+        if (count <= n && p) return;
+        release();
+        size_t c = std::max<size_t>(count, 1);
+        cudaError_t e = cudaMalloc(&p, c * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            throw StatusError(MFS_OOM, std::string("cudaMalloc of ") + std::to_string(c * sizeof(T)) +
+                                           " bytes failed: " + cudaGetErrorString(e));
+        }
+        n = c;
+    }
+    template <typename U>
+    void upload(const std::vector<U> &v, cudaStream_t st) {
+        ensure(v.size());
+        if (v.empty()) return;
+        std::vector<T> tmp(v.begin(), v.end());
+        MFS_CUDA(cudaMemcpyAsync(p, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        MFS_CUDA(cudaStreamSynchronize(st));
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+constexpr int kNB = 64;   // column block of the tiled large-front factorization
+
+struct LevelPlan {
+    int small_off = 0, small_count = 0, small_max_front = 0;
+    int all_off = 0, all_count = 0, all_max_front = 0;
+    int large_count = 0;
+    int asm_off = 0, asm_n = 0, asm_tiles = 0;
+    struct Step {
+        int potrf_off, potrf_n, potrf_maxnb;
+        int trsm_off, trsm_n, trsm_tiles, trsm_maxnb;
+        int gemm_off, gemm_n, gemm_tiles;
+    };
+    std::vector<Step> steps;
+    int syrk_off = 0, syrk_n = 0, syrk_tiles = 0;
+};
+
+struct DevSym {
+    std::shared_ptr<Symbolic> S;
+    DBuf<int32_t> w, d, f, col0, child_ptr, child_list, struct_rows, rel, small_list, all_list;
+    DBuf<int64_t> pan_off, upd_off, sol_off, struct_ptr, diag_off;
+    DBuf<PlanEntryDev> plan;
+    DBuf<AssembleTask> asm_tasks;
+    DBuf<PotrfTask> potrf_tasks;
+    DBuf<TrsmTask> trsm_tasks;
+    DBuf<GemmTask> gemm_tasks;
+    DBuf<int64_t> spmv_ptr, spmv_src;
+    DBuf<int32_t> spmv_col, spmv_flag;
+    DBuf<int64_t> prrfr, sperm;
+    std::vector<LevelPlan> levels;
+    SnDev sd{};
+    int64_t ax_len = 0;
+    std::vector<int64_t> Ap_full, Ai_full;   // caller's pattern (for the element slot map)
+    int num_large = 0;
+    size_t bytes() const {
+        return w.bytes() * 4 + col0.bytes() + child_ptr.bytes() + child_list.bytes() + struct_rows.bytes() +
+               rel.bytes() + small_list.bytes() + all_list.bytes() + pan_off.bytes() + upd_off.bytes() +
+               sol_off.bytes() + struct_ptr.bytes() + diag_off.bytes() + plan.bytes() + asm_tasks.bytes() +
+               potrf_tasks.bytes() + trsm_tasks.bytes() + gemm_tasks.bytes() + spmv_ptr.bytes() +
+               spmv_src.bytes() + spmv_col.bytes() + spmv_flag.bytes() + prrfr.bytes() + sperm.bytes();
+    }
+};
+
+struct State {
+    std::shared_ptr<DevSym> sym;
+    std::shared_ptr<DBuf<double>> f64;
+    std::shared_ptr<DBuf<float>> f32;
+    std::shared_ptr<DBuf<double>> ax, bx;   // values the numeric factor was computed from
+    int type = 0;   // 0 none, 1 symbolic, 2 numeric
+    double sigma = 0.0;
+};
+
+}  // namespace mfs
+
+using namespace mfs;
+
+struct mfs_handle {
+    mfs_options opt{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    State cur, stash;
+    bool has_stash = false;
+    DBuf<double> upd64;
+    DBuf<float> upd32;
+    DBuf<double> sol;
+    std::shared_ptr<DBuf<double>> asm_ax;   // output of the last mfs_assemble (device resident)
+    DBuf<double> rhs, work_r, work_z, work_p, work_ap, work_x, work_s, io;
+    DBuf<double> partials, dots;
+    DBuf<int> active;
+    DBuf<int> fail;
+    int *fail_host = nullptr;
+    double *dots_host = nullptr;
+    // assembly
+    DBuf<int64_t> slot_ptr, contrib;
+    int64_t nslots = 0, nelem = 0;
+    DBuf<double> ke;
+    std::string err;
+    mfs_stats stats{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+void set_device(mfs_handle *h) {
+    if (h->opt.device < 0) throw StatusError(MFS_INVALID_ARG, "analysis-only handle (device -1) has no GPU state");
+    MFS_CUDA(cudaSetDevice(h->opt.device));
+}
+
+template <typename F>
+mfs_status guarded(mfs_handle *h, F &&fn) {
+    try {
+        fn();
+        if (h) h->err.clear();
+        return MFS_OK;
+    } catch (const StatusError &e) {
+        if (h) h->err = e.what();
+        return e.status;
+    } catch (const CudaError &e) {
+        if (h) h->err = e.what();
+        return MFS_CUDA_ERROR;
+    } catch (const std::bad_alloc &e) {
+        if (h) h->err = "host allocation failed";
+        return MFS_OOM;
+    } catch (const std::exception &e) {
+        if (h) h->err = e.what();
+        return MFS_INTERNAL;
+    }
+}
+
+int small_front_limit(const mfs_handle *h) {
+    if (h->opt.small_front_max > 0) return h->opt.small_front_max;
+    return h->opt.precision == MFS_PREC_FP32 ? 160 : 128;
+}
+
+std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic> Sp) {
+    const Symbolic &S = *Sp;
+    cudaStream_t st = h->stream;
+    auto ds = std::make_shared<DevSym>();
+    ds->S = Sp;
+    const idx nsn = S.nsn;
+    std::vector<int32_t> col0(nsn), w32(nsn), d32(nsn), f32v(nsn);
+    for (idx s = 0; s < nsn; ++s) {
+        col0[s] = int32_t(S.vb * S.sn_start[s]);
+        w32[s] = int32_t(S.w[s]);
+        d32[s] = int32_t(S.d[s]);
+        f32v[s] = int32_t(S.f[s]);
+    }
+    ds->w.upload(w32, st);
+    ds->d.upload(d32, st);
+    ds->f.upload(f32v, st);
+    ds->col0.upload(col0, st);
+    ds->child_ptr.upload(S.child_ptr, st);
+    ds->child_list.upload(S.child_list, st);
+    ds->struct_rows.upload(S.struct_rows, st);
+    ds->rel.upload(S.rel, st);
+    ds->pan_off.upload(S.pan_off, st);
+    ds->upd_off.upload(S.upd_off, st);
+    ds->sol_off.upload(S.sol_off, st);
+    ds->struct_ptr.upload(S.struct_ptr, st);
+    std::vector<int64_t> diag(S.n);
+    for (idx s = 0; s < nsn; ++s)
+        for (idx k = 0; k < S.w[s]; ++k) diag[S.vb * S.sn_start[s] + k] = S.pan_off[s] + k * S.f[s] + k;
+    ds->diag_off.upload(diag, st);
+    {
+        std::vector<PlanEntryDev> pl(S.plan.size());
+        for (size_t k = 0; k < pl.size(); ++k) {
+            pl[k].dst = S.plan[k].dst;
+            pl[k].src = S.plan[k].src;
+            pl[k].ld = S.plan[k].ld;
+            pl[k].flags = S.plan[k].flags;
+        }
+        ds->plan.ensure(pl.size());
+        if (!pl.empty())
+            MFS_CUDA(cudaMemcpyAsync(ds->plan.p, pl.data(), pl.size() * sizeof(PlanEntryDev),
+                                     cudaMemcpyHostToDevice, st));
+        MFS_CUDA(cudaStreamSynchronize(st));
+    }
+    ds->spmv_ptr.upload(S.spmv_ptr, st);
+    ds->spmv_src.upload(S.spmv_src, st);
+    ds->spmv_col.upload(S.spmv_col, st);
+    ds->spmv_flag.upload(S.spmv_flag, st);
+    ds->prrfr.upload(S.permuted_reduced_row_for_row, st);
+    ds->sperm.upload(S.scalar_perm, st);
+
+    // level schedule and tiled task lists
+    const int small_max = small_front_limit(h);
+    std::vector<int32_t> small_list, all_list;
+    std::vector<AssembleTask> asm_tasks;
+    std::vector<PotrfTask> potrf_tasks;
+    std::vector<TrsmTask> trsm_tasks;
+    std::vector<GemmTask> gemm_tasks;
+    ds->levels.resize(S.nlevels);
+    ds->num_large = 0;
+    for (idx l = 0; l < S.nlevels; ++l) {
+        LevelPlan &L = ds->levels[l];
+        std::vector<idx> large;
+        L.small_off = int(small_list.size());
+        L.all_off = int(all_list.size());
+        for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
+            idx s = S.level_list[k];
+            all_list.push_back(int32_t(s));
+            L.all_max_front = std::max<int>(L.all_max_front, int(S.f[s]));
+            if (S.f[s] <= small_max) {
+                small_list.push_back(int32_t(s));
+                L.small_max_front = std::max<int>(L.small_max_front, int(S.f[s]));
+            } else large.push_back(s);
+        }
+        L.small_count = int(small_list.size()) - L.small_off;
+        L.all_count = int(all_list.size()) - L.all_off;
+        L.large_count = int(large.size());
+        ds->num_large += L.large_count;
+        if (large.empty()) continue;
+        L.asm_off = int(asm_tasks.size());
+        int base = 0;
+        idx maxw = 0;
+        for (idx s : large) {
+            asm_tasks.push_back({int32_t(s), base});
+            base += int((S.f[s] + kAsmCols - 1) / kAsmCols);
+            maxw = std::max(maxw, S.w[s]);
+        }
+        L.asm_n = int(large.size());
+        L.asm_tiles = base;
+        for (idx kb = 0; kb < maxw; kb += kNB) {
+            LevelPlan::Step sp{};
+            sp.potrf_off = int(potrf_tasks.size());
+            sp.trsm_off = int(trsm_tasks.size());
+            sp.gemm_off = int(gemm_tasks.size());
+            int tb = 0, gb = 0;
+            for (idx s : large) {
+                const idx w = S.w[s], f = S.f[s], pan = S.pan_off[s];
+                if (w <= kb) continue;
+                const int nb = int(std::min<idx>(kNB, w - kb));
+                potrf_tasks.push_back({pan + kb * f + kb, int32_t(f), nb, int32_t(col0[s] + kb), 0});
+                sp.potrf_maxnb = std::max(sp.potrf_maxnb, nb);
+                const idx m = f - kb - nb;
+                if (m > 0) {
+                    TrsmTask t{};
+                    t.l_off = pan + kb * f + kb;
+                    t.b_off = pan + kb * f + kb + nb;
+                    t.ld = int32_t(f);
+                    t.nb = nb;
+                    t.m = int32_t(m);
+                    t.tile_base = tb;
+                    tb += int((m + kTrsmRows - 1) / kTrsmRows);
+                    trsm_tasks.push_back(t);
+                    sp.trsm_maxnb = std::max(sp.trsm_maxnb, nb);
+                }
+                const idx n = w - kb - nb;
+                if (n > 0) {
+                    GemmTask g{};
+                    g.a_off = pan + kb * f + kb + nb;
+                    g.b_off = g.a_off;
+                    g.c_off = pan + (kb + nb) * f + kb + nb;
+                    g.lda = int32_t(f);
+                    g.ldc = int32_t(f);
+                    g.m = int32_t(m);
+                    g.n = int32_t(n);
+                    g.k = nb;
+                    g.tiles_m = int32_t((m + kGemmTile - 1) / kGemmTile);
+                    g.tiles_n = int32_t((n + kGemmTile - 1) / kGemmTile);
+                    g.tile_base = gb;
+                    g.lower = 1;
+                    gb += g.tiles_m * g.tiles_n;
+                    gemm_tasks.push_back(g);
+                }
+            }
+            sp.potrf_n = int(potrf_tasks.size()) - sp.potrf_off;
+            sp.trsm_n = int(trsm_tasks.size()) - sp.trsm_off;
+            sp.trsm_tiles = tb;
+            sp.gemm_n = int(gemm_tasks.size()) - sp.gemm_off;
+            sp.gemm_tiles = gb;
+            L.steps.push_back(sp);
+        }
+        L.syrk_off = int(gemm_tasks.size());
+        int sb = 0;
+        for (idx s : large) {
+            if (S.d[s] == 0 || S.upd_off[s] < 0) continue;
+            GemmTask g{};
+            g.a_off = S.pan_off[s] + S.w[s];
+            g.b_off = g.a_off;
+            g.c_off = S.upd_off[s];
+            g.lda = int32_t(S.f[s]);
+            g.ldc = int32_t(S.d[s]);
+            g.m = g.n = int32_t(S.d[s]);
+            g.k = int32_t(S.w[s]);
+            g.tiles_m = g.tiles_n = int32_t((S.d[s] + kGemmTile - 1) / kGemmTile);
+            g.tile_base = sb;
+            g.lower = 1;
+            sb += g.tiles_m * g.tiles_n;
+            gemm_tasks.push_back(g);
+        }
+        L.syrk_n = int(gemm_tasks.size()) - L.syrk_off;
+        L.syrk_tiles = sb;
+    }
+    ds->small_list.upload(small_list, st);
+    ds->all_list.upload(all_list, st);
+    auto up = [&](auto &buf, const auto &vec) {
+        buf.ensure(vec.size());
+        if (!vec.empty())
+            MFS_CUDA(cudaMemcpyAsync(buf.p, vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice, st));
+    };
+    up(ds->asm_tasks, asm_tasks);
+    up(ds->potrf_tasks, potrf_tasks);
+    up(ds->trsm_tasks, trsm_tasks);
+    up(ds->gemm_tasks, gemm_tasks);
+    MFS_CUDA(cudaStreamSynchronize(st));
+
+    SnDev &sd = ds->sd;
+    sd.w = ds->w.p;
+    sd.d = ds->d.p;
+    sd.f = ds->f.p;
+    sd.col0 = ds->col0.p;
+    sd.pan_off = ds->pan_off.p;
+    sd.upd_off = ds->upd_off.p;
+    sd.sol_off = ds->sol_off.p;
+    sd.child_ptr = ds->child_ptr.p;
+    sd.child_list = ds->child_list.p;
+    sd.struct_ptr = ds->struct_ptr.p;
+    sd.struct_rows = ds->struct_rows.p;
+    sd.rel = ds->rel.p;
+    sd.vb = S.vb;
+    return ds;
+}
+
+template <typename T>
+void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, const double *Ax, const double *Bx, double sigma) {
+    const Symbolic &S = *ds.S;
+    cudaStream_t st = h->stream;
+    launch_zero<T>(factor, S.factor_size, st);
+    MFS_LAUNCHED();
+    launch_inject<T>(ds.plan.p, int64_t(S.plan.size()), S.vb, S.src_ld, Ax, Bx, Bx ? sigma : 0.0, factor, st);
+    MFS_LAUNCHED();
+    if (!Bx && sigma != 0.0) {
+        launch_diag_shift<T>(ds.diag_off.p, S.n, sigma, factor, st);
+        MFS_LAUNCHED();
+    }
+    for (const LevelPlan &L : ds.levels) {
+        if (L.small_count > 0) {
+            launch_small_factor<T>(ds.small_list.p + L.small_off, L.small_count, L.small_max_front, ds.sd, factor,
+                                   upd, h->fail.p, st);
+            MFS_LAUNCHED();
+        }
+        if (L.large_count == 0) continue;
+        launch_assemble_large<T>(ds.asm_tasks.p + L.asm_off, L.asm_n, L.asm_tiles, ds.sd, factor, upd, st);
+        MFS_LAUNCHED();
+        for (const auto &sp : L.steps) {
+            launch_potrf<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, h->fail.p, st);
+            MFS_LAUNCHED();
+            if (sp.trsm_n > 0) {
+                launch_trsm<T>(ds.trsm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, sp.trsm_maxnb, factor, st);
+                MFS_LAUNCHED();
+            }
+            if (sp.gemm_n > 0) {
+                launch_gemm_update<T>(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor,
+                                      h->opt.tensor_cores, st);
+                MFS_LAUNCHED();
+            }
+        }
+        if (L.syrk_n > 0) {
+            launch_gemm_update<T>(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, upd,
+                                  h->opt.tensor_cores, st);
+            MFS_LAUNCHED();
+        }
+    }
+}
+
+template <typename T>
+void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) {
+    const Symbolic &S = *ds.S;
+    cudaStream_t st = h->stream;
+    h->sol.ensure(size_t(std::max<idx>(S.sol_size, 1)) * nrhs);
+    for (size_t l = 0; l < ds.levels.size(); ++l) {
+        const LevelPlan &L = ds.levels[l];
+        launch_fwd_level<T>(ds.all_list.p + L.all_off, L.all_count, L.all_max_front, ds.sd, factor, X, S.n, nrhs,
+                            h->sol.p, st);
+        MFS_LAUNCHED();
+    }
+    for (size_t l = ds.levels.size(); l-- > 0;) {
+        const LevelPlan &L = ds.levels[l];
+        launch_bwd_level<T>(ds.all_list.p + L.all_off, L.all_count, L.all_max_front, ds.sd, factor, X, S.n, nrhs, st);
+        MFS_LAUNCHED();
+    }
+}
+
+void solve_current(mfs_handle *h, double *X, int nrhs) {
+    DevSym &ds = *h->cur.sym;
+    if (h->opt.precision == MFS_PREC_FP32) run_solve<float>(h, ds, h->cur.f32->p, X, nrhs);
+    else run_solve<double>(h, ds, h->cur.f64->p, X, nrhs);
+}
+
+// Y = (A + sigma I | A + sigma B) X on the permuted reduced system.
+void apply_current(mfs_handle *h, const double *Ax, const double *Bx, double sigma, const double *X, double *Y,
+                   int nrhs) {
+    DevSym &ds = *h->cur.sym;
+    const Symbolic &S = *ds.S;
+    launch_spmv(ds.spmv_ptr.p, ds.spmv_src.p, ds.spmv_col.p, ds.spmv_flag.p, S.nv, S.vb, S.src_ld, Ax, X, Y, S.n,
+                nrhs, h->stream);
+    MFS_LAUNCHED();
+    if (sigma == 0.0) return;
+    const int64_t cnt = int64_t(S.n) * nrhs;
+    if (Bx) {
+        h->work_s.ensure(size_t(cnt));
+        launch_spmv(ds.spmv_ptr.p, ds.spmv_src.p, ds.spmv_col.p, ds.spmv_flag.p, S.nv, S.vb, S.src_ld, Bx, X,
+                    h->work_s.p, S.n, nrhs, h->stream);
+        launch_axpy(Y, h->work_s.p, sigma, cnt, h->stream);
+    } else {
+        launch_axpy(Y, X, sigma, cnt, h->stream);
+    }
+    MFS_LAUNCHED();
+}
+
+// Preconditioned CG on the permuted reduced system, preconditioned by the
+// current (FP32) factor, everything else FP64. B and X are n x nrhs (ld n).
+void refine_solve(mfs_handle *h, const double *B, double *X, int nrhs) {
+    DevSym &ds = *h->cur.sym;
+    const Symbolic &S = *ds.S;
+    const int64_t n = S.n;
+    const size_t sz = size_t(n) * nrhs;
+    cudaStream_t st = h->stream;
+    if (nrhs > 64) throw StatusError(MFS_INVALID_ARG, "refined solves support at most 64 right-hand sides");
+    h->work_r.ensure(sz);
+    h->work_z.ensure(sz);
+    h->work_p.ensure(sz);
+    h->work_ap.ensure(sz);
+    const int np = reduce_partials_count();
+    h->partials.ensure(size_t(np) * 64);
+    h->dots.ensure(4 * 64);
+    h->active.ensure(64);
+    double *bb = h->dots.p, *rz = h->dots.p + 64, *rz2 = h->dots.p + 128, *pap = h->dots.p + 192;
+    if (!h->cur.ax) throw StatusError(MFS_NO_FACTOR, "matrix values of the current factor are not available");
+    const double *Ax = h->cur.ax->p;
+    const double *Bx = h->cur.bx ? h->cur.bx->p : nullptr;
+    const double sigma = h->cur.sigma;
+    std::vector<int> act(nrhs, 1);
+    MFS_CUDA(cudaMemcpyAsync(h->active.p, act.data(), nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
+    launch_colnorm2(B, n, nrhs, h->partials.p, bb, st);
+    MFS_CUDA(cudaMemsetAsync(X, 0, sz * sizeof(double), st));
+    launch_copy(h->work_r.p, B, int64_t(sz), st);
+    launch_copy(h->work_z.p, B, int64_t(sz), st);
+    MFS_LAUNCHED();
+    solve_current(h, h->work_z.p, nrhs);
+    launch_copy(h->work_p.p, h->work_z.p, int64_t(sz), st);
+    launch_coldot(h->work_r.p, h->work_z.p, n, nrhs, h->partials.p, rz, st);
+    MFS_LAUNCHED();
+    std::vector<double> hb(nrhs), hr(nrhs);
+    MFS_CUDA(cudaMemcpyAsync(hb.data(), bb, nrhs * sizeof(double), cudaMemcpyDeviceToHost, st));
+    MFS_CUDA(cudaStreamSynchronize(st));
+    const double tol = h->opt.refine_tol > 0 ? h->opt.refine_tol : 1e-10;
+    const int maxit = h->opt.refine_maxit > 0 ? h->opt.refine_maxit : 50;
+    int it = 0;
+    double worst = 0.0;
+    bool all_done = false;
+    for (int r = 0; r < nrhs; ++r) if (hb[r] == 0.0) act[r] = 0;
+    while (it < maxit) {
+        ++it;
+        apply_current(h, Ax, Bx, sigma, h->work_p.p, h->work_ap.p, nrhs);
+        launch_coldot(h->work_p.p, h->work_ap.p, n, nrhs, h->partials.p, pap, st);
+        launch_pcg_update_x_r(X, h->work_r.p, h->work_p.p, h->work_ap.p, rz, pap, h->active.p, n, nrhs, st);
+        launch_colnorm2(h->work_r.p, n, nrhs, h->partials.p, rz2, st);
+        MFS_LAUNCHED();
+        MFS_CUDA(cudaMemcpyAsync(hr.data(), rz2, nrhs * sizeof(double), cudaMemcpyDeviceToHost, st));
+        MFS_CUDA(cudaStreamSynchronize(st));
+        worst = 0.0;
+        all_done = true;
+        for (int r = 0; r < nrhs; ++r) {
+            double rel = hb[r] > 0 ? std::sqrt(hr[r] / hb[r]) : 0.0;
+            if (act[r] && rel <= tol) act[r] = 0;
+            if (act[r]) all_done = false;
+            worst = std::max(worst, rel);
+        }
+        if (all_done) break;
+        MFS_CUDA(cudaMemcpyAsync(h->active.p, act.data(), nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
+        launch_copy(h->work_z.p, h->work_r.p, int64_t(sz), st);
+        MFS_LAUNCHED();
+        solve_current(h, h->work_z.p, nrhs);
+        launch_coldot(h->work_r.p, h->work_z.p, n, nrhs, h->partials.p, rz2, st);
+        launch_pcg_update_p(h->work_p.p, h->work_z.p, rz2, rz, h->active.p, n, nrhs, st);
+        MFS_LAUNCHED();
+        MFS_CUDA(cudaMemcpyAsync(rz, rz2, nrhs * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    h->stats.refine_iterations = it;
+    h->stats.residual = worst;
+    if (!all_done)
+        throw StatusError(MFS_NOT_POSDEF, "refinement did not reach the residual target within the iteration cap (" +
+                                              std::to_string(worst) + ")");
+}
+
+void require_symbolic(mfs_handle *h) {
+    if (!h->cur.sym || h->cur.type < 1) throw StatusError(MFS_NO_FACTOR, "Symbolic factorization does not exist");
+}
+void require_numeric(mfs_handle *h) {
+    if (!h->cur.sym || h->cur.type < 2) throw StatusError(MFS_NO_FACTOR, "Numeric factorization does not exist");
+}
+
+const double *stage_input(mfs_handle *h, DBuf<double> &buf, const double *src, size_t count, bool on_device) {
+    if (on_device) return src;
+    buf.ensure(count);
+    if (count) MFS_CUDA(cudaMemcpyAsync(buf.p, src, count * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    return buf.p;
+}
+
+}  // namespace
+
+extern "C" {
+
+mfs_status mfs_default_options(mfs_options *opt) {
+    if (!opt) return MFS_INVALID_ARG;
+    std::memset(opt, 0, sizeof(*opt));
+    opt->precision = MFS_PREC_FP64;
+    opt->ordering = MFS_ORDER_ND;
+    opt->relax = 1;
+    opt->device = 0;
+    opt->relax_zeros = 128;
+    opt->relax_ratio = 0.01;
+    opt->nd_leaf_size = 120;
+    opt->seed = 12345;
+    opt->stream = nullptr;
+    opt->small_front_max = 0;
+    opt->refine = 0;
+    opt->refine_tol = 1e-10;
+    opt->refine_maxit = 50;
+    opt->use_graphs = 0;
+    opt->tensor_cores = 1;
+    return MFS_OK;
+}
+
+mfs_status mfs_create(mfs_handle **out, const mfs_options *opt) {
+    if (!out) return MFS_INVALID_ARG;
+    *out = nullptr;
+    auto h = std::make_unique<mfs_handle>();
+    if (opt) h->opt = *opt;
+    else mfs_default_options(&h->opt);
+    mfs_status s = guarded(h.get(), [&] {
+        if (h->opt.precision != MFS_PREC_FP64 && h->opt.precision != MFS_PREC_FP32)
+            throw StatusError(MFS_INVALID_ARG, "unknown precision");
+        h->stats.failed_column = -1;
+        if (h->opt.device == -1) return;   // analysis-only handle: no CUDA context is touched
+        int ndev = 0;
+        MFS_CUDA(cudaGetDeviceCount(&ndev));
+        if (h->opt.device < 0 || h->opt.device >= ndev) throw StatusError(MFS_INVALID_ARG, "invalid CUDA device");
+        set_device(h.get());
+        if (h->opt.stream) h->stream = static_cast<cudaStream_t>(h->opt.stream);
+        else {
+            MFS_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+            h->own_stream = true;
+        }
+        MFS_CUDA(cudaEventCreate(&h->ev0));
+        MFS_CUDA(cudaEventCreate(&h->ev1));
+        MFS_CUDA(cudaMallocHost(&h->fail_host, sizeof(int)));
+        MFS_CUDA(cudaMallocHost(&h->dots_host, 64 * sizeof(double)));
+        h->fail.ensure(1);
+        h->stats.failed_column = -1;
+    });
+    if (s != MFS_OK) {
+        // keep the message reachable for callers that only get a status
+        return s;
+    }
+    *out = h.release();
+    return MFS_OK;
+}
+
+mfs_status mfs_set_options(mfs_handle *h, const mfs_options *opt) {
+    if (!h || !opt) return MFS_INVALID_ARG;
+    if (opt->precision != h->opt.precision || opt->device != h->opt.device)
+        return MFS_INVALID_ARG;   // fixed for the lifetime of a handle
+    void *stream = h->opt.stream;
+    h->opt = *opt;
+    h->opt.stream = stream;
+    return MFS_OK;
+}
+
+mfs_status mfs_destroy(mfs_handle *h) {
+    if (!h) return MFS_OK;
+    if (h->opt.device == -1) {
+        delete h;
+        return MFS_OK;
+    }
+    cudaSetDevice(h->opt.device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->fail_host) cudaFreeHost(h->fail_host);
+    if (h->dots_host) cudaFreeHost(h->dots_host);
+    delete h;
+    return MFS_OK;
+}
+
+mfs_status mfs_last_error(const mfs_handle *h, char *buf, size_t len) {
+    if (!h || !buf || len == 0) return MFS_INVALID_ARG;
+    std::strncpy(buf, h->err.c_str(), len - 1);
+    buf[len - 1] = 0;
+    return MFS_OK;
+}
+
+mfs_status mfs_build_pattern(int64_t nvars, int64_t nelem, int32_t npe, const int64_t *conn, int64_t *Ap,
+                             int64_t *Ai, int64_t *nnz) {
+    if (nvars < 0 || nelem < 0 || npe <= 0 || !Ap || !nnz || (nelem > 0 && !conn)) return MFS_INVALID_ARG;
+    try {
+        Pattern P = build_block_pattern(nvars, nelem, npe, conn);
+        std::copy(P.Ap.begin(), P.Ap.end(), Ap);
+        *nnz = P.nnz();
+        if (Ai) std::copy(P.Ai.begin(), P.Ai.end(), Ai);
+        return MFS_OK;
+    } catch (const std::invalid_argument &) {
+        return MFS_INVALID_ARG;
+    } catch (...) {
+        return MFS_INTERNAL;
+    }
+}
+
+mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, const int64_t *Ai, int32_t block_size,
+                        const int64_t *pinned, int64_t n_pinned, const int64_t *user_perm,
+                        const int64_t *supernode_sizes, int64_t num_supernodes) {
+    if (!h) return MFS_INVALID_ARG;
+    return guarded(h, [&] {
+        if (!Ap || (n_pinned > 0 && !pinned) || n_blocks < 0) throw StatusError(MFS_INVALID_ARG, "null pattern");
+        if (Ap[n_blocks] > 0 && !Ai) throw StatusError(MFS_INVALID_ARG, "null Ai");
+        const bool host_only = h->opt.device == -1;
+        if (!host_only) set_device(h);
+        // A new analysis replaces the current factorization (the stash is kept).
+        h->cur = State();
+        h->asm_ax.reset();
+        h->nslots = 0;
+        h->nelem = 0;
+        auto Sp = std::make_shared<Symbolic>();
+        SymbolicOptions so;
+        so.ordering = h->opt.ordering;
+        so.relax = h->opt.relax != 0;
+        so.relax_zeros = h->opt.relax_zeros;
+        so.relax_ratio = h->opt.relax_ratio;
+        so.nd.leaf_size = h->opt.nd_leaf_size > 0 ? h->opt.nd_leaf_size : 120;
+        so.nd.seed = h->opt.seed;
+        std::string e = analyze(n_blocks, Ap, Ai, block_size, pinned, n_pinned, so, user_perm, *Sp, supernode_sizes,
+                                supernode_sizes ? num_supernodes : 0);
+        if (!e.empty())
+            throw StatusError(e.rfind("Fixed variable index out of range", 0) == 0 ? MFS_SIZE_MISMATCH : MFS_INVALID_ARG,
+                              e);
+        if (host_only) {
+            auto ds = std::make_shared<DevSym>();
+            ds->S = Sp;
+            ds->ax_len = Ap[n_blocks] * int64_t(block_size) * block_size;
+            h->cur.sym = ds;
+            h->cur.type = 1;
+            h->stats.num_levels = int(Sp->nlevels);
+            return;
+        }
+        auto ds = upload_symbolic(h, Sp);
+        ds->ax_len = Ap[n_blocks] * int64_t(block_size) * block_size;
+        ds->Ap_full.assign(Ap, Ap + n_blocks + 1);
+        ds->Ai_full.assign(Ai, Ai + Ap[n_blocks]);
+        const Symbolic &S = *Sp;
+        if (h->opt.precision == MFS_PREC_FP32) h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
+        else h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
+        h->cur.sym = ds;
+        h->cur.type = 1;
+        h->stats.num_levels = int(S.nlevels);
+        h->stats.num_large = ds->num_large;
+    });
+}
+
+mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double sigma, int32_t flags) {
+    if (!h) return MFS_INVALID_ARG;
+    return guarded(h, [&] {
+        require_symbolic(h);
+        set_device(h);
+        DevSym &ds = *h->cur.sym;
+        const Symbolic &S = *ds.S;
+        const bool dev = (flags & MFS_DEVICE_POINTERS) != 0;
+        cudaStream_t st = h->stream;
+        // The numeric factor becomes invalid from here until success.
+        h->cur.type = 1;
+        const size_t axn = size_t(ds.ax_len);
+        auto take_values = [&](std::shared_ptr<DBuf<double>> &dst, const double *src) {
+            if (!dst || dst.use_count() > 1) dst = std::make_shared<DBuf<double>>();
+            dst->ensure(axn);
+            if (axn)
+                MFS_CUDA(cudaMemcpyAsync(dst->p, src, axn * sizeof(double),
+                                         dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+        };
+        if (Ax) {
+            take_values(h->cur.ax, Ax);
+        } else {
+            if (!h->asm_ax) throw StatusError(MFS_INVALID_ARG, "no values: pass Ax or assemble first");
+            h->cur.ax = h->asm_ax;
+        }
+        if (Bx) take_values(h->cur.bx, Bx);
+        else h->cur.bx.reset();
+        const double *dBx = h->cur.bx ? h->cur.bx->p : nullptr;
+        const int big = INT_MAX;
+        MFS_CUDA(cudaMemcpyAsync(h->fail.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+        MFS_CUDA(cudaEventRecord(h->ev0, st));
+        if (h->opt.precision == MFS_PREC_FP32) {
+            if (!h->cur.f32 || h->cur.f32.use_count() > 1) h->cur.f32 = std::make_shared<DBuf<float>>();
+            h->cur.f32->ensure(size_t(std::max<idx>(S.factor_size, 1)));
+            h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
+            run_factor<float>(h, ds, h->cur.f32->p, h->upd32.p, h->cur.ax->p, dBx, sigma);
+        } else {
+            if (!h->cur.f64 || h->cur.f64.use_count() > 1) h->cur.f64 = std::make_shared<DBuf<double>>();
+            h->cur.f64->ensure(size_t(std::max<idx>(S.factor_size, 1)));
+            h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
+            run_factor<double>(h, ds, h->cur.f64->p, h->upd64.p, h->cur.ax->p, dBx, sigma);
+        }
+        MFS_CUDA(cudaEventRecord(h->ev1, st));
+        MFS_CUDA(cudaMemcpyAsync(h->fail_host, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        MFS_CUDA(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        h->stats.factor_ms = ms;
+        h->cur.sigma = sigma;
+        if (*h->fail_host != INT_MAX) {
+            h->stats.failed_column = *h->fail_host;
+            throw StatusError(MFS_NOT_POSDEF, std::to_string(*h->fail_host) + "/" + std::to_string(S.n) +
+                                                  "  pivots successful in numeric factorization (non-positive definite?)");
+        }
+        h->stats.failed_column = -1;
+        h->cur.type = 2;
+    });
+}
+
+mfs_status mfs_solve(mfs_handle *h, const double *B, double *X, int64_t nrhs, int64_t ldb, int32_t flags) {
+    if (!h) return MFS_INVALID_ARG;
+    return guarded(h, [&] {
+        require_numeric(h);
+        set_device(h);
+        DevSym &ds = *h->cur.sym;
+        const Symbolic &S = *ds.S;
+        const int mode = flags & 3;
+        const bool dev = (flags & MFS_DEVICE_POINTERS) != 0;
+        if (nrhs < 1) throw StatusError(MFS_INVALID_ARG, "Must specify at least one rhs.");
+        const int64_t rows = mode == MFS_SOLVE_FULL ? S.n_full : S.n;
+        if (ldb < rows) throw StatusError(MFS_SIZE_MISMATCH, "Incorrect RHS size");
+        if (!B || !X) throw StatusError(MFS_INVALID_ARG, "null vector");
+        cudaStream_t st = h->stream;
+        const size_t sz = size_t(S.n) * nrhs;
+        h->rhs.ensure(sz);
+        const double *Bd = B;
+        double *Xd = X;
+        const size_t io_sz = size_t(ldb) * nrhs;
+        if (!dev) {
+            h->io.ensure(io_sz);
+            MFS_CUDA(cudaMemcpyAsync(h->io.p, B, io_sz * sizeof(double), cudaMemcpyHostToDevice, st));
+            Bd = h->io.p;
+            Xd = h->io.p;
+        }
+        MFS_CUDA(cudaEventRecord(h->ev0, st));
+        const int64_t *map = mode == MFS_SOLVE_FULL ? ds.prrfr.p : (mode == MFS_SOLVE_REDUCED ? ds.sperm.p : nullptr);
+        launch_gather_rows(map, rows, Bd, ldb, h->rhs.p, S.n, int(nrhs), st);
+        MFS_LAUNCHED();
+        double *result = h->rhs.p;
+        const bool refine = h->opt.refine && h->opt.precision == MFS_PREC_FP32;
+        if (refine) {
+            h->work_x.ensure(sz);
+            refine_solve(h, h->rhs.p, h->work_x.p, int(nrhs));
+            result = h->work_x.p;
+        } else {
+            solve_current(h, h->rhs.p, int(nrhs));
+        }
+        launch_scatter_rows(map, rows, result, S.n, Xd, ldb, int(nrhs), st);
+        MFS_LAUNCHED();
+        MFS_CUDA(cudaEventRecord(h->ev1, st));
+        if (!dev) MFS_CUDA(cudaMemcpyAsync(X, h->io.p, io_sz * sizeof(double), cudaMemcpyDeviceToHost, st));
+        MFS_CUDA(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        h->stats.solve_ms = ms;
+    });
+}
+
+mfs_status mfs_apply(mfs_handle *h, const double *x, double *y, int64_t nrhs, int64_t ld, int32_t flags) {
+    if (!h) return MFS_INVALID_ARG;
+    return guarded(h, [&] {
+        require_symbolic(h);
+        std::shared_ptr<DBuf<double>> vals = h->cur.ax ? h->cur.ax : h->asm_ax;
+        if (!vals) throw StatusError(MFS_NO_FACTOR, "no matrix values on the device");
+        set_device(h);
+        DevSym &ds = *h->cur.sym;
+        const Symbolic &S = *ds.S;
+        const int mode = flags & 3;
+        const bool dev = (flags & MFS_DEVICE_POINTERS) != 0;
+        const int64_t rows = mode == MFS_SOLVE_FULL ? S.n_full : S.n;
+        if (ld < rows || nrhs < 1) throw StatusError(MFS_SIZE_MISMATCH, "Incorrect vector size");
+        cudaStream_t st = h->stream;
+        const size_t sz = size_t(S.n) * nrhs;
+        const size_t io_sz = size_t(ld) * nrhs;
+        h->rhs.ensure(sz);
+        h->work_x.ensure(sz);
+        const double *xd = x;
+        double *yd = y;
+        if (!dev) {
+            h->io.ensure(io_sz);
+            MFS_CUDA(cudaMemcpyAsync(h->io.p, x, io_sz * sizeof(double), cudaMemcpyHostToDevice, st));
+            xd = h->io.p;
+            yd = h->io.p;
+        }
+        const int64_t *map = mode == MFS_SOLVE_FULL ? ds.prrfr.p : (mode == MFS_SOLVE_REDUCED ? ds.sperm.p : nullptr);
+        launch_gather_rows(map, rows, xd, ld, h->rhs.p, S.n, int(nrhs), st);
+        apply_current(h, vals->p, nullptr, 0.0, h->rhs.p, h->work_x.p, int(nrhs));
+        launch_scatter_rows(map, rows, h->work_x.p, S.n, yd, ld, int(nrhs), st);
+        MFS_LAUNCHED();
+        if (!dev) MFS_CUDA(cudaMemcpyAsync(y, h->io.p, io_sz * sizeof(double), cudaMemcpyDeviceToHost, st));
+        MFS_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+mfs_status mfs_assembly_setup(mfs_handle *h, int64_t nelem, const int64_t *conn) {
+    if (!h) return MFS_INVALID_ARG;
+    return guarded(h, [&] {
+        require_symbolic(h);
+        set_device(h);
+        DevSym &ds = *h->cur.sym;
+        if (ds.S->bs != 3) throw StatusError(MFS_INVALID_ARG, "element assembly expects 3x3 blocks");
+        if (nelem < 0 || (nelem > 0 && !conn)) throw StatusError(MFS_INVALID_ARG, "bad connectivity");
+        const int64_t nb = int64_t(ds.Ap_full.size()) - 1;
+        const int64_t nslots = ds.Ap_full[nb];
+        // Per element, in the reference's order (SystemAssembler.hh:60-98): columns by
+        // sorted global index; an upper block (bi, bj) takes He(i_loc, j_loc) when the
+        // local order agrees with the global one, else the transpose of He(j_loc, i_loc);
+        // the diagonal block adds its upper triangle only.
+        std::vector<int64_t> cnt(nslots + 1, 0);
+        auto find_slot = [&](int64_t bi, int64_t bj) -> int64_t {
+            const int64_t *b = ds.Ai_full.data() + ds.Ap_full[bj];
+            const int64_t *e = ds.Ai_full.data() + ds.Ap_full[bj + 1];
+            const int64_t *it = std::lower_bound(b, e, bi);
+            if (it == e || *it != bi) throw StatusError(MFS_INVALID_ARG, "element block not in the pattern");
+            return it - ds.Ai_full.data();
+        };
+        std::vector<int64_t> slots(size_t(nelem) * 10), codes(size_t(nelem) * 10);
+        for (int64_t e = 0; e < nelem; ++e) {
+            const int64_t *v = conn + 4 * e;
+            int order[4] = {0, 1, 2, 3};
+            for (int k = 0; k < 4; ++k) {
+                if (v[k] < 0 || v[k] >= nb) throw StatusError(MFS_INVALID_ARG, "element node out of range");
+            }
+            std::stable_sort(order, order + 4, [&](int a, int b) { return v[a] < v[b]; });
+            int q = 0;
+            for (int jj = 0; jj < 4; ++jj) {
+                const int lj = order[jj];
+                const int64_t bj = v[lj];
+                for (int ii = 0; ii < jj; ++ii) {
+                    const int li = order[ii];
+                    const int64_t bi = v[li];
+                    const int64_t slot = find_slot(bi, bj);
+                    int64_t code;
+                    if (li < lj) code = ((e * 144 + (3 * li) * 12 + 3 * lj) << 2) | 0;
+                    else code = ((e * 144 + (3 * lj) * 12 + 3 * li) << 2) | 1;
+                    slots[e * 10 + q] = slot;
+                    codes[e * 10 + q] = code;
+                    ++q;
+                }
+                const int64_t slot = find_slot(bj, bj);
+                slots[e * 10 + q] = slot;
+                codes[e * 10 + q] = ((e * 144 + (3 * lj) * 12 + 3 * lj) << 2) | 2;
+                ++q;
+            }
+        }
+        for (size_t k = 0; k < slots.size(); ++k) cnt[slots[k] + 1]++;
+        for (int64_t s = 0; s < nslots; ++s) cnt[s + 1] += cnt[s];
+        std::vector<int64_t> contrib(slots.size());
+        std::vector<int64_t> back(cnt.begin(), cnt.end() - 1);
+        for (size_t k = 0; k < slots.size(); ++k) contrib[back[slots[k]]++] = codes[k];
+        h->slot_ptr.upload(cnt, h->stream);
+        h->contrib.upload(contrib, h->stream);
+        h->nslots = nslots;
+        h->nelem = nelem;
+    });
+}
+
+mfs_status mfs_assemble(mfs_handle *h, const double *Ke, double *Ax_out, int32_t flags) {
+    if (!h) return MFS_INVALID_ARG;
+    return guarded(h, [&] {
+        require_symbolic(h);
+        if (h->nslots == 0 && h->nelem == 0) throw StatusError(MFS_INVALID_ARG, "call mfs_assembly_setup first");
+        set_device(h);
+        DevSym &ds = *h->cur.sym;
+        cudaStream_t st = h->stream;
+        const bool dev = (flags & MFS_DEVICE_POINTERS) != 0;
+        const size_t ke_n = size_t(h->nelem) * 144;
+        const double *Ked = dev ? Ke : stage_input(h, h->ke, Ke, ke_n, false);
+        if (!h->asm_ax || h->asm_ax.use_count() > 1) h->asm_ax = std::make_shared<DBuf<double>>();
+        h->asm_ax->ensure(size_t(ds.ax_len));
+        MFS_CUDA(cudaEventRecord(h->ev0, st));
+        launch_assemble_elements(h->slot_ptr.p, h->contrib.p, h->nslots, Ked, h->asm_ax->p, st);
+        MFS_LAUNCHED();
+        MFS_CUDA(cudaEventRecord(h->ev1, st));
+        if (Ax_out) {
+            MFS_CUDA(cudaMemcpyAsync(Ax_out, h->asm_ax->p, size_t(ds.ax_len) * sizeof(double),
+                                     dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+        }
+        MFS_CUDA(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        h->stats.assemble_ms = ms;
+    });
+}
+
+mfs_status mfs_info(const mfs_handle *h, int64_t *n_full, int64_t *n_reduced, int64_t *factor_nnz, double *flops,
+                    int64_t *num_supernodes, int32_t *factorization_type) {
+    if (!h) return MFS_INVALID_ARG;
+    const bool has = h->cur.sym && h->cur.type >= 1;
+    if (factorization_type) *factorization_type = h->cur.type;
+    if (!has) return MFS_NO_FACTOR;
+    const Symbolic &S = *h->cur.sym->S;
+    if (n_full) *n_full = S.n_full;
+    if (n_reduced) *n_reduced = S.n;
+    if (factor_nnz) *factor_nnz = S.factor_nnz;
+    if (flops) *flops = S.flops;
+    if (num_supernodes) *num_supernodes = S.nsn;
+    return MFS_OK;
+}
+
+mfs_status mfs_inverse_permutation(const mfs_handle *h, int64_t *iperm_out) {
+    if (!h || !iperm_out) return MFS_INVALID_ARG;
+    if (!h->cur.sym || h->cur.type < 1) return MFS_NO_FACTOR;
+    const Symbolic &S = *h->cur.sym->S;
+    std::copy(S.scalar_iperm.begin(), S.scalar_iperm.end(), iperm_out);
+    return MFS_OK;
+}
+
+mfs_status mfs_nd_ordering(const mfs_handle *h, int64_t *ncomp, int64_t *nmember, int64_t *cparent,
+                           int64_t *cmember) {
+    if (!h || !ncomp || !nmember) return MFS_INVALID_ARG;
+    if (!h->cur.sym || h->cur.type < 1) return MFS_NO_FACTOR;
+    const Symbolic &S = *h->cur.sym->S;
+    *ncomp = int64_t(S.nd_cparent.size());
+    *nmember = int64_t(S.nd_cmember.size());
+    if (cparent) std::copy(S.nd_cparent.begin(), S.nd_cparent.end(), cparent);
+    if (cmember) std::copy(S.nd_cmember.begin(), S.nd_cmember.end(), cmember);
+    return MFS_OK;
+}
+
+mfs_status mfs_supernodes(const mfs_handle *h, int64_t *nsn, int64_t *nstruct, int32_t *vb, int64_t *sn_start,
+                          int64_t *parent, int64_t *struct_ptr, int64_t *struct_rows, int64_t *rel) {
+    if (!h || !nsn || !nstruct) return MFS_INVALID_ARG;
+    if (!h->cur.sym || h->cur.type < 1) return MFS_NO_FACTOR;
+    const Symbolic &S = *h->cur.sym->S;
+    *nsn = S.nsn;
+    *nstruct = int64_t(S.struct_rows.size());
+    if (vb) *vb = S.vb;
+    if (sn_start) std::copy(S.sn_start.begin(), S.sn_start.end(), sn_start);
+    if (parent) std::copy(S.sn_parent.begin(), S.sn_parent.end(), parent);
+    if (struct_ptr) std::copy(S.struct_ptr.begin(), S.struct_ptr.end(), struct_ptr);
+    if (struct_rows) std::copy(S.struct_rows.begin(), S.struct_rows.end(), struct_rows);
+    if (rel) std::copy(S.rel.begin(), S.rel.end(), rel);
+    return MFS_OK;
+}
+
+mfs_status mfs_conversion_plan(const mfs_handle *h, int64_t *nv, int64_t *nentries, int64_t *column_offsets,
+                               int64_t *entries) {
+    if (!h || !nv || !nentries) return MFS_INVALID_ARG;
+    if (!h->cur.sym || h->cur.type < 1) return MFS_NO_FACTOR;
+    const Symbolic &S = *h->cur.sym->S;
+    *nv = S.nv;
+    *nentries = int64_t(S.plan.size());
+    if (column_offsets) std::copy(S.plan_ptr.begin(), S.plan_ptr.end(), column_offsets);
+    if (entries)
+        for (size_t k = 0; k < S.plan.size(); ++k) {
+            entries[4 * k] = S.plan[k].dst;
+            entries[4 * k + 1] = S.plan[k].src;
+            entries[4 * k + 2] = S.plan[k].ld;
+            entries[4 * k + 3] = S.plan[k].flags;
+        }
+    return MFS_OK;
+}
+
+mfs_status mfs_factor_values(const mfs_handle *h, int64_t *factor_size, double *out) {
+    if (!h || !factor_size) return MFS_INVALID_ARG;
+    if (!h->cur.sym || h->cur.type < 2) return MFS_NO_FACTOR;
+    const Symbolic &S = *h->cur.sym->S;
+    *factor_size = S.factor_size;
+    if (!out) return MFS_OK;
+    mfs_handle *hm = const_cast<mfs_handle *>(h);
+    return guarded(hm, [&] {
+        set_device(hm);
+        if (h->opt.precision == MFS_PREC_FP32) {
+            std::vector<float> tmp(S.factor_size);
+            MFS_CUDA(cudaMemcpy(tmp.data(), h->cur.f32->p, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost));
+            std::copy(tmp.begin(), tmp.end(), out);
+        } else {
+            MFS_CUDA(cudaMemcpy(out, h->cur.f64->p, size_t(S.factor_size) * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+    });
+}
+
+mfs_status mfs_stash(mfs_handle *h) {
+    if (!h) return MFS_INVALID_ARG;
+    return guarded(h, [&] {
+        require_symbolic(h);
+        set_device(h);
+        State s;
+        s.sym = h->cur.sym;
+        s.type = h->cur.type;
+        s.sigma = h->cur.sigma;
+        s.ax = h->cur.ax;
+        s.bx = h->cur.bx;
+        const size_t fs = size_t(std::max<idx>(h->cur.sym->S->factor_size, 1));
+        if (h->cur.type >= 2) {
+            if (h->cur.f64) {
+                s.f64 = std::make_shared<DBuf<double>>();
+                s.f64->ensure(fs);
+                MFS_CUDA(cudaMemcpyAsync(s.f64->p, h->cur.f64->p, fs * sizeof(double), cudaMemcpyDeviceToDevice,
+                                         h->stream));
+            }
+            if (h->cur.f32) {
+                s.f32 = std::make_shared<DBuf<float>>();
+                s.f32->ensure(fs);
+                MFS_CUDA(cudaMemcpyAsync(s.f32->p, h->cur.f32->p, fs * sizeof(float), cudaMemcpyDeviceToDevice,
+                                         h->stream));
+            }
+        }
+        MFS_CUDA(cudaStreamSynchronize(h->stream));
+        h->stash = s;
+        h->has_stash = true;
+    });
+}
+
+mfs_status mfs_swap_stash(mfs_handle *h) {
+    if (!h) return MFS_INVALID_ARG;
+    return guarded(h, [&] {
+        if (!h->has_stash) throw StatusError(MFS_NO_FACTOR, "No stashed factorization");
+        std::swap(h->cur, h->stash);
+        if (h->cur.sym) {
+            const Symbolic &S = *h->cur.sym->S;
+            if (h->opt.precision == MFS_PREC_FP32) h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
+            else h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
+        }
+    });
+}
+
+mfs_status mfs_clear_stash(mfs_handle *h) {
+    if (!h) return MFS_INVALID_ARG;
+    h->stash = State();
+    h->has_stash = false;
+    return MFS_OK;
+}
+
+mfs_status mfs_has_stash(const mfs_handle *h, int32_t *has) {
+    if (!h || !has) return MFS_INVALID_ARG;
+    *has = h->has_stash ? 1 : 0;
+    return MFS_OK;
+}
+
+mfs_status mfs_clear_factors(mfs_handle *h) {
+    if (!h) return MFS_INVALID_ARG;
+    h->cur = State();
+    h->asm_ax.reset();
+    h->nslots = 0;
+    h->nelem = 0;
+    return MFS_OK;
+}
+
+mfs_status mfs_get_stats(const mfs_handle *h, mfs_stats *st) {
+    if (!h || !st) return MFS_INVALID_ARG;
+    *st = h->stats;
+    int64_t bytes = 0;
+    if (h->cur.sym) bytes += int64_t(h->cur.sym->bytes());
+    if (h->cur.f64) bytes += int64_t(h->cur.f64->bytes());
+    if (h->cur.f32) bytes += int64_t(h->cur.f32->bytes());
+    if (h->cur.ax) bytes += int64_t(h->cur.ax->bytes());
+    bytes += int64_t(h->upd64.bytes() + h->upd32.bytes() + h->sol.bytes() + h->rhs.bytes());
+    st->device_bytes = bytes;
+    st->kernel_launches = g_kernel_launches;
+    return MFS_OK;
+}
+
+}  // extern "C"

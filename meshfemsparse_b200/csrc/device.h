@@ -1,0 +1,137 @@
+// Device-side data layout and kernel launchers shared by the CUDA sources.
+//
+// Storage in HBM (all column-major):
+//   factor values  : one panel per supernode, (w+d) x w, ld = w+d, panels back to back
+//                    (catamari layout, CatamariConversionPlan.hh:366)
+//   update arena   : U_s (d x d, ld d) of the multifrontal assembly tree; offsets from
+//                    the static level-lifetime plan built on the host
+//   solve arena    : u_s (d x nrhs, ld d) forward-substitution update vectors; offsets
+//                    are the same plan computed with unit size d, scaled by nrhs
+//   right-hand sides: permuted reduced order, n x nrhs, ld = n
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mfs {
+
+// Kernels launched by this library since load (every launcher increments it).
+extern long long g_kernel_launches;
+
+struct SnDev {
+    const int32_t *w, *d, *f;           // scalar width / degree / front size
+    const int32_t *col0;                // first scalar column of the supernode
+    const int64_t *pan_off;             // panel offset in the factor array
+    const int64_t *upd_off;             // U_s offset in the update arena (-1: none)
+    const int64_t *sol_off;             // u_s offset (units of one RHS) in the solve arena
+    const int32_t *child_ptr, *child_list;
+    const int64_t *struct_ptr;          // per supernode, into struct_rows / rel
+    const int32_t *struct_rows;         // analysis-variable rows (permuted)
+    const int32_t *rel;                 // per struct entry: scalar row in the parent's front
+    int vb;                             // analysis block size
+};
+
+// Plan entry mirror of host_symbolic.h PlanEntry.
+struct PlanEntryDev {
+    int64_t dst;
+    int64_t src;
+    int32_t ld;
+    int32_t flags;
+};
+
+// C(i,j) -= sum_k A(i,k) * A'(j,k) over a tile grid; A and A' share the
+// leading dimension lda (both are column ranges of one panel).
+struct GemmTask {
+    int64_t a_off, b_off, c_off;
+    int32_t lda, ldc;
+    int32_t m, n, k;
+    int32_t tiles_m, tiles_n;
+    int32_t tile_base;                  // prefix over tasks of tiles_m*tiles_n
+    int32_t lower;                      // 1: only i >= j is updated
+};
+
+// Dense Cholesky of an nb x nb diagonal block held in a panel.
+struct PotrfTask {
+    int64_t off;                        // offset of the block's (0,0) entry
+    int32_t ld, nb;
+    int32_t col;                        // global scalar column of the block's first pivot
+    int32_t pad;
+};
+
+// X L^T = B for the rows below a factored diagonal block.
+struct TrsmTask {
+    int64_t l_off;                      // diagonal block (nb x nb, lower)
+    int64_t b_off;                      // first row of the block column below
+    int32_t ld, nb, m;                  // m rows
+    int32_t tile_base;                  // prefix over tasks of row tiles
+};
+
+// Extend-add of all children of a large supernode, split by front columns.
+struct AssembleTask {
+    int32_t sn;
+    int32_t tile_base;                  // prefix over tasks of column chunks
+};
+
+constexpr int kAsmCols = 32;            // front columns per assemble CTA
+constexpr int kGemmTile = 64;           // C tile edge of the update kernels
+constexpr int kTrsmRows = 64;           // rows per TRSM CTA
+
+// ---------------------------------------------------------------- launchers
+template <typename T>
+void launch_zero(T *p, int64_t n, cudaStream_t st);
+template <typename T>
+void launch_inject(const PlanEntryDev *plan, int64_t nplan, int vb, int src_ld, const double *Ax,
+                   const double *Bx, double sigma_b, T *factor, cudaStream_t st);
+template <typename T>
+void launch_diag_shift(const int64_t *diag_off, int64_t n, double sigma, T *factor, cudaStream_t st);
+template <typename T>
+void launch_small_factor(const int32_t *list, int count, int max_front, SnDev sd, T *factor, T *upd,
+                         int *fail_col, cudaStream_t st);
+template <typename T>
+void launch_assemble_large(const AssembleTask *tasks, int ntasks, int ntiles, SnDev sd, T *factor, T *upd,
+                           cudaStream_t st);
+template <typename T>
+void launch_potrf(const PotrfTask *tasks, int ntasks, int max_nb, T *factor, int *fail_col, cudaStream_t st);
+template <typename T>
+void launch_trsm(const TrsmTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, cudaStream_t st);
+template <typename T>
+void launch_gemm_update(const GemmTask *tasks, int ntasks, int ntiles, const T *a, T *c, int use_tc,
+                        cudaStream_t st);
+
+// Solves (the factor type T may be float while vectors stay double).
+template <typename T>
+void launch_fwd_level(const int32_t *list, int count, int max_front, SnDev sd, const T *factor, double *X,
+                      int64_t ldx, int nrhs, double *sol, cudaStream_t st);
+template <typename T>
+void launch_bwd_level(const int32_t *list, int count, int max_front, SnDev sd, const T *factor, double *X,
+                      int64_t ldx, int nrhs, cudaStream_t st);
+
+// Symmetric block SpMV over permuted reduced rows: Y = A X (both ld = n).
+void launch_spmv(const int64_t *ptr, const int64_t *src, const int32_t *col, const int32_t *flag, int64_t nrows,
+                 int vb, int src_ld, const double *Ax, const double *X, double *Y, int64_t ld, int nrhs,
+                 cudaStream_t st);
+
+// Gather/scatter between the caller's (full or reduced) order and the permuted reduced order.
+void launch_gather_rows(const int64_t *map, int64_t n_in, const double *in, int64_t ld_in, double *out,
+                        int64_t ld_out, int nrhs, cudaStream_t st);
+void launch_scatter_rows(const int64_t *map, int64_t n_out, const double *in, int64_t ld_in, double *out,
+                         int64_t ld_out, int nrhs, cudaStream_t st);
+
+// Assembly (K1): Ax[slot*9 + c*3 + r] = sum of contributions in element order.
+void launch_assemble_elements(const int64_t *slot_ptr, const int64_t *contrib, int64_t nslots, const double *Ke,
+                              double *Ax, cudaStream_t st);
+
+// Refinement / PCG vector kernels (column-wise over nrhs columns, ld = n).
+void launch_residual(const double *B, const double *AX, double *R, int64_t n, int nrhs, cudaStream_t st);
+void launch_colnorm2(const double *X, int64_t n, int nrhs, double *partials, double *out, cudaStream_t st);
+void launch_coldot(const double *X, const double *Y, int64_t n, int nrhs, double *partials, double *out,
+                   cudaStream_t st);
+void launch_pcg_update_x_r(double *X, double *R, const double *P, const double *AP, const double *rz,
+                           const double *pap, const int *active, int64_t n, int nrhs, cudaStream_t st);
+void launch_pcg_update_p(double *P, const double *Z, const double *rz_new, const double *rz_old, const int *active,
+                         int64_t n, int nrhs, cudaStream_t st);
+void launch_copy(double *dst, const double *src, int64_t count, cudaStream_t st);
+void launch_axpy(double *y, const double *x, double alpha, int64_t count, cudaStream_t st);
+
+int reduce_partials_count();
+
+}  // namespace mfs
