@@ -88,6 +88,10 @@ struct LevelPlan {
     };
     std::vector<Step> steps;
     int syrk_off = 0, syrk_n = 0, syrk_tiles = 0;
+    // solve task lists of this level
+    int sasm_off = 0, sasm_n = 0, sasm_tiles = 0;
+    int ftri_off = 0, ftri_n = 0;
+    int btri_off = 0, btri_n = 0;
 };
 
 struct DevSym {
@@ -99,6 +103,9 @@ struct DevSym {
     DBuf<PotrfTask> potrf_tasks;
     DBuf<TrsmTask> trsm_tasks;
     DBuf<GemmTask> gemm_tasks;
+    DBuf<SolveAsmTask> sasm_tasks;
+    DBuf<SolveTask> ftri_tasks, btri_tasks;
+    DBuf<int> flags;                     // one per 64-row diagonal block of every front
     DBuf<int64_t> spmv_ptr, spmv_src;
     DBuf<int32_t> spmv_col, spmv_flag;
     DBuf<int64_t> prrfr, sperm;
@@ -143,6 +150,8 @@ struct mfs_handle {
     DBuf<double> partials, dots;
     DBuf<int> active;
     DBuf<int> fail;
+    DBuf<int> solve_err;          // set by a solve kernel whose dependency wait timed out
+    int epoch = 0;                // flag epoch of the cooperative solve kernels
     int *fail_host = nullptr;
     double *dots_host = nullptr;
     // assembly
@@ -347,6 +356,50 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         L.syrk_n = int(gemm_tasks.size()) - L.syrk_off;
         L.syrk_tiles = sb;
     }
+    // ---- solve tasks (all supernodes, level by level)
+    const int RB = solve_rows_per_task();
+    std::vector<int32_t> flag_base(nsn);
+    int nflags = 0;
+    for (idx s = 0; s < nsn; ++s) {
+        flag_base[s] = nflags;
+        nflags += int((S.w[s] + RB - 1) / RB);
+    }
+    std::vector<SolveAsmTask> sasm;
+    std::vector<SolveTask> ftri, btri;
+    for (idx l = 0; l < S.nlevels; ++l) {
+        LevelPlan &L = ds->levels[l];
+        L.sasm_off = int(sasm.size());
+        L.ftri_off = int(ftri.size());
+        L.btri_off = int(btri.size());
+        int base = 0, maxblk = 0, maxnbw = 0;
+        for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
+            const idx s = S.level_list[k];
+            if (S.child_ptr[s + 1] > S.child_ptr[s] || S.d[s] > 0) {
+                sasm.push_back({int32_t(s), base});
+                base += int((S.f[s] + kSolveAsmRows - 1) / kSolveAsmRows);
+            }
+            const int nbw = int((S.w[s] + RB - 1) / RB), nbd = int((S.d[s] + RB - 1) / RB);
+            maxblk = std::max(maxblk, nbw + nbd);
+            maxnbw = std::max(maxnbw, nbw);
+        }
+        L.sasm_n = int(sasm.size()) - L.sasm_off;
+        L.sasm_tiles = base;
+        // ascending block index across the level's fronts: every dependency precedes its task
+        for (int b = 0; b < maxblk; ++b)
+            for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
+                const idx s = S.level_list[k];
+                const int nbw = int((S.w[s] + RB - 1) / RB), nbd = int((S.d[s] + RB - 1) / RB);
+                if (b < nbw + nbd) ftri.push_back({int32_t(s), b, flag_base[s], 0});
+            }
+        for (int p = 0; p < maxnbw; ++p)
+            for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
+                const idx s = S.level_list[k];
+                const int nbw = int((S.w[s] + RB - 1) / RB);
+                if (p < nbw) btri.push_back({int32_t(s), nbw - 1 - p, flag_base[s], 0});
+            }
+        L.ftri_n = int(ftri.size()) - L.ftri_off;
+        L.btri_n = int(btri.size()) - L.btri_off;
+    }
     ds->small_list.upload(small_list, st);
     ds->all_list.upload(all_list, st);
     auto up = [&](auto &buf, const auto &vec) {
@@ -358,6 +411,11 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     up(ds->potrf_tasks, potrf_tasks);
     up(ds->trsm_tasks, trsm_tasks);
     up(ds->gemm_tasks, gemm_tasks);
+    up(ds->sasm_tasks, sasm);
+    up(ds->ftri_tasks, ftri);
+    up(ds->btri_tasks, btri);
+    ds->flags.ensure(size_t(std::max(nflags, 1)));
+    MFS_CUDA(cudaMemsetAsync(ds->flags.p, 0, ds->flags.bytes(), st));
     MFS_CUDA(cudaStreamSynchronize(st));
 
     SnDev &sd = ds->sd;
@@ -423,17 +481,33 @@ template <typename T>
 void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) {
     const Symbolic &S = *ds.S;
     cudaStream_t st = h->stream;
-    h->sol.ensure(size_t(std::max<idx>(S.sol_size, 1)) * nrhs);
-    for (size_t l = 0; l < ds.levels.size(); ++l) {
-        const LevelPlan &L = ds.levels[l];
-        launch_fwd_level<T>(ds.all_list.p + L.all_off, L.all_count, L.all_max_front, ds.sd, factor, X, S.n, nrhs,
-                            h->sol.p, st);
-        MFS_LAUNCHED();
+    const int chunk = std::min(nrhs, kMaxSolveRhs);
+    h->sol.ensure(size_t(std::max<idx>(S.sol_size, 1)) * chunk);
+    for (int r0 = 0; r0 < nrhs; r0 += kMaxSolveRhs) {
+        const int nr = std::min(kMaxSolveRhs, nrhs - r0);
+        double *Xc = X + int64_t(r0) * S.n;
+        for (size_t l = 0; l < ds.levels.size(); ++l) {
+            const LevelPlan &L = ds.levels[l];
+            launch_fwd_asm(ds.sasm_tasks.p + L.sasm_off, L.sasm_n, L.sasm_tiles, ds.sd, Xc, S.n, nr, h->sol.p, st);
+            MFS_LAUNCHED();
+            MFS_CUDA(launch_fwd_tri<T>(ds.ftri_tasks.p + L.ftri_off, L.ftri_n, ds.sd, factor, Xc, S.n, nr, h->sol.p,
+                                       ds.flags.p, ++h->epoch, h->solve_err.p, st));
+        }
+        for (size_t l = ds.levels.size(); l-- > 0;) {
+            const LevelPlan &L = ds.levels[l];
+            MFS_CUDA(launch_bwd_tri<T>(ds.btri_tasks.p + L.btri_off, L.btri_n, ds.sd, factor, Xc, S.n, nr, ds.flags.p,
+                                       ++h->epoch, h->solve_err.p, st));
+        }
     }
-    for (size_t l = ds.levels.size(); l-- > 0;) {
-        const LevelPlan &L = ds.levels[l];
-        launch_bwd_level<T>(ds.all_list.p + L.all_off, L.all_count, L.all_max_front, ds.sd, factor, X, S.n, nrhs, st);
-        MFS_LAUNCHED();
+}
+
+// After a stream synchronisation: a solve wait that timed out is an error.
+void check_solve_error(mfs_handle *h) {
+    int e = 0;
+    MFS_CUDA(cudaMemcpy(&e, h->solve_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        MFS_CUDA(cudaMemset(h->solve_err.p, 0, sizeof(int)));
+        throw StatusError(MFS_TIMEOUT, "triangular solve: a dependency wait timed out");
     }
 }
 
@@ -515,6 +589,7 @@ void refine_solve(mfs_handle *h, const double *B, double *X, int nrhs) {
         MFS_LAUNCHED();
         MFS_CUDA(cudaMemcpyAsync(hr.data(), rz2, nrhs * sizeof(double), cudaMemcpyDeviceToHost, st));
         MFS_CUDA(cudaStreamSynchronize(st));
+        check_solve_error(h);
         worst = 0.0;
         all_done = true;
         for (int r = 0; r < nrhs; ++r) {
@@ -604,7 +679,8 @@ mfs_status mfs_create(mfs_handle **out, const mfs_options *opt) {
         MFS_CUDA(cudaMallocHost(&h->fail_host, sizeof(int)));
         MFS_CUDA(cudaMallocHost(&h->dots_host, 64 * sizeof(double)));
         h->fail.ensure(1);
-        h->stats.failed_column = -1;
+        h->solve_err.ensure(1);
+        MFS_CUDA(cudaMemset(h->solve_err.p, 0, sizeof(int)));
     });
     if (s != MFS_OK) {
         // keep the message reachable for callers that only get a status
@@ -816,6 +892,7 @@ mfs_status mfs_solve(mfs_handle *h, const double *B, double *X, int64_t nrhs, in
         MFS_CUDA(cudaEventRecord(h->ev1, st));
         if (!dev) MFS_CUDA(cudaMemcpyAsync(X, h->io.p, io_sz * sizeof(double), cudaMemcpyDeviceToHost, st));
         MFS_CUDA(cudaStreamSynchronize(st));
+        check_solve_error(h);
         float ms = 0;
         cudaEventElapsedTime(&ms, h->ev0, h->ev1);
         h->stats.solve_ms = ms;

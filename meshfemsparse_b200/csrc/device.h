@@ -71,6 +71,20 @@ struct AssembleTask {
     int32_t tile_base;                  // prefix over tasks of column chunks
 };
 
+// Solve tasks: one 64-row block of a front (blk < ceil(w/64): diagonal block,
+// otherwise structure block blk - ceil(w/64)); flag_base indexes the front's
+// first diagonal-block flag.
+struct SolveTask {
+    int32_t sn, blk, flag_base, pad;
+};
+// Forward extend-add of children's update vectors, split by front rows.
+struct SolveAsmTask {
+    int32_t sn;
+    int32_t tile_base;
+};
+constexpr int kSolveAsmRows = 256;      // front rows per forward extend-add CTA
+constexpr int kMaxSolveRhs = 32;        // right-hand sides per solve pass (more are chunked)
+
 constexpr int kAsmCols = 32;            // front columns per assemble CTA
 constexpr int kGemmTile = 64;           // C tile edge of the update kernels
 constexpr int kTrsmRows = 64;           // rows per TRSM CTA
@@ -98,12 +112,15 @@ void launch_gemm_update(const GemmTask *tasks, int ntasks, int ntiles, const T *
                         cudaStream_t st);
 
 // Solves (the factor type T may be float while vectors stay double).
+void launch_fwd_asm(const SolveAsmTask *tasks, int ntasks, int ntiles, SnDev sd, double *X, int64_t ldx, int nrhs,
+                    double *sol, cudaStream_t st);
 template <typename T>
-void launch_fwd_level(const int32_t *list, int count, int max_front, SnDev sd, const T *factor, double *X,
-                      int64_t ldx, int nrhs, double *sol, cudaStream_t st);
+cudaError_t launch_fwd_tri(const SolveTask *tasks, int ntasks, SnDev sd, const T *factor, double *X, int64_t ldx,
+                           int nrhs, double *sol, int *flags, int epoch, int *err, cudaStream_t st);
 template <typename T>
-void launch_bwd_level(const int32_t *list, int count, int max_front, SnDev sd, const T *factor, double *X,
-                      int64_t ldx, int nrhs, cudaStream_t st);
+cudaError_t launch_bwd_tri(const SolveTask *tasks, int ntasks, SnDev sd, const T *factor, double *X, int64_t ldx,
+                           int nrhs, int *flags, int epoch, int *err, cudaStream_t st);
+int solve_rows_per_task();
 
 // Symmetric block SpMV over permuted reduced rows: Y = A X (both ld = n).
 void launch_spmv(const int64_t *ptr, const int64_t *src, const int32_t *col, const int32_t *flag, int64_t nrows,

@@ -1,4 +1,4 @@
-// Triangular solves (K6), symmetric block SpMV (K7), the fused
+// Symmetric block SpMV (K7), the fused
 // pin-removal/permutation gathers, element assembly (K1) and the FP64
 // vector kernels of the refinement loop.
 //
@@ -11,10 +11,7 @@
 //   ..................................... BlockCSCHessian.hh:1080-1120
 //   ElementHessianContribAssembler<true>::run + ColumnScanner::addBlockAtLoc
 //   ..................................... SystemAssembler.hh:60-98, BlockCSCHessian.hh:371-381
-// The forward solve follows the multifrontal assembly tree: every supernode
-// solves with its diagonal block and hands an update vector u_s = (front rows
-// below the block) to its parent, which pulls it through the same relative
-// indices as the factorization. No atomics; results are run-to-run identical.
+// The triangular solves themselves live in kernels_trisolve.cu.
 #include "device.h"
 
 namespace mfs {
@@ -23,85 +20,6 @@ namespace {
 
 constexpr int kReduceBlocks = 296;   // 2 x SM count; fixed so reductions are deterministic
 
-__device__ __forceinline__ int child_rel(const int32_t *rel, int i, int vb) { return rel[i / vb] + i % vb; }
-
-template <typename T>
-__global__ void __launch_bounds__(256) fwd_level_kernel(const int32_t *__restrict__ list, SnDev sd,
-                                                        const T *__restrict__ factor, double *__restrict__ X,
-                                                        int64_t ldx, int nrhs, double *__restrict__ sol) {
-    const int s = list[blockIdx.x];
-    const int w = sd.w[s], d = sd.d[s], f = w + d;
-    const int c0 = sd.col0[s];
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int vb = sd.vb;
-    double *us = (d > 0 && sd.sol_off[s] >= 0) ? sol + sd.sol_off[s] * nrhs : nullptr;
-    if (us)
-        for (int t = tid; t < d * nrhs; t += nt) us[t] = 0.0;
-    __syncthreads();
-    for (int ci = sd.child_ptr[s]; ci < sd.child_ptr[s + 1]; ++ci) {
-        const int c = sd.child_list[ci];
-        const int dc = sd.d[c];
-        const double *uc = sol + sd.sol_off[c] * nrhs;
-        const int32_t *rel = sd.rel + sd.struct_ptr[c];
-        for (int t = tid; t < dc * nrhs; t += nt) {
-            const int r = t / dc, i = t - r * dc;
-            const int ri = child_rel(rel, i, vb);
-            const double v = uc[t];
-            if (ri < w) X[c0 + ri + r * ldx] += v;
-            else us[(ri - w) + r * d] += v;
-        }
-        __syncthreads();
-    }
-    const T *pan = factor + sd.pan_off[s];
-    for (int k = 0; k < w; ++k) {
-        const T *Lk = pan + int64_t(k) * f;
-        for (int r = tid; r < nrhs; r += nt) X[c0 + k + r * ldx] /= double(Lk[k]);
-        __syncthreads();
-        const int m = f - k - 1;
-        for (int t = tid; t < m * nrhs; t += nt) {
-            const int r = t / m, i = k + 1 + (t - r * m);
-            const double xk = X[c0 + k + r * ldx];
-            const double l = double(Lk[i]);
-            if (i < w) X[c0 + i + r * ldx] -= l * xk;
-            else us[(i - w) + r * d] -= l * xk;
-        }
-        __syncthreads();
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) bwd_level_kernel(const int32_t *__restrict__ list, SnDev sd,
-                                                        const T *__restrict__ factor, double *__restrict__ X,
-                                                        int64_t ldx, int nrhs) {
-    const int s = list[blockIdx.x];
-    const int w = sd.w[s], d = sd.d[s], f = w + d;
-    const int c0 = sd.col0[s];
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int vb = sd.vb;
-    const T *pan = factor + sd.pan_off[s];
-    const int32_t *rows = sd.struct_rows + sd.struct_ptr[s];
-    // y_k -= sum_{i in struct} L(i,k) x_i  (thread per (k, rhs))
-    for (int t = tid; t < w * nrhs; t += nt) {
-        const int r = t / w, k = t - r * w;
-        const T *col = pan + int64_t(k) * f + w;
-        double acc = 0.0;
-        for (int i = 0; i < d; ++i) {
-            const int gi = rows[i / vb] * vb + i % vb;
-            acc += double(col[i]) * X[gi + r * ldx];
-        }
-        X[c0 + k + r * ldx] -= acc;
-    }
-    __syncthreads();
-    for (int i = w - 1; i >= 0; --i) {
-        for (int r = tid; r < nrhs; r += nt) X[c0 + i + r * ldx] /= double(pan[int64_t(i) * f + i]);
-        __syncthreads();
-        for (int t = tid; t < i * nrhs; t += nt) {
-            const int r = t / i, k = t - r * i;
-            X[c0 + k + r * ldx] -= double(pan[int64_t(k) * f + i]) * X[c0 + i + r * ldx];
-        }
-        __syncthreads();
-    }
-}
 
 __global__ void spmv_kernel(const int64_t *__restrict__ ptr, const int64_t *__restrict__ src,
                             const int32_t *__restrict__ col, const int32_t *__restrict__ flag, int64_t nrows, int vb,
@@ -261,33 +179,6 @@ inline int grid_for(int64_t n, int threads) {
 }  // namespace
 
 int reduce_partials_count() { return kReduceBlocks; }
-
-template <typename T>
-void launch_fwd_level(const int32_t *list, int count, int max_front, SnDev sd, const T *factor, double *X,
-                      int64_t ldx, int nrhs, double *sol, cudaStream_t st) {
-    (void)max_front;
-    if (count <= 0) return;
-    ++g_kernel_launches;
-    fwd_level_kernel<T><<<count, 256, 0, st>>>(list, sd, factor, X, ldx, nrhs, sol);
-}
-
-template <typename T>
-void launch_bwd_level(const int32_t *list, int count, int max_front, SnDev sd, const T *factor, double *X,
-                      int64_t ldx, int nrhs, cudaStream_t st) {
-    (void)max_front;
-    if (count <= 0) return;
-    ++g_kernel_launches;
-    bwd_level_kernel<T><<<count, 256, 0, st>>>(list, sd, factor, X, ldx, nrhs);
-}
-
-template void launch_fwd_level<double>(const int32_t *, int, int, SnDev, const double *, double *, int64_t, int,
-                                       double *, cudaStream_t);
-template void launch_fwd_level<float>(const int32_t *, int, int, SnDev, const float *, double *, int64_t, int,
-                                      double *, cudaStream_t);
-template void launch_bwd_level<double>(const int32_t *, int, int, SnDev, const double *, double *, int64_t, int,
-                                       cudaStream_t);
-template void launch_bwd_level<float>(const int32_t *, int, int, SnDev, const float *, double *, int64_t, int,
-                                      cudaStream_t);
 
 void launch_spmv(const int64_t *ptr, const int64_t *src, const int32_t *col, const int32_t *flag, int64_t nrows,
                  int vb, int src_ld, const double *Ax, const double *X, double *Y, int64_t ld, int nrhs,

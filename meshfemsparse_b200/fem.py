@@ -126,7 +126,7 @@ def neo_hookean_hessians(nodes, tets, u, E, nu, clamp: float = 1e-8, device: str
     lam, mu = lame(np.broadcast_to(E, (ne,)), np.broadcast_to(nu, (ne,)))
     dev = torch.device(device) if device else torch.device("cpu")
     out = np.empty((ne, 12, 12))
-    chunk = 1 << 18
+    chunk = 1 << 16
     for s in range(0, ne, chunk):
         e = slice(s, min(ne, s + chunk))
         G = torch.as_tensor(g[e], device=dev)                               # m,4,3  (a, J)
@@ -147,11 +147,14 @@ def neo_hookean_hessians(nodes, tets, u, E, nu, clamp: float = 1e-8, device: str
         K = torch.einsum("maJ,miJkL,mbL->maibk", G, A, G).reshape(-1, 12, 12)
         K = K * torch.as_tensor(V[e], device=dev)[:, None, None]
         K = 0.5 * (K + K.transpose(1, 2))
-        w, Q = torch.linalg.eigh(K)
+        # SPD projection on the host (batched syevd from the CUDA math library
+        # rejects these batch shapes on some driver/library combinations)
+        Kc = K.cpu()
+        w, Q = torch.linalg.eigh(Kc)
         w = torch.clamp(w, min=clamp)
-        K = (Q * w[:, None, :]) @ Q.transpose(1, 2)
-        K = 0.5 * (K + K.transpose(1, 2))
-        out[e] = K.cpu().numpy()
+        Kc = (Q * w[:, None, :]) @ Q.transpose(1, 2)
+        Kc = 0.5 * (Kc + Kc.transpose(1, 2))
+        out[e] = Kc.numpy()
     return out
 
 
