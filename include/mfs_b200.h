@@ -73,7 +73,8 @@ typedef struct {
     double refine_tol;          /* relative residual target ||b - Hx|| / ||b|| (1e-10) */
     int32_t refine_maxit;       /* iteration cap (50) */
     int32_t use_graphs;         /* capture the factorization / solve launch sequence in CUDA graphs */
-    int32_t tensor_cores;       /* FP32 path: 0 FMA, 1 TF32 tensor cores, 2 split 3xTF32 */
+    int32_t tensor_cores;       /* FP32 Schur updates: 0 auto (TF32 with refinement, else split 3xTF32),
+                                   1 TF32, 2 split 3xTF32 (FP32-level products) */
     int32_t reserved[7];
 } mfs_options;
 

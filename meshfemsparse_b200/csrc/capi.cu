@@ -74,7 +74,6 @@ struct DBuf {
     size_t bytes() const { return n * sizeof(T); }
 };
 
-constexpr int kNB = 64;   // column block of the tiled large-front factorization
 
 struct LevelPlan {
     int small_off = 0, small_count = 0, small_max_front = 0;
@@ -101,7 +100,6 @@ struct DevSym {
     DBuf<PlanEntryDev> plan;
     DBuf<AssembleTask> asm_tasks;
     DBuf<PotrfTask> potrf_tasks;
-    DBuf<TrsmTask> trsm_tasks;
     DBuf<GemmTask> gemm_tasks;
     DBuf<SolveAsmTask> sasm_tasks;
     DBuf<SolveTask> ftri_tasks, btri_tasks;
@@ -114,11 +112,12 @@ struct DevSym {
     int64_t ax_len = 0;
     std::vector<int64_t> Ap_full, Ai_full;   // caller's pattern (for the element slot map)
     int num_large = 0;
+    int inv_slots = 0;                   // diagonal-block inverses needed by one factorization step
     size_t bytes() const {
         return w.bytes() * 4 + col0.bytes() + child_ptr.bytes() + child_list.bytes() + struct_rows.bytes() +
                rel.bytes() + small_list.bytes() + all_list.bytes() + pan_off.bytes() + upd_off.bytes() +
                sol_off.bytes() + struct_ptr.bytes() + diag_off.bytes() + plan.bytes() + asm_tasks.bytes() +
-               potrf_tasks.bytes() + trsm_tasks.bytes() + gemm_tasks.bytes() + spmv_ptr.bytes() +
+               potrf_tasks.bytes() + gemm_tasks.bytes() + spmv_ptr.bytes() +
                spmv_src.bytes() + spmv_col.bytes() + spmv_flag.bytes() + prrfr.bytes() + sperm.bytes();
     }
 };
@@ -142,8 +141,8 @@ struct mfs_handle {
     bool own_stream = false;
     State cur, stash;
     bool has_stash = false;
-    DBuf<double> upd64;
-    DBuf<float> upd32;
+    DBuf<double> upd64, inv64;     // update arena, diagonal-block inverses (scratch)
+    DBuf<float> upd32, inv32;
     DBuf<double> sol;
     std::shared_ptr<DBuf<double>> asm_ax;   // output of the last mfs_assemble (device resident)
     DBuf<double> rhs, work_r, work_z, work_p, work_ap, work_x, work_s, io;
@@ -251,8 +250,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     std::vector<int32_t> small_list, all_list;
     std::vector<AssembleTask> asm_tasks;
     std::vector<PotrfTask> potrf_tasks;
-    std::vector<TrsmTask> trsm_tasks;
     std::vector<GemmTask> gemm_tasks;
+    int max_inv_slots = 0;
     ds->levels.resize(S.nlevels);
     ds->num_large = 0;
     for (idx l = 0; l < S.nlevels; ++l) {
@@ -284,53 +283,69 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         }
         L.asm_n = int(large.size());
         L.asm_tiles = base;
-        for (idx kb = 0; kb < maxw; kb += kNB) {
+        const bool f64 = h->opt.precision != MFS_PREC_FP32;
+        const int NB = f64 ? 64 : 128;                  // <= GEMM tile N: the in-place panel solve needs one column tile
+        const int TM = gemm_tile_m(f64), TN = gemm_tile_n(f64);
+        auto gemm = [&](int64_t a_off, int64_t b_off, int64_t c_off, int lda, int ldb, int ldc, idx m, idx n, idx k,
+                        int lower, int mode, int &base) {
+            GemmTask g{};
+            g.a_off = a_off; g.b_off = b_off; g.c_off = c_off;
+            g.lda = lda; g.ldb = ldb; g.ldc = ldc;
+            g.m = int32_t(m); g.n = int32_t(n); g.k = int32_t(k);
+            g.tiles_m = int32_t((m + TM - 1) / TM);
+            g.tiles_n = int32_t((n + TN - 1) / TN);
+            g.tile_base = base;
+            g.lower = lower;
+            g.mode = mode;
+            base += g.tiles_m * g.tiles_n;
+            gemm_tasks.push_back(g);
+        };
+        for (idx kb = 0; kb < maxw; kb += NB) {
             LevelPlan::Step sp{};
             sp.potrf_off = int(potrf_tasks.size());
-            sp.trsm_off = int(trsm_tasks.size());
-            sp.gemm_off = int(gemm_tasks.size());
-            int tb = 0, gb = 0;
+            int slot = 0;
             for (idx s : large) {
                 const idx w = S.w[s], f = S.f[s], pan = S.pan_off[s];
                 if (w <= kb) continue;
-                const int nb = int(std::min<idx>(kNB, w - kb));
-                potrf_tasks.push_back({pan + kb * f + kb, int32_t(f), nb, int32_t(col0[s] + kb), 0});
+                const int nb = int(std::min<idx>(NB, w - kb));
+                PotrfTask pt{};
+                pt.off = pan + kb * f + kb;
+                pt.inv_off = int64_t(slot++) * NB * NB;
+                pt.ld = int32_t(f);
+                pt.nb = nb;
+                pt.col = int32_t(col0[s] + kb);
+                potrf_tasks.push_back(pt);
                 sp.potrf_maxnb = std::max(sp.potrf_maxnb, nb);
-                const idx m = f - kb - nb;
-                if (m > 0) {
-                    TrsmTask t{};
-                    t.l_off = pan + kb * f + kb;
-                    t.b_off = pan + kb * f + kb + nb;
-                    t.ld = int32_t(f);
-                    t.nb = nb;
-                    t.m = int32_t(m);
-                    t.tile_base = tb;
-                    tb += int((m + kTrsmRows - 1) / kTrsmRows);
-                    trsm_tasks.push_back(t);
-                    sp.trsm_maxnb = std::max(sp.trsm_maxnb, nb);
-                }
-                const idx n = w - kb - nb;
-                if (n > 0) {
-                    GemmTask g{};
-                    g.a_off = pan + kb * f + kb + nb;
-                    g.b_off = g.a_off;
-                    g.c_off = pan + (kb + nb) * f + kb + nb;
-                    g.lda = int32_t(f);
-                    g.ldc = int32_t(f);
-                    g.m = int32_t(m);
-                    g.n = int32_t(n);
-                    g.k = nb;
-                    g.tiles_m = int32_t((m + kGemmTile - 1) / kGemmTile);
-                    g.tiles_n = int32_t((n + kGemmTile - 1) / kGemmTile);
-                    g.tile_base = gb;
-                    g.lower = 1;
-                    gb += g.tiles_m * g.tiles_n;
-                    gemm_tasks.push_back(g);
-                }
             }
             sp.potrf_n = int(potrf_tasks.size()) - sp.potrf_off;
-            sp.trsm_n = int(trsm_tasks.size()) - sp.trsm_off;
+            max_inv_slots = std::max(max_inv_slots, slot);
+            // panel rows below the diagonal block: B := B inv(L_kk)^T (in place, one column tile)
+            sp.trsm_off = int(gemm_tasks.size());
+            int tb = 0;
+            slot = 0;
+            for (idx s : large) {
+                const idx w = S.w[s], f = S.f[s], pan = S.pan_off[s];
+                if (w <= kb) continue;
+                const int nb = int(std::min<idx>(NB, w - kb));
+                const idx m = f - kb - nb;
+                const int64_t inv = int64_t(slot++) * NB * NB;
+                if (m > 0) gemm(pan + kb * f + kb + nb, inv, pan + kb * f + kb + nb, int(f), nb, int(f), m, nb, nb, 0, 1, tb);
+            }
+            sp.trsm_n = int(gemm_tasks.size()) - sp.trsm_off;
             sp.trsm_tiles = tb;
+            // trailing update of the remaining panel columns
+            sp.gemm_off = int(gemm_tasks.size());
+            int gb = 0;
+            for (idx s : large) {
+                const idx w = S.w[s], f = S.f[s], pan = S.pan_off[s];
+                if (w <= kb) continue;
+                const int nb = int(std::min<idx>(NB, w - kb));
+                const idx m = f - kb - nb, n = w - kb - nb;
+                if (n > 0) {
+                    const int64_t a = pan + kb * f + kb + nb;
+                    gemm(a, a, pan + (kb + nb) * f + kb + nb, int(f), int(f), int(f), m, n, nb, 1, 0, gb);
+                }
+            }
             sp.gemm_n = int(gemm_tasks.size()) - sp.gemm_off;
             sp.gemm_tiles = gb;
             L.steps.push_back(sp);
@@ -339,23 +354,13 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         int sb = 0;
         for (idx s : large) {
             if (S.d[s] == 0 || S.upd_off[s] < 0) continue;
-            GemmTask g{};
-            g.a_off = S.pan_off[s] + S.w[s];
-            g.b_off = g.a_off;
-            g.c_off = S.upd_off[s];
-            g.lda = int32_t(S.f[s]);
-            g.ldc = int32_t(S.d[s]);
-            g.m = g.n = int32_t(S.d[s]);
-            g.k = int32_t(S.w[s]);
-            g.tiles_m = g.tiles_n = int32_t((S.d[s] + kGemmTile - 1) / kGemmTile);
-            g.tile_base = sb;
-            g.lower = 1;
-            sb += g.tiles_m * g.tiles_n;
-            gemm_tasks.push_back(g);
+            const int64_t a = S.pan_off[s] + S.w[s];
+            gemm(a, a, S.upd_off[s], int(S.f[s]), int(S.f[s]), int(S.d[s]), S.d[s], S.d[s], S.w[s], 1, 0, sb);
         }
         L.syrk_n = int(gemm_tasks.size()) - L.syrk_off;
         L.syrk_tiles = sb;
     }
+    ds->inv_slots = max_inv_slots;
     // ---- solve tasks (all supernodes, level by level)
     const int RB = solve_rows_per_task();
     std::vector<int32_t> flag_base(nsn);
@@ -409,7 +414,6 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     };
     up(ds->asm_tasks, asm_tasks);
     up(ds->potrf_tasks, potrf_tasks);
-    up(ds->trsm_tasks, trsm_tasks);
     up(ds->gemm_tasks, gemm_tasks);
     up(ds->sasm_tasks, sasm);
     up(ds->ftri_tasks, ftri);
@@ -436,9 +440,13 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
 }
 
 template <typename T>
-void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, const double *Ax, const double *Bx, double sigma) {
+void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *inv, const double *Ax, const double *Bx,
+                double sigma) {
     const Symbolic &S = *ds.S;
     cudaStream_t st = h->stream;
+    // FP32 factors: single-pass TF32 when FP64 refinement recovers the accuracy,
+    // split 3xTF32 (FP32-level products) otherwise or when asked for.
+    const int split = (h->opt.tensor_cores == 2 || (h->opt.tensor_cores == 0 && !h->opt.refine)) ? 3 : 1;
     launch_zero<T>(factor, S.factor_size, st);
     MFS_LAUNCHED();
     launch_inject<T>(ds.plan.p, int64_t(S.plan.size()), S.vb, S.src_ld, Ax, Bx, Bx ? sigma : 0.0, factor, st);
@@ -457,21 +465,16 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, const double *Ax, 
         launch_assemble_large<T>(ds.asm_tasks.p + L.asm_off, L.asm_n, L.asm_tiles, ds.sd, factor, upd, st);
         MFS_LAUNCHED();
         for (const auto &sp : L.steps) {
-            launch_potrf<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, h->fail.p, st);
+            launch_potrf_inv<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, inv, h->fail.p,
+                                st);
             MFS_LAUNCHED();
-            if (sp.trsm_n > 0) {
-                launch_trsm<T>(ds.trsm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, sp.trsm_maxnb, factor, st);
-                MFS_LAUNCHED();
-            }
-            if (sp.gemm_n > 0) {
-                launch_gemm_update<T>(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor,
-                                      h->opt.tensor_cores, st);
-                MFS_LAUNCHED();
-            }
+            launch_gemm<T>(ds.gemm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, factor, inv, factor, split, st);
+            MFS_LAUNCHED();
+            launch_gemm<T>(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor, factor, split, st);
+            MFS_LAUNCHED();
         }
         if (L.syrk_n > 0) {
-            launch_gemm_update<T>(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, upd,
-                                  h->opt.tensor_cores, st);
+            launch_gemm<T>(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, factor, upd, split, st);
             MFS_LAUNCHED();
         }
     }
@@ -650,7 +653,7 @@ mfs_status mfs_default_options(mfs_options *opt) {
     opt->refine_tol = 1e-10;
     opt->refine_maxit = 50;
     opt->use_graphs = 0;
-    opt->tensor_cores = 1;
+    opt->tensor_cores = 0;
     return MFS_OK;
 }
 
@@ -825,12 +828,14 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
             if (!h->cur.f32 || h->cur.f32.use_count() > 1) h->cur.f32 = std::make_shared<DBuf<float>>();
             h->cur.f32->ensure(size_t(std::max<idx>(S.factor_size, 1)));
             h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
-            run_factor<float>(h, ds, h->cur.f32->p, h->upd32.p, h->cur.ax->p, dBx, sigma);
+            h->inv32.ensure(size_t(std::max(ds.inv_slots, 1)) * 128 * 128);
+            run_factor<float>(h, ds, h->cur.f32->p, h->upd32.p, h->inv32.p, h->cur.ax->p, dBx, sigma);
         } else {
             if (!h->cur.f64 || h->cur.f64.use_count() > 1) h->cur.f64 = std::make_shared<DBuf<double>>();
             h->cur.f64->ensure(size_t(std::max<idx>(S.factor_size, 1)));
             h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
-            run_factor<double>(h, ds, h->cur.f64->p, h->upd64.p, h->cur.ax->p, dBx, sigma);
+            h->inv64.ensure(size_t(std::max(ds.inv_slots, 1)) * 64 * 64);
+            run_factor<double>(h, ds, h->cur.f64->p, h->upd64.p, h->inv64.p, h->cur.ax->p, dBx, sigma);
         }
         MFS_CUDA(cudaEventRecord(h->ev1, st));
         MFS_CUDA(cudaMemcpyAsync(h->fail_host, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -38,31 +38,27 @@ struct PlanEntryDev {
     int32_t flags;
 };
 
-// C(i,j) -= sum_k A(i,k) * A'(j,k) over a tile grid; A and A' share the
-// leading dimension lda (both are column ranges of one panel).
+// C(i,j) -= sum_k A(i,k) B(j,k)  (mode 0)  or  C(i,j) = sum_k A(i,k) B(j,k)  (mode 1)
+// for i < m, j < n over a grid of tiles_m x tiles_n CTA tiles; A, B, C are
+// column-major blocks at the given offsets of the launch's three base arrays.
 struct GemmTask {
     int64_t a_off, b_off, c_off;
-    int32_t lda, ldc;
+    int32_t lda, ldb, ldc;
     int32_t m, n, k;
     int32_t tiles_m, tiles_n;
     int32_t tile_base;                  // prefix over tasks of tiles_m*tiles_n
-    int32_t lower;                      // 1: only i >= j is updated
+    int32_t lower;                      // 1: only i >= j is touched
+    int32_t mode;
 };
 
-// Dense Cholesky of an nb x nb diagonal block held in a panel.
+// Dense Cholesky of an nb x nb diagonal block held in a panel; inv(L) of the
+// block goes to scratch slot inv_off (nb x nb, ld nb).
 struct PotrfTask {
     int64_t off;                        // offset of the block's (0,0) entry
+    int64_t inv_off;
     int32_t ld, nb;
     int32_t col;                        // global scalar column of the block's first pivot
     int32_t pad;
-};
-
-// X L^T = B for the rows below a factored diagonal block.
-struct TrsmTask {
-    int64_t l_off;                      // diagonal block (nb x nb, lower)
-    int64_t b_off;                      // first row of the block column below
-    int32_t ld, nb, m;                  // m rows
-    int32_t tile_base;                  // prefix over tasks of row tiles
 };
 
 // Extend-add of all children of a large supernode, split by front columns.
@@ -86,8 +82,6 @@ constexpr int kSolveAsmRows = 256;      // front rows per forward extend-add CTA
 constexpr int kMaxSolveRhs = 32;        // right-hand sides per solve pass (more are chunked)
 
 constexpr int kAsmCols = 32;            // front columns per assemble CTA
-constexpr int kGemmTile = 64;           // C tile edge of the update kernels
-constexpr int kTrsmRows = 64;           // rows per TRSM CTA
 
 // ---------------------------------------------------------------- launchers
 template <typename T>
@@ -104,12 +98,14 @@ template <typename T>
 void launch_assemble_large(const AssembleTask *tasks, int ntasks, int ntiles, SnDev sd, T *factor, T *upd,
                            cudaStream_t st);
 template <typename T>
-void launch_potrf(const PotrfTask *tasks, int ntasks, int max_nb, T *factor, int *fail_col, cudaStream_t st);
+void launch_potrf_inv(const PotrfTask *tasks, int ntasks, int max_nb, T *factor, T *inv, int *fail_col,
+                      cudaStream_t st);
+// Tensor-core tile GEMM (TF32 / split 3xTF32 for float, DMMA for double).
 template <typename T>
-void launch_trsm(const TrsmTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, cudaStream_t st);
-template <typename T>
-void launch_gemm_update(const GemmTask *tasks, int ntasks, int ntiles, const T *a, T *c, int use_tc,
-                        cudaStream_t st);
+void launch_gemm(const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int split,
+                 cudaStream_t st);
+int gemm_tile_m(bool fp64);
+int gemm_tile_n(bool fp64);
 
 // Solves (the factor type T may be float while vectors stay double).
 void launch_fwd_asm(const SolveAsmTask *tasks, int ntasks, int ntiles, SnDev sd, double *X, int64_t ldx, int nrhs,

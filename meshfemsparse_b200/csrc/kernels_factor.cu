@@ -182,149 +182,66 @@ __global__ void __launch_bounds__(256) assemble_large_kernel(const AssembleTask 
     }
 }
 
-// K3: Cholesky of one nb x nb diagonal block per CTA.
+// K3 (+ the inverse used by the K4 panel solve): Cholesky of one nb x nb
+// diagonal block per CTA. Right-looking on an unscaled working copy S with the
+// scaled column written to a separate output, so each column costs one barrier:
+//   L(k,k) = sqrt(S(k,k)),  L(i,k) = S(i,k) / L(k,k),
+//   S(i,j) -= S(i,k) S(j,k) / S(k,k)   for k < j <= i.
+// Then inv(L) is formed column by column (forward substitution on e_j) and
+// written to the scratch slot of the task; the panel below is solved as the
+// GEMM  B := B inv(L)^T.
 template <typename T>
-__global__ void __launch_bounds__(256) potrf_kernel(const PotrfTask *__restrict__ tasks, T *__restrict__ factor,
-                                                    int *__restrict__ fail_col) {
+__global__ void __launch_bounds__(256) potrf_inv_kernel(const PotrfTask *__restrict__ tasks, T *__restrict__ factor,
+                                                        T *__restrict__ inv, int *__restrict__ fail_col) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *S = reinterpret_cast<T *>(smem_raw);
     const PotrfTask tk = tasks[blockIdx.x];
     const int nb = tk.nb, ld = tk.ld;
+    T *S = reinterpret_cast<T *>(smem_raw);
+    T *Lo = S + nb * nb;
     T *blk = factor + tk.off;
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int k = tid; k < nb * nb; k += nt) {
         const int j = k / nb, i = k - j * nb;
-        S[k] = i >= j ? blk[int64_t(j) * ld + i] : T(0);
+        const T v = i >= j ? blk[int64_t(j) * ld + i] : T(0);
+        S[k] = v;
+        Lo[k] = T(0);
     }
     __syncthreads();
     for (int k = 0; k < nb; ++k) {
-        T *colk = S + k * nb;
-        if (tid == 0) {
-            T a = colk[k];
-            if (!(a > T(0))) { atomicMin(fail_col, tk.col + k); a = T(1); }
-            colk[k] = dev_sqrt(a);
+        T akk = S[k * nb + k];
+        if (!(akk > T(0))) {
+            if (tid == 0) atomicMin(fail_col, tk.col + k);
+            akk = T(1);
         }
-        __syncthreads();
-        const T piv = colk[k];
-        for (int i = k + 1 + tid; i < nb; i += nt) colk[i] = colk[i] / piv;
-        __syncthreads();
+        const T rs = dev_sqrt(akk);
+        const T rinv = T(1) / akk;
+        const T *Sk = S + k * nb;
+        for (int i = k + tid; i < nb; i += nt) Lo[k * nb + i] = (i == k) ? rs : Sk[i] / rs;
         const int m = nb - k - 1;
         for (int t = tid; t < m * m; t += nt) {
             const int jj = t / m, ii = t - jj * m;
             if (ii < jj) continue;
-            S[(k + 1 + jj) * nb + (k + 1 + ii)] -= colk[k + 1 + ii] * colk[k + 1 + jj];
+            const int j = k + 1 + jj, i = k + 1 + ii;
+            S[j * nb + i] -= Sk[i] * Sk[j] * rinv;
         }
         __syncthreads();
     }
+    // inv(L): column j solves L x = e_j (x_i = 0 for i < j); stored in S
+    for (int j = tid; j < nb; j += nt) {
+        for (int i = 0; i < j; ++i) S[j * nb + i] = T(0);
+        S[j * nb + j] = T(1) / Lo[j * nb + j];
+        for (int i = j + 1; i < nb; ++i) {
+            T a = T(0);
+            for (int k = j; k < i; ++k) a += Lo[k * nb + i] * S[j * nb + k];
+            S[j * nb + i] = -a / Lo[i * nb + i];
+        }
+    }
+    __syncthreads();
+    T *Iv = inv + tk.inv_off;
     for (int k = tid; k < nb * nb; k += nt) {
         const int j = k / nb, i = k - j * nb;
-        if (i >= j) blk[int64_t(j) * ld + i] = S[k];
-    }
-}
-
-// K4: rows below a factored diagonal block, X L^T = B, one thread per row.
-template <typename T>
-__global__ void __launch_bounds__(kTrsmRows) trsm_kernel(const TrsmTask *__restrict__ tasks, int ntasks,
-                                                          T *__restrict__ factor) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int t = blockIdx.x;
-    int lo = 0, hi = ntasks - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (tasks[mid].tile_base <= t) lo = mid; else hi = mid - 1;
-    }
-    const TrsmTask tk = tasks[lo];
-    const int tile = t - tk.tile_base;
-    const int nb = tk.nb, ld = tk.ld;
-    T *L = reinterpret_cast<T *>(smem_raw);             // nb x nb
-    T *B = L + nb * nb;                                 // kTrsmRows x (nb+1), row-major
-    const int bld = nb + 1;
-    const int tid = threadIdx.x;
-    for (int k = tid; k < nb * nb; k += blockDim.x) {
-        const int j = k / nb, i = k - j * nb;
-        L[k] = i >= j ? factor[tk.l_off + int64_t(j) * ld + i] : T(0);
-    }
-    const int r0 = tile * kTrsmRows;
-    const int rows = min(kTrsmRows, tk.m - r0);
-    for (int k = tid; k < kTrsmRows * nb; k += blockDim.x) {
-        const int j = k / kTrsmRows, i = k - j * kTrsmRows;
-        if (i < rows) B[i * bld + j] = factor[tk.b_off + int64_t(j) * ld + r0 + i];
-    }
-    __syncthreads();
-    if (tid < rows) {
-        T *x = B + tid * bld;
-        for (int j = 0; j < nb; ++j) {
-            T acc = x[j];
-            for (int k = 0; k < j; ++k) acc -= x[k] * L[k * nb + j];
-            x[j] = acc / L[j * nb + j];
-        }
-    }
-    __syncthreads();
-    for (int k = tid; k < kTrsmRows * nb; k += blockDim.x) {
-        const int j = k / kTrsmRows, i = k - j * kTrsmRows;
-        if (i < rows) factor[tk.b_off + int64_t(j) * ld + r0 + i] = B[i * bld + j];
-    }
-}
-
-// K5: C(i,j) -= sum_k A(i,k) A(j,k), 64x64 tile per CTA, FMA path.
-template <typename T>
-__global__ void __launch_bounds__(256) gemm_update_kernel(const GemmTask *__restrict__ tasks, int ntasks,
-                                                          const T *__restrict__ A, T *__restrict__ C) {
-    const int t = blockIdx.x;
-    int lo = 0, hi = ntasks - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (tasks[mid].tile_base <= t) lo = mid; else hi = mid - 1;
-    }
-    const GemmTask tk = tasks[lo];
-    const int local = t - tk.tile_base;
-    const int ti = local % tk.tiles_m, tj = local / tk.tiles_m;
-    const int i0 = ti * kGemmTile, j0 = tj * kGemmTile;
-    if (tk.lower && i0 + kGemmTile - 1 < j0) return;
-    constexpr int KC = 16;
-    __shared__ T As[KC][kGemmTile + 1];
-    __shared__ T Bs[KC][kGemmTile + 1];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    T acc[4][4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = T(0);
-    const T *Aa = A + tk.a_off;
-    const T *Ab = A + tk.b_off;
-    for (int k0 = 0; k0 < tk.k; k0 += KC) {
-        for (int l = threadIdx.x; l < KC * kGemmTile; l += 256) {
-            const int kk = l / kGemmTile, ii = l - kk * kGemmTile;
-            const int gk = k0 + kk;
-            const int gi = i0 + ii, gj = j0 + ii;
-            As[kk][ii] = (gi < tk.m && gk < tk.k) ? Aa[int64_t(gk) * tk.lda + gi] : T(0);
-            Bs[kk][ii] = (gj < tk.n && gk < tk.k) ? Ab[int64_t(gk) * tk.lda + gj] : T(0);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < KC; ++kk) {
-            T a[4], b[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) a[r] = As[kk][tx + 16 * r];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) b[c] = Bs[kk][ty + 16 * c];
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) acc[r][c] += a[r] * b[c];
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const int j = j0 + ty + 16 * c;
-        if (j >= tk.n) continue;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int i = i0 + tx + 16 * r;
-            if (i >= tk.m || (tk.lower && i < j)) continue;
-            C[tk.c_off + int64_t(j) * tk.ldc + i] -= acc[r][c];
-        }
+        if (i >= j) blk[int64_t(j) * ld + i] = Lo[k];
+        Iv[k] = S[k];
     }
 }
 
@@ -379,30 +296,13 @@ void launch_assemble_large(const AssembleTask *tasks, int ntasks, int ntiles, Sn
 }
 
 template <typename T>
-void launch_potrf(const PotrfTask *tasks, int ntasks, int max_nb, T *factor, int *fail_col, cudaStream_t st) {
+void launch_potrf_inv(const PotrfTask *tasks, int ntasks, int max_nb, T *factor, T *inv, int *fail_col,
+                      cudaStream_t st) {
     if (ntasks <= 0) return;
-    const size_t smem = size_t(max_nb) * max_nb * sizeof(T);
-    cudaFuncSetAttribute(potrf_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const size_t smem = size_t(2) * max_nb * max_nb * sizeof(T);
+    cudaFuncSetAttribute(potrf_inv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     ++g_kernel_launches;
-    potrf_kernel<T><<<ntasks, 256, smem, st>>>(tasks, factor, fail_col);
-}
-
-template <typename T>
-void launch_trsm(const TrsmTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, cudaStream_t st) {
-    if (ntiles <= 0) return;
-    const size_t smem = (size_t(max_nb) * max_nb + size_t(kTrsmRows) * (max_nb + 1)) * sizeof(T);
-    cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    ++g_kernel_launches;
-    trsm_kernel<T><<<ntiles, kTrsmRows, smem, st>>>(tasks, ntasks, factor);
-}
-
-template <typename T>
-void launch_gemm_update(const GemmTask *tasks, int ntasks, int ntiles, const T *a, T *c, int use_tc,
-                        cudaStream_t st) {
-    (void)use_tc;
-    if (ntiles <= 0) return;
-    ++g_kernel_launches;
-    gemm_update_kernel<T><<<ntiles, 256, 0, st>>>(tasks, ntasks, a, c);
+    potrf_inv_kernel<T><<<ntasks, 256, smem, st>>>(tasks, factor, inv, fail_col);
 }
 
 #define MFS_INSTANTIATE(T)                                                                                        \
@@ -412,9 +312,7 @@ void launch_gemm_update(const GemmTask *tasks, int ntasks, int ntiles, const T *
     template void launch_diag_shift<T>(const int64_t *, int64_t, double, T *, cudaStream_t);                       \
     template void launch_small_factor<T>(const int32_t *, int, int, SnDev, T *, T *, int *, cudaStream_t);         \
     template void launch_assemble_large<T>(const AssembleTask *, int, int, SnDev, T *, T *, cudaStream_t);         \
-    template void launch_potrf<T>(const PotrfTask *, int, int, T *, int *, cudaStream_t);                          \
-    template void launch_trsm<T>(const TrsmTask *, int, int, int, T *, cudaStream_t);                              \
-    template void launch_gemm_update<T>(const GemmTask *, int, int, const T *, T *, int, cudaStream_t);
+    template void launch_potrf_inv<T>(const PotrfTask *, int, int, T *, T *, int *, cudaStream_t);
 
 MFS_INSTANTIATE(double)
 MFS_INSTANTIATE(float)

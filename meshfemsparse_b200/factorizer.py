@@ -88,7 +88,7 @@ class B200Factorizer:
 
     def __init__(self, singlePrecision: bool = False, *, refine: bool = False, device: int = 0,
                  orderingMethod: OrderingMethod = OrderingMethod.CholmodNesdisParallel, refine_tol: float = 1e-10,
-                 refine_maxit: int = 50, small_front_max: int = 0, tensor_cores: int = 1, relax: bool = True,
+                 refine_maxit: int = 50, small_front_max: int = 0, tensor_cores: int = 0, relax: bool = True,
                  relax_zeros: int = 128, relax_ratio: float = 0.01, nd_leaf_size: int = 120, seed: int = 12345,
                  stream: int | None = None):
         self._lib = _lib.load()
