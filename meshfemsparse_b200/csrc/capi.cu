@@ -81,8 +81,7 @@ struct LevelPlan {
     int large_count = 0;
     int asm_off = 0, asm_n = 0, asm_tiles = 0;
     struct Step {
-        int potrf_off, potrf_n, potrf_maxnb;
-        int trsm_off, trsm_n, trsm_tiles, trsm_maxnb;
+        int potrf_off, potrf_n, potrf_tiles, potrf_maxnb;
         int gemm_off, gemm_n, gemm_tiles;
     };
     std::vector<Step> steps;
@@ -91,6 +90,8 @@ struct LevelPlan {
     int sasm_off = 0, sasm_n = 0, sasm_tiles = 0;
     int ftri_off = 0, ftri_n = 0;
     int btri_off = 0, btri_n = 0;
+    int fstr_off = 0, fstr_n = 0, fred_off = 0, fred_n = 0;
+    int bstr_off = 0, bstr_n = 0, bred_off = 0, bred_n = 0;
 };
 
 struct DevSym {
@@ -99,10 +100,13 @@ struct DevSym {
     DBuf<int64_t> pan_off, upd_off, sol_off, struct_ptr, diag_off;
     DBuf<PlanEntryDev> plan;
     DBuf<AssembleTask> asm_tasks;
-    DBuf<PotrfTask> potrf_tasks;
+    DBuf<PanelTask> potrf_tasks;
     DBuf<GemmTask> gemm_tasks;
     DBuf<SolveAsmTask> sasm_tasks;
     DBuf<SolveTask> ftri_tasks, btri_tasks;
+    DBuf<StrTask> fstr_tasks, bstr_tasks;
+    DBuf<StrReduce> fred, bred;
+    int max_str_tasks = 0;
     DBuf<int> flags;                     // one per 64-row diagonal block of every front
     DBuf<int64_t> spmv_ptr, spmv_src;
     DBuf<int32_t> spmv_col, spmv_flag;
@@ -112,7 +116,6 @@ struct DevSym {
     int64_t ax_len = 0;
     std::vector<int64_t> Ap_full, Ai_full;   // caller's pattern (for the element slot map)
     int num_large = 0;
-    int inv_slots = 0;                   // diagonal-block inverses needed by one factorization step
     size_t bytes() const {
         return w.bytes() * 4 + col0.bytes() + child_ptr.bytes() + child_list.bytes() + struct_rows.bytes() +
                rel.bytes() + small_list.bytes() + all_list.bytes() + pan_off.bytes() + upd_off.bytes() +
@@ -141,8 +144,8 @@ struct mfs_handle {
     bool own_stream = false;
     State cur, stash;
     bool has_stash = false;
-    DBuf<double> upd64, inv64;     // update arena, diagonal-block inverses (scratch)
-    DBuf<float> upd32, inv32;
+    DBuf<double> upd64;            // update arena (multifrontal Schur complements)
+    DBuf<float> upd32;
     DBuf<double> sol;
     std::shared_ptr<DBuf<double>> asm_ax;   // output of the last mfs_assemble (device resident)
     DBuf<double> rhs, work_r, work_z, work_p, work_ap, work_x, work_s, io;
@@ -150,7 +153,7 @@ struct mfs_handle {
     DBuf<int> active;
     DBuf<int> fail;
     DBuf<int> solve_err;          // set by a solve kernel whose dependency wait timed out
-    int epoch = 0;                // flag epoch of the cooperative solve kernels
+    DBuf<double> str_partials;    // chunk partial sums of the solve structure phases (scratch)
     int *fail_host = nullptr;
     double *dots_host = nullptr;
     // assembly
@@ -249,9 +252,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     const int small_max = small_front_limit(h);
     std::vector<int32_t> small_list, all_list;
     std::vector<AssembleTask> asm_tasks;
-    std::vector<PotrfTask> potrf_tasks;
+    std::vector<PanelTask> potrf_tasks;
     std::vector<GemmTask> gemm_tasks;
-    int max_inv_slots = 0;
     ds->levels.resize(S.nlevels);
     ds->num_large = 0;
     for (idx l = 0; l < S.nlevels; ++l) {
@@ -284,7 +286,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         L.asm_n = int(large.size());
         L.asm_tiles = base;
         const bool f64 = h->opt.precision != MFS_PREC_FP32;
-        const int NB = f64 ? 64 : 128;                  // <= GEMM tile N: the in-place panel solve needs one column tile
+        const int NB = f64 ? 64 : 128;                  // column block of the large-front factorization
         const int TM = gemm_tile_m(f64), TN = gemm_tile_n(f64);
         auto gemm = [&](int64_t a_off, int64_t b_off, int64_t c_off, int lda, int ldb, int ldc, idx m, idx n, idx k,
                         int lower, int mode, int &base) {
@@ -303,36 +305,24 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         for (idx kb = 0; kb < maxw; kb += NB) {
             LevelPlan::Step sp{};
             sp.potrf_off = int(potrf_tasks.size());
-            int slot = 0;
+            int pb = 0;
             for (idx s : large) {
                 const idx w = S.w[s], f = S.f[s], pan = S.pan_off[s];
                 if (w <= kb) continue;
                 const int nb = int(std::min<idx>(NB, w - kb));
-                PotrfTask pt{};
+                PanelTask pt{};
                 pt.off = pan + kb * f + kb;
-                pt.inv_off = int64_t(slot++) * NB * NB;
                 pt.ld = int32_t(f);
                 pt.nb = nb;
+                pt.m = int32_t(f - kb - nb);
                 pt.col = int32_t(col0[s] + kb);
+                pt.tile_base = pb;
+                pb += std::max(1, int((pt.m + kPanelRows - 1) / kPanelRows));
                 potrf_tasks.push_back(pt);
                 sp.potrf_maxnb = std::max(sp.potrf_maxnb, nb);
             }
             sp.potrf_n = int(potrf_tasks.size()) - sp.potrf_off;
-            max_inv_slots = std::max(max_inv_slots, slot);
-            // panel rows below the diagonal block: B := B inv(L_kk)^T (in place, one column tile)
-            sp.trsm_off = int(gemm_tasks.size());
-            int tb = 0;
-            slot = 0;
-            for (idx s : large) {
-                const idx w = S.w[s], f = S.f[s], pan = S.pan_off[s];
-                if (w <= kb) continue;
-                const int nb = int(std::min<idx>(NB, w - kb));
-                const idx m = f - kb - nb;
-                const int64_t inv = int64_t(slot++) * NB * NB;
-                if (m > 0) gemm(pan + kb * f + kb + nb, inv, pan + kb * f + kb + nb, int(f), nb, int(f), m, nb, nb, 0, 1, tb);
-            }
-            sp.trsm_n = int(gemm_tasks.size()) - sp.trsm_off;
-            sp.trsm_tiles = tb;
+            sp.potrf_tiles = pb;
             // trailing update of the remaining panel columns
             sp.gemm_off = int(gemm_tasks.size());
             int gb = 0;
@@ -360,7 +350,6 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         L.syrk_n = int(gemm_tasks.size()) - L.syrk_off;
         L.syrk_tiles = sb;
     }
-    ds->inv_slots = max_inv_slots;
     // ---- solve tasks (all supernodes, level by level)
     const int RB = solve_rows_per_task();
     std::vector<int32_t> flag_base(nsn);
@@ -371,6 +360,9 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     }
     std::vector<SolveAsmTask> sasm;
     std::vector<SolveTask> ftri, btri;
+    std::vector<StrTask> fstr, bstr;
+    std::vector<StrReduce> fred, bred;
+    int max_str = 0;
     for (idx l = 0; l < S.nlevels; ++l) {
         LevelPlan &L = ds->levels[l];
         L.sasm_off = int(sasm.size());
@@ -390,12 +382,36 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         L.sasm_n = int(sasm.size()) - L.sasm_off;
         L.sasm_tiles = base;
         // ascending block index across the level's fronts: every dependency precedes its task
-        for (int b = 0; b < maxblk; ++b)
+        for (int b = 0; b < maxnbw; ++b)
             for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
                 const idx s = S.level_list[k];
-                const int nbw = int((S.w[s] + RB - 1) / RB), nbd = int((S.d[s] + RB - 1) / RB);
-                if (b < nbw + nbd) ftri.push_back({int32_t(s), b, flag_base[s], 0});
+                const int nbw = int((S.w[s] + RB - 1) / RB);
+                if (b < nbw) ftri.push_back({int32_t(s), b, flag_base[s], 0});
             }
+        // structure slabs: forward 64-row slabs x kStrChunk-column chunks, backward 64-column slabs x row chunks
+        L.fstr_off = int(fstr.size());
+        L.fred_off = int(fred.size());
+        L.bstr_off = int(bstr.size());
+        L.bred_off = int(bred.size());
+        for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
+            const idx s = S.level_list[k];
+            if (S.d[s] == 0) continue;
+            const int nrs = int((S.d[s] + RB - 1) / RB), ncs = int((S.w[s] + kStrChunk - 1) / kStrChunk);
+            for (int a = 0; a < nrs; ++a) {
+                fred.push_back({int32_t(s), a, int32_t(fstr.size()) - L.fstr_off, ncs});
+                for (int c = 0; c < ncs; ++c) fstr.push_back({int32_t(s), a, c, 0});
+            }
+            const int nws = int((S.w[s] + RB - 1) / RB), nds = int((S.d[s] + kStrChunk - 1) / kStrChunk);
+            for (int a = 0; a < nws; ++a) {
+                bred.push_back({int32_t(s), a, int32_t(bstr.size()) - L.bstr_off, nds});
+                for (int c = 0; c < nds; ++c) bstr.push_back({int32_t(s), a, c, 0});
+            }
+        }
+        L.fstr_n = int(fstr.size()) - L.fstr_off;
+        L.fred_n = int(fred.size()) - L.fred_off;
+        L.bstr_n = int(bstr.size()) - L.bstr_off;
+        L.bred_n = int(bred.size()) - L.bred_off;
+        max_str = std::max(max_str, std::max(L.fstr_n, L.bstr_n));
         for (int p = 0; p < maxnbw; ++p)
             for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
                 const idx s = S.level_list[k];
@@ -418,6 +434,11 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     up(ds->sasm_tasks, sasm);
     up(ds->ftri_tasks, ftri);
     up(ds->btri_tasks, btri);
+    up(ds->fstr_tasks, fstr);
+    up(ds->bstr_tasks, bstr);
+    up(ds->fred, fred);
+    up(ds->bred, bred);
+    ds->max_str_tasks = max_str;
     ds->flags.ensure(size_t(std::max(nflags, 1)));
     MFS_CUDA(cudaMemsetAsync(ds->flags.p, 0, ds->flags.bytes(), st));
     MFS_CUDA(cudaStreamSynchronize(st));
@@ -440,8 +461,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
 }
 
 template <typename T>
-void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *inv, const double *Ax, const double *Bx,
-                double sigma) {
+void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, const double *Ax, const double *Bx, double sigma) {
     const Symbolic &S = *ds.S;
     cudaStream_t st = h->stream;
     // FP32 factors: single-pass TF32 when FP64 refinement recovers the accuracy,
@@ -465,10 +485,8 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *inv, const doub
         launch_assemble_large<T>(ds.asm_tasks.p + L.asm_off, L.asm_n, L.asm_tiles, ds.sd, factor, upd, st);
         MFS_LAUNCHED();
         for (const auto &sp : L.steps) {
-            launch_potrf_inv<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, inv, h->fail.p,
-                                st);
-            MFS_LAUNCHED();
-            launch_gemm<T>(ds.gemm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, factor, inv, factor, split, st);
+            launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_tiles, sp.potrf_maxnb, factor,
+                            h->fail.p, st);
             MFS_LAUNCHED();
             launch_gemm<T>(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor, factor, split, st);
             MFS_LAUNCHED();
@@ -486,20 +504,28 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
     cudaStream_t st = h->stream;
     const int chunk = std::min(nrhs, kMaxSolveRhs);
     h->sol.ensure(size_t(std::max<idx>(S.sol_size, 1)) * chunk);
+    h->str_partials.ensure(size_t(std::max(ds.max_str_tasks, 1)) * solve_rows_per_task() * chunk);
     for (int r0 = 0; r0 < nrhs; r0 += kMaxSolveRhs) {
         const int nr = std::min(kMaxSolveRhs, nrhs - r0);
         double *Xc = X + int64_t(r0) * S.n;
+        MFS_CUDA(cudaMemsetAsync(ds.flags.p, 0, ds.flags.bytes(), st));
         for (size_t l = 0; l < ds.levels.size(); ++l) {
             const LevelPlan &L = ds.levels[l];
             launch_fwd_asm(ds.sasm_tasks.p + L.sasm_off, L.sasm_n, L.sasm_tiles, ds.sd, Xc, S.n, nr, h->sol.p, st);
             MFS_LAUNCHED();
-            MFS_CUDA(launch_fwd_tri<T>(ds.ftri_tasks.p + L.ftri_off, L.ftri_n, ds.sd, factor, Xc, S.n, nr, h->sol.p,
-                                       ds.flags.p, ++h->epoch, h->solve_err.p, st));
+            MFS_CUDA(launch_diag<T>(true, ds.ftri_tasks.p + L.ftri_off, L.ftri_n, ds.sd, factor, Xc, S.n, nr,
+                                    ds.flags.p, h->solve_err.p, st));
+            launch_str<T>(true, ds.fstr_tasks.p + L.fstr_off, L.fstr_n, ds.fred.p + L.fred_off, L.fred_n, ds.sd,
+                          factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
+            MFS_LAUNCHED();
         }
         for (size_t l = ds.levels.size(); l-- > 0;) {
             const LevelPlan &L = ds.levels[l];
-            MFS_CUDA(launch_bwd_tri<T>(ds.btri_tasks.p + L.btri_off, L.btri_n, ds.sd, factor, Xc, S.n, nr, ds.flags.p,
-                                       ++h->epoch, h->solve_err.p, st));
+            launch_str<T>(false, ds.bstr_tasks.p + L.bstr_off, L.bstr_n, ds.bred.p + L.bred_off, L.bred_n, ds.sd,
+                          factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
+            MFS_LAUNCHED();
+            MFS_CUDA(launch_diag<T>(false, ds.btri_tasks.p + L.btri_off, L.btri_n, ds.sd, factor, Xc, S.n, nr,
+                                    ds.flags.p, h->solve_err.p, st));
         }
     }
 }
@@ -828,14 +854,12 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
             if (!h->cur.f32 || h->cur.f32.use_count() > 1) h->cur.f32 = std::make_shared<DBuf<float>>();
             h->cur.f32->ensure(size_t(std::max<idx>(S.factor_size, 1)));
             h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
-            h->inv32.ensure(size_t(std::max(ds.inv_slots, 1)) * 128 * 128);
-            run_factor<float>(h, ds, h->cur.f32->p, h->upd32.p, h->inv32.p, h->cur.ax->p, dBx, sigma);
+            run_factor<float>(h, ds, h->cur.f32->p, h->upd32.p, h->cur.ax->p, dBx, sigma);
         } else {
             if (!h->cur.f64 || h->cur.f64.use_count() > 1) h->cur.f64 = std::make_shared<DBuf<double>>();
             h->cur.f64->ensure(size_t(std::max<idx>(S.factor_size, 1)));
             h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
-            h->inv64.ensure(size_t(std::max(ds.inv_slots, 1)) * 64 * 64);
-            run_factor<double>(h, ds, h->cur.f64->p, h->upd64.p, h->inv64.p, h->cur.ax->p, dBx, sigma);
+            run_factor<double>(h, ds, h->cur.f64->p, h->upd64.p, h->cur.ax->p, dBx, sigma);
         }
         MFS_CUDA(cudaEventRecord(h->ev1, st));
         MFS_CUDA(cudaMemcpyAsync(h->fail_host, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));

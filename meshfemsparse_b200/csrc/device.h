@@ -51,15 +51,16 @@ struct GemmTask {
     int32_t mode;
 };
 
-// Dense Cholesky of an nb x nb diagonal block held in a panel; inv(L) of the
-// block goes to scratch slot inv_off (nb x nb, ld nb).
-struct PotrfTask {
-    int64_t off;                        // offset of the block's (0,0) entry
-    int64_t inv_off;
-    int32_t ld, nb;
+// One column block of a large front: factor its nb x nb diagonal block and
+// solve the m rows below it (X := B L^{-T}) in tiles of kPanelRows rows.
+struct PanelTask {
+    int64_t off;                        // offset of the diagonal block's (0,0) entry
+    int32_t ld, nb, m;
     int32_t col;                        // global scalar column of the block's first pivot
+    int32_t tile_base;                  // prefix over tasks of max(1, ceil(m / kPanelRows))
     int32_t pad;
 };
+constexpr int kPanelRows = 128;
 
 // Extend-add of all children of a large supernode, split by front columns.
 struct AssembleTask {
@@ -78,6 +79,16 @@ struct SolveAsmTask {
     int32_t sn;
     int32_t tile_base;
 };
+// Structure part of a solve level: one 64-row (forward) or 64-column (backward)
+// slab `idx` of L21 times one kStrChunk-wide chunk of the other dimension.
+struct StrTask {
+    int32_t sn, idx, chunk, pad;
+};
+// Fixed-order reduction of the chunk partials [first, first + nchunks) of a slab.
+struct StrReduce {
+    int32_t sn, idx, first, nchunks;
+};
+constexpr int kStrChunk = 512;
 constexpr int kSolveAsmRows = 256;      // front rows per forward extend-add CTA
 constexpr int kMaxSolveRhs = 32;        // right-hand sides per solve pass (more are chunked)
 
@@ -98,8 +109,8 @@ template <typename T>
 void launch_assemble_large(const AssembleTask *tasks, int ntasks, int ntiles, SnDev sd, T *factor, T *upd,
                            cudaStream_t st);
 template <typename T>
-void launch_potrf_inv(const PotrfTask *tasks, int ntasks, int max_nb, T *factor, T *inv, int *fail_col,
-                      cudaStream_t st);
+void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, int *fail_col,
+                  cudaStream_t st);
 // Tensor-core tile GEMM (TF32 / split 3xTF32 for float, DMMA for double).
 template <typename T>
 void launch_gemm(const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int split,
@@ -111,11 +122,11 @@ int gemm_tile_n(bool fp64);
 void launch_fwd_asm(const SolveAsmTask *tasks, int ntasks, int ntiles, SnDev sd, double *X, int64_t ldx, int nrhs,
                     double *sol, cudaStream_t st);
 template <typename T>
-cudaError_t launch_fwd_tri(const SolveTask *tasks, int ntasks, SnDev sd, const T *factor, double *X, int64_t ldx,
-                           int nrhs, double *sol, int *flags, int epoch, int *err, cudaStream_t st);
+cudaError_t launch_diag(bool forward, const SolveTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
+                        int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st);
 template <typename T>
-cudaError_t launch_bwd_tri(const SolveTask *tasks, int ntasks, SnDev sd, const T *factor, double *X, int64_t ldx,
-                           int nrhs, int *flags, int epoch, int *err, cudaStream_t st);
+void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce *red, int nred, SnDev sd,
+                const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st);
 int solve_rows_per_task();
 
 // Symmetric block SpMV over permuted reduced rows: Y = A X (both ld = n).

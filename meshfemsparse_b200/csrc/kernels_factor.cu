@@ -182,66 +182,117 @@ __global__ void __launch_bounds__(256) assemble_large_kernel(const AssembleTask 
     }
 }
 
-// K3 (+ the inverse used by the K4 panel solve): Cholesky of one nb x nb
-// diagonal block per CTA. Right-looking on an unscaled working copy S with the
-// scaled column written to a separate output, so each column costs one barrier:
-//   L(k,k) = sqrt(S(k,k)),  L(i,k) = S(i,k) / L(k,k),
-//   S(i,j) -= S(i,k) S(j,k) / S(k,k)   for k < j <= i.
-// Then inv(L) is formed column by column (forward substitution on e_j) and
-// written to the scratch slot of the task; the panel below is solved as the
-// GEMM  B := B inv(L)^T.
+// K3 + K4 fused: one launch per column block of the large fronts of a level.
+// Every CTA of a task loads the nb x nb diagonal block, factors it in shared
+// memory (redundantly: no CTA waits for another) and solves its own tile of up
+// to kPanelRows rows of the panel below, X := B L^{-T}. The first CTA of the
+// task writes the factored diagonal block back.
+// The diagonal factorization is blocked by 32 columns: warp 0 factors the
+// 32 x 32 diagonal sub-block (lane i owns row i), the rows below are solved one
+// thread per row, and the trailing sub-block gets the rank-32 update, so a
+// 128-column block costs 12 barriers instead of one or more per column.
 template <typename T>
-__global__ void __launch_bounds__(256) potrf_inv_kernel(const PotrfTask *__restrict__ tasks, T *__restrict__ factor,
-                                                        T *__restrict__ inv, int *__restrict__ fail_col) {
+__global__ void __launch_bounds__(256) panel_kernel(const PanelTask *__restrict__ tasks, int ntasks,
+                                                    T *__restrict__ factor, int *__restrict__ fail_col) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const PotrfTask tk = tasks[blockIdx.x];
+    const int t = blockIdx.x;
+    int lo = 0, hi = ntasks - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (tasks[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+    }
+    const PanelTask tk = tasks[lo];
+    const int tile = t - tk.tile_base;
     const int nb = tk.nb, ld = tk.ld;
-    T *S = reinterpret_cast<T *>(smem_raw);
-    T *Lo = S + nb * nb;
+    const int LDD = nb + 1;
+    T *D = reinterpret_cast<T *>(smem_raw);           // nb x nb, column-major, ld LDD
+    T *X = D + nb * LDD;                              // kPanelRows x nb, column-major, ld kPanelRows
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     T *blk = factor + tk.off;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int k = tid; k < nb * nb; k += nt) {
-        const int j = k / nb, i = k - j * nb;
-        const T v = i >= j ? blk[int64_t(j) * ld + i] : T(0);
-        S[k] = v;
-        Lo[k] = T(0);
+    for (int q = tid; q < nb * nb; q += nt) {
+        const int j = q / nb, i = q - j * nb;
+        D[j * LDD + i] = i >= j ? blk[int64_t(j) * ld + i] : T(0);
+    }
+    const int r0 = tile * kPanelRows;
+    const int rows = max(0, min(kPanelRows, tk.m - r0));
+    for (int q = tid; q < rows * nb; q += nt) {
+        const int j = q / rows, i = q - j * rows;
+        X[j * kPanelRows + i] = blk[int64_t(j) * ld + nb + r0 + i];
     }
     __syncthreads();
-    for (int k = 0; k < nb; ++k) {
-        T akk = S[k * nb + k];
-        if (!(akk > T(0))) {
-            if (tid == 0) atomicMin(fail_col, tk.col + k);
-            akk = T(1);
+    for (int c0 = 0; c0 < nb; c0 += 32) {
+        const int cw = min(32, nb - c0);
+        if (warp == 0) {
+            for (int k = 0; k < cw; ++k) {
+                T dkk = D[(c0 + k) * LDD + c0 + k];
+                if (!(dkk > T(0))) {
+                    if (lane == 0 && tile == 0) atomicMin(fail_col, tk.col + c0 + k);
+                    dkk = T(1);
+                }
+                const T lkk = dev_sqrt(dkk);
+                __syncwarp();
+                if (lane > k && lane < cw) D[(c0 + k) * LDD + c0 + lane] /= lkk;
+                if (lane == 0) D[(c0 + k) * LDD + c0 + k] = lkk;
+                __syncwarp();
+                if (lane > k && lane < cw) {
+                    const T lik = D[(c0 + k) * LDD + c0 + lane];
+                    for (int j = k + 1; j <= lane; ++j)
+                        D[(c0 + j) * LDD + c0 + lane] -= lik * D[(c0 + k) * LDD + c0 + j];
+                }
+                __syncwarp();
+            }
         }
-        const T rs = dev_sqrt(akk);
-        const T rinv = T(1) / akk;
-        const T *Sk = S + k * nb;
-        for (int i = k + tid; i < nb; i += nt) Lo[k * nb + i] = (i == k) ? rs : Sk[i] / rs;
-        const int m = nb - k - 1;
-        for (int t = tid; t < m * m; t += nt) {
-            const int jj = t / m, ii = t - jj * m;
+        __syncthreads();
+        // rows below the sub-block inside the diagonal block: D[r, c] := D[r, c] L_cc^{-T}
+        for (int r = c0 + cw + tid; r < nb; r += nt) {
+            for (int j = 0; j < cw; ++j) {
+                T x = D[(c0 + j) * LDD + r];
+                for (int k = 0; k < j; ++k) x -= D[(c0 + k) * LDD + r] * D[(c0 + k) * LDD + c0 + j];
+                D[(c0 + j) * LDD + r] = x / D[(c0 + j) * LDD + c0 + j];
+            }
+        }
+        __syncthreads();
+        // rank-cw update of the trailing part of the diagonal block
+        const int mm = nb - c0 - cw;
+        for (int q = tid; q < mm * mm; q += nt) {
+            const int jj = q / mm, ii = q - jj * mm;
             if (ii < jj) continue;
-            const int j = k + 1 + jj, i = k + 1 + ii;
-            S[j * nb + i] -= Sk[i] * Sk[j] * rinv;
+            const int i = c0 + cw + ii, j = c0 + cw + jj;
+            T a = T(0);
+            for (int k = 0; k < cw; ++k) a += D[(c0 + k) * LDD + i] * D[(c0 + k) * LDD + j];
+            D[j * LDD + i] -= a;
         }
         __syncthreads();
     }
-    // inv(L): column j solves L x = e_j (x_i = 0 for i < j); stored in S
-    for (int j = tid; j < nb; j += nt) {
-        for (int i = 0; i < j; ++i) S[j * nb + i] = T(0);
-        S[j * nb + j] = T(1) / Lo[j * nb + j];
-        for (int i = j + 1; i < nb; ++i) {
-            T a = T(0);
-            for (int k = j; k < i; ++k) a += Lo[k * nb + i] * S[j * nb + k];
-            S[j * nb + i] = -a / Lo[i * nb + i];
+    if (tile == 0)
+        for (int q = tid; q < nb * nb; q += nt) {
+            const int j = q / nb, i = q - j * nb;
+            if (i >= j) blk[int64_t(j) * ld + i] = D[j * LDD + i];
         }
+    if (rows == 0) return;
+    // panel tile: X := X L^{-T}, 32 columns at a time
+    for (int c0 = 0; c0 < nb; c0 += 32) {
+        const int cw = min(32, nb - c0);
+        if (c0 > 0)
+            for (int q = tid; q < rows * cw; q += nt) {
+                const int j = q / rows, i = q - j * rows;
+                T a = T(0);
+                for (int k = 0; k < c0; ++k) a += X[k * kPanelRows + i] * D[k * LDD + c0 + j];
+                X[(c0 + j) * kPanelRows + i] -= a;
+            }
+        __syncthreads();
+        for (int i = tid; i < rows; i += nt) {
+            for (int j = 0; j < cw; ++j) {
+                T x = X[(c0 + j) * kPanelRows + i];
+                for (int k = 0; k < j; ++k) x -= X[(c0 + k) * kPanelRows + i] * D[(c0 + k) * LDD + c0 + j];
+                X[(c0 + j) * kPanelRows + i] = x / D[(c0 + j) * LDD + c0 + j];
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    T *Iv = inv + tk.inv_off;
-    for (int k = tid; k < nb * nb; k += nt) {
-        const int j = k / nb, i = k - j * nb;
-        if (i >= j) blk[int64_t(j) * ld + i] = Lo[k];
-        Iv[k] = S[k];
+    for (int q = tid; q < rows * nb; q += nt) {
+        const int j = q / rows, i = q - j * rows;
+        blk[int64_t(j) * ld + nb + r0 + i] = X[j * kPanelRows + i];
     }
 }
 
@@ -296,13 +347,13 @@ void launch_assemble_large(const AssembleTask *tasks, int ntasks, int ntiles, Sn
 }
 
 template <typename T>
-void launch_potrf_inv(const PotrfTask *tasks, int ntasks, int max_nb, T *factor, T *inv, int *fail_col,
-                      cudaStream_t st) {
-    if (ntasks <= 0) return;
-    const size_t smem = size_t(2) * max_nb * max_nb * sizeof(T);
-    cudaFuncSetAttribute(potrf_inv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, int *fail_col,
+                  cudaStream_t st) {
+    if (ntiles <= 0) return;
+    const size_t smem = (size_t(max_nb) * (max_nb + 1) + size_t(kPanelRows) * max_nb) * sizeof(T);
+    cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     ++g_kernel_launches;
-    potrf_inv_kernel<T><<<ntasks, 256, smem, st>>>(tasks, factor, inv, fail_col);
+    panel_kernel<T><<<ntiles, 256, smem, st>>>(tasks, ntasks, factor, fail_col);
 }
 
 #define MFS_INSTANTIATE(T)                                                                                        \
@@ -312,7 +363,7 @@ void launch_potrf_inv(const PotrfTask *tasks, int ntasks, int max_nb, T *factor,
     template void launch_diag_shift<T>(const int64_t *, int64_t, double, T *, cudaStream_t);                       \
     template void launch_small_factor<T>(const int32_t *, int, int, SnDev, T *, T *, int *, cudaStream_t);         \
     template void launch_assemble_large<T>(const AssembleTask *, int, int, SnDev, T *, T *, cudaStream_t);         \
-    template void launch_potrf_inv<T>(const PotrfTask *, int, int, T *, T *, int *, cudaStream_t);
+    template void launch_panel<T>(const PanelTask *, int, int, int, T *, int *, cudaStream_t);
 
 MFS_INSTANTIATE(double)
 MFS_INSTANTIATE(float)

@@ -6,23 +6,27 @@
 // (trs_kernels::SolveLowerTri / MultiplyLowerBlock, solve_kernels::fused_forward /
 // fused_backward, tests/test_catamari_solve_kernels.cc).
 //
-// Per elimination-tree level:
-//   forward   1. fwd_asm: zero u_s and pull every child's update vector u_c into
-//                the front (x rows of the supernode, or u_s) through child_rel_indices,
-//                children in order (deterministic, no atomics);
-//             2. fwd_tri: one task per 64-row block of every front. A diagonal row
-//                block r subtracts L(r, k) y_k for k < r, solves its triangle and
-//                publishes y_r through an epoch flag; a structure row block
-//                subtracts all L(r, k) y_k into u_s.
-//   backward  bwd_tri: one task per diagonal block, descending: subtract
-//                L(struct, r)^T x_struct (ancestors are final) and L(k, r)^T x_k for
-//                k > r (waiting on their flags), then solve the transposed triangle.
-// The tri kernels are cooperative launches (all CTAs co-resident); every CTA
+// A front of supernode s is [L11; L21] (w + d rows, w columns). Per level:
+//   forward   fwd_asm      zero u_s and pull every child's update vector u_c into the
+//                          front through child_rel_indices (children in order);
+//             fwd_diag     L11 y = v, one task per 64-row diagonal block; block r
+//                          subtracts L11(r, k) y_k for k < r (waiting on block k's
+//                          epoch flag) and solves its triangle;
+//             str_partial  P = L21(rows, chunk) y(chunk) for 64-row tiles of L21 and
+//                          512-column chunks (independent tasks);
+//             fwd_reduce   u_s(rows) -= sum over chunks of P, in chunk order.
+//   backward  str_partial  P = L21(chunk, cols)^T x_struct for 64-column blocks and
+//                          512-row chunks of L21 (ancestors are final);
+//             bwd_reduce   x(cols) -= sum over chunks of P, in chunk order;
+//             bwd_diag     L11^T x = y, blocks descending, waiting on flags.
+// Everything is summed in a fixed order: results are run-to-run identical.
+// The diag kernels are cooperative launches (all CTAs co-resident); every CTA
 // walks its tasks in ascending order and a task only waits on lower-numbered
 // tasks of the same front, so the lowest unfinished task can always proceed.
-// Every wait is bounded in time: after kWaitNs the kernel records an error and
-// stops waiting (later waits return at once) so the launch always completes;
-// the host then reports MFS_TIMEOUT.
+// Every wait is bounded in time (kWaitNs): on expiry the kernel records an
+// error and stops waiting so the launch completes; the host reports MFS_TIMEOUT.
+// Flags are cleared before each solve; the forward pass publishes epoch 1 and
+// the backward pass epoch 2, so the launch sequence is fixed (graph-capturable).
 #include "device.h"
 
 #include <algorithm>
@@ -31,7 +35,7 @@ namespace mfs {
 
 namespace {
 
-constexpr int kRB = 64;                     // rows per task
+constexpr int kRB = 64;                     // rows / columns per task
 constexpr int kTriThreads = 128;
 constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s per wait at most
 
@@ -62,11 +66,20 @@ __device__ __forceinline__ void wait_flag(const int *flag, int epoch, int *err) 
                     atomicExch(err, 1);
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(32);
             }
         }
     }
     __syncthreads();
+}
+
+__device__ __forceinline__ int find_base(const int32_t *base, int n, int t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (base[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
 }
 
 __global__ void __launch_bounds__(256) fwd_asm_kernel(const SolveAsmTask *__restrict__ tasks, int ntasks, SnDev sd,
@@ -118,17 +131,16 @@ __global__ void __launch_bounds__(256) fwd_asm_kernel(const SolveAsmTask *__rest
     }
 }
 
-// shared memory: acc[kRB * nrhs] | vec[kRB * nrhs] | tile[kRB][kRB + 1]
+// shared memory of the diag kernels: acc[kRB * nrhs] | vec[kRB * nrhs] | tile[kRB][kRB + 1]
 __host__ __device__ inline size_t tri_smem(int nrhs) {
     return (size_t(2) * kRB * nrhs + size_t(kRB) * (kRB + 1)) * sizeof(double);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kTriThreads) fwd_tri_kernel(const SolveTask *__restrict__ tasks, int ntasks, SnDev sd,
-                                                              const T *__restrict__ factor, double *__restrict__ X,
-                                                              int64_t ldx, int nrhs, double *__restrict__ sol,
-                                                              int *__restrict__ flags, int epoch,
-                                                              int *__restrict__ err) {
+__global__ void __launch_bounds__(kTriThreads) fwd_diag_kernel(const SolveTask *__restrict__ tasks, int ntasks,
+                                                               SnDev sd, const T *__restrict__ factor,
+                                                               double *__restrict__ X, int64_t ldx, int nrhs,
+                                                               int *__restrict__ flags, int *__restrict__ err) {
     extern __shared__ __align__(16) double smem_d[];
     double *acc = smem_d;
     double *yk = acc + kRB * nrhs;
@@ -137,29 +149,22 @@ __global__ void __launch_bounds__(kTriThreads) fwd_tri_kernel(const SolveTask *_
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SolveTask tk = tasks[t];
         const int s = tk.sn;
-        const int w = sd.w[s], d = sd.d[s], f = w + d;
+        const int w = sd.w[s], f = w + sd.d[s];
         const int c0 = sd.col0[s];
-        const int nbw = (w + kRB - 1) / kRB;
-        const bool diag = tk.blk < nbw;
-        const int r0 = diag ? tk.blk * kRB : w + (tk.blk - nbw) * kRB;
-        const int r1 = diag ? min(w, r0 + kRB) : min(f, r0 + kRB);
-        const int nr = r1 - r0;
+        const int r0 = tk.blk * kRB, nr = min(kRB, w - r0);
         const T *pan = factor + sd.pan_off[s];
-        double *us = (d > 0 && sd.sol_off[s] >= 0) ? sol + sd.sol_off[s] * nrhs : nullptr;
         for (int q = tid; q < nr * nrhs; q += kTriThreads) {
             const int i = q / nrhs, r = q % nrhs;
-            acc[q] = diag ? X[c0 + r0 + i + r * ldx] : us[(r0 - w + i) + r * d];
+            acc[q] = X[c0 + r0 + i + r * ldx];
         }
-        const int kend = diag ? tk.blk : nbw;
-        for (int k = 0; k < kend; ++k) {
-            const int k0 = k * kRB, nk = min(kRB, w - k0);
-            // the L tile does not depend on the flag: load it first
-            for (int q = tid; q < nr * nk; q += kTriThreads) {
+        for (int k = 0; k < tk.blk; ++k) {
+            const int k0 = k * kRB;      // full block: k < blk
+            for (int q = tid; q < nr * kRB; q += kTriThreads) {
                 const int j = q / nr, i = q % nr;
                 tile[i * (kRB + 1) + j] = double(pan[int64_t(k0 + j) * f + r0 + i]);
             }
-            wait_flag(flags + tk.flag_base + k, epoch, err);
-            for (int q = tid; q < nk * nrhs; q += kTriThreads) {
+            wait_flag(flags + tk.flag_base + k, 1, err);
+            for (int q = tid; q < kRB * nrhs; q += kTriThreads) {
                 const int j = q / nrhs, r = q % nrhs;
                 yk[q] = __ldcg(&X[c0 + k0 + j + r * ldx]);
             }
@@ -168,94 +173,73 @@ __global__ void __launch_bounds__(kTriThreads) fwd_tri_kernel(const SolveTask *_
                 const int i = q / nrhs, r = q % nrhs;
                 const double *trow = tile + i * (kRB + 1);
                 double a = 0.0;
-                for (int j = 0; j < nk; ++j) a += trow[j] * yk[j * nrhs + r];
+#pragma unroll 8
+                for (int j = 0; j < kRB; ++j) a += trow[j] * yk[j * nrhs + r];
                 acc[q] -= a;
             }
             __syncthreads();
         }
-        if (diag) {
-            for (int q = tid; q < nr * nr; q += kTriThreads) {
-                const int j = q / nr, i = q % nr;
-                tile[i * (kRB + 1) + j] = i >= j ? double(pan[int64_t(r0 + j) * f + r0 + i]) : 0.0;
-            }
-            __syncthreads();
-            if (tid < 32) {
-                for (int j = 0; j < nr; ++j) {
-                    const double ljj = tile[j * (kRB + 1) + j];
-                    for (int r = tid; r < nrhs; r += 32) acc[j * nrhs + r] /= ljj;
-                    __syncwarp();
-                    for (int i = j + 1 + tid; i < nr; i += 32) {
-                        const double lij = tile[i * (kRB + 1) + j];
-                        for (int r = 0; r < nrhs; ++r) acc[i * nrhs + r] -= lij * acc[j * nrhs + r];
-                    }
-                    __syncwarp();
+        for (int q = tid; q < nr * nr; q += kTriThreads) {
+            const int j = q / nr, i = q % nr;
+            tile[i * (kRB + 1) + j] = i >= j ? double(pan[int64_t(r0 + j) * f + r0 + i]) : 0.0;
+        }
+        __syncthreads();
+        if (tid < 32) {
+            for (int j = 0; j < nr; ++j) {
+                const double ljj = tile[j * (kRB + 1) + j];
+                for (int r = tid; r < nrhs; r += 32) acc[j * nrhs + r] /= ljj;
+                __syncwarp();
+                for (int i = j + 1 + tid; i < nr; i += 32) {
+                    const double lij = tile[i * (kRB + 1) + j];
+                    for (int r = 0; r < nrhs; ++r) acc[i * nrhs + r] -= lij * acc[j * nrhs + r];
                 }
-            }
-            __syncthreads();
-            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-                const int i = q / nrhs, r = q % nrhs;
-                X[c0 + r0 + i + r * ldx] = acc[q];
-            }
-            __threadfence();
-            __syncthreads();
-            if (tid == 0) st_release(flags + tk.flag_base + tk.blk, epoch);
-        } else {
-            __syncthreads();
-            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-                const int i = q / nrhs, r = q % nrhs;
-                us[(r0 - w + i) + r * d] = acc[q];
+                __syncwarp();
             }
         }
+        __syncthreads();
+        for (int q = tid; q < nr * nrhs; q += kTriThreads) {
+            const int i = q / nrhs, r = q % nrhs;
+            X[c0 + r0 + i + r * ldx] = acc[q];
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_release(flags + tk.flag_base + tk.blk, 1);
         __syncthreads();
     }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kTriThreads) bwd_tri_kernel(const SolveTask *__restrict__ tasks, int ntasks, SnDev sd,
-                                                              const T *__restrict__ factor, double *__restrict__ X,
-                                                              int64_t ldx, int nrhs, int *__restrict__ flags, int epoch,
-                                                              int *__restrict__ err) {
+__global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *__restrict__ tasks, int ntasks,
+                                                               SnDev sd, const T *__restrict__ factor,
+                                                               double *__restrict__ X, int64_t ldx, int nrhs,
+                                                               int *__restrict__ flags, int *__restrict__ err) {
     extern __shared__ __align__(16) double smem_d[];
     double *acc = smem_d;
     double *xk = acc + kRB * nrhs;
     double *tile = xk + kRB * nrhs;            // tile[i * (kRB+1) + j] = L(i0+i, r0+j)
     const int tid = threadIdx.x;
-    const int vb = sd.vb;
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SolveTask tk = tasks[t];
         const int s = tk.sn;
-        const int w = sd.w[s], d = sd.d[s], f = w + d;
+        const int w = sd.w[s], f = w + sd.d[s];
         const int c0 = sd.col0[s];
         const int nbw = (w + kRB - 1) / kRB;
         const int r0 = tk.blk * kRB, nr = min(kRB, w - r0);
         const T *pan = factor + sd.pan_off[s];
-        const int32_t *rows = sd.struct_rows + sd.struct_ptr[s];
         for (int q = tid; q < nr * nrhs; q += kTriThreads) {
             const int j = q / nrhs, r = q % nrhs;
             acc[q] = X[c0 + r0 + j + r * ldx];
         }
-        // chunks: structure rows first (no dependency), then diagonal blocks k > blk, descending
-        const int nsc = (d + kRB - 1) / kRB;
-        const int nchunks = nsc + (nbw - 1 - tk.blk);
-        for (int ch = 0; ch < nchunks; ++ch) {
-            const bool st = ch < nsc;
-            const int k = st ? -1 : nbw - 1 - (ch - nsc);
-            const int i0 = st ? w + ch * kRB : k * kRB;
-            const int ni = st ? min(kRB, f - i0) : min(kRB, w - i0);
+        for (int k = nbw - 1; k > tk.blk; --k) {
+            const int i0 = k * kRB, ni = min(kRB, w - i0);
             for (int q = tid; q < ni * nr; q += kTriThreads) {
                 const int j = q / ni, i = q % ni;
                 tile[i * (kRB + 1) + j] = double(pan[int64_t(r0 + j) * f + i0 + i]);
             }
-            if (!st) wait_flag(flags + tk.flag_base + k, epoch, err);
+            wait_flag(flags + tk.flag_base + k, 2, err);
             for (int q = tid; q < ni * nrhs; q += kTriThreads) {
                 const int i = q / nrhs, r = q % nrhs;
-                if (st) {
-                    const int li = i0 - w + i;
-                    const int64_t gi = int64_t(rows[li / vb]) * vb + li % vb;
-                    xk[q] = X[gi + r * ldx];
-                } else {
-                    xk[q] = __ldcg(&X[c0 + i0 + i + r * ldx]);
-                }
+                xk[q] = __ldcg(&X[c0 + i0 + i + r * ldx]);
             }
             __syncthreads();
             for (int q = tid; q < nr * nrhs; q += kTriThreads) {
@@ -266,7 +250,6 @@ __global__ void __launch_bounds__(kTriThreads) bwd_tri_kernel(const SolveTask *_
             }
             __syncthreads();
         }
-        // transposed triangle: x_j = (acc_j - sum_{i>j} L(i,j) x_i) / L(j,j), descending
         for (int q = tid; q < nr * nr; q += kTriThreads) {
             const int j = q / nr, i = q % nr;
             tile[i * (kRB + 1) + j] = i >= j ? double(pan[int64_t(r0 + j) * f + r0 + i]) : 0.0;
@@ -290,8 +273,96 @@ __global__ void __launch_bounds__(kTriThreads) bwd_tri_kernel(const SolveTask *_
         }
         __threadfence();
         __syncthreads();
-        if (tid == 0) st_release(flags + tk.flag_base + tk.blk, epoch);
+        if (tid == 0) st_release(flags + tk.flag_base + tk.blk, 2);
         __syncthreads();
+    }
+}
+
+// Structure part, forward: P(task) = L21(rows, cols) y(cols); backward:
+// P(task) = L21(rows, cols)^T x(struct rows). One 64 x kStrChunk (or
+// kStrChunk x 64) slab of L21 per CTA, read as 64 x 64 tiles.
+template <typename T, bool FWD>
+__global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restrict__ tasks, SnDev sd,
+                                                          const T *__restrict__ factor,
+                                                          const double *__restrict__ X, int64_t ldx, int nrhs,
+                                                          double *__restrict__ P) {
+    extern __shared__ __align__(16) double smem_d[];
+    double *out = smem_d;                      // [kRB * nrhs]
+    double *vec = out + kRB * nrhs;            // [kRB * nrhs]
+    double *tile = vec + kRB * nrhs;           // [kRB][kRB + 1]
+    const StrTask tk = tasks[blockIdx.x];
+    const int s = tk.sn;
+    const int w = sd.w[s], d = sd.d[s], f = w + d;
+    const int c0 = sd.col0[s];
+    const int vb = sd.vb;
+    const T *pan = factor + sd.pan_off[s];
+    const int32_t *rows = sd.struct_rows + sd.struct_ptr[s];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    // FWD: fixed 64 struct rows [a0, a0+na), loop over 64-col blocks of the chunk
+    // BWD: fixed 64 columns [a0, a0+na), loop over 64-row blocks of the chunk
+    const int a0 = tk.idx * kRB;
+    const int na = FWD ? min(kRB, d - a0) : min(kRB, w - a0);
+    const int lim = FWD ? w : d;
+    const int b_begin = tk.chunk * kStrChunk, b_end = min(lim, b_begin + kStrChunk);
+    for (int q = tid; q < na * nrhs; q += nt) out[q] = 0.0;
+    for (int b0 = b_begin; b0 < b_end; b0 += kRB) {
+        const int nbk = min(kRB, b_end - b0);
+        __syncthreads();
+        if (FWD) {
+            // tile[i][j] = L(w + a0 + i, b0 + j), vec[j] = y(b0 + j)
+            for (int q = tid; q < na * nbk; q += nt) {
+                const int j = q / na, i = q % na;
+                tile[i * (kRB + 1) + j] = double(pan[int64_t(b0 + j) * f + w + a0 + i]);
+            }
+            for (int q = tid; q < nbk * nrhs; q += nt) {
+                const int j = q / nrhs, r = q % nrhs;
+                vec[q] = X[c0 + b0 + j + r * ldx];
+            }
+        } else {
+            // tile[i][j] = L(w + b0 + i, a0 + j), vec[i] = x(struct row b0 + i)
+            for (int q = tid; q < nbk * na; q += nt) {
+                const int j = q / nbk, i = q % nbk;
+                tile[i * (kRB + 1) + j] = double(pan[int64_t(a0 + j) * f + w + b0 + i]);
+            }
+            for (int q = tid; q < nbk * nrhs; q += nt) {
+                const int i = q / nrhs, r = q % nrhs;
+                const int li = b0 + i;
+                const int64_t gi = int64_t(rows[li / vb]) * vb + li % vb;
+                vec[q] = X[gi + r * ldx];
+            }
+        }
+        __syncthreads();
+        for (int q = tid; q < na * nrhs; q += nt) {
+            const int a = q / nrhs, r = q % nrhs;
+            double acc = 0.0;
+            if (FWD)
+                for (int j = 0; j < nbk; ++j) acc += tile[a * (kRB + 1) + j] * vec[j * nrhs + r];
+            else
+                for (int i = 0; i < nbk; ++i) acc += tile[i * (kRB + 1) + a] * vec[i * nrhs + r];
+            out[q] += acc;
+        }
+    }
+    __syncthreads();
+    double *Pt = P + int64_t(blockIdx.x) * kRB * nrhs;
+    for (int q = tid; q < na * nrhs; q += nt) Pt[q] = out[q];
+}
+
+// Subtract the chunk partials of one 64-row (FWD: of u_s) or 64-column (BWD: of x) slab, in chunk order.
+template <bool FWD>
+__global__ void __launch_bounds__(256) str_reduce_kernel(const StrReduce *__restrict__ red, SnDev sd,
+                                                         double *__restrict__ X, int64_t ldx, int nrhs,
+                                                         double *__restrict__ sol, const double *__restrict__ P) {
+    const StrReduce rd = red[blockIdx.x];
+    const int s = rd.sn;
+    const int w = sd.w[s], d = sd.d[s];
+    const int a0 = rd.idx * kRB;
+    const int na = FWD ? min(kRB, d - a0) : min(kRB, w - a0);
+    for (int q = threadIdx.x; q < na * nrhs; q += blockDim.x) {
+        const int a = q / nrhs, r = q % nrhs;
+        double acc = 0.0;
+        for (int c = 0; c < rd.nchunks; ++c) acc += P[int64_t(rd.first + c) * kRB * nrhs + q];
+        if (FWD) sol[sd.sol_off[s] * nrhs + (a0 + a) + int64_t(r) * d] -= acc;
+        else X[sd.col0[s] + a0 + a + r * ldx] -= acc;
     }
 }
 
@@ -323,41 +394,45 @@ void launch_fwd_asm(const SolveAsmTask *tasks, int ntasks, int ntiles, SnDev sd,
 }
 
 template <typename T>
-cudaError_t launch_fwd_tri(const SolveTask *tasks, int ntasks, SnDev sd, const T *factor, double *X, int64_t ldx,
-                           int nrhs, double *sol, int *flags, int epoch, int *err, cudaStream_t st) {
+cudaError_t launch_diag(bool forward, const SolveTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
+                        int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st) {
     if (ntasks <= 0) return cudaSuccess;
-    auto kern = fwd_tri_kernel<T>;
+    void *kern = forward ? (void *)fwd_diag_kernel<T> : (void *)bwd_diag_kernel<T>;
     const size_t smem = tri_smem(nrhs);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tri_smem(kMaxSolveRhs)));
-    const int grid = coop_grid(kern, smem, ntasks);
+    const int grid = forward ? coop_grid(fwd_diag_kernel<T>, smem, ntasks) : coop_grid(bwd_diag_kernel<T>, smem, ntasks);
     void *args[] = {(void *)&tasks, (void *)&ntasks, (void *)&sd, (void *)&factor, (void *)&X, (void *)&ldx,
-                    (void *)&nrhs, (void *)&sol, (void *)&flags, (void *)&epoch, (void *)&err};
+                    (void *)&nrhs, (void *)&flags, (void *)&err};
     ++g_kernel_launches;
-    return cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(kTriThreads), args, smem, st);
+    return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kTriThreads), args, smem, st);
 }
 
 template <typename T>
-cudaError_t launch_bwd_tri(const SolveTask *tasks, int ntasks, SnDev sd, const T *factor, double *X, int64_t ldx,
-                           int nrhs, int *flags, int epoch, int *err, cudaStream_t st) {
-    if (ntasks <= 0) return cudaSuccess;
-    auto kern = bwd_tri_kernel<T>;
+void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce *red, int nred, SnDev sd,
+                const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st) {
+    if (ntasks <= 0) return;
+    g_kernel_launches += 2;
     const size_t smem = tri_smem(nrhs);
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tri_smem(kMaxSolveRhs)));
-    const int grid = coop_grid(kern, smem, ntasks);
-    void *args[] = {(void *)&tasks, (void *)&ntasks, (void *)&sd, (void *)&factor, (void *)&X, (void *)&ldx,
-                    (void *)&nrhs, (void *)&flags, (void *)&epoch, (void *)&err};
-    ++g_kernel_launches;
-    return cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(kTriThreads), args, smem, st);
+    if (forward) {
+        cudaFuncSetAttribute(str_partial_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(tri_smem(kMaxSolveRhs)));
+        str_partial_kernel<T, true><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
+        str_reduce_kernel<true><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
+    } else {
+        cudaFuncSetAttribute(str_partial_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(tri_smem(kMaxSolveRhs)));
+        str_partial_kernel<T, false><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
+        str_reduce_kernel<false><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
+    }
 }
 
-template cudaError_t launch_fwd_tri<double>(const SolveTask *, int, SnDev, const double *, double *, int64_t, int,
-                                            double *, int *, int, int *, cudaStream_t);
-template cudaError_t launch_fwd_tri<float>(const SolveTask *, int, SnDev, const float *, double *, int64_t, int,
-                                           double *, int *, int, int *, cudaStream_t);
-template cudaError_t launch_bwd_tri<double>(const SolveTask *, int, SnDev, const double *, double *, int64_t, int,
-                                            int *, int, int *, cudaStream_t);
-template cudaError_t launch_bwd_tri<float>(const SolveTask *, int, SnDev, const float *, double *, int64_t, int,
-                                           int *, int, int *, cudaStream_t);
+#define MFS_TRI_INSTANTIATE(T)                                                                                    \
+    template cudaError_t launch_diag<T>(bool, const SolveTask *, int, SnDev, const T *, double *, int64_t, int,   \
+                                        int *, int *, cudaStream_t);                                              \
+    template void launch_str<T>(bool, const StrTask *, int, const StrReduce *, int, SnDev, const T *, double *,   \
+                                int64_t, int, double *, double *, cudaStream_t);
+MFS_TRI_INSTANTIATE(double)
+MFS_TRI_INSTANTIATE(float)
 
 int solve_rows_per_task() { return kRB; }
 
