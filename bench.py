@@ -86,7 +86,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                          "-lms", "500", "-i", str(self.gpu)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -247,7 +247,7 @@ def run_b200(args, rank, world, local, dist):
         "clocks": clocks,
         "roofline": roofline,
         "residual": res32,
-        "refine_iterations": st32["refine_iterations"],
+        "refine_iterations": st32["refine_iterations"], "perturbed_pivots": st32["perturbed_pivots"],
         "factor_ms": st32["factor_ms"], "solve_ms": st32["solve_ms"], "assemble_ms": st32["assemble_ms"],
         "factor_nnz": f32.getFactorNNZ(), "flops": flops, "symbolic_s": t_sym, "input_gen_s": t_gen,
         **out64,

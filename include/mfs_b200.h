@@ -178,6 +178,9 @@ typedef struct {
     int32_t num_levels;          /* levels of the assembly tree */
     int32_t num_large;           /* supernodes on the tiled large-front path */
     int64_t kernel_launches;     /* kernels launched by the library since it was loaded */
+    int32_t perturbed_pivots;    /* FP32 factor under refinement: non-positive pivots replaced by a
+                                    floor relative to the injected diagonal (last numeric) */
+    int32_t reserved_stats;
 } mfs_stats;
 mfs_status mfs_get_stats(const mfs_handle *h, mfs_stats *st);
 

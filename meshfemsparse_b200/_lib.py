@@ -44,7 +44,7 @@ class Stats(C.Structure):
         ("factor_ms", C.c_double), ("solve_ms", C.c_double), ("assemble_ms", C.c_double),
         ("refine_iterations", C.c_int32), ("failed_column", C.c_int32), ("residual", C.c_double),
         ("device_bytes", C.c_int64), ("num_levels", C.c_int32), ("num_large", C.c_int32),
-        ("kernel_launches", C.c_int64),
+        ("kernel_launches", C.c_int64), ("perturbed_pivots", C.c_int32), ("reserved_stats", C.c_int32),
     ]
 
 

@@ -152,6 +152,8 @@ struct mfs_handle {
     DBuf<double> partials, dots;
     DBuf<int> active;
     DBuf<int> fail;
+    DBuf<int> perturbed;          // pivots perturbed in the last numeric factorization
+    DBuf<double> dorig;           // injected diagonal (perturbation reference)
     DBuf<int> solve_err;          // set by a solve kernel whose dependency wait timed out
     DBuf<double> str_partials;    // chunk partial sums of the solve structure phases (scratch)
     int *fail_host = nullptr;
@@ -475,10 +477,19 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, const double *Ax, 
         launch_diag_shift<T>(ds.diag_off.p, S.n, sigma, factor, st);
         MFS_LAUNCHED();
     }
+    // The FP32 factor preconditions FP64 refinement: non-positive pivots are
+    // perturbed (relative to the injected diagonal) instead of failing.
+    PivotCtl pv{h->fail.p, h->perturbed.p, nullptr};
+    if (h->opt.precision == MFS_PREC_FP32 && h->opt.refine) {
+        h->dorig.ensure(size_t(std::max<idx>(S.n, 1)));
+        launch_extract_diag<T>(ds.diag_off.p, S.n, factor, h->dorig.p, st);
+        MFS_LAUNCHED();
+        pv.dorig = h->dorig.p;
+    }
     for (const LevelPlan &L : ds.levels) {
         if (L.small_count > 0) {
             launch_small_factor<T>(ds.small_list.p + L.small_off, L.small_count, L.small_max_front, ds.sd, factor,
-                                   upd, h->fail.p, st);
+                                   upd, pv, st);
             MFS_LAUNCHED();
         }
         if (L.large_count == 0) continue;
@@ -486,7 +497,7 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, const double *Ax, 
         MFS_LAUNCHED();
         for (const auto &sp : L.steps) {
             launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_tiles, sp.potrf_maxnb, factor,
-                            h->fail.p, st);
+                            pv, st);
             MFS_LAUNCHED();
             launch_gemm<T>(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor, factor, split, st);
             MFS_LAUNCHED();
@@ -705,9 +716,10 @@ mfs_status mfs_create(mfs_handle **out, const mfs_options *opt) {
         }
         MFS_CUDA(cudaEventCreate(&h->ev0));
         MFS_CUDA(cudaEventCreate(&h->ev1));
-        MFS_CUDA(cudaMallocHost(&h->fail_host, sizeof(int)));
+        MFS_CUDA(cudaMallocHost(&h->fail_host, 2 * sizeof(int)));
         MFS_CUDA(cudaMallocHost(&h->dots_host, 64 * sizeof(double)));
         h->fail.ensure(1);
+        h->perturbed.ensure(1);
         h->solve_err.ensure(1);
         MFS_CUDA(cudaMemset(h->solve_err.p, 0, sizeof(int)));
     });
@@ -849,6 +861,7 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
         const double *dBx = h->cur.bx ? h->cur.bx->p : nullptr;
         const int big = INT_MAX;
         MFS_CUDA(cudaMemcpyAsync(h->fail.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+        MFS_CUDA(cudaMemsetAsync(h->perturbed.p, 0, sizeof(int), st));
         MFS_CUDA(cudaEventRecord(h->ev0, st));
         if (h->opt.precision == MFS_PREC_FP32) {
             if (!h->cur.f32 || h->cur.f32.use_count() > 1) h->cur.f32 = std::make_shared<DBuf<float>>();
@@ -863,10 +876,12 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
         }
         MFS_CUDA(cudaEventRecord(h->ev1, st));
         MFS_CUDA(cudaMemcpyAsync(h->fail_host, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        MFS_CUDA(cudaMemcpyAsync(h->fail_host + 1, h->perturbed.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         MFS_CUDA(cudaStreamSynchronize(st));
         float ms = 0;
         cudaEventElapsedTime(&ms, h->ev0, h->ev1);
         h->stats.factor_ms = ms;
+        h->stats.perturbed_pivots = h->fail_host[1];
         h->cur.sigma = sigma;
         if (*h->fail_host != INT_MAX) {
             h->stats.failed_column = *h->fail_host;

@@ -30,6 +30,14 @@ struct SnDev {
     int vb;                             // analysis block size
 };
 
+// Pivot handling of the factorization kernels: smallest failing column, count
+// of perturbed pivots, and (perturbation mode only) the injected diagonal.
+struct PivotCtl {
+    int *fail_col;
+    int *perturbed;
+    const double *dorig;                // nullptr: no perturbation, failures are reported
+};
+
 // Plan entry mirror of host_symbolic.h PlanEntry.
 struct PlanEntryDev {
     int64_t dst;
@@ -93,6 +101,7 @@ constexpr int kSolveAsmRows = 256;      // front rows per forward extend-add CTA
 constexpr int kMaxSolveRhs = 32;        // right-hand sides per solve pass (more are chunked)
 
 constexpr int kAsmCols = 32;            // front columns per assemble CTA
+constexpr int kMaxSmemOptin = 232448;   // opt-in dynamic shared memory per CTA (227 KB)
 
 // ---------------------------------------------------------------- launchers
 template <typename T>
@@ -103,13 +112,15 @@ void launch_inject(const PlanEntryDev *plan, int64_t nplan, int vb, int src_ld, 
 template <typename T>
 void launch_diag_shift(const int64_t *diag_off, int64_t n, double sigma, T *factor, cudaStream_t st);
 template <typename T>
+void launch_extract_diag(const int64_t *diag_off, int64_t n, const T *factor, double *out, cudaStream_t st);
+template <typename T>
 void launch_small_factor(const int32_t *list, int count, int max_front, SnDev sd, T *factor, T *upd,
-                         int *fail_col, cudaStream_t st);
+                         PivotCtl pv, cudaStream_t st);
 template <typename T>
 void launch_assemble_large(const AssembleTask *tasks, int ntasks, int ntiles, SnDev sd, T *factor, T *upd,
                            cudaStream_t st);
 template <typename T>
-void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, int *fail_col,
+void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, PivotCtl pv,
                   cudaStream_t st);
 // Tensor-core tile GEMM (TF32 / split 3xTF32 for float, DMMA for double).
 template <typename T>

@@ -67,11 +67,37 @@ __global__ void diag_shift_kernel(const int64_t *__restrict__ diag_off, int64_t 
 
 __device__ __forceinline__ int child_rel(const int32_t *rel, int i, int vb) { return rel[i / vb] + i % vb; }
 
+// A non-positive (or NaN) pivot. Without perturbation (plain solves, the
+// reference's semantics) the smallest failing column is recorded and 1 is used
+// so the launch completes; the host then reports the failure. With
+// perturbation (the FP32 factor used as a preconditioner under FP64
+// refinement) the pivot becomes max(|a|, kPivotFloor * A(col,col)) of the
+// injected matrix, which keeps the factor SPD, and the event is counted.
+constexpr double kPivotFloor = 1e-3;
+template <typename T>
+__device__ __forceinline__ T bad_pivot(T a, int col, const PivotCtl &pv, bool record) {
+    if (pv.dorig) {
+        const T floor_v = T(kPivotFloor * fabs(pv.dorig[col]));
+        const T m = fabs(a);
+        if (record) atomicAdd(pv.perturbed, 1);
+        return (m > floor_v) ? m : (floor_v > T(0) ? floor_v : T(1));
+    }
+    if (record) atomicMin(pv.fail_col, col);
+    return T(1);
+}
+
+template <typename T>
+__global__ void extract_diag_kernel(const int64_t *__restrict__ diag_off, int64_t n, const T *__restrict__ factor,
+                                    double *__restrict__ out) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        out[i] = double(factor[diag_off[i]]);
+}
+
 // Small fronts: the whole (w+d)^2 front lives in shared memory.
 template <typename T>
 __global__ void __launch_bounds__(256) small_factor_kernel(const int32_t *__restrict__ list, SnDev sd,
                                                            T *__restrict__ factor, T *__restrict__ upd,
-                                                           int *__restrict__ fail_col) {
+                                                           PivotCtl pv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *F = reinterpret_cast<T *>(smem_raw);
     const int s = list[blockIdx.x];
@@ -98,7 +124,7 @@ __global__ void __launch_bounds__(256) small_factor_kernel(const int32_t *__rest
         T *colk = F + k * f;
         if (tid == 0) {
             T a = colk[k];
-            if (!(a > T(0))) { atomicMin(fail_col, sd.col0[s] + k); a = T(1); }
+            if (!(a > T(0))) a = bad_pivot(a, sd.col0[s] + k, pv, true);
             colk[k] = dev_sqrt(a);
         }
         __syncthreads();
@@ -193,7 +219,7 @@ __global__ void __launch_bounds__(256) assemble_large_kernel(const AssembleTask 
 // 128-column block costs 12 barriers instead of one or more per column.
 template <typename T>
 __global__ void __launch_bounds__(256) panel_kernel(const PanelTask *__restrict__ tasks, int ntasks,
-                                                    T *__restrict__ factor, int *__restrict__ fail_col) {
+                                                    T *__restrict__ factor, PivotCtl pv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int t = blockIdx.x;
     int lo = 0, hi = ntasks - 1;
@@ -225,10 +251,7 @@ __global__ void __launch_bounds__(256) panel_kernel(const PanelTask *__restrict_
         if (warp == 0) {
             for (int k = 0; k < cw; ++k) {
                 T dkk = D[(c0 + k) * LDD + c0 + k];
-                if (!(dkk > T(0))) {
-                    if (lane == 0 && tile == 0) atomicMin(fail_col, tk.col + c0 + k);
-                    dkk = T(1);
-                }
+                if (!(dkk > T(0))) dkk = bad_pivot(dkk, tk.col + c0 + k, pv, lane == 0 && tile == 0);
                 const T lkk = dev_sqrt(dkk);
                 __syncwarp();
                 if (lane > k && lane < cw) D[(c0 + k) * LDD + c0 + lane] /= lkk;
@@ -329,13 +352,14 @@ void launch_diag_shift(const int64_t *diag_off, int64_t n, double sigma, T *fact
 }
 
 template <typename T>
-void launch_small_factor(const int32_t *list, int count, int max_front, SnDev sd, T *factor, T *upd, int *fail_col,
+void launch_small_factor(const int32_t *list, int count, int max_front, SnDev sd, T *factor, T *upd, PivotCtl pv,
                          cudaStream_t st) {
     if (count <= 0) return;
     const size_t smem = size_t(max_front) * max_front * sizeof(T);
-    cudaFuncSetAttribute(small_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    static const bool smem_ok = (cudaFuncSetAttribute(small_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin), true);
+    (void)smem_ok;
     ++g_kernel_launches;
-    small_factor_kernel<T><<<count, 256, smem, st>>>(list, sd, factor, upd, fail_col);
+    small_factor_kernel<T><<<count, 256, smem, st>>>(list, sd, factor, upd, pv);
 }
 
 template <typename T>
@@ -347,13 +371,21 @@ void launch_assemble_large(const AssembleTask *tasks, int ntasks, int ntiles, Sn
 }
 
 template <typename T>
-void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, int *fail_col,
+void launch_extract_diag(const int64_t *diag_off, int64_t n, const T *factor, double *out, cudaStream_t st) {
+    if (n <= 0) return;
+    ++g_kernel_launches;
+    extract_diag_kernel<T><<<grid_for(n, 256), 256, 0, st>>>(diag_off, n, factor, out);
+}
+
+template <typename T>
+void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, PivotCtl pv,
                   cudaStream_t st) {
     if (ntiles <= 0) return;
     const size_t smem = (size_t(max_nb) * (max_nb + 1) + size_t(kPanelRows) * max_nb) * sizeof(T);
-    cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    static const bool smem_ok = (cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin), true);
+    (void)smem_ok;
     ++g_kernel_launches;
-    panel_kernel<T><<<ntiles, 256, smem, st>>>(tasks, ntasks, factor, fail_col);
+    panel_kernel<T><<<ntiles, 256, smem, st>>>(tasks, ntasks, factor, pv);
 }
 
 #define MFS_INSTANTIATE(T)                                                                                        \
@@ -361,9 +393,10 @@ void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T 
     template void launch_inject<T>(const PlanEntryDev *, int64_t, int, int, const double *, const double *, double, \
                                    T *, cudaStream_t);                                                            \
     template void launch_diag_shift<T>(const int64_t *, int64_t, double, T *, cudaStream_t);                       \
-    template void launch_small_factor<T>(const int32_t *, int, int, SnDev, T *, T *, int *, cudaStream_t);         \
+    template void launch_small_factor<T>(const int32_t *, int, int, SnDev, T *, T *, PivotCtl, cudaStream_t);      \
     template void launch_assemble_large<T>(const AssembleTask *, int, int, SnDev, T *, T *, cudaStream_t);         \
-    template void launch_panel<T>(const PanelTask *, int, int, int, T *, int *, cudaStream_t);
+    template void launch_panel<T>(const PanelTask *, int, int, int, T *, PivotCtl, cudaStream_t);                 \
+    template void launch_extract_diag<T>(const int64_t *, int64_t, const T *, double *, cudaStream_t);
 
 MFS_INSTANTIATE(double)
 MFS_INSTANTIATE(float)

@@ -289,10 +289,12 @@ void launch_gemm<float>(const GemmTask *tasks, int ntasks, int ntiles, const flo
     if (ntiles <= 0) return;
     ++g_kernel_launches;
     if (split == 3) {
-        cudaFuncSetAttribute(gemm_tf32_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTF32Smem);
+        static const bool ok3 = (cudaFuncSetAttribute(gemm_tf32_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTF32Smem), true);
+        (void)ok3;
         gemm_tf32_kernel<3><<<ntiles, 256, kTF32Smem, st>>>(tasks, ntasks, A, B, C);
     } else {
-        cudaFuncSetAttribute(gemm_tf32_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTF32Smem);
+        static const bool ok1 = (cudaFuncSetAttribute(gemm_tf32_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTF32Smem), true);
+        (void)ok1;
         gemm_tf32_kernel<1><<<ntiles, 256, kTF32Smem, st>>>(tasks, ntasks, A, B, C);
     }
 }
@@ -303,7 +305,8 @@ void launch_gemm<double>(const GemmTask *tasks, int ntasks, int ntiles, const do
     (void)split;
     if (ntiles <= 0) return;
     ++g_kernel_launches;
-    cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kF64Smem);
+    static const bool ok = (cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kF64Smem), true);
+    (void)ok;
     gemm_f64_kernel<<<ntiles, 256, kF64Smem, st>>>(tasks, ntasks, A, B, C);
 }
 

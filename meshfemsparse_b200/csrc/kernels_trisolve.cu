@@ -399,8 +399,18 @@ cudaError_t launch_diag(bool forward, const SolveTask *tasks, int ntasks, SnDev 
     if (ntasks <= 0) return cudaSuccess;
     void *kern = forward ? (void *)fwd_diag_kernel<T> : (void *)bwd_diag_kernel<T>;
     const size_t smem = tri_smem(nrhs);
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tri_smem(kMaxSolveRhs)));
-    const int grid = forward ? coop_grid(fwd_diag_kernel<T>, smem, ntasks) : coop_grid(bwd_diag_kernel<T>, smem, ntasks);
+    // one-time per kernel: shared-memory opt-in and co-resident grid per RHS count
+    static const bool attr_ok =
+        (cudaFuncSetAttribute(fwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(tri_smem(kMaxSolveRhs))),
+         cudaFuncSetAttribute(bwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(tri_smem(kMaxSolveRhs))),
+         true);
+    (void)attr_ok;
+    static int grid_cache[2][kMaxSolveRhs + 1] = {};
+    int &gmax = grid_cache[forward ? 0 : 1][nrhs];
+    if (!gmax) gmax = forward ? coop_grid(fwd_diag_kernel<T>, smem, 1 << 30) : coop_grid(bwd_diag_kernel<T>, smem, 1 << 30);
+    const int grid = std::min(gmax, ntasks);
     void *args[] = {(void *)&tasks, (void *)&ntasks, (void *)&sd, (void *)&factor, (void *)&X, (void *)&ldx,
                     (void *)&nrhs, (void *)&flags, (void *)&err};
     ++g_kernel_launches;
@@ -413,14 +423,17 @@ void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce 
     if (ntasks <= 0) return;
     g_kernel_launches += 2;
     const size_t smem = tri_smem(nrhs);
+    static const bool attr_ok =
+        (cudaFuncSetAttribute(str_partial_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(tri_smem(kMaxSolveRhs))),
+         cudaFuncSetAttribute(str_partial_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(tri_smem(kMaxSolveRhs))),
+         true);
+    (void)attr_ok;
     if (forward) {
-        cudaFuncSetAttribute(str_partial_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(tri_smem(kMaxSolveRhs)));
         str_partial_kernel<T, true><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
         str_reduce_kernel<true><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
     } else {
-        cudaFuncSetAttribute(str_partial_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(tri_smem(kMaxSolveRhs)));
         str_partial_kernel<T, false><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
         str_reduce_kernel<false><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
     }

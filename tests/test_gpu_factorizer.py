@@ -156,6 +156,20 @@ def test_rounding_induced_loss_of_positive_definiteness():
         single.solveMultiRHS(np.ones((2, 1)))
 
 
+def test_refined_fp32_perturbs_instead_of_failing():
+    """Under FP64 refinement the FP32 factor is a preconditioner: a pivot lost to
+    rounding is perturbed (and counted) and the refined solve still reaches 1e-10."""
+    S = ScalarCSC(2, np.array([0, 1, 3]), np.array([0, 0, 1]), np.array([1.0, 1.0, 1.0 + 1e-8]))
+    A = BlockCSCHessian(2, S.Ap, S.Ai, 1, S.Ax)
+    f = B200Factorizer(True, refine=True, orderingMethod=OrderingMethod.AMD, refine_maxit=20)
+    f.factorize(A)
+    assert f.stats()["perturbed_pivots"] >= 1
+    b = np.array([1.0, 2.0])
+    x = f.solve(b)
+    r = S.apply(x) - b
+    assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(b)
+
+
 @pytest.mark.parametrize("single", [False, True])
 def test_symbolic_reuse_resets_scalar_fallback(single):
     S = plain_scalar_path(6)
