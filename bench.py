@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--k", type=int, default=None, help="override the cube side (smaller runs)")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison arm")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--tc", type=int, default=0, help="FP32 Schur updates: 0 auto, 1 TF32, 2 split 3xTF32")
+    p.add_argument("--maxit", type=int, default=50, help="refinement iteration cap")
     p.add_argument("--cpu-budget", type=float, default=2.5e11, help="flops of the CPU factorization sample")
     return p.parse_args()
 
@@ -139,7 +141,8 @@ def run_b200(args, rank, world, local, dist):
     nrhs = wl.nrhs
 
     def make(single):
-        f = B200Factorizer(single, refine=single, stream=stream.cuda_stream, device=local)
+        f = B200Factorizer(single, refine=single, stream=stream.cuda_stream, device=local, tensor_cores=args.tc,
+                           refine_maxit=args.maxit)
         t = time.time()
         f.factorizeSymbolic(wl.H, wl.pins)
         f.setElements(wl.tets)

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -86,6 +87,7 @@ struct LevelPlan {
     };
     std::vector<Step> steps;
     int syrk_off = 0, syrk_n = 0, syrk_tiles = 0;
+    int panel_first = 0, panel_count = 0;   // all panel tasks of the level (diagonal write-back)
     // solve task lists of this level
     int sasm_off = 0, sasm_n = 0, sasm_tiles = 0;
     int ftri_off = 0, ftri_n = 0;
@@ -116,6 +118,7 @@ struct DevSym {
     int64_t ax_len = 0;
     std::vector<int64_t> Ap_full, Ai_full;   // caller's pattern (for the element slot map)
     int num_large = 0;
+    int64_t diag_scratch = 0;            // elements of factored diagonal blocks held per level
     size_t bytes() const {
         return w.bytes() * 4 + col0.bytes() + child_ptr.bytes() + child_list.bytes() + struct_rows.bytes() +
                rel.bytes() + small_list.bytes() + all_list.bytes() + pan_off.bytes() + upd_off.bytes() +
@@ -146,6 +149,8 @@ struct mfs_handle {
     bool has_stash = false;
     DBuf<double> upd64;            // update arena (multifrontal Schur complements)
     DBuf<float> upd32;
+    DBuf<double> dscr64;           // factored diagonal blocks of one level (written back per level)
+    DBuf<float> dscr32;
     DBuf<double> sol;
     std::shared_ptr<DBuf<double>> asm_ax;   // output of the last mfs_assemble (device resident)
     DBuf<double> rhs, work_r, work_z, work_p, work_ap, work_x, work_s, io;
@@ -304,6 +309,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             base += g.tiles_m * g.tiles_n;
             gemm_tasks.push_back(g);
         };
+        L.panel_first = int(potrf_tasks.size());
+        int64_t dslot = 0;
         for (idx kb = 0; kb < maxw; kb += NB) {
             LevelPlan::Step sp{};
             sp.potrf_off = int(potrf_tasks.size());
@@ -314,6 +321,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
                 const int nb = int(std::min<idx>(NB, w - kb));
                 PanelTask pt{};
                 pt.off = pan + kb * f + kb;
+                pt.diag_out = dslot;
+                dslot += int64_t(nb) * nb;
                 pt.ld = int32_t(f);
                 pt.nb = nb;
                 pt.m = int32_t(f - kb - nb);
@@ -342,6 +351,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             sp.gemm_tiles = gb;
             L.steps.push_back(sp);
         }
+        L.panel_count = int(potrf_tasks.size()) - L.panel_first;
+        ds->diag_scratch = std::max<int64_t>(ds->diag_scratch, dslot);
         L.syrk_off = int(gemm_tasks.size());
         int sb = 0;
         for (idx s : large) {
@@ -463,7 +474,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
 }
 
 template <typename T>
-void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, const double *Ax, const double *Bx, double sigma) {
+void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const double *Ax, const double *Bx,
+                double sigma) {
     const Symbolic &S = *ds.S;
     cudaStream_t st = h->stream;
     // FP32 factors: single-pass TF32 when FP64 refinement recovers the accuracy,
@@ -497,11 +509,13 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, const double *Ax, 
         MFS_LAUNCHED();
         for (const auto &sp : L.steps) {
             launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_tiles, sp.potrf_maxnb, factor,
-                            pv, st);
+                            dscr, pv, st);
             MFS_LAUNCHED();
             launch_gemm<T>(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor, factor, split, st);
             MFS_LAUNCHED();
         }
+        launch_diag_writeback<T>(ds.potrf_tasks.p + L.panel_first, L.panel_count, dscr, factor, st);
+        MFS_LAUNCHED();
         if (L.syrk_n > 0) {
             launch_gemm<T>(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, factor, upd, split, st);
             MFS_LAUNCHED();
@@ -650,9 +664,12 @@ void refine_solve(mfs_handle *h, const double *B, double *X, int nrhs) {
     }
     h->stats.refine_iterations = it;
     h->stats.residual = worst;
-    if (!all_done)
-        throw StatusError(MFS_NOT_POSDEF, "refinement did not reach the residual target within the iteration cap (" +
-                                              std::to_string(worst) + ")");
+    if (!all_done) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf),
+                      "refinement did not reach the residual target within %d iterations (worst %.3e)", it, worst);
+        throw StatusError(MFS_NOT_POSDEF, buf);
+    }
 }
 
 void require_symbolic(mfs_handle *h) {
@@ -867,12 +884,14 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
             if (!h->cur.f32 || h->cur.f32.use_count() > 1) h->cur.f32 = std::make_shared<DBuf<float>>();
             h->cur.f32->ensure(size_t(std::max<idx>(S.factor_size, 1)));
             h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
-            run_factor<float>(h, ds, h->cur.f32->p, h->upd32.p, h->cur.ax->p, dBx, sigma);
+            h->dscr32.ensure(size_t(std::max<int64_t>(ds.diag_scratch, 1)));
+            run_factor<float>(h, ds, h->cur.f32->p, h->upd32.p, h->dscr32.p, h->cur.ax->p, dBx, sigma);
         } else {
             if (!h->cur.f64 || h->cur.f64.use_count() > 1) h->cur.f64 = std::make_shared<DBuf<double>>();
             h->cur.f64->ensure(size_t(std::max<idx>(S.factor_size, 1)));
             h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
-            run_factor<double>(h, ds, h->cur.f64->p, h->upd64.p, h->cur.ax->p, dBx, sigma);
+            h->dscr64.ensure(size_t(std::max<int64_t>(ds.diag_scratch, 1)));
+            run_factor<double>(h, ds, h->cur.f64->p, h->upd64.p, h->dscr64.p, h->cur.ax->p, dBx, sigma);
         }
         MFS_CUDA(cudaEventRecord(h->ev1, st));
         MFS_CUDA(cudaMemcpyAsync(h->fail_host, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));

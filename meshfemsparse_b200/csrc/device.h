@@ -61,8 +61,12 @@ struct GemmTask {
 
 // One column block of a large front: factor its nb x nb diagonal block and
 // solve the m rows below it (X := B L^{-T}) in tiles of kPanelRows rows.
+// Tile 0 of a task stores the factored diagonal block at scratch offset
+// `diag_out` (nb x nb, ld nb): the other CTAs of the task may still be reading
+// the unfactored block in place, so it is copied back once the level is done.
 struct PanelTask {
     int64_t off;                        // offset of the diagonal block's (0,0) entry
+    int64_t diag_out;                   // scratch offset of the factored diagonal block
     int32_t ld, nb, m;
     int32_t col;                        // global scalar column of the block's first pivot
     int32_t tile_base;                  // prefix over tasks of max(1, ceil(m / kPanelRows))
@@ -120,8 +124,11 @@ template <typename T>
 void launch_assemble_large(const AssembleTask *tasks, int ntasks, int ntiles, SnDev sd, T *factor, T *upd,
                            cudaStream_t st);
 template <typename T>
-void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, PivotCtl pv,
-                  cudaStream_t st);
+void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, T *diag_scratch,
+                  PivotCtl pv, cudaStream_t st);
+// Copy the factored diagonal blocks of a level's panel tasks back into the factor.
+template <typename T>
+void launch_diag_writeback(const PanelTask *tasks, int ntasks, const T *diag_scratch, T *factor, cudaStream_t st);
 // Tensor-core tile GEMM (TF32 / split 3xTF32 for float, DMMA for double).
 template <typename T>
 void launch_gemm(const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int split,

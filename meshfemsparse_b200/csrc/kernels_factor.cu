@@ -219,7 +219,8 @@ __global__ void __launch_bounds__(256) assemble_large_kernel(const AssembleTask 
 // 128-column block costs 12 barriers instead of one or more per column.
 template <typename T>
 __global__ void __launch_bounds__(256) panel_kernel(const PanelTask *__restrict__ tasks, int ntasks,
-                                                    T *__restrict__ factor, PivotCtl pv) {
+                                                    T *__restrict__ factor, T *__restrict__ diag_scratch,
+                                                    PivotCtl pv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int t = blockIdx.x;
     int lo = 0, hi = ntasks - 1;
@@ -287,11 +288,14 @@ __global__ void __launch_bounds__(256) panel_kernel(const PanelTask *__restrict_
         }
         __syncthreads();
     }
-    if (tile == 0)
+    if (tile == 0) {
+        // not in place: other CTAs of this task may not have read the block yet
+        T *out = diag_scratch + tk.diag_out;
         for (int q = tid; q < nb * nb; q += nt) {
             const int j = q / nb, i = q - j * nb;
-            if (i >= j) blk[int64_t(j) * ld + i] = D[j * LDD + i];
+            out[q] = D[j * LDD + i];
         }
+    }
     if (rows == 0) return;
     // panel tile: X := X L^{-T}, 32 columns at a time
     for (int c0 = 0; c0 < nb; c0 += 32) {
@@ -378,14 +382,33 @@ void launch_extract_diag(const int64_t *diag_off, int64_t n, const T *factor, do
 }
 
 template <typename T>
-void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, PivotCtl pv,
-                  cudaStream_t st) {
+void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, T *diag_scratch,
+                  PivotCtl pv, cudaStream_t st) {
     if (ntiles <= 0) return;
     const size_t smem = (size_t(max_nb) * (max_nb + 1) + size_t(kPanelRows) * max_nb) * sizeof(T);
     static const bool smem_ok = (cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin), true);
     (void)smem_ok;
     ++g_kernel_launches;
-    panel_kernel<T><<<ntiles, 256, smem, st>>>(tasks, ntasks, factor, pv);
+    panel_kernel<T><<<ntiles, 256, smem, st>>>(tasks, ntasks, factor, diag_scratch, pv);
+}
+
+template <typename T>
+__global__ void diag_writeback_kernel(const PanelTask *__restrict__ tasks, const T *__restrict__ scratch,
+                                      T *__restrict__ factor) {
+    const PanelTask tk = tasks[blockIdx.x];
+    const T *src = scratch + tk.diag_out;
+    T *blk = factor + tk.off;
+    for (int q = threadIdx.x; q < tk.nb * tk.nb; q += blockDim.x) {
+        const int j = q / tk.nb, i = q - j * tk.nb;
+        if (i >= j) blk[int64_t(j) * tk.ld + i] = src[q];
+    }
+}
+
+template <typename T>
+void launch_diag_writeback(const PanelTask *tasks, int ntasks, const T *diag_scratch, T *factor, cudaStream_t st) {
+    if (ntasks <= 0) return;
+    ++g_kernel_launches;
+    diag_writeback_kernel<T><<<ntasks, 256, 0, st>>>(tasks, diag_scratch, factor);
 }
 
 #define MFS_INSTANTIATE(T)                                                                                        \
@@ -395,7 +418,8 @@ void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T 
     template void launch_diag_shift<T>(const int64_t *, int64_t, double, T *, cudaStream_t);                       \
     template void launch_small_factor<T>(const int32_t *, int, int, SnDev, T *, T *, PivotCtl, cudaStream_t);      \
     template void launch_assemble_large<T>(const AssembleTask *, int, int, SnDev, T *, T *, cudaStream_t);         \
-    template void launch_panel<T>(const PanelTask *, int, int, int, T *, PivotCtl, cudaStream_t);                 \
+    template void launch_panel<T>(const PanelTask *, int, int, int, T *, T *, PivotCtl, cudaStream_t);            \
+    template void launch_diag_writeback<T>(const PanelTask *, int, const T *, T *, cudaStream_t);                 \
     template void launch_extract_diag<T>(const int64_t *, int64_t, const T *, double *, cudaStream_t);
 
 MFS_INSTANTIATE(double)

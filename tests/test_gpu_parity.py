@@ -72,6 +72,24 @@ def test_tiled_path_large_fronts(single):
     assert rel_err(got, ref) <= (1e-4 if single else 1e-11)
 
 
+@pytest.mark.parametrize("single", [False, True])
+def test_large_cube_many_panel_tiles(single):
+    """k=24 cube: large fronts whose panel tasks span several CTA waves (the diagonal
+    block is read by every CTA of a task while the factored copy is written elsewhere)."""
+    H, tets, Ke, pins, nodes = cube_problem(24)
+    f = B200Factorizer(single, tensor_cores=2)
+    f.factorizeSymbolic(H, pins)
+    f.factorizeNumeric(H)
+    sn = f.supernodes()
+    plan = f.conversionPlan()
+    w, d, fr, pan, col0 = pyoracle.panel_layout(sn)
+    ref = pyoracle.inject(plan["entries"], sn["vb"], H.bs, H.Ax, int(pan[-1]))
+    pyoracle.load_blas()
+    assert pyoracle.mf_factor(sn, ref, 8) == -1
+    got = f.factorValues()
+    assert rel_err(got, ref) <= (1e-4 if single else 1e-11)
+
+
 @pytest.mark.parametrize("k", [2, 4])
 def test_assembly_bit_exact(k):
     nodes, tets = fem.tet_cube(k, jitter=0.1, seed=7)
