@@ -100,6 +100,7 @@ struct DevSym {
     std::shared_ptr<Symbolic> S;
     DBuf<int32_t> w, d, f, col0, child_ptr, child_list, struct_rows, rel, small_list, all_list;
     DBuf<int64_t> pan_off, upd_off, sol_off, struct_ptr, diag_off;
+    DBuf<int64_t> inv_off;               // 64 x 64 diagonal inverses of large fronts (-1: none)
     DBuf<PlanEntryDev> plan;
     DBuf<AssembleTask> asm_tasks;
     DBuf<PanelTask> potrf_tasks;
@@ -119,10 +120,11 @@ struct DevSym {
     std::vector<int64_t> Ap_full, Ai_full;   // caller's pattern (for the element slot map)
     int num_large = 0;
     int64_t diag_scratch = 0;            // elements of factored diagonal blocks held per level
+    int64_t factor_alloc = 0;            // panels followed by the diagonal inverses
     size_t bytes() const {
         return w.bytes() * 4 + col0.bytes() + child_ptr.bytes() + child_list.bytes() + struct_rows.bytes() +
                rel.bytes() + small_list.bytes() + all_list.bytes() + pan_off.bytes() + upd_off.bytes() +
-               sol_off.bytes() + struct_ptr.bytes() + diag_off.bytes() + plan.bytes() + asm_tasks.bytes() +
+               sol_off.bytes() + struct_ptr.bytes() + diag_off.bytes() + inv_off.bytes() + plan.bytes() + asm_tasks.bytes() +
                potrf_tasks.bytes() + gemm_tasks.bytes() + spmv_ptr.bytes() +
                spmv_src.bytes() + spmv_col.bytes() + spmv_flag.bytes() + prrfr.bytes() + sperm.bytes();
     }
@@ -263,6 +265,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     std::vector<GemmTask> gemm_tasks;
     ds->levels.resize(S.nlevels);
     ds->num_large = 0;
+    std::vector<int64_t> inv_off(nsn, -1);
+    int64_t inv_end = S.factor_size;
     for (idx l = 0; l < S.nlevels; ++l) {
         LevelPlan &L = ds->levels[l];
         std::vector<idx> large;
@@ -286,6 +290,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         int base = 0;
         idx maxw = 0;
         for (idx s : large) {
+            inv_off[s] = inv_end;
+            inv_end += ((S.w[s] + 63) / 64) * 4096;
             asm_tasks.push_back({int32_t(s), base});
             base += int((S.f[s] + kAsmCols - 1) / kAsmCols);
             maxw = std::max(maxw, S.w[s]);
@@ -323,6 +329,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
                 pt.off = pan + kb * f + kb;
                 pt.diag_out = dslot;
                 dslot += int64_t(nb) * nb;
+                pt.inv_out = inv_off[s] + (kb / 64) * 4096;
                 pt.ld = int32_t(f);
                 pt.nb = nb;
                 pt.m = int32_t(f - kb - nb);
@@ -436,6 +443,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     }
     ds->small_list.upload(small_list, st);
     ds->all_list.upload(all_list, st);
+    ds->inv_off.upload(inv_off, st);
+    ds->factor_alloc = std::max<int64_t>(inv_end, 1);
     auto up = [&](auto &buf, const auto &vec) {
         buf.ensure(vec.size());
         if (!vec.empty())
@@ -464,6 +473,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     sd.pan_off = ds->pan_off.p;
     sd.upd_off = ds->upd_off.p;
     sd.sol_off = ds->sol_off.p;
+    sd.inv_off = ds->inv_off.p;
     sd.child_ptr = ds->child_ptr.p;
     sd.child_list = ds->child_list.p;
     sd.struct_ptr = ds->struct_ptr.p;
@@ -882,13 +892,13 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
         MFS_CUDA(cudaEventRecord(h->ev0, st));
         if (h->opt.precision == MFS_PREC_FP32) {
             if (!h->cur.f32 || h->cur.f32.use_count() > 1) h->cur.f32 = std::make_shared<DBuf<float>>();
-            h->cur.f32->ensure(size_t(std::max<idx>(S.factor_size, 1)));
+            h->cur.f32->ensure(size_t(ds.factor_alloc));
             h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
             h->dscr32.ensure(size_t(std::max<int64_t>(ds.diag_scratch, 1)));
             run_factor<float>(h, ds, h->cur.f32->p, h->upd32.p, h->dscr32.p, h->cur.ax->p, dBx, sigma);
         } else {
             if (!h->cur.f64 || h->cur.f64.use_count() > 1) h->cur.f64 = std::make_shared<DBuf<double>>();
-            h->cur.f64->ensure(size_t(std::max<idx>(S.factor_size, 1)));
+            h->cur.f64->ensure(size_t(ds.factor_alloc));
             h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
             h->dscr64.ensure(size_t(std::max<int64_t>(ds.diag_scratch, 1)));
             run_factor<double>(h, ds, h->cur.f64->p, h->upd64.p, h->dscr64.p, h->cur.ax->p, dBx, sigma);
@@ -1188,7 +1198,7 @@ mfs_status mfs_stash(mfs_handle *h) {
         s.sigma = h->cur.sigma;
         s.ax = h->cur.ax;
         s.bx = h->cur.bx;
-        const size_t fs = size_t(std::max<idx>(h->cur.sym->S->factor_size, 1));
+        const size_t fs = size_t(h->cur.sym->factor_alloc);
         if (h->cur.type >= 2) {
             if (h->cur.f64) {
                 s.f64 = std::make_shared<DBuf<double>>();

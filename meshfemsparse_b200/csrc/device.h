@@ -2,7 +2,9 @@
 //
 // Storage in HBM (all column-major):
 //   factor values  : one panel per supernode, (w+d) x w, ld = w+d, panels back to back
-//                    (catamari layout, CatamariConversionPlan.hh:366)
+//                    (catamari layout, CatamariConversionPlan.hh:366), followed by the
+//                    64 x 64 inverses of the diagonal blocks of every large front's L11
+//                    (written by the panel kernel, read by the triangular solves)
 //   update arena   : U_s (d x d, ld d) of the multifrontal assembly tree; offsets from
 //                    the static level-lifetime plan built on the host
 //   solve arena    : u_s (d x nrhs, ld d) forward-substitution update vectors; offsets
@@ -23,6 +25,8 @@ struct SnDev {
     const int64_t *pan_off;             // panel offset in the factor array
     const int64_t *upd_off;             // U_s offset in the update arena (-1: none)
     const int64_t *sol_off;             // u_s offset (units of one RHS) in the solve arena
+    const int64_t *inv_off;             // factor-array offset of the 64 x 64 inverses of L11's
+                                        // diagonal blocks, ceil(w/64) blocks (-1: not stored)
     const int32_t *child_ptr, *child_list;
     const int64_t *struct_ptr;          // per supernode, into struct_rows / rel
     const int32_t *struct_rows;         // analysis-variable rows (permuted)
@@ -64,9 +68,12 @@ struct GemmTask {
 // Tile 0 of a task stores the factored diagonal block at scratch offset
 // `diag_out` (nb x nb, ld nb): the other CTAs of the task may still be reading
 // the unfactored block in place, so it is copied back once the level is done.
+// It also stores the 64 x 64 diagonal blocks of inv(L) at `inv_out` of the factor
+// array (-1: not stored), which the triangular solves apply as small GEMVs.
 struct PanelTask {
     int64_t off;                        // offset of the diagonal block's (0,0) entry
     int64_t diag_out;                   // scratch offset of the factored diagonal block
+    int64_t inv_out;                    // factor-array offset of the 64 x 64 inverse blocks
     int32_t ld, nb, m;
     int32_t col;                        // global scalar column of the block's first pivot
     int32_t tile_base;                  // prefix over tasks of max(1, ceil(m / kPanelRows))

@@ -208,121 +208,6 @@ __global__ void __launch_bounds__(256) assemble_large_kernel(const AssembleTask 
     }
 }
 
-// K3 + K4 fused: one launch per column block of the large fronts of a level.
-// Every CTA of a task loads the nb x nb diagonal block, factors it in shared
-// memory (redundantly: no CTA waits for another) and solves its own tile of up
-// to kPanelRows rows of the panel below, X := B L^{-T}. The first CTA of the
-// task writes the factored diagonal block back.
-// The diagonal factorization is blocked by 32 columns: warp 0 factors the
-// 32 x 32 diagonal sub-block (lane i owns row i), the rows below are solved one
-// thread per row, and the trailing sub-block gets the rank-32 update, so a
-// 128-column block costs 12 barriers instead of one or more per column.
-template <typename T>
-__global__ void __launch_bounds__(256) panel_kernel(const PanelTask *__restrict__ tasks, int ntasks,
-                                                    T *__restrict__ factor, T *__restrict__ diag_scratch,
-                                                    PivotCtl pv) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int t = blockIdx.x;
-    int lo = 0, hi = ntasks - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (tasks[mid].tile_base <= t) lo = mid; else hi = mid - 1;
-    }
-    const PanelTask tk = tasks[lo];
-    const int tile = t - tk.tile_base;
-    const int nb = tk.nb, ld = tk.ld;
-    const int LDD = nb + 1;
-    T *D = reinterpret_cast<T *>(smem_raw);           // nb x nb, column-major, ld LDD
-    T *X = D + nb * LDD;                              // kPanelRows x nb, column-major, ld kPanelRows
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    T *blk = factor + tk.off;
-    for (int q = tid; q < nb * nb; q += nt) {
-        const int j = q / nb, i = q - j * nb;
-        D[j * LDD + i] = i >= j ? blk[int64_t(j) * ld + i] : T(0);
-    }
-    const int r0 = tile * kPanelRows;
-    const int rows = max(0, min(kPanelRows, tk.m - r0));
-    for (int q = tid; q < rows * nb; q += nt) {
-        const int j = q / rows, i = q - j * rows;
-        X[j * kPanelRows + i] = blk[int64_t(j) * ld + nb + r0 + i];
-    }
-    __syncthreads();
-    for (int c0 = 0; c0 < nb; c0 += 32) {
-        const int cw = min(32, nb - c0);
-        if (warp == 0) {
-            for (int k = 0; k < cw; ++k) {
-                T dkk = D[(c0 + k) * LDD + c0 + k];
-                if (!(dkk > T(0))) dkk = bad_pivot(dkk, tk.col + c0 + k, pv, lane == 0 && tile == 0);
-                const T lkk = dev_sqrt(dkk);
-                __syncwarp();
-                if (lane > k && lane < cw) D[(c0 + k) * LDD + c0 + lane] /= lkk;
-                if (lane == 0) D[(c0 + k) * LDD + c0 + k] = lkk;
-                __syncwarp();
-                if (lane > k && lane < cw) {
-                    const T lik = D[(c0 + k) * LDD + c0 + lane];
-                    for (int j = k + 1; j <= lane; ++j)
-                        D[(c0 + j) * LDD + c0 + lane] -= lik * D[(c0 + k) * LDD + c0 + j];
-                }
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-        // rows below the sub-block inside the diagonal block: D[r, c] := D[r, c] L_cc^{-T}
-        for (int r = c0 + cw + tid; r < nb; r += nt) {
-            for (int j = 0; j < cw; ++j) {
-                T x = D[(c0 + j) * LDD + r];
-                for (int k = 0; k < j; ++k) x -= D[(c0 + k) * LDD + r] * D[(c0 + k) * LDD + c0 + j];
-                D[(c0 + j) * LDD + r] = x / D[(c0 + j) * LDD + c0 + j];
-            }
-        }
-        __syncthreads();
-        // rank-cw update of the trailing part of the diagonal block
-        const int mm = nb - c0 - cw;
-        for (int q = tid; q < mm * mm; q += nt) {
-            const int jj = q / mm, ii = q - jj * mm;
-            if (ii < jj) continue;
-            const int i = c0 + cw + ii, j = c0 + cw + jj;
-            T a = T(0);
-            for (int k = 0; k < cw; ++k) a += D[(c0 + k) * LDD + i] * D[(c0 + k) * LDD + j];
-            D[j * LDD + i] -= a;
-        }
-        __syncthreads();
-    }
-    if (tile == 0) {
-        // not in place: other CTAs of this task may not have read the block yet
-        T *out = diag_scratch + tk.diag_out;
-        for (int q = tid; q < nb * nb; q += nt) {
-            const int j = q / nb, i = q - j * nb;
-            out[q] = D[j * LDD + i];
-        }
-    }
-    if (rows == 0) return;
-    // panel tile: X := X L^{-T}, 32 columns at a time
-    for (int c0 = 0; c0 < nb; c0 += 32) {
-        const int cw = min(32, nb - c0);
-        if (c0 > 0)
-            for (int q = tid; q < rows * cw; q += nt) {
-                const int j = q / rows, i = q - j * rows;
-                T a = T(0);
-                for (int k = 0; k < c0; ++k) a += X[k * kPanelRows + i] * D[k * LDD + c0 + j];
-                X[(c0 + j) * kPanelRows + i] -= a;
-            }
-        __syncthreads();
-        for (int i = tid; i < rows; i += nt) {
-            for (int j = 0; j < cw; ++j) {
-                T x = X[(c0 + j) * kPanelRows + i];
-                for (int k = 0; k < j; ++k) x -= X[(c0 + k) * kPanelRows + i] * D[(c0 + k) * LDD + c0 + j];
-                X[(c0 + j) * kPanelRows + i] = x / D[(c0 + j) * LDD + c0 + j];
-            }
-        }
-        __syncthreads();
-    }
-    for (int q = tid; q < rows * nb; q += nt) {
-        const int j = q / rows, i = q - j * rows;
-        blk[int64_t(j) * ld + nb + r0 + i] = X[j * kPanelRows + i];
-    }
-}
-
 inline int grid_for(int64_t n, int threads) {
     int64_t g = (n + threads - 1) / threads;
     if (g > 148 * 32) g = 148 * 32;
@@ -381,36 +266,6 @@ void launch_extract_diag(const int64_t *diag_off, int64_t n, const T *factor, do
     extract_diag_kernel<T><<<grid_for(n, 256), 256, 0, st>>>(diag_off, n, factor, out);
 }
 
-template <typename T>
-void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, T *diag_scratch,
-                  PivotCtl pv, cudaStream_t st) {
-    if (ntiles <= 0) return;
-    const size_t smem = (size_t(max_nb) * (max_nb + 1) + size_t(kPanelRows) * max_nb) * sizeof(T);
-    static const bool smem_ok = (cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin), true);
-    (void)smem_ok;
-    ++g_kernel_launches;
-    panel_kernel<T><<<ntiles, 256, smem, st>>>(tasks, ntasks, factor, diag_scratch, pv);
-}
-
-template <typename T>
-__global__ void diag_writeback_kernel(const PanelTask *__restrict__ tasks, const T *__restrict__ scratch,
-                                      T *__restrict__ factor) {
-    const PanelTask tk = tasks[blockIdx.x];
-    const T *src = scratch + tk.diag_out;
-    T *blk = factor + tk.off;
-    for (int q = threadIdx.x; q < tk.nb * tk.nb; q += blockDim.x) {
-        const int j = q / tk.nb, i = q - j * tk.nb;
-        if (i >= j) blk[int64_t(j) * tk.ld + i] = src[q];
-    }
-}
-
-template <typename T>
-void launch_diag_writeback(const PanelTask *tasks, int ntasks, const T *diag_scratch, T *factor, cudaStream_t st) {
-    if (ntasks <= 0) return;
-    ++g_kernel_launches;
-    diag_writeback_kernel<T><<<ntasks, 256, 0, st>>>(tasks, diag_scratch, factor);
-}
-
 #define MFS_INSTANTIATE(T)                                                                                        \
     template void launch_zero<T>(T *, int64_t, cudaStream_t);                                                      \
     template void launch_inject<T>(const PlanEntryDev *, int64_t, int, int, const double *, const double *, double, \
@@ -418,8 +273,6 @@ void launch_diag_writeback(const PanelTask *tasks, int ntasks, const T *diag_scr
     template void launch_diag_shift<T>(const int64_t *, int64_t, double, T *, cudaStream_t);                       \
     template void launch_small_factor<T>(const int32_t *, int, int, SnDev, T *, T *, PivotCtl, cudaStream_t);      \
     template void launch_assemble_large<T>(const AssembleTask *, int, int, SnDev, T *, T *, cudaStream_t);         \
-    template void launch_panel<T>(const PanelTask *, int, int, int, T *, T *, PivotCtl, cudaStream_t);            \
-    template void launch_diag_writeback<T>(const PanelTask *, int, const T *, T *, cudaStream_t);                 \
     template void launch_extract_diag<T>(const int64_t *, int64_t, const T *, double *, cudaStream_t);
 
 MFS_INSTANTIATE(double)

@@ -66,7 +66,6 @@ __device__ __forceinline__ void wait_flag(const int *flag, int epoch, int *err) 
                     atomicExch(err, 1);
                     break;
                 }
-                __nanosleep(32);
             }
         }
     }
@@ -131,9 +130,36 @@ __global__ void __launch_bounds__(256) fwd_asm_kernel(const SolveAsmTask *__rest
     }
 }
 
-// shared memory of the diag kernels: acc[kRB * nrhs] | vec[kRB * nrhs] | tile[kRB][kRB + 1]
-__host__ __device__ inline size_t tri_smem(int nrhs) {
+// shared memory of the structure kernels: out[kRB * nrhs] | vec[kRB * nrhs] | tile[kRB][kRB + 1]
+__host__ __device__ inline size_t str_smem(int nrhs) {
     return (size_t(2) * kRB * nrhs + size_t(kRB) * (kRB + 1)) * sizeof(double);
+}
+// shared memory of the diag kernels: acc[kRB * nrhs] | vec[kRB * nrhs] (double) |
+// tile[kRB][kRB + 1] | dblk[kRB][kRB + 1] (factor type)
+template <typename T>
+__host__ __device__ inline size_t diag_smem(int nrhs) {
+    return size_t(2) * kRB * nrhs * sizeof(double) + size_t(2) * kRB * (kRB + 1) * sizeof(T);
+}
+
+// Diagonal block of the task into dblk (row-major, ld kRB + 1): the stored
+// inverse of L(r, r) when the front has one, else the lower triangle of L(r, r).
+template <typename T>
+__device__ __forceinline__ bool load_diag_block(T *dblk, const T *factor, const T *pan, int64_t inv, int f, int r0,
+                                                int nr, int blk) {
+    const int tid = threadIdx.x;
+    if (inv >= 0) {
+        const T *src = factor + inv + int64_t(blk) * kRB * kRB;   // column-major 64 x 64
+        for (int q = tid; q < kRB * kRB; q += kTriThreads) {
+            const int j = q >> 6, i = q & 63;
+            dblk[i * (kRB + 1) + j] = src[q];
+        }
+        return true;
+    }
+    for (int q = tid; q < nr * nr; q += kTriThreads) {
+        const int j = q / nr, i = q % nr;
+        dblk[i * (kRB + 1) + j] = i >= j ? pan[int64_t(r0 + j) * f + r0 + i] : T(0);
+    }
+    return false;
 }
 
 template <typename T>
@@ -144,7 +170,8 @@ __global__ void __launch_bounds__(kTriThreads) fwd_diag_kernel(const SolveTask *
     extern __shared__ __align__(16) double smem_d[];
     double *acc = smem_d;
     double *yk = acc + kRB * nrhs;
-    double *tile = yk + kRB * nrhs;            // tile[i * (kRB+1) + j] = L(r0+i, k0+j)
+    T *tile = reinterpret_cast<T *>(yk + kRB * nrhs);   // tile[i * (kRB+1) + j] = L(r0+i, k0+j)
+    T *dblk = tile + kRB * (kRB + 1);
     const int tid = threadIdx.x;
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SolveTask tk = tasks[t];
@@ -153,15 +180,18 @@ __global__ void __launch_bounds__(kTriThreads) fwd_diag_kernel(const SolveTask *
         const int c0 = sd.col0[s];
         const int r0 = tk.blk * kRB, nr = min(kRB, w - r0);
         const T *pan = factor + sd.pan_off[s];
+        // everything that does not depend on earlier blocks is loaded before the first wait
+        const bool has_inv = load_diag_block(dblk, factor, pan, sd.inv_off[s], f, r0, nr, tk.blk);
         for (int q = tid; q < nr * nrhs; q += kTriThreads) {
             const int i = q / nrhs, r = q % nrhs;
             acc[q] = X[c0 + r0 + i + r * ldx];
         }
         for (int k = 0; k < tk.blk; ++k) {
             const int k0 = k * kRB;      // full block: k < blk
+            __syncthreads();
             for (int q = tid; q < nr * kRB; q += kTriThreads) {
                 const int j = q / nr, i = q % nr;
-                tile[i * (kRB + 1) + j] = double(pan[int64_t(k0 + j) * f + r0 + i]);
+                tile[i * (kRB + 1) + j] = pan[int64_t(k0 + j) * f + r0 + i];
             }
             wait_flag(flags + tk.flag_base + k, 1, err);
             for (int q = tid; q < kRB * nrhs; q += kTriThreads) {
@@ -171,40 +201,53 @@ __global__ void __launch_bounds__(kTriThreads) fwd_diag_kernel(const SolveTask *
             __syncthreads();
             for (int q = tid; q < nr * nrhs; q += kTriThreads) {
                 const int i = q / nrhs, r = q % nrhs;
-                const double *trow = tile + i * (kRB + 1);
-                double a = 0.0;
+                const T *trow = tile + i * (kRB + 1);
+                double a0 = 0.0, a1 = 0.0;
 #pragma unroll 8
-                for (int j = 0; j < kRB; ++j) a += trow[j] * yk[j * nrhs + r];
-                acc[q] -= a;
+                for (int j = 0; j < kRB; j += 2) {
+                    a0 += double(trow[j]) * yk[j * nrhs + r];
+                    a1 += double(trow[j + 1]) * yk[(j + 1) * nrhs + r];
+                }
+                acc[q] -= a0 + a1;
+            }
+        }
+        __syncthreads();
+        if (has_inv) {
+            // y = inv(L(r, r)) acc, written straight to X
+            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
+                const int i = q / nrhs, r = q % nrhs;
+                const T *irow = dblk + i * (kRB + 1);
+                double a0 = 0.0, a1 = 0.0;
+                int j = 0;
+                for (; j + 1 <= i; j += 2) {
+                    a0 += double(irow[j]) * acc[j * nrhs + r];
+                    a1 += double(irow[j + 1]) * acc[(j + 1) * nrhs + r];
+                }
+                if (j == i) a0 += double(irow[j]) * acc[j * nrhs + r];
+                X[c0 + r0 + i + r * ldx] = a0 + a1;
+            }
+        } else {
+            if (tid < 32) {
+                for (int j = 0; j < nr; ++j) {
+                    const double ljj = double(dblk[j * (kRB + 1) + j]);
+                    for (int r = tid; r < nrhs; r += 32) acc[j * nrhs + r] /= ljj;
+                    __syncwarp();
+                    for (int i = j + 1 + tid; i < nr; i += 32) {
+                        const double lij = double(dblk[i * (kRB + 1) + j]);
+                        for (int r = 0; r < nrhs; ++r) acc[i * nrhs + r] -= lij * acc[j * nrhs + r];
+                    }
+                    __syncwarp();
+                }
             }
             __syncthreads();
-        }
-        for (int q = tid; q < nr * nr; q += kTriThreads) {
-            const int j = q / nr, i = q % nr;
-            tile[i * (kRB + 1) + j] = i >= j ? double(pan[int64_t(r0 + j) * f + r0 + i]) : 0.0;
-        }
-        __syncthreads();
-        if (tid < 32) {
-            for (int j = 0; j < nr; ++j) {
-                const double ljj = tile[j * (kRB + 1) + j];
-                for (int r = tid; r < nrhs; r += 32) acc[j * nrhs + r] /= ljj;
-                __syncwarp();
-                for (int i = j + 1 + tid; i < nr; i += 32) {
-                    const double lij = tile[i * (kRB + 1) + j];
-                    for (int r = 0; r < nrhs; ++r) acc[i * nrhs + r] -= lij * acc[j * nrhs + r];
-                }
-                __syncwarp();
+            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
+                const int i = q / nrhs, r = q % nrhs;
+                X[c0 + r0 + i + r * ldx] = acc[q];
             }
-        }
-        __syncthreads();
-        for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-            const int i = q / nrhs, r = q % nrhs;
-            X[c0 + r0 + i + r * ldx] = acc[q];
         }
         __threadfence();
         __syncthreads();
         if (tid == 0) st_release(flags + tk.flag_base + tk.blk, 1);
-        __syncthreads();
     }
 }
 
@@ -216,7 +259,8 @@ __global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *
     extern __shared__ __align__(16) double smem_d[];
     double *acc = smem_d;
     double *xk = acc + kRB * nrhs;
-    double *tile = xk + kRB * nrhs;            // tile[i * (kRB+1) + j] = L(i0+i, r0+j)
+    T *tile = reinterpret_cast<T *>(xk + kRB * nrhs);   // tile[i * (kRB+1) + j] = L(i0+i, r0+j)
+    T *dblk = tile + kRB * (kRB + 1);
     const int tid = threadIdx.x;
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SolveTask tk = tasks[t];
@@ -226,15 +270,17 @@ __global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *
         const int nbw = (w + kRB - 1) / kRB;
         const int r0 = tk.blk * kRB, nr = min(kRB, w - r0);
         const T *pan = factor + sd.pan_off[s];
+        const bool has_inv = load_diag_block(dblk, factor, pan, sd.inv_off[s], f, r0, nr, tk.blk);
         for (int q = tid; q < nr * nrhs; q += kTriThreads) {
             const int j = q / nrhs, r = q % nrhs;
             acc[q] = X[c0 + r0 + j + r * ldx];
         }
         for (int k = nbw - 1; k > tk.blk; --k) {
             const int i0 = k * kRB, ni = min(kRB, w - i0);
+            __syncthreads();
             for (int q = tid; q < ni * nr; q += kTriThreads) {
                 const int j = q / ni, i = q % ni;
-                tile[i * (kRB + 1) + j] = double(pan[int64_t(r0 + j) * f + i0 + i]);
+                tile[i * (kRB + 1) + j] = pan[int64_t(r0 + j) * f + i0 + i];
             }
             wait_flag(flags + tk.flag_base + k, 2, err);
             for (int q = tid; q < ni * nrhs; q += kTriThreads) {
@@ -245,36 +291,45 @@ __global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *
             for (int q = tid; q < nr * nrhs; q += kTriThreads) {
                 const int j = q / nrhs, r = q % nrhs;
                 double a = 0.0;
-                for (int i = 0; i < ni; ++i) a += tile[i * (kRB + 1) + j] * xk[i * nrhs + r];
+                for (int i = 0; i < ni; ++i) a += double(tile[i * (kRB + 1) + j]) * xk[i * nrhs + r];
                 acc[q] -= a;
             }
-            __syncthreads();
-        }
-        for (int q = tid; q < nr * nr; q += kTriThreads) {
-            const int j = q / nr, i = q % nr;
-            tile[i * (kRB + 1) + j] = i >= j ? double(pan[int64_t(r0 + j) * f + r0 + i]) : 0.0;
         }
         __syncthreads();
-        if (tid < 32) {
-            for (int j = nr - 1; j >= 0; --j) {
-                for (int r = tid; r < nrhs; r += 32) acc[j * nrhs + r] /= tile[j * (kRB + 1) + j];
-                __syncwarp();
-                for (int i = tid; i < j; i += 32) {
-                    const double lji = tile[j * (kRB + 1) + i];
-                    for (int r = 0; r < nrhs; ++r) acc[i * nrhs + r] -= lji * acc[j * nrhs + r];
+        if (has_inv) {
+            // x = inv(L(r, r))^T acc
+            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
+                const int j = q / nrhs, r = q % nrhs;
+                double a0 = 0.0, a1 = 0.0;
+                int i = j;
+                for (; i + 1 < nr; i += 2) {
+                    a0 += double(dblk[i * (kRB + 1) + j]) * acc[i * nrhs + r];
+                    a1 += double(dblk[(i + 1) * (kRB + 1) + j]) * acc[(i + 1) * nrhs + r];
                 }
-                __syncwarp();
+                if (i < nr) a0 += double(dblk[i * (kRB + 1) + j]) * acc[i * nrhs + r];
+                X[c0 + r0 + j + r * ldx] = a0 + a1;
             }
-        }
-        __syncthreads();
-        for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-            const int j = q / nrhs, r = q % nrhs;
-            X[c0 + r0 + j + r * ldx] = acc[q];
+        } else {
+            if (tid < 32) {
+                for (int j = nr - 1; j >= 0; --j) {
+                    for (int r = tid; r < nrhs; r += 32) acc[j * nrhs + r] /= double(dblk[j * (kRB + 1) + j]);
+                    __syncwarp();
+                    for (int i = tid; i < j; i += 32) {
+                        const double lji = double(dblk[j * (kRB + 1) + i]);
+                        for (int r = 0; r < nrhs; ++r) acc[i * nrhs + r] -= lji * acc[j * nrhs + r];
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
+                const int j = q / nrhs, r = q % nrhs;
+                X[c0 + r0 + j + r * ldx] = acc[q];
+            }
         }
         __threadfence();
         __syncthreads();
         if (tid == 0) st_release(flags + tk.flag_base + tk.blk, 2);
-        __syncthreads();
     }
 }
 
@@ -398,13 +453,13 @@ cudaError_t launch_diag(bool forward, const SolveTask *tasks, int ntasks, SnDev 
                         int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st) {
     if (ntasks <= 0) return cudaSuccess;
     void *kern = forward ? (void *)fwd_diag_kernel<T> : (void *)bwd_diag_kernel<T>;
-    const size_t smem = tri_smem(nrhs);
+    const size_t smem = diag_smem<T>(nrhs);
     // one-time per kernel: shared-memory opt-in and co-resident grid per RHS count
     static const bool attr_ok =
         (cudaFuncSetAttribute(fwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(tri_smem(kMaxSolveRhs))),
+                              int(diag_smem<T>(kMaxSolveRhs))),
          cudaFuncSetAttribute(bwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(tri_smem(kMaxSolveRhs))),
+                              int(diag_smem<T>(kMaxSolveRhs))),
          true);
     (void)attr_ok;
     static int grid_cache[2][kMaxSolveRhs + 1] = {};
@@ -422,12 +477,12 @@ void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce 
                 const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st) {
     if (ntasks <= 0) return;
     g_kernel_launches += 2;
-    const size_t smem = tri_smem(nrhs);
+    const size_t smem = str_smem(nrhs);
     static const bool attr_ok =
         (cudaFuncSetAttribute(str_partial_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(tri_smem(kMaxSolveRhs))),
+                              int(str_smem(kMaxSolveRhs))),
          cudaFuncSetAttribute(str_partial_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(tri_smem(kMaxSolveRhs))),
+                              int(str_smem(kMaxSolveRhs))),
          true);
     (void)attr_ok;
     if (forward) {
