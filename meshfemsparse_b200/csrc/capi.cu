@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <type_traits>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -82,12 +83,12 @@ struct LevelPlan {
     int large_count = 0;
     int asm_off = 0, asm_n = 0, asm_tiles = 0;
     struct Step {
-        int potrf_off, potrf_n, potrf_tiles, potrf_maxnb;
-        int gemm_off, gemm_n, gemm_tiles;
+        int potrf_off, potrf_n, potrf_maxnb;
+        int trsm_off, trsm_n, trsm_tiles;   // X := X inv(L)^T of the rows below the block
+        int gemm_off, gemm_n, gemm_tiles;   // trailing update of the remaining panel columns
     };
     std::vector<Step> steps;
     int syrk_off = 0, syrk_n = 0, syrk_tiles = 0;
-    int panel_first = 0, panel_count = 0;   // all panel tasks of the level (diagonal write-back)
     // solve task lists of this level
     int sasm_off = 0, sasm_n = 0, sasm_tiles = 0;
     int ftri_off = 0, ftri_n = 0;
@@ -98,7 +99,7 @@ struct LevelPlan {
 
 struct DevSym {
     std::shared_ptr<Symbolic> S;
-    DBuf<int32_t> w, d, f, col0, child_ptr, child_list, struct_rows, rel, small_list, all_list;
+    DBuf<int32_t> w, d, f, ld, col0, child_ptr, child_list, struct_rows, rel, small_list, all_list;
     DBuf<int64_t> pan_off, upd_off, sol_off, struct_ptr, diag_off;
     DBuf<int64_t> inv_off;               // 64 x 64 diagonal inverses of large fronts (-1: none)
     DBuf<PlanEntryDev> plan;
@@ -119,10 +120,13 @@ struct DevSym {
     int64_t ax_len = 0;
     std::vector<int64_t> Ap_full, Ai_full;   // caller's pattern (for the element slot map)
     int num_large = 0;
-    int64_t diag_scratch = 0;            // elements of factored diagonal blocks held per level
+    int64_t inv_scratch = 0;             // elements of the block inverses of one column-block step
     int64_t factor_alloc = 0;            // panels followed by the diagonal inverses
+    std::vector<int64_t> dpan;           // device panel offsets (leading dimension padded to 4)
+    std::vector<int32_t> dld;            // device panel leading dimensions
+    int64_t panel_alloc = 0;             // elements of the padded panels
     size_t bytes() const {
-        return w.bytes() * 4 + col0.bytes() + child_ptr.bytes() + child_list.bytes() + struct_rows.bytes() +
+        return w.bytes() * 5 + col0.bytes() + child_ptr.bytes() + child_list.bytes() + struct_rows.bytes() +
                rel.bytes() + small_list.bytes() + all_list.bytes() + pan_off.bytes() + upd_off.bytes() +
                sol_off.bytes() + struct_ptr.bytes() + diag_off.bytes() + inv_off.bytes() + plan.bytes() + asm_tasks.bytes() +
                potrf_tasks.bytes() + gemm_tasks.bytes() + spmv_ptr.bytes() +
@@ -151,10 +155,11 @@ struct mfs_handle {
     bool has_stash = false;
     DBuf<double> upd64;            // update arena (multifrontal Schur complements)
     DBuf<float> upd32;
-    DBuf<double> dscr64;           // factored diagonal blocks of one level (written back per level)
+    DBuf<double> dscr64;           // inverses of the diagonal blocks of one column-block step
     DBuf<float> dscr32;
     DBuf<double> sol;
     std::shared_ptr<DBuf<double>> asm_ax;   // output of the last mfs_assemble (device resident)
+    std::shared_ptr<DBuf<double>> asm_spare;   // an earlier assembly buffer, reused once nothing holds it
     DBuf<double> rhs, work_r, work_z, work_p, work_ap, work_x, work_s, io;
     DBuf<double> partials, dots;
     DBuf<int> active;
@@ -162,6 +167,7 @@ struct mfs_handle {
     DBuf<int> perturbed;          // pivots perturbed in the last numeric factorization
     DBuf<double> dorig;           // injected diagonal (perturbation reference)
     DBuf<int> solve_err;          // set by a solve kernel whose dependency wait timed out
+    DBuf<int> gemm_err;           // set by a tensor-core GEMM whose pipeline wait timed out
     DBuf<double> str_partials;    // chunk partial sums of the solve structure phases (scratch)
     int *fail_host = nullptr;
     double *dots_host = nullptr;
@@ -220,28 +226,45 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         d32[s] = int32_t(S.d[s]);
         f32v[s] = int32_t(S.f[s]);
     }
+    // Device panel layout: the catamari panel with its leading dimension rounded up
+    // to a multiple of 4, so every column starts 16-byte aligned.
+    ds->dpan.assign(nsn + 1, 0);
+    ds->dld.assign(nsn, 0);
+    for (idx s = 0; s < nsn; ++s) {
+        ds->dld[s] = int32_t((S.f[s] + 3) & ~idx(3));
+        ds->dpan[s + 1] = ds->dpan[s] + int64_t(ds->dld[s]) * S.w[s];
+    }
+    ds->panel_alloc = ds->dpan[nsn];
+    const std::vector<int64_t> &dpan = ds->dpan;
+    const std::vector<int32_t> &dld = ds->dld;
     ds->w.upload(w32, st);
     ds->d.upload(d32, st);
     ds->f.upload(f32v, st);
+    ds->ld.upload(dld, st);
     ds->col0.upload(col0, st);
     ds->child_ptr.upload(S.child_ptr, st);
     ds->child_list.upload(S.child_list, st);
     ds->struct_rows.upload(S.struct_rows, st);
     ds->rel.upload(S.rel, st);
-    ds->pan_off.upload(S.pan_off, st);
+    ds->pan_off.upload(dpan, st);
     ds->upd_off.upload(S.upd_off, st);
     ds->sol_off.upload(S.sol_off, st);
     ds->struct_ptr.upload(S.struct_ptr, st);
     std::vector<int64_t> diag(S.n);
     for (idx s = 0; s < nsn; ++s)
-        for (idx k = 0; k < S.w[s]; ++k) diag[S.vb * S.sn_start[s] + k] = S.pan_off[s] + k * S.f[s] + k;
+        for (idx k = 0; k < S.w[s]; ++k) diag[S.vb * S.sn_start[s] + k] = dpan[s] + k * dld[s] + k;
     ds->diag_off.upload(diag, st);
     {
+        // plan destinations move from the catamari layout to the padded device layout
         std::vector<PlanEntryDev> pl(S.plan.size());
         for (size_t k = 0; k < pl.size(); ++k) {
-            pl[k].dst = S.plan[k].dst;
+            const idx dst = S.plan[k].dst;
+            const idx s = idx(std::upper_bound(S.pan_off.begin(), S.pan_off.begin() + nsn + 1, dst) -
+                              S.pan_off.begin()) - 1;
+            const idx rel = dst - S.pan_off[s];
+            pl[k].dst = dpan[s] + (rel / S.f[s]) * dld[s] + rel % S.f[s];
             pl[k].src = S.plan[k].src;
-            pl[k].ld = S.plan[k].ld;
+            pl[k].ld = dld[s];
             pl[k].flags = S.plan[k].flags;
         }
         ds->plan.ensure(pl.size());
@@ -266,7 +289,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     ds->levels.resize(S.nlevels);
     ds->num_large = 0;
     std::vector<int64_t> inv_off(nsn, -1);
-    int64_t inv_end = S.factor_size;
+    int64_t inv_end = ds->panel_alloc;
     for (idx l = 0; l < S.nlevels; ++l) {
         LevelPlan &L = ds->levels[l];
         std::vector<idx> large;
@@ -301,71 +324,94 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         const bool f64 = h->opt.precision != MFS_PREC_FP32;
         const int NB = f64 ? 64 : 128;                  // column block of the large-front factorization
         const int TM = gemm_tile_m(f64), TN = gemm_tile_n(f64);
+        // The in-place row solve needs every CTA tile to span the block's columns
+        // (with the FP32 tiles' alignment shift of up to 3 columns).
+        if (NB + (f64 ? 0 : 3) > TN) throw StatusError(MFS_INTERNAL, "column block wider than the GEMM tile");
         auto gemm = [&](int64_t a_off, int64_t b_off, int64_t c_off, int lda, int ldb, int ldc, idx m, idx n, idx k,
                         int lower, int mode, int &base) {
             GemmTask g{};
             g.a_off = a_off; g.b_off = b_off; g.c_off = c_off;
             g.lda = lda; g.ldb = ldb; g.ldc = ldc;
             g.m = int32_t(m); g.n = int32_t(n); g.k = int32_t(k);
-            g.tiles_m = int32_t((m + TM - 1) / TM);
-            g.tiles_n = int32_t((n + TN - 1) / TN);
+            // FP32 operands are staged in 16-byte chunks: a tile starts at the
+            // aligned element at or before the operand (leading dimensions are
+            // multiples of 4, so the shift is the same for every column).
+            int da = 0, db = 0;
+            if (!f64) {
+                if ((lda & 3) || (ldb & 3)) throw StatusError(MFS_INTERNAL, "unaligned GEMM operand");
+                da = int(a_off & 3);
+                db = int(b_off & 3);
+            }
+            g.shift = da | (db << 8);
+            g.tiles_m = int32_t((m + da + TM - 1) / TM);
+            g.tiles_n = int32_t((n + db + TN - 1) / TN);
             g.tile_base = base;
             g.lower = lower;
             g.mode = mode;
             base += g.tiles_m * g.tiles_n;
             gemm_tasks.push_back(g);
         };
-        L.panel_first = int(potrf_tasks.size());
-        int64_t dslot = 0;
         for (idx kb = 0; kb < maxw; kb += NB) {
             LevelPlan::Step sp{};
             sp.potrf_off = int(potrf_tasks.size());
-            int pb = 0;
+            int64_t dslot = 0;
             for (idx s : large) {
-                const idx w = S.w[s], f = S.f[s], pan = S.pan_off[s];
+                const idx w = S.w[s], ld = dld[s], pan = dpan[s];
                 if (w <= kb) continue;
                 const int nb = int(std::min<idx>(NB, w - kb));
                 PanelTask pt{};
-                pt.off = pan + kb * f + kb;
-                pt.diag_out = dslot;
-                dslot += int64_t(nb) * nb;
+                pt.off = pan + kb * ld + kb;
+                pt.ldi = (nb + 3) & ~3;
+                pt.inv_full = dslot;
+                dslot += int64_t(pt.ldi) * nb;
                 pt.inv_out = inv_off[s] + (kb / 64) * 4096;
-                pt.ld = int32_t(f);
+                pt.ld = int32_t(ld);
                 pt.nb = nb;
-                pt.m = int32_t(f - kb - nb);
                 pt.col = int32_t(col0[s] + kb);
-                pt.tile_base = pb;
-                pb += std::max(1, int((pt.m + kPanelRows - 1) / kPanelRows));
                 potrf_tasks.push_back(pt);
                 sp.potrf_maxnb = std::max(sp.potrf_maxnb, nb);
             }
             sp.potrf_n = int(potrf_tasks.size()) - sp.potrf_off;
-            sp.potrf_tiles = pb;
+            ds->inv_scratch = std::max<int64_t>(ds->inv_scratch, dslot);
+            // rows below the diagonal block: X := X inv(L)^T (in place; one CTA tile spans all nb columns)
+            sp.trsm_off = int(gemm_tasks.size());
+            int tb = 0;
+            {
+                int q = sp.potrf_off;
+                for (idx s : large) {
+                    if (S.w[s] <= kb) continue;
+                    const PanelTask &pt = potrf_tasks[q++];
+                    const idx m = S.f[s] - (kb + pt.nb);   // rows of the front below the block
+                    if (m > 0)
+                        gemm(pt.off + pt.nb, pt.inv_full, pt.off + pt.nb, pt.ld, pt.ldi, pt.ld, m, pt.nb, pt.nb, 0, 1,
+                             tb);
+                }
+            }
+            sp.trsm_n = int(gemm_tasks.size()) - sp.trsm_off;
+            sp.trsm_tiles = tb;
             // trailing update of the remaining panel columns
             sp.gemm_off = int(gemm_tasks.size());
             int gb = 0;
             for (idx s : large) {
-                const idx w = S.w[s], f = S.f[s], pan = S.pan_off[s];
+                const idx w = S.w[s], f = S.f[s], ld = dld[s], pan = dpan[s];
                 if (w <= kb) continue;
                 const int nb = int(std::min<idx>(NB, w - kb));
                 const idx m = f - kb - nb, n = w - kb - nb;
                 if (n > 0) {
-                    const int64_t a = pan + kb * f + kb + nb;
-                    gemm(a, a, pan + (kb + nb) * f + kb + nb, int(f), int(f), int(f), m, n, nb, 1, 0, gb);
+                    const int64_t a = pan + kb * ld + kb + nb;
+                    gemm(a, a, pan + (kb + nb) * ld + kb + nb, int(ld), int(ld), int(ld), m, n, nb, 1, 0, gb);
                 }
             }
             sp.gemm_n = int(gemm_tasks.size()) - sp.gemm_off;
             sp.gemm_tiles = gb;
             L.steps.push_back(sp);
         }
-        L.panel_count = int(potrf_tasks.size()) - L.panel_first;
-        ds->diag_scratch = std::max<int64_t>(ds->diag_scratch, dslot);
         L.syrk_off = int(gemm_tasks.size());
         int sb = 0;
         for (idx s : large) {
             if (S.d[s] == 0 || S.upd_off[s] < 0) continue;
-            const int64_t a = S.pan_off[s] + S.w[s];
-            gemm(a, a, S.upd_off[s], int(S.f[s]), int(S.f[s]), int(S.d[s]), S.d[s], S.d[s], S.w[s], 1, 0, sb);
+            const int64_t a = dpan[s] + S.w[s];
+            gemm(a, a, S.upd_off[s], dld[s], dld[s], int(S.d[s]), S.d[s], S.d[s], S.w[s], 1, 0, sb);
         }
         L.syrk_n = int(gemm_tasks.size()) - L.syrk_off;
         L.syrk_tiles = sb;
@@ -473,6 +519,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     sd.pan_off = ds->pan_off.p;
     sd.upd_off = ds->upd_off.p;
     sd.sol_off = ds->sol_off.p;
+    sd.ld = ds->ld.p;
     sd.inv_off = ds->inv_off.p;
     sd.child_ptr = ds->child_ptr.p;
     sd.child_list = ds->child_list.p;
@@ -490,8 +537,10 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
     cudaStream_t st = h->stream;
     // FP32 factors: single-pass TF32 when FP64 refinement recovers the accuracy,
     // split 3xTF32 (FP32-level products) otherwise or when asked for.
-    const int split = (h->opt.tensor_cores == 2 || (h->opt.tensor_cores == 0 && !h->opt.refine)) ? 3 : 1;
-    launch_zero<T>(factor, S.factor_size, st);
+    // 1: single-pass TF32 on tcgen05, 3: split 3xTF32 (mma.sync), 0: single-pass TF32 on mma.sync
+    const int tc = h->opt.tensor_cores;
+    const int split = tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : (h->opt.refine ? 1 : 3);
+    launch_zero<T>(factor, ds.panel_alloc, st);
     MFS_LAUNCHED();
     launch_inject<T>(ds.plan.p, int64_t(S.plan.size()), S.vb, S.src_ld, Ax, Bx, Bx ? sigma : 0.0, factor, st);
     MFS_LAUNCHED();
@@ -518,16 +567,18 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         launch_assemble_large<T>(ds.asm_tasks.p + L.asm_off, L.asm_n, L.asm_tiles, ds.sd, factor, upd, st);
         MFS_LAUNCHED();
         for (const auto &sp : L.steps) {
-            launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_tiles, sp.potrf_maxnb, factor,
-                            dscr, pv, st);
+            launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, dscr, pv, split == 1,
+                            st);
             MFS_LAUNCHED();
-            launch_gemm<T>(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor, factor, split, st);
+            launch_gemm<T>(ds.gemm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, factor, dscr, factor, split,
+                           h->gemm_err.p, st);
+            MFS_LAUNCHED();
+            launch_gemm<T>(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor, factor, split,
+                           h->gemm_err.p, st);
             MFS_LAUNCHED();
         }
-        launch_diag_writeback<T>(ds.potrf_tasks.p + L.panel_first, L.panel_count, dscr, factor, st);
-        MFS_LAUNCHED();
         if (L.syrk_n > 0) {
-            launch_gemm<T>(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, factor, upd, split, st);
+            launch_gemm<T>(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, factor, upd, split, h->gemm_err.p, st);
             MFS_LAUNCHED();
         }
     }
@@ -743,12 +794,14 @@ mfs_status mfs_create(mfs_handle **out, const mfs_options *opt) {
         }
         MFS_CUDA(cudaEventCreate(&h->ev0));
         MFS_CUDA(cudaEventCreate(&h->ev1));
-        MFS_CUDA(cudaMallocHost(&h->fail_host, 2 * sizeof(int)));
+        MFS_CUDA(cudaMallocHost(&h->fail_host, 3 * sizeof(int)));
         MFS_CUDA(cudaMallocHost(&h->dots_host, 64 * sizeof(double)));
         h->fail.ensure(1);
         h->perturbed.ensure(1);
         h->solve_err.ensure(1);
         MFS_CUDA(cudaMemset(h->solve_err.p, 0, sizeof(int)));
+        h->gemm_err.ensure(1);
+        MFS_CUDA(cudaMemset(h->gemm_err.p, 0, sizeof(int)));
     });
     if (s != MFS_OK) {
         // keep the message reachable for callers that only get a status
@@ -820,6 +873,7 @@ mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, cons
         // A new analysis replaces the current factorization (the stash is kept).
         h->cur = State();
         h->asm_ax.reset();
+        h->asm_spare.reset();
         h->nslots = 0;
         h->nelem = 0;
         auto Sp = std::make_shared<Symbolic>();
@@ -894,24 +948,29 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
             if (!h->cur.f32 || h->cur.f32.use_count() > 1) h->cur.f32 = std::make_shared<DBuf<float>>();
             h->cur.f32->ensure(size_t(ds.factor_alloc));
             h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
-            h->dscr32.ensure(size_t(std::max<int64_t>(ds.diag_scratch, 1)));
+            h->dscr32.ensure(size_t(std::max<int64_t>(ds.inv_scratch, 1)));
             run_factor<float>(h, ds, h->cur.f32->p, h->upd32.p, h->dscr32.p, h->cur.ax->p, dBx, sigma);
         } else {
             if (!h->cur.f64 || h->cur.f64.use_count() > 1) h->cur.f64 = std::make_shared<DBuf<double>>();
             h->cur.f64->ensure(size_t(ds.factor_alloc));
             h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
-            h->dscr64.ensure(size_t(std::max<int64_t>(ds.diag_scratch, 1)));
+            h->dscr64.ensure(size_t(std::max<int64_t>(ds.inv_scratch, 1)));
             run_factor<double>(h, ds, h->cur.f64->p, h->upd64.p, h->dscr64.p, h->cur.ax->p, dBx, sigma);
         }
         MFS_CUDA(cudaEventRecord(h->ev1, st));
         MFS_CUDA(cudaMemcpyAsync(h->fail_host, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         MFS_CUDA(cudaMemcpyAsync(h->fail_host + 1, h->perturbed.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        MFS_CUDA(cudaMemcpyAsync(h->fail_host + 2, h->gemm_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         MFS_CUDA(cudaStreamSynchronize(st));
         float ms = 0;
         cudaEventElapsedTime(&ms, h->ev0, h->ev1);
         h->stats.factor_ms = ms;
         h->stats.perturbed_pivots = h->fail_host[1];
         h->cur.sigma = sigma;
+        if (h->fail_host[2]) {
+            MFS_CUDA(cudaMemset(h->gemm_err.p, 0, sizeof(int)));
+            throw StatusError(MFS_TIMEOUT, "Schur update: a tensor-core pipeline wait timed out");
+        }
         if (*h->fail_host != INT_MAX) {
             h->stats.failed_column = *h->fail_host;
             throw StatusError(MFS_NOT_POSDEF, std::to_string(*h->fail_host) + "/" + std::to_string(S.n) +
@@ -1082,7 +1141,16 @@ mfs_status mfs_assemble(mfs_handle *h, const double *Ke, double *Ax_out, int32_t
         const bool dev = (flags & MFS_DEVICE_POINTERS) != 0;
         const size_t ke_n = size_t(h->nelem) * 144;
         const double *Ked = dev ? Ke : stage_input(h, h->ke, Ke, ke_n, false);
-        if (!h->asm_ax || h->asm_ax.use_count() > 1) h->asm_ax = std::make_shared<DBuf<double>>();
+        // The current factor may still hold the previous assembly (its values drive
+        // refinement): assemble into another buffer then, alternating between two.
+        if (!h->asm_ax || h->asm_ax.use_count() > 1) {
+            if (h->asm_spare && h->asm_spare.use_count() == 1) std::swap(h->asm_ax, h->asm_spare);
+            else {
+                h->asm_spare = h->asm_ax;
+                h->asm_ax = std::make_shared<DBuf<double>>();
+            }
+            if (h->asm_ax.use_count() > 1) h->asm_ax = std::make_shared<DBuf<double>>();
+        }
         h->asm_ax->ensure(size_t(ds.ax_len));
         MFS_CUDA(cudaEventRecord(h->ev0, st));
         launch_assemble_elements(h->slot_ptr.p, h->contrib.p, h->nslots, Ked, h->asm_ax->p, st);
@@ -1177,13 +1245,19 @@ mfs_status mfs_factor_values(const mfs_handle *h, int64_t *factor_size, double *
     mfs_handle *hm = const_cast<mfs_handle *>(h);
     return guarded(hm, [&] {
         set_device(hm);
-        if (h->opt.precision == MFS_PREC_FP32) {
-            std::vector<float> tmp(S.factor_size);
-            MFS_CUDA(cudaMemcpy(tmp.data(), h->cur.f32->p, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost));
-            std::copy(tmp.begin(), tmp.end(), out);
-        } else {
-            MFS_CUDA(cudaMemcpy(out, h->cur.f64->p, size_t(S.factor_size) * sizeof(double), cudaMemcpyDeviceToHost));
-        }
+        // the device panels carry padded leading dimensions: repack into the catamari layout
+        const DevSym &ds = *h->cur.sym;
+        auto repack = [&](const auto *dev) {
+            using T = std::remove_const_t<std::remove_pointer_t<decltype(dev)>>;
+            std::vector<T> tmp(size_t(ds.panel_alloc));
+            MFS_CUDA(cudaMemcpy(tmp.data(), dev, tmp.size() * sizeof(T), cudaMemcpyDeviceToHost));
+            for (size_t s = 0; s + 1 < ds.dpan.size(); ++s)
+                for (idx j = 0; j < S.w[s]; ++j)
+                    for (idx i = 0; i < S.f[s]; ++i)
+                        out[S.pan_off[s] + j * S.f[s] + i] = double(tmp[ds.dpan[s] + j * ds.dld[s] + i]);
+        };
+        if (h->opt.precision == MFS_PREC_FP32) repack(static_cast<const float *>(h->cur.f32->p));
+        else repack(static_cast<const double *>(h->cur.f64->p));
     });
 }
 
@@ -1249,6 +1323,7 @@ mfs_status mfs_clear_factors(mfs_handle *h) {
     if (!h) return MFS_INVALID_ARG;
     h->cur = State();
     h->asm_ax.reset();
+    h->asm_spare.reset();
     h->nslots = 0;
     h->nelem = 0;
     return MFS_OK;

@@ -1,8 +1,11 @@
 // Device-side data layout and kernel launchers shared by the CUDA sources.
 //
 // Storage in HBM (all column-major):
-//   factor values  : one panel per supernode, (w+d) x w, ld = w+d, panels back to back
-//                    (catamari layout, CatamariConversionPlan.hh:366), followed by the
+//   factor values  : one panel per supernode, (w+d) x w with ld = w+d rounded up to a
+//                    multiple of 4 (16-byte aligned columns for the tensor-core
+//                    GEMM loads), panels back to back; the catamari layout
+//                    (CatamariConversionPlan.hh:366, ld = w+d) is produced on export;
+//                    followed by the
 //                    64 x 64 inverses of the diagonal blocks of every large front's L11
 //                    (written by the panel kernel, read by the triangular solves)
 //   update arena   : U_s (d x d, ld d) of the multifrontal assembly tree; offsets from
@@ -21,8 +24,9 @@ extern long long g_kernel_launches;
 
 struct SnDev {
     const int32_t *w, *d, *f;           // scalar width / degree / front size
+    const int32_t *ld;                  // panel leading dimension: f rounded up to a multiple of 4
     const int32_t *col0;                // first scalar column of the supernode
-    const int64_t *pan_off;             // panel offset in the factor array
+    const int64_t *pan_off;             // panel offset in the factor array (a multiple of 4)
     const int64_t *upd_off;             // U_s offset in the update arena (-1: none)
     const int64_t *sol_off;             // u_s offset (units of one RHS) in the solve arena
     const int64_t *inv_off;             // factor-array offset of the 64 x 64 inverses of L11's
@@ -61,25 +65,24 @@ struct GemmTask {
     int32_t tile_base;                  // prefix over tasks of tiles_m*tiles_n
     int32_t lower;                      // 1: only i >= j is touched
     int32_t mode;
+    int32_t shift;                      // FP32: tiles start da = shift & 255 rows before A and
+                                        // db = shift >> 8 rows before B (16-byte aligned starts);
+                                        // tiles_m / tiles_n cover m + da / n + db
 };
 
-// One column block of a large front: factor its nb x nb diagonal block and
-// solve the m rows below it (X := B L^{-T}) in tiles of kPanelRows rows.
-// Tile 0 of a task stores the factored diagonal block at scratch offset
-// `diag_out` (nb x nb, ld nb): the other CTAs of the task may still be reading
-// the unfactored block in place, so it is copied back once the level is done.
-// It also stores the 64 x 64 diagonal blocks of inv(L) at `inv_out` of the factor
+// One column block of a large front: factor its nb x nb diagonal block in
+// place, store inv(L) of the block (nb x nb, ld ldi) at `inv_full` of the
+// inverse scratch for the row solve X := X inv(L)^T that follows as a GEMM,
+// and store the 64 x 64 diagonal blocks of inv(L) at `inv_out` of the factor
 // array (-1: not stored), which the triangular solves apply as small GEMVs.
 struct PanelTask {
     int64_t off;                        // offset of the diagonal block's (0,0) entry
-    int64_t diag_out;                   // scratch offset of the factored diagonal block
+    int64_t inv_full;                   // scratch offset of inv(L) of the block
     int64_t inv_out;                    // factor-array offset of the 64 x 64 inverse blocks
-    int32_t ld, nb, m;
+    int32_t ld, nb;
     int32_t col;                        // global scalar column of the block's first pivot
-    int32_t tile_base;                  // prefix over tasks of max(1, ceil(m / kPanelRows))
-    int32_t pad;
+    int32_t ldi;                        // leading dimension of inv(L) in scratch (nb rounded up to 4)
 };
-constexpr int kPanelRows = 128;
 
 // Extend-add of all children of a large supernode, split by front columns.
 struct AssembleTask {
@@ -131,15 +134,16 @@ template <typename T>
 void launch_assemble_large(const AssembleTask *tasks, int ntasks, int ntiles, SnDev sd, T *factor, T *upd,
                            cudaStream_t st);
 template <typename T>
-void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, T *diag_scratch,
-                  PivotCtl pv, cudaStream_t st);
-// Copy the factored diagonal blocks of a level's panel tasks back into the factor.
+void launch_panel(const PanelTask *tasks, int ntasks, int max_nb, T *factor, T *inv_scratch, PivotCtl pv,
+                  bool round_inv, cudaStream_t st);
+// Tensor-core tile GEMM. float: split 1 = single-pass TF32 on tcgen05, 3 = split
+// 3xTF32 on mma.sync, 0 = single-pass TF32 on mma.sync; double: DMMA. A wait of
+// the tcgen05 pipeline that times out sets *err.
 template <typename T>
-void launch_diag_writeback(const PanelTask *tasks, int ntasks, const T *diag_scratch, T *factor, cudaStream_t st);
-// Tensor-core tile GEMM (TF32 / split 3xTF32 for float, DMMA for double).
-template <typename T>
-void launch_gemm(const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int split,
+void launch_gemm(const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int split, int *err,
                  cudaStream_t st);
+void launch_gemm_tc(const GemmTask *tasks, int ntasks, int ntiles, const float *A, const float *B, float *C, int *err,
+                    cudaStream_t st);
 int gemm_tile_m(bool fp64);
 int gemm_tile_n(bool fp64);
 

@@ -104,8 +104,9 @@ __global__ void __launch_bounds__(256) small_factor_kernel(const int32_t *__rest
     const int w = sd.w[s], d = sd.d[s], f = w + d;
     const int tid = threadIdx.x, nt = blockDim.x;
     T *pan = factor + sd.pan_off[s];
+    const int ld = sd.ld[s];
     const int fw = f * w;
-    for (int k = tid; k < f * f; k += nt) F[k] = k < fw ? pan[k] : T(0);
+    for (int k = tid; k < f * f; k += nt) F[k] = k < fw ? pan[(k / f) * ld + k % f] : T(0);
     __syncthreads();
     const int vb = sd.vb;
     for (int ci = sd.child_ptr[s]; ci < sd.child_ptr[s + 1]; ++ci) {
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(256) small_factor_kernel(const int32_t *__rest
         }
         __syncthreads();
     }
-    for (int k = tid; k < fw; k += nt) pan[k] = F[k];
+    for (int k = tid; k < fw; k += nt) pan[(k / f) * ld + k % f] = F[k];
     if (d > 0 && sd.upd_off[s] >= 0) {
         T *U = upd + sd.upd_off[s];
         for (int k = tid; k < d * d; k += nt) {
@@ -167,6 +168,7 @@ __global__ void __launch_bounds__(256) assemble_large_kernel(const AssembleTask 
     const int w = sd.w[s], d = sd.d[s], f = w + d;
     const int c0 = chunk * kAsmCols, c1 = min(f, c0 + kAsmCols);
     T *pan = factor + sd.pan_off[s];
+    const int ld = sd.ld[s];
     T *Us = (d > 0 && sd.upd_off[s] >= 0) ? upd + sd.upd_off[s] : nullptr;
     const int tid = threadIdx.x, nt = blockDim.x;
     // zero the U_s columns of this chunk
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(256) assemble_large_kernel(const AssembleTask 
                 for (int ic = jc + tid; ic < dc; ic += nt) {
                     const int ri = child_rel(rel, ic, vb);
                     const T v = Ucol[ic];
-                    if (rj < w) pan[int64_t(rj) * f + ri] += v;
+                    if (rj < w) pan[int64_t(rj) * ld + ri] += v;
                     else Us[int64_t(rj - w) * d + (ri - w)] += v;
                 }
             }

@@ -7,11 +7,14 @@
 // mask (only i >= j is touched, tiles strictly above the diagonal exit early).
 // One launch carries the tasks of every large front of a level.
 //
-// FP32 factors run on TF32 tensor cores (mma.sync m16n8k8, FP32 accumulate),
-// optionally as split 3xTF32 (a = a_hi + a_lo, three products) for FP32-level
-// accuracy. FP64 factors run on the FP64 tensor-core path (mma.sync m8n8k4 DMMA).
-// Tiles are staged through shared memory with cp.async (4/8-byte copies: the
-// panel leading dimension w+d carries no alignment guarantee), double buffered.
+// FP32 factors: single-pass TF32 runs on the 5th-generation tensor cores
+// (tcgen05, kernels_gemm_tc.cu); the split 3xTF32 form (a = a_hi + a_lo, three
+// products, FP32-level accuracy) and a legacy single-pass form run here on
+// mma.sync m16n8k8. FP64 factors run on the FP64 tensor-core path (mma.sync
+// m8n8k4 DMMA). Tiles are staged through shared memory with 4/8-byte cp.async,
+// double buffered. An FP32 task tile is 128 x 256 (the tcgen05 tile); the
+// mma.sync kernel covers it as two 128 x 128 halves and ignores the tcgen05
+// alignment shift (its extra tiles find no rows or columns).
 #include "device.h"
 
 #include <cstdint>
@@ -72,20 +75,11 @@ __device__ __forceinline__ int find_task(const GemmTask *tasks, int ntasks, int 
 // ---------------------------------------------------------------- TF32 ----
 constexpr int TBM = 128, TBN = 128, TBK = 32, TLD = TBM + 8;   // TLD % 32 == 8: conflict-free fragments
 constexpr int kTF32Smem = 2 * 2 * TBK * TLD * 4;
+constexpr int kTaskTileN32 = 256;                                // FP32 task tile width
 
 template <int SPLIT>
-__global__ void __launch_bounds__(256) gemm_tf32_kernel(const GemmTask *__restrict__ tasks, int ntasks,
-                                                        const float *__restrict__ Abase,
-                                                        const float *__restrict__ Bbase, float *__restrict__ Cbase) {
-    extern __shared__ __align__(16) float sm[];
-    float *As = sm;                           // [2][TBK][TLD]
-    float *Bs = sm + 2 * TBK * TLD;           // [2][TBK][TLD]
-    const int t = blockIdx.x;
-    const GemmTask tk = tasks[find_task(tasks, ntasks, t)];
-    const int local = t - tk.tile_base;
-    const int ti = local % tk.tiles_m, tj = local / tk.tiles_m;
-    const int i0 = ti * TBM, j0 = tj * TBN;
-    if (tk.lower && i0 + TBM - 1 < j0) return;
+__device__ __forceinline__ void tf32_tile(const GemmTask &tk, int i0, int j0, const float *Abase,
+                                          const float *__restrict__ Bbase, float *Cbase, float *As, float *Bs) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 1, wn = warp >> 1;        // 2 x 4 warps, warp tile 64 x 32
     const int gid = lane >> 2, tig = lane & 3;
@@ -185,13 +179,35 @@ __global__ void __launch_bounds__(256) gemm_tf32_kernel(const GemmTask *__restri
             }
 }
 
+template <int SPLIT>
+__global__ void __launch_bounds__(256) gemm_tf32_kernel(const GemmTask *__restrict__ tasks, int ntasks,
+                                                        const float *Abase, const float *__restrict__ Bbase,
+                                                        float *Cbase) {
+    extern __shared__ __align__(16) float sm[];
+    float *As = sm;                           // [2][TBK][TLD]
+    float *Bs = sm + 2 * TBK * TLD;           // [2][TBK][TLD]
+    const int t = blockIdx.x;
+    const GemmTask tk = tasks[find_task(tasks, ntasks, t)];
+    const int local = t - tk.tile_base;
+    const int ti = local % tk.tiles_m, tj = local / tk.tiles_m;
+    const int i0 = ti * TBM;
+    // The halves run in order; an in-place task (C == A, n <= 128) is finished
+    // by the first half before the second one (which has no columns) starts.
+    for (int h = 0; h < kTaskTileN32 / TBN; ++h) {
+        const int j0 = tj * kTaskTileN32 + h * TBN;
+        if (j0 >= tk.n || (tk.lower && i0 + TBM - 1 < j0)) break;
+        if (h) __syncthreads();
+        tf32_tile<SPLIT>(tk, i0, j0, Abase, Bbase, Cbase, As, Bs);
+    }
+}
+
 // ---------------------------------------------------------------- FP64 ----
 constexpr int DBM = 128, DBN = 64, DBK = 16, DLDA = DBM + 4, DLDB = DBN + 4;
 constexpr int kF64Smem = 2 * DBK * (DLDA + DLDB) * 8;
 
 __global__ void __launch_bounds__(256) gemm_f64_kernel(const GemmTask *__restrict__ tasks, int ntasks,
-                                                       const double *__restrict__ Abase,
-                                                       const double *__restrict__ Bbase, double *__restrict__ Cbase) {
+                                                       const double *Abase, const double *__restrict__ Bbase,
+                                                       double *Cbase) {
     extern __shared__ __align__(16) double smd[];
     double *As = smd;                          // [2][DBK][DLDA]
     double *Bs = smd + 2 * DBK * DLDA;         // [2][DBK][DLDB]
@@ -281,12 +297,16 @@ __global__ void __launch_bounds__(256) gemm_f64_kernel(const GemmTask *__restric
 }  // namespace
 
 int gemm_tile_m(bool fp64) { return fp64 ? DBM : TBM; }
-int gemm_tile_n(bool fp64) { return fp64 ? DBN : TBN; }
+int gemm_tile_n(bool fp64) { return fp64 ? DBN : kTaskTileN32; }
 
 template <>
 void launch_gemm<float>(const GemmTask *tasks, int ntasks, int ntiles, const float *A, const float *B, float *C,
-                        int split, cudaStream_t st) {
+                        int split, int *err, cudaStream_t st) {
     if (ntiles <= 0) return;
+    if (split == 1) {
+        launch_gemm_tc(tasks, ntasks, ntiles, A, B, C, err, st);
+        return;
+    }
     ++g_kernel_launches;
     if (split == 3) {
         static const bool ok3 = (cudaFuncSetAttribute(gemm_tf32_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTF32Smem), true);
@@ -301,8 +321,9 @@ void launch_gemm<float>(const GemmTask *tasks, int ntasks, int ntiles, const flo
 
 template <>
 void launch_gemm<double>(const GemmTask *tasks, int ntasks, int ntiles, const double *A, const double *B, double *C,
-                         int split, cudaStream_t st) {
+                         int split, int *err, cudaStream_t st) {
     (void)split;
+    (void)err;
     if (ntiles <= 0) return;
     ++g_kernel_launches;
     static const bool ok = (cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kF64Smem), true);

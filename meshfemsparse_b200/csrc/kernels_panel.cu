@@ -1,15 +1,13 @@
-// Large-front column block (K3 + K4 fused): factor the nb x nb diagonal block,
-// invert it, and solve the panel rows below with the inverse.
+// Large-front column block, first half of K3 + K4: factor the nb x nb
+// diagonal block of one column block and invert it.
 //
-// One launch per column block of all large fronts of a level; a task has
-// ceil(m / kPanelRows) CTAs, each owning up to kPanelRows rows of the panel
-// below the diagonal block. Every CTA factors the diagonal block itself
-// (identical results, no inter-CTA waiting) and then computes
-//     X := B L^{-T} = B inv(L)^T
-// for its rows. Tile 0 also stores the factored block to per-level scratch
-// (written back after the level: other CTAs may still be reading the
-// unfactored block in place) and the 64 x 64 diagonal inverses that the
-// triangular solves use.
+// One launch per column block of all large fronts of a level, one CTA per
+// front. The CTA factors the block in shared memory, writes L back in place,
+// stores the full inverse inv(L) (nb x nb, column-major, ld ldi) to scratch and
+// the 64 x 64 diagonal blocks of inv(L) after the panels for the triangular
+// solves. The rows below the block are then solved on the tensor cores as the
+// GEMM  X := X inv(L)^T  (launched by the host right after this kernel), so
+// the O(m nb^2) part of the TRSM runs at GEMM speed.
 //
 // The diagonal block is processed in 32-column sub-panels:
 //   warp 0 factors the 32 x 32 sub-block with each lane holding its row in
@@ -30,6 +28,17 @@ template <>
 __device__ __forceinline__ double psqrt<double>(double x) { return sqrt(x); }
 template <>
 __device__ __forceinline__ float psqrt<float>(float x) { return sqrtf(x); }
+
+// inv(L) feeding a single-pass TF32 tensor-core row solve is stored rounded to
+// TF32 (nearest); the tensor cores would truncate it.
+template <typename T>
+__device__ __forceinline__ T round_operand(T x) { return x; }
+template <>
+__device__ __forceinline__ float round_operand<float>(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
 
 // Same rule as the small-front kernel: report (plain) or perturb (refined FP32).
 template <typename T>
@@ -72,25 +81,17 @@ __device__ __forceinline__ void warp_potrf32(T *D, int LDD, int c0, int cw, int 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, 1) panel_kernel(const PanelTask *__restrict__ tasks, int ntasks,
-                                                       T *__restrict__ factor, T *__restrict__ diag_scratch,
-                                                       PivotCtl pv) {
+__global__ void __launch_bounds__(256, 1) panel_kernel(const PanelTask *__restrict__ tasks,
+                                                       T *__restrict__ factor, T *__restrict__ inv_scratch,
+                                                       PivotCtl pv, bool round_inv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int t = blockIdx.x;
-    int lo = 0, hi = ntasks - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (tasks[mid].tile_base <= t) lo = mid; else hi = mid - 1;
-    }
-    const PanelTask tk = tasks[lo];
-    const int tile = t - tk.tile_base;
+    const PanelTask tk = tasks[blockIdx.x];
     const int nb = tk.nb, ld = tk.ld;
     const int LDD = nb + 1;
     const int nblk = (nb + 31) / 32;
     T *D = reinterpret_cast<T *>(smem_raw);          // L, column-major, ld LDD
     T *Iv = D + nb * LDD;                            // inv(L), column-major, ld LDD
     T *Tm = Iv + nb * LDD;                           // 3 x [32][33] temporaries of the blocked inverse
-    T *X = Tm + 3 * 32 * 33;                         // panel rows, column-major, ld kPanelRows
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     T *blk = factor + tk.off;
     for (int q = tid; q < nb * nb; q += nt) {
@@ -98,17 +99,11 @@ __global__ void __launch_bounds__(256, 1) panel_kernel(const PanelTask *__restri
         D[j * LDD + i] = i >= j ? blk[int64_t(j) * ld + i] : T(0);
         Iv[j * LDD + i] = T(0);
     }
-    const int r0 = tile * kPanelRows;
-    const int rows = max(0, min(kPanelRows, tk.m - r0));
-    for (int q = tid; q < rows * nb; q += nt) {
-        const int j = q / rows, i = q - j * rows;
-        X[j * kPanelRows + i] = blk[int64_t(j) * ld + nb + r0 + i];
-    }
     __syncthreads();
     // ---- factor D
     for (int c0 = 0; c0 < nb; c0 += 32) {
         const int cw = min(32, nb - c0);
-        if (warp == 0) warp_potrf32(D, LDD, c0, cw, lane, tk.col + c0, pv, tile == 0);
+        if (warp == 0) warp_potrf32(D, LDD, c0, cw, lane, tk.col + c0, pv, true);
         __syncthreads();
         for (int row = c0 + cw + tid; row < nb; row += nt) {
             T x[32];
@@ -190,44 +185,23 @@ __global__ void __launch_bounds__(256, 1) panel_kernel(const PanelTask *__restri
         }
         __syncthreads();
     }
-    if (tile == 0) {
-        T *out = diag_scratch + tk.diag_out;
-        for (int q = tid; q < nb * nb; q += nt) {
-            const int j = q / nb, i = q - j * nb;
-            out[q] = D[j * LDD + i];
-        }
-        if (tk.inv_out >= 0) {
-            // 64 x 64 diagonal blocks of inv(L) (the inverses of L's 64 x 64 diagonal blocks)
-            const int nb64 = (nb + 63) / 64;
-            T *inv = factor + tk.inv_out;
-            for (int q = tid; q < nb64 * 4096; q += nt) {
-                const int b = q >> 12, e = q & 4095;
-                const int j = e >> 6, i = e & 63;
-                const int gi = b * 64 + i, gj = b * 64 + j;
-                inv[q] = (gi < nb && gj < nb && gi >= gj) ? Iv[gj * LDD + gi] : T(0);
-            }
-        }
+    for (int q = tid; q < nb * nb; q += nt) {
+        const int j = q / nb, i = q - j * nb;
+        if (i >= j) blk[int64_t(j) * ld + i] = D[j * LDD + i];
+        T v = i >= j ? Iv[j * LDD + i] : T(0);
+        if (round_inv) v = round_operand(v);
+        inv_scratch[tk.inv_full + int64_t(j) * tk.ldi + i] = v;
     }
-    if (rows == 0) return;
-    // ---- X := X inv(L)^T, written straight back (X in shared memory is only read)
-    for (int q = tid; q < rows * nb; q += nt) {
-        const int j = q / rows, i = q - j * rows;
-        T a = T(0);
-#pragma unroll 4
-        for (int k = 0; k <= j; ++k) a += X[k * kPanelRows + i] * Iv[k * LDD + j];
-        blk[int64_t(j) * ld + nb + r0 + i] = a;
-    }
-}
-
-template <typename T>
-__global__ void diag_writeback_kernel(const PanelTask *__restrict__ tasks, const T *__restrict__ scratch,
-                                      T *__restrict__ factor) {
-    const PanelTask tk = tasks[blockIdx.x];
-    const T *src = scratch + tk.diag_out;
-    T *blk = factor + tk.off;
-    for (int q = threadIdx.x; q < tk.nb * tk.nb; q += blockDim.x) {
-        const int j = q / tk.nb, i = q - j * tk.nb;
-        if (i >= j) blk[int64_t(j) * tk.ld + i] = src[q];
+    if (tk.inv_out >= 0) {
+        // 64 x 64 diagonal blocks of inv(L) (the inverses of L's 64 x 64 diagonal blocks)
+        const int nb64 = (nb + 63) / 64;
+        T *inv = factor + tk.inv_out;
+        for (int q = tid; q < nb64 * 4096; q += nt) {
+            const int b = q >> 12, e = q & 4095;
+            const int j = e >> 6, i = e & 63;
+            const int gi = b * 64 + i, gj = b * 64 + j;
+            inv[q] = (gi < nb && gj < nb && gi >= gj) ? Iv[gj * LDD + gi] : T(0);
+        }
     }
 }
 
@@ -235,31 +209,22 @@ __global__ void diag_writeback_kernel(const PanelTask *__restrict__ tasks, const
 
 size_t panel_smem_bytes(int nb, bool fp64) {
     const size_t el = fp64 ? 8 : 4;
-    return (size_t(2) * nb * (nb + 1) + 3 * 32 * 33 + size_t(kPanelRows) * nb) * el;
+    return (size_t(2) * nb * (nb + 1) + 3 * 32 * 33) * el;
 }
 
 template <typename T>
-void launch_panel(const PanelTask *tasks, int ntasks, int ntiles, int max_nb, T *factor, T *diag_scratch,
-                  PivotCtl pv, cudaStream_t st) {
-    if (ntiles <= 0) return;
+void launch_panel(const PanelTask *tasks, int ntasks, int max_nb, T *factor, T *inv_scratch, PivotCtl pv,
+                  bool round_inv, cudaStream_t st) {
+    if (ntasks <= 0) return;
     const size_t smem = panel_smem_bytes(max_nb, sizeof(T) == 8);
     static const bool smem_ok =
         (cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin), true);
     (void)smem_ok;
     ++g_kernel_launches;
-    panel_kernel<T><<<ntiles, 256, smem, st>>>(tasks, ntasks, factor, diag_scratch, pv);
+    panel_kernel<T><<<ntasks, 256, smem, st>>>(tasks, factor, inv_scratch, pv, round_inv);
 }
 
-template <typename T>
-void launch_diag_writeback(const PanelTask *tasks, int ntasks, const T *diag_scratch, T *factor, cudaStream_t st) {
-    if (ntasks <= 0) return;
-    ++g_kernel_launches;
-    diag_writeback_kernel<T><<<ntasks, 256, 0, st>>>(tasks, diag_scratch, factor);
-}
-
-template void launch_panel<float>(const PanelTask *, int, int, int, float *, float *, PivotCtl, cudaStream_t);
-template void launch_panel<double>(const PanelTask *, int, int, int, double *, double *, PivotCtl, cudaStream_t);
-template void launch_diag_writeback<float>(const PanelTask *, int, const float *, float *, cudaStream_t);
-template void launch_diag_writeback<double>(const PanelTask *, int, const double *, double *, cudaStream_t);
+template void launch_panel<float>(const PanelTask *, int, int, float *, float *, PivotCtl, bool, cudaStream_t);
+template void launch_panel<double>(const PanelTask *, int, int, double *, double *, PivotCtl, bool, cudaStream_t);
 
 }  // namespace mfs

@@ -144,7 +144,7 @@ __host__ __device__ inline size_t diag_smem(int nrhs) {
 // Diagonal block of the task into dblk (row-major, ld kRB + 1): the stored
 // inverse of L(r, r) when the front has one, else the lower triangle of L(r, r).
 template <typename T>
-__device__ __forceinline__ bool load_diag_block(T *dblk, const T *factor, const T *pan, int64_t inv, int f, int r0,
+__device__ __forceinline__ bool load_diag_block(T *dblk, const T *factor, const T *pan, int64_t inv, int ld, int r0,
                                                 int nr, int blk) {
     const int tid = threadIdx.x;
     if (inv >= 0) {
@@ -157,7 +157,7 @@ __device__ __forceinline__ bool load_diag_block(T *dblk, const T *factor, const 
     }
     for (int q = tid; q < nr * nr; q += kTriThreads) {
         const int j = q / nr, i = q % nr;
-        dblk[i * (kRB + 1) + j] = i >= j ? pan[int64_t(r0 + j) * f + r0 + i] : T(0);
+        dblk[i * (kRB + 1) + j] = i >= j ? pan[int64_t(r0 + j) * ld + r0 + i] : T(0);
     }
     return false;
 }
@@ -176,12 +176,12 @@ __global__ void __launch_bounds__(kTriThreads) fwd_diag_kernel(const SolveTask *
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SolveTask tk = tasks[t];
         const int s = tk.sn;
-        const int w = sd.w[s], f = w + sd.d[s];
+        const int w = sd.w[s], ld = sd.ld[s];
         const int c0 = sd.col0[s];
         const int r0 = tk.blk * kRB, nr = min(kRB, w - r0);
         const T *pan = factor + sd.pan_off[s];
         // everything that does not depend on earlier blocks is loaded before the first wait
-        const bool has_inv = load_diag_block(dblk, factor, pan, sd.inv_off[s], f, r0, nr, tk.blk);
+        const bool has_inv = load_diag_block(dblk, factor, pan, sd.inv_off[s], ld, r0, nr, tk.blk);
         for (int q = tid; q < nr * nrhs; q += kTriThreads) {
             const int i = q / nrhs, r = q % nrhs;
             acc[q] = X[c0 + r0 + i + r * ldx];
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kTriThreads) fwd_diag_kernel(const SolveTask *
             __syncthreads();
             for (int q = tid; q < nr * kRB; q += kTriThreads) {
                 const int j = q / nr, i = q % nr;
-                tile[i * (kRB + 1) + j] = pan[int64_t(k0 + j) * f + r0 + i];
+                tile[i * (kRB + 1) + j] = pan[int64_t(k0 + j) * ld + r0 + i];
             }
             wait_flag(flags + tk.flag_base + k, 1, err);
             for (int q = tid; q < kRB * nrhs; q += kTriThreads) {
@@ -265,12 +265,12 @@ __global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SolveTask tk = tasks[t];
         const int s = tk.sn;
-        const int w = sd.w[s], f = w + sd.d[s];
+        const int w = sd.w[s], ld = sd.ld[s];
         const int c0 = sd.col0[s];
         const int nbw = (w + kRB - 1) / kRB;
         const int r0 = tk.blk * kRB, nr = min(kRB, w - r0);
         const T *pan = factor + sd.pan_off[s];
-        const bool has_inv = load_diag_block(dblk, factor, pan, sd.inv_off[s], f, r0, nr, tk.blk);
+        const bool has_inv = load_diag_block(dblk, factor, pan, sd.inv_off[s], ld, r0, nr, tk.blk);
         for (int q = tid; q < nr * nrhs; q += kTriThreads) {
             const int j = q / nrhs, r = q % nrhs;
             acc[q] = X[c0 + r0 + j + r * ldx];
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *
             __syncthreads();
             for (int q = tid; q < ni * nr; q += kTriThreads) {
                 const int j = q / ni, i = q % ni;
-                tile[i * (kRB + 1) + j] = pan[int64_t(r0 + j) * f + i0 + i];
+                tile[i * (kRB + 1) + j] = pan[int64_t(r0 + j) * ld + i0 + i];
             }
             wait_flag(flags + tk.flag_base + k, 2, err);
             for (int q = tid; q < ni * nrhs; q += kTriThreads) {
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restr
     double *tile = vec + kRB * nrhs;           // [kRB][kRB + 1]
     const StrTask tk = tasks[blockIdx.x];
     const int s = tk.sn;
-    const int w = sd.w[s], d = sd.d[s], f = w + d;
+    const int w = sd.w[s], d = sd.d[s], ld = sd.ld[s];
     const int c0 = sd.col0[s];
     const int vb = sd.vb;
     const T *pan = factor + sd.pan_off[s];
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restr
             // tile[i][j] = L(w + a0 + i, b0 + j), vec[j] = y(b0 + j)
             for (int q = tid; q < na * nbk; q += nt) {
                 const int j = q / na, i = q % na;
-                tile[i * (kRB + 1) + j] = double(pan[int64_t(b0 + j) * f + w + a0 + i]);
+                tile[i * (kRB + 1) + j] = double(pan[int64_t(b0 + j) * ld + w + a0 + i]);
             }
             for (int q = tid; q < nbk * nrhs; q += nt) {
                 const int j = q / nrhs, r = q % nrhs;
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restr
             // tile[i][j] = L(w + b0 + i, a0 + j), vec[i] = x(struct row b0 + i)
             for (int q = tid; q < nbk * na; q += nt) {
                 const int j = q / nbk, i = q % nbk;
-                tile[i * (kRB + 1) + j] = double(pan[int64_t(a0 + j) * f + w + b0 + i]);
+                tile[i * (kRB + 1) + j] = double(pan[int64_t(a0 + j) * ld + w + b0 + i]);
             }
             for (int q = tid; q < nbk * nrhs; q += nt) {
                 const int i = q / nrhs, r = q % nrhs;

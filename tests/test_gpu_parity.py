@@ -55,9 +55,10 @@ def test_factor_panels_cube(k, small):
 
 
 @pytest.mark.parametrize("small", [0, 16])
-@pytest.mark.parametrize("tc,tol", [(2, 1e-4), (1, 3e-2)])
+@pytest.mark.parametrize("tc,tol", [(2, 1e-4), (1, 3e-2), (3, 3e-2)])
 def test_factor_panels_single_precision(small, tc, tol):
-    """FP32 factor: split 3xTF32 Schur updates keep FP32-level error; single-pass TF32 is looser."""
+    """FP32 factor: split 3xTF32 Schur updates keep FP32-level error; single-pass TF32
+    (tcgen05: tc=1, mma.sync: tc=3) is looser."""
     H, tets, Ke, pins, nodes = cube_problem(5)
     f, sn, ref, got = gpu_and_oracle(H, pins, single=True, small_front_max=small, tensor_cores=tc)
     assert rel_err(got, ref) <= tol
