@@ -137,6 +137,19 @@ mfs_status mfs_assemble(mfs_handle *h, const double *Ke, double *Ax_out, int32_t
  * variables; BlockCSCHessian.hh:723-732). flags: MFS_SOLVE_FULL / REDUCED / REDUCED_PERMUTED
  * select the vector layout as for mfs_solve; pinned rows of a full y are 0. */
 mfs_status mfs_apply(mfs_handle *h, const double *x, double *y, int64_t nrhs, int64_t ld, int32_t flags);
+/* No counterpart in the reference. mfs_apply for callers that cannot allocate
+ * device memory at the point where they apply H: a process whose caching
+ * allocator has already reserved the device, or a loop where the device-wide
+ * synchronisation of cudaMalloc / cudaFree is not acceptable. x and y must be
+ * device pointers (flags must include MFS_DEVICE_POINTERS); the vector layouts
+ * are those of mfs_apply. Temporaries live in one fixed device array of
+ * 2 x 2^20 doubles (16 MiB, on every GPU that loads the library, until exit),
+ * so (free variables) x nrhs may not exceed 1048576 (MFS_SIZE_MISMATCH
+ * otherwise). The first call on a device looks up that array's address; make
+ * it before any stream capture. All calls on a device share the array: calls
+ * that overlap on the GPU (other handles, other streams) race and must be
+ * serialised by the caller. Returns after the result is written. */
+mfs_status mfs_apply_noalloc(mfs_handle *h, const double *x, double *y, int64_t nrhs, int64_t ld, int32_t flags);
 /* Conversion-plan entries are exported as 4 int64 each: (dst, src, ld, flags);
  * flags bit0 = source block transposed, bit1 = diagonal block (lower part only). */
 

@@ -25,7 +25,7 @@ EXPORTED = [
     "mfs_numeric", "mfs_solve", "mfs_assembly_setup", "mfs_assemble", "mfs_apply", "mfs_info",
     "mfs_inverse_permutation", "mfs_nd_ordering", "mfs_supernodes", "mfs_conversion_plan", "mfs_factor_values",
     "mfs_stash", "mfs_swap_stash", "mfs_clear_stash", "mfs_has_stash", "mfs_clear_factors", "mfs_get_stats",
-    "mfs_set_options",
+    "mfs_set_options", "mfs_apply_noalloc",
 ]
 
 
@@ -73,6 +73,7 @@ def load() -> C.CDLL:
     lib.mfs_assembly_setup.argtypes = [P, C.c_int64, i64p]
     lib.mfs_assemble.argtypes = [P, P, P, C.c_int32]
     lib.mfs_apply.argtypes = [P, P, P, C.c_int64, C.c_int64, C.c_int32]
+    lib.mfs_apply_noalloc.argtypes = [P, P, P, C.c_int64, C.c_int64, C.c_int32]
     lib.mfs_info.argtypes = [P, i64p, i64p, i64p, C.POINTER(C.c_double), i64p, C.POINTER(C.c_int32)]
     lib.mfs_inverse_permutation.argtypes = [P, i64p]
     lib.mfs_nd_ordering.argtypes = [P, i64p, i64p, i64p, i64p]

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <type_traits>
 #include <stdexcept>
 #include <string>
@@ -749,6 +750,32 @@ const double *stage_input(mfs_handle *h, DBuf<double> &buf, const double *src, s
 
 }  // namespace
 
+// Scratch of mfs_apply_noalloc: the permuted reduced copies of x and of y,
+// kNoAllocApplyEntries doubles each (16 MiB on every GPU that loads this
+// library, held until the process exits). In host code the name only stands in
+// for the array; its device address comes from cudaGetSymbolAddress.
+constexpr int64_t kNoAllocApplyEntries = int64_t(1) << 20;
+static __device__ __align__(256) double g_noalloc_apply_scratch[2 * kNoAllocApplyEntries];
+
+namespace {
+
+// Device address of the scratch on device `dev` (which must be current),
+// looked up on the first call for that device and cached.
+double *noalloc_apply_scratch(int dev) {
+    static std::mutex mu;
+    static double *addr[256] = {};
+    if (dev < 0 || dev >= 256) throw StatusError(MFS_INVALID_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        MFS_CUDA(cudaGetSymbolAddress(&p, g_noalloc_apply_scratch));
+        addr[dev] = static_cast<double *>(p);
+    }
+    return addr[dev];
+}
+
+}  // namespace
+
 extern "C" {
 
 mfs_status mfs_default_options(mfs_options *opt) {
@@ -1327,6 +1354,43 @@ mfs_status mfs_clear_factors(mfs_handle *h) {
     h->nslots = 0;
     h->nelem = 0;
     return MFS_OK;
+}
+
+// y = H x like mfs_apply, with device vectors only and every temporary in the
+// fixed array above: nothing is allocated, on the device or pinned, during the
+// call. Every entry of the scratch that is read was written earlier in the same
+// call (gather, then the SpMV overwrites y), so nothing needs clearing between
+// calls.
+mfs_status mfs_apply_noalloc(mfs_handle *h, const double *x, double *y, int64_t nrhs, int64_t ld, int32_t flags) {
+    if (!h) return MFS_INVALID_ARG;
+    return guarded(h, [&] {
+        require_symbolic(h);
+        const double *vals = h->cur.ax ? h->cur.ax->p : (h->asm_ax ? h->asm_ax->p : nullptr);
+        if (!vals) throw StatusError(MFS_NO_FACTOR, "no matrix values on the device");
+        if (!(flags & MFS_DEVICE_POINTERS))
+            throw StatusError(MFS_INVALID_ARG, "mfs_apply_noalloc takes device vectors only (MFS_DEVICE_POINTERS)");
+        if (!x || !y) throw StatusError(MFS_INVALID_ARG, "null vector");
+        set_device(h);
+        DevSym &ds = *h->cur.sym;
+        const Symbolic &S = *ds.S;
+        const int mode = flags & 3;
+        const int64_t rows = mode == MFS_SOLVE_FULL ? S.n_full : S.n;
+        if (ld < rows || nrhs < 1) throw StatusError(MFS_SIZE_MISMATCH, "Incorrect vector size");
+        if (int64_t(S.n) * nrhs > kNoAllocApplyEntries)
+            throw StatusError(MFS_SIZE_MISMATCH,
+                              "mfs_apply_noalloc: free variables x right-hand sides = " +
+                                  std::to_string(int64_t(S.n) * nrhs) + " exceeds its fixed scratch of " +
+                                  std::to_string(kNoAllocApplyEntries) + " entries");
+        double *xs = noalloc_apply_scratch(h->opt.device);
+        double *ys = xs + kNoAllocApplyEntries;
+        cudaStream_t st = h->stream;
+        const int64_t *map = mode == MFS_SOLVE_FULL ? ds.prrfr.p : (mode == MFS_SOLVE_REDUCED ? ds.sperm.p : nullptr);
+        launch_gather_rows(map, rows, x, ld, xs, S.n, int(nrhs), st);
+        apply_current(h, vals, nullptr, 0.0, xs, ys, int(nrhs));
+        launch_scatter_rows(map, rows, ys, S.n, y, ld, int(nrhs), st);
+        MFS_LAUNCHED();
+        MFS_CUDA(cudaStreamSynchronize(st));
+    });
 }
 
 mfs_status mfs_get_stats(const mfs_handle *h, mfs_stats *st) {
