@@ -9,25 +9,36 @@
 // GEMM  X := X inv(L)^T  (launched by the host right after this kernel), so
 // the O(m nb^2) part of the TRSM runs at GEMM speed.
 //
-// The diagonal block is processed in 32-column sub-panels:
-//   warp 0 factors the 32 x 32 sub-block with each lane holding its row in
-//   registers (column broadcast by warp shuffles), the rows below are solved one
-//   thread per row with the row in registers, and the trailing part of the block
-//   gets the rank-32 update. The inverse is built blockwise: 32 x 32 diagonal
-//   inverses (one warp each, lane = column), then off-diagonal blocks
-//   inv(L)_IJ = -inv(L_II) sum_{K=J}^{I-1} L_IK inv(L)_KJ by block distance.
+// The block (padded to a multiple of 32 with an identity tail) is processed in
+// 32 x 32 tiles I = 0 .. nblk-1, right-looking, two barriers per tile column:
+//   phase A  one warp per tile: the tiles below, L_RI = A_RI inv(L_II)^T, and the
+//            inverse tiles inv(L)_IJ = -inv(L_II) sum_K P_IJK (J < I).
+//   phase B  warp 0 updates tile (I+1, I+1) and at once factors it left-looking
+//            (lane = row, reciprocal square root per pivot) and inverts it
+//            (lane = column); warps 1-7 meanwhile run the other trailing updates
+//            A_RC -= L_RI L_CI^T (R >= C > I) and the products
+//            P_{I+1,J,K} = L_{I+1,K} inv(L)_KJ (J <= K <= I) that the next
+//            off-diagonal inverse tiles need (they only read final tiles).
+// Every tile product runs as a warp-level register-tiled 32 x 32 x 32 GEMM
+// (each lane owns a 4 x 8 patch), so the chain of dependent work per tile is
+// the 32 pivots of its diagonal factorization and three 32-deep products.
+// The code is kept compact (rolled loops, one product routine): the work per
+// CTA is small, and fully unrolled variants spent most of their time refetching
+// instructions.
 #include "device.h"
 
 namespace mfs {
 
 namespace {
 
+constexpr int kPanelThreads = 256;
+
 template <typename T>
-__device__ __forceinline__ T psqrt(T x);
+__device__ __forceinline__ T recip_sqrt(T x);
 template <>
-__device__ __forceinline__ double psqrt<double>(double x) { return sqrt(x); }
+__device__ __forceinline__ double recip_sqrt<double>(double x) { return 1.0 / sqrt(x); }
 template <>
-__device__ __forceinline__ float psqrt<float>(float x) { return sqrtf(x); }
+__device__ __forceinline__ float recip_sqrt<float>(float x) { return rsqrtf(x); }
 
 // inv(L) feeding a single-pass TF32 tensor-core row solve is stored rounded to
 // TF32 (nearest); the tensor cores would truncate it.
@@ -41,150 +52,211 @@ __device__ __forceinline__ float round_operand<float>(float x) {
 }
 
 // Same rule as the small-front kernel: report (plain) or perturb (refined FP32).
+// Kept out of line: it is rare, and inlined into the unrolled pivot loop it
+// stops that loop from being unrolled.
 template <typename T>
-__device__ __forceinline__ T panel_bad_pivot(T a, int col, const PivotCtl &pv, bool record) {
+__device__ __noinline__ T panel_bad_pivot(T a, int col, PivotCtl pv) {
+    if (col < 0) return T(1);
     if (pv.dorig) {
         const T floor_v = T(1e-3 * fabs(pv.dorig[col]));
         const T m = fabs(a);
-        if (record) atomicAdd(pv.perturbed, 1);
+        atomicAdd(pv.perturbed, 1);
         return (m > floor_v) ? m : (floor_v > T(0) ? floor_v : T(1));
     }
-    if (record) atomicMin(pv.fail_col, col);
+    atomicMin(pv.fail_col, col);
     return T(1);
 }
 
-// Cholesky of the cw x cw sub-block at (c0, c0) of D (ld LDD) by one warp.
+// Warp-level tile product: c[r][q] += sum_{k < 32} A(4 rq + r, k) * B(8 cq + q, k)
+// with rq = lane % 8, cq = lane / 8; A(i, k) = A0[k * lda + i], B(j, k) = B0[j * sj + k * sk].
 template <typename T>
-__device__ __forceinline__ void warp_potrf32(T *D, int LDD, int c0, int cw, int lane, int col_base,
-                                             const PivotCtl &pv, bool record) {
-    T r[32];
-#pragma unroll
-    for (int j = 0; j < 32; ++j) r[j] = (j < cw && lane < cw && j <= lane) ? D[(c0 + j) * LDD + c0 + lane] : T(0);
-#pragma unroll
+__device__ __forceinline__ void tile_mma(T (&c)[4][8], const T *A0, int lda, const T *B0, int sj, int sk,
+                                         int lane) {
+    const int rq = lane & 7, cq = lane >> 3;
+    const T *a = A0 + 4 * rq;
+    const T *b = B0 + 8 * cq * sj;
+#pragma unroll 1
     for (int k = 0; k < 32; ++k) {
-        if (k < cw) {
-            T piv = __shfl_sync(0xffffffffu, r[k], k);
-            if (!(piv > T(0))) piv = panel_bad_pivot(piv, col_base + k, pv, record && lane == 0);
-            const T lkk = psqrt(piv);
-            const T lik = (lane == k) ? lkk : r[k] / lkk;
-            if (lane >= k) r[k] = lik;
+        T av[4], bv[8];
 #pragma unroll
-            for (int j = k + 1; j < 32; ++j) {
-                const T ljk = __shfl_sync(0xffffffffu, lik, j);
-                if (lane >= j && j < cw) r[j] -= lik * ljk;
-            }
-        }
+        for (int r = 0; r < 4; ++r) av[r] = a[k * lda + r];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) bv[q] = b[q * sj + k * sk];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) c[r][q] += av[r] * bv[q];
     }
-#pragma unroll
-    for (int j = 0; j < 32; ++j)
-        if (j < cw && lane < cw && j <= lane) D[(c0 + j) * LDD + c0 + lane] = r[j];
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, 1) panel_kernel(const PanelTask *__restrict__ tasks,
-                                                       T *__restrict__ factor, T *__restrict__ inv_scratch,
-                                                       PivotCtl pv, bool round_inv) {
+__device__ __forceinline__ void tile_zero(T (&c)[4][8]) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) c[r][q] = T(0);
+}
+
+// Store a lane's 4 x 8 patch into a column-major tile (element (i, j) at M[j * ldm + i]),
+// scaled by s (and added to the old value when add is set).
+template <typename T>
+__device__ __forceinline__ void tile_store(T *M, int ldm, const T (&c)[4][8], T s, bool add, int lane) {
+    const int rq = lane & 7, cq = lane >> 3;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            T *p = M + (8 * cq + q) * ldm + 4 * rq + r;
+            *p = add ? *p + s * c[r][q] : s * c[r][q];
+        }
+}
+
+// Cholesky of the 32 x 32 tile at (c0, c0) of D by one warp, then its inverse.
+// Both keep a 32-entry vector per lane in registers and rotate it by one entry
+// per step, so the current column (row) is always entry 0: the step loop stays
+// rolled (compact code) while every register index is static.
+//   factor : lane = row i, r[j] = A(i, k + j); pivot from lane k by shuffle,
+//            reciprocal square root, rank-1 update with L(k + j, k) from lane k + j;
+//   inverse: lane = column c, y[i] = Y(k + i, c); y_k = y[0] / L(k, k), then
+//            y[i] -= L(k + i, k) y_k (L read from shared memory, broadcast).
+template <typename T>
+__device__ __noinline__ void warp_diag_tile(T *D, T *Iv, T *rdiag, int LDD, int c0, int nb, int lane, int col_base,
+                                            int *fail_col, int *perturbed, const double *dorig) {
+    const PivotCtl pv{fail_col, perturbed, dorig};
+    T *Dt = D + c0 * LDD + c0;                       // tile element (i, j) at Dt[j * LDD + i]
+    T r[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) r[j] = (j <= lane) ? Dt[j * LDD + lane] : T(0);
+#pragma unroll 1
+    for (int k = 0; k < 32; ++k) {
+        T piv = __shfl_sync(0xffffffffu, r[0], k);
+        if (!(piv > T(0))) piv = panel_bad_pivot(piv, c0 + k < nb ? col_base + c0 + k : -1, pv);
+        const T rs = recip_sqrt(piv);
+        const T lik = (lane == k) ? piv * rs : r[0] * rs;
+        if (lane >= k) Dt[k * LDD + lane] = lik;
+        if (lane == k) rdiag[c0 + k] = rs;
+#pragma unroll
+        for (int j = 1; j < 32; ++j) r[j] -= lik * __shfl_sync(0xffffffffu, lik, (k + j) & 31);
+#pragma unroll
+        for (int j = 0; j < 31; ++j) r[j] = r[j + 1];
+    }
+    __syncwarp();
+    T *It = Iv + c0 * LDD + c0;
+    T y[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) y[i] = (i == lane) ? T(1) : T(0);
+#pragma unroll 1
+    for (int k = 0; k < 32; ++k) {
+        const T yk = y[0] * rdiag[c0 + k];
+        if (k >= lane) It[lane * LDD + k] = yk;
+        const T *lk = Dt + k * LDD;                  // column k of L
+#pragma unroll
+        for (int i = 1; i < 32; ++i) y[i] -= lk[(k + i) & 31] * yk;
+#pragma unroll
+        for (int i = 0; i < 31; ++i) y[i] = y[i + 1];
+    }
+    __syncwarp();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask *__restrict__ tasks,
+                                                                 T *__restrict__ factor, T *__restrict__ inv_scratch,
+                                                                 PivotCtl pv, bool round_inv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const PanelTask tk = tasks[blockIdx.x];
     const int nb = tk.nb, ld = tk.ld;
-    const int LDD = nb + 1;
-    const int nblk = (nb + 31) / 32;
-    T *D = reinterpret_cast<T *>(smem_raw);          // L, column-major, ld LDD
-    T *Iv = D + nb * LDD;                            // inv(L), column-major, ld LDD
-    T *Tm = Iv + nb * LDD;                           // 3 x [32][33] temporaries of the blocked inverse
+    const int nblk = (nb + 31) / 32, NBP = nblk * 32;
+    const int LDD = NBP + 1;
+    T *D = reinterpret_cast<T *>(smem_raw);          // L, column-major, ld LDD (identity-padded)
+    T *Iv = D + NBP * LDD;                           // inv(L), column-major, ld LDD
+    T *P = Iv + NBP * LDD;                           // 6 x [32][33] partial products
+    T *rdiag = P + 6 * 32 * 33;                      // reciprocal diagonal of L
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     T *blk = factor + tk.off;
-    for (int q = tid; q < nb * nb; q += nt) {
-        const int j = q / nb, i = q - j * nb;
-        D[j * LDD + i] = i >= j ? blk[int64_t(j) * ld + i] : T(0);
+    // unrolled so that many global loads are in flight per thread
+#pragma unroll 8
+    for (int q = tid; q < NBP * NBP; q += nt) {
+        const int j = q / NBP, i = q - j * NBP;
+        T v = T(0);
+        if (i < nb && j < nb) v = i >= j ? blk[int64_t(j) * ld + i] : T(0);
+        else if (i == j) v = T(1);
+        D[j * LDD + i] = v;
         Iv[j * LDD + i] = T(0);
     }
     __syncthreads();
-    // ---- factor D
-    for (int c0 = 0; c0 < nb; c0 += 32) {
-        const int cw = min(32, nb - c0);
-        if (warp == 0) warp_potrf32(D, LDD, c0, cw, lane, tk.col + c0, pv, true);
-        __syncthreads();
-        for (int row = c0 + cw + tid; row < nb; row += nt) {
-            T x[32];
-#pragma unroll
-            for (int j = 0; j < 32; ++j) x[j] = j < cw ? D[(c0 + j) * LDD + row] : T(0);
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                if (j < cw) {
-                    T a = x[j];
-#pragma unroll
-                    for (int k = 0; k < j; ++k) a -= x[k] * D[(c0 + k) * LDD + c0 + j];
-                    x[j] = a / D[(c0 + j) * LDD + c0 + j];
+    if (warp == 0) warp_diag_tile(D, Iv, rdiag, LDD, 0, nb, lane, tk.col, pv.fail_col, pv.perturbed, pv.dorig);
+    __syncthreads();
+    for (int I = 0; I < nblk; ++I) {
+        const int c0 = 32 * I;
+        // ---- phase A: tiles below (L_RI) and off-diagonal inverse tiles (inv(L)_IJ)
+        {
+            const int nbelow = nblk - 1 - I;
+            for (int u = warp; u < nbelow + I; u += 8) {
+                T c[4][8];
+                tile_zero(c);
+                if (u < nbelow) {
+                    const int R = I + 1 + u;
+                    // B(j, k) = inv(L_II)(j, k)
+                    tile_mma(c, D + c0 * LDD + 32 * R, LDD, Iv + c0 * LDD + c0, 1, LDD, lane);
+                    __syncwarp();
+                    tile_store(D + c0 * LDD + 32 * R, LDD, c, T(1), false, lane);
+                } else {
+                    const int J = u - nbelow;
+                    // T_IJ = sum_{K=J}^{I-1} P_IJK, gathered into the K = J slot; B(j, t) = T_IJ(t, j)
+                    T *Pj = P + (J * (J + 1) / 2 + J) * 32 * 33;
+                    for (int K = J + 1; K < I; ++K) {
+                        const T *Pk = P + (K * (K + 1) / 2 + J) * 32 * 33;
+                        for (int e = lane; e < 32 * 33; e += 32) Pj[e] += Pk[e];
+                    }
+                    __syncwarp();
+                    tile_mma(c, Iv + c0 * LDD + c0, LDD, Pj, 33, 1, lane);
+                    tile_store(Iv + (32 * J) * LDD + c0, LDD, c, T(-1), false, lane);
                 }
             }
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-                if (j < cw) D[(c0 + j) * LDD + row] = x[j];
         }
         __syncthreads();
-        const int mm = nb - c0 - cw;
-        for (int q = tid; q < mm * mm; q += nt) {
-            const int jj = q / mm, ii = q - jj * mm;
-            if (ii < jj) continue;
-            const int i = c0 + cw + ii, j = c0 + cw + jj;
-            T a = T(0);
-#pragma unroll 8
-            for (int k = 0; k < cw; ++k) a += D[(c0 + k) * LDD + i] * D[(c0 + k) * LDD + j];
-            D[j * LDD + i] -= a;
-        }
-        __syncthreads();
-    }
-    // ---- inv(L): diagonal 32 x 32 blocks, one warp each, lane = column
-    if (warp < nblk) {
-        const int b0 = warp * 32, bw = min(32, nb - b0);
-        T y[32];
-#pragma unroll
-        for (int i = 0; i < 32; ++i) {
-            if (i < bw) {
-                T a = (i == lane) ? T(1) : T(0);
-#pragma unroll
-                for (int k = 0; k < i; ++k) a -= D[(b0 + k) * LDD + b0 + i] * y[k];
-                y[i] = (i >= lane) ? a / D[(b0 + i) * LDD + b0 + i] : T(0);
+        if (I + 1 == nblk) break;
+        // ---- phase B: trailing updates of tile column I; tile I+1 factored and inverted
+        //      as soon as its update is in; products for the next inverse tiles
+        {
+            const int m = nblk - 1 - I;                          // trailing tile rows / columns
+            const int ntrail = m * (m + 1) / 2;                  // u = 0 is tile (I+1, I+1)
+            const int nterm = (I + 1) * (I + 2) / 2;             // P_{I+1,J,K}, J <= K <= I
+            if (warp == 0) {
+                T c[4][8];
+                tile_zero(c);
+                const int R = I + 1;
+                tile_mma(c, D + c0 * LDD + 32 * R, LDD, D + c0 * LDD + 32 * R, 1, LDD, lane);
+                tile_store(D + (32 * R) * LDD + 32 * R, LDD, c, T(-1), true, lane);
+                __syncwarp();
+                warp_diag_tile(D, Iv, rdiag, LDD, 32 * R, nb, lane, tk.col, pv.fail_col, pv.perturbed, pv.dorig);
             } else {
-                y[i] = T(0);
-            }
-        }
-        if (lane < bw)
-#pragma unroll
-            for (int i = 0; i < 32; ++i)
-                if (i < bw && i >= lane) Iv[(b0 + lane) * LDD + b0 + i] = y[i];
-    }
-    __syncthreads();
-    // ---- off-diagonal blocks by distance
-    for (int dist = 1; dist < nblk; ++dist) {
-        const int nbl = nblk - dist;                 // blocks (I, J = I - dist), I = dist .. nblk-1
-        // Tm[J] = sum_{K=J}^{I-1} L_IK inv(L)_KJ
-        for (int q = tid; q < nbl * 1024; q += nt) {
-            const int bq = q >> 10, e = q & 1023;
-            const int j = e >> 5, i = e & 31;
-            const int J = bq, I = bq + dist;
-            const int gi = I * 32 + i, gj = J * 32 + j;
-            T a = T(0);
-            if (gi < nb && gj < nb)
-                for (int k = J * 32; k < I * 32; ++k) a += D[k * LDD + gi] * Iv[gj * LDD + k];
-            Tm[bq * 32 * 33 + j * 33 + i] = a;
-        }
-        __syncthreads();
-        // inv(L)_IJ = -inv(L_II) Tm
-        for (int q = tid; q < nbl * 1024; q += nt) {
-            const int bq = q >> 10, e = q & 1023;
-            const int j = e >> 5, i = e & 31;
-            const int J = bq, I = bq + dist;
-            const int gi = I * 32 + i, gj = J * 32 + j;
-            if (gi < nb && gj < nb) {
-                T a = T(0);
-                for (int k = 0; k <= i; ++k) a += Iv[(I * 32 + k) * LDD + gi] * Tm[bq * 32 * 33 + j * 33 + k];
-                Iv[gj * LDD + gi] = -a;
+                for (int u = warp; u < ntrail + nterm; u += 7) {
+                    T c[4][8];
+                    tile_zero(c);
+                    if (u < ntrail) {
+                        int a = 0;
+                        while ((a + 1) * (a + 2) / 2 <= u) ++a;
+                        const int R = I + 1 + a, C = I + 1 + (u - a * (a + 1) / 2);   // R >= C
+                        // B(j, k) = L_CI(j, k)
+                        tile_mma(c, D + c0 * LDD + 32 * R, LDD, D + c0 * LDD + 32 * C, 1, LDD, lane);
+                        tile_store(D + (32 * C) * LDD + 32 * R, LDD, c, T(-1), true, lane);
+                    } else {
+                        const int t = u - ntrail;                 // t = K (K + 1) / 2 + J
+                        int K = 0;
+                        while ((K + 1) * (K + 2) / 2 <= t) ++K;
+                        const int J = t - K * (K + 1) / 2;
+                        // B(j, k) = inv(L)_KJ(k, j)
+                        tile_mma(c, D + (32 * K) * LDD + 32 * (I + 1), LDD, Iv + (32 * J) * LDD + 32 * K, LDD, 1,
+                                 lane);
+                        tile_store(P + t * 32 * 33, 33, c, T(1), false, lane);
+                    }
+                }
             }
         }
         __syncthreads();
     }
+#pragma unroll 4
     for (int q = tid; q < nb * nb; q += nt) {
         const int j = q / nb, i = q - j * nb;
         if (i >= j) blk[int64_t(j) * ld + i] = D[j * LDD + i];
@@ -209,7 +281,8 @@ __global__ void __launch_bounds__(256, 1) panel_kernel(const PanelTask *__restri
 
 size_t panel_smem_bytes(int nb, bool fp64) {
     const size_t el = fp64 ? 8 : 4;
-    return (size_t(2) * nb * (nb + 1) + 3 * 32 * 33) * el;
+    const size_t nbp = size_t((nb + 31) / 32) * 32;
+    return (2 * nbp * (nbp + 1) + 6 * 32 * 33 + nbp) * el;
 }
 
 template <typename T>
@@ -221,7 +294,7 @@ void launch_panel(const PanelTask *tasks, int ntasks, int max_nb, T *factor, T *
         (cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin), true);
     (void)smem_ok;
     ++g_kernel_launches;
-    panel_kernel<T><<<ntasks, 256, smem, st>>>(tasks, factor, inv_scratch, pv, round_inv);
+    panel_kernel<T><<<ntasks, kPanelThreads, smem, st>>>(tasks, factor, inv_scratch, pv, round_inv);
 }
 
 template void launch_panel<float>(const PanelTask *, int, int, float *, float *, PivotCtl, bool, cudaStream_t);
