@@ -130,15 +130,67 @@ __global__ void __launch_bounds__(256) fwd_asm_kernel(const SolveAsmTask *__rest
     }
 }
 
-// shared memory of the structure kernels: out[kRB * nrhs] | vec[kRB * nrhs] | tile[kRB][kRB + 1]
-__host__ __device__ inline size_t str_smem(int nrhs) {
-    return (size_t(2) * kRB * nrhs + size_t(kRB) * (kRB + 1)) * sizeof(double);
+// Tiles of L in shared memory are column-major with leading dimension TL
+// (64 rows + room for the 16-byte alignment shift of the first row).
+template <typename T>
+struct TileLd;
+template <>
+struct TileLd<float> {
+    static constexpr int v = 68;
+};
+template <>
+struct TileLd<double> {
+    static constexpr int v = 66;
+};
+
+__device__ __forceinline__ void cpa16(void *dst_smem, const void *src, int bytes) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
 }
-// shared memory of the diag kernels: acc[kRB * nrhs] | vec[kRB * nrhs] (double) |
-// tile[kRB][kRB + 1] | dblk[kRB][kRB + 1] (factor type)
+__device__ __forceinline__ void cpa8(void *dst_smem, const void *src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Stage panel rows [row0, row0 + nrows) x columns [col0, col0 + ncols) (at most
+// 64 x 64) into dst: element (i, j) lands at dst[j * TL + sh + i], sh = row0 % E
+// (E elements per 16 bytes; panel columns start 16-byte aligned). The rows of the
+// first 16-byte chunk before row0 belong to the same column and are copied too;
+// the last chunk is zero-filled past the range.
+template <typename T, int TL>
+__device__ __forceinline__ int stage_tile(T *dst, const T *pan, int64_t ld, int row0, int nrows, int col0,
+                                          int ncols, int tid, int nth) {
+    constexpr int E = 16 / int(sizeof(T));
+    const int sh = row0 % E;
+    const int start = row0 - sh;
+    const int nch = (nrows + sh + E - 1) / E;
+    const int tot = ncols * nch;
+#pragma unroll 4
+    for (int q = tid; q < tot; q += nth) {
+        const int j = q / nch, c = q - j * nch;
+        const int r = start + c * E;
+        const int nv = min(E, row0 + nrows - r);
+        cpa16(dst + j * TL + c * E, pan + int64_t(col0 + j) * ld + r, nv * int(sizeof(T)));
+    }
+    return sh;
+}
+
+// shared memory of the structure kernels: out[kRB * nrhs] | vec[2][kRB * nrhs] (double) | tile[2][kRB][TL]
+template <typename T>
+__host__ __device__ inline size_t str_smem(int nrhs) {
+    return size_t(3) * kRB * nrhs * sizeof(double) + size_t(2) * kRB * TileLd<T>::v * sizeof(T);
+}
+// shared memory of the diag kernels: acc[kRB * nrhs] | vec[kRB * nrhs] (double) | tile[2][kRB][TL] |
+// dblk[kRB][kRB + 1] (factor type)
 template <typename T>
 __host__ __device__ inline size_t diag_smem(int nrhs) {
-    return size_t(2) * kRB * nrhs * sizeof(double) + size_t(2) * kRB * (kRB + 1) * sizeof(T);
+    return size_t(2) * kRB * nrhs * sizeof(double) + size_t(2) * kRB * TileLd<T>::v * sizeof(T) +
+           size_t(kRB) * (kRB + 1) * sizeof(T);
 }
 
 // Diagonal block of the task into dblk (row-major, ld kRB + 1): the stored
@@ -149,6 +201,7 @@ __device__ __forceinline__ bool load_diag_block(T *dblk, const T *factor, const 
     const int tid = threadIdx.x;
     if (inv >= 0) {
         const T *src = factor + inv + int64_t(blk) * kRB * kRB;   // column-major 64 x 64
+#pragma unroll 8
         for (int q = tid; q < kRB * kRB; q += kTriThreads) {
             const int j = q >> 6, i = q & 63;
             dblk[i * (kRB + 1) + j] = src[q];
@@ -162,17 +215,20 @@ __device__ __forceinline__ bool load_diag_block(T *dblk, const T *factor, const 
     return false;
 }
 
+// Vectors in shared memory are column-major per right-hand side: v[r * kRB + i].
 template <typename T>
 __global__ void __launch_bounds__(kTriThreads) fwd_diag_kernel(const SolveTask *__restrict__ tasks, int ntasks,
                                                                SnDev sd, const T *__restrict__ factor,
                                                                double *__restrict__ X, int64_t ldx, int nrhs,
                                                                int *__restrict__ flags, int *__restrict__ err) {
+    constexpr int TL = TileLd<T>::v;
     extern __shared__ __align__(16) double smem_d[];
     double *acc = smem_d;
     double *yk = acc + kRB * nrhs;
-    T *tile = reinterpret_cast<T *>(yk + kRB * nrhs);   // tile[i * (kRB+1) + j] = L(r0+i, k0+j)
-    T *dblk = tile + kRB * (kRB + 1);
+    T *tiles = reinterpret_cast<T *>(yk + kRB * nrhs);   // two tiles: (i, j) = L(r0+i, k0+j) at [j * TL + i]
+    T *dblk = tiles + 2 * kRB * TL;
     const int tid = threadIdx.x;
+    const int nq = kRB * nrhs;
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SolveTask tk = tasks[t];
         const int s = tk.sn;
@@ -180,69 +236,77 @@ __global__ void __launch_bounds__(kTriThreads) fwd_diag_kernel(const SolveTask *
         const int c0 = sd.col0[s];
         const int r0 = tk.blk * kRB, nr = min(kRB, w - r0);
         const T *pan = factor + sd.pan_off[s];
-        // everything that does not depend on earlier blocks is loaded before the first wait
+        __syncthreads();                             // previous task done with shared memory
+        // everything that does not depend on earlier blocks is requested before the first wait
+        if (tk.blk > 0) stage_tile<T, TL>(tiles, pan, ld, r0, nr, 0, kRB, tid, kTriThreads);
+        cpa_commit();
         const bool has_inv = load_diag_block(dblk, factor, pan, sd.inv_off[s], ld, r0, nr, tk.blk);
-        for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-            const int i = q / nrhs, r = q % nrhs;
-            acc[q] = X[c0 + r0 + i + r * ldx];
+        for (int q = tid; q < nq; q += kTriThreads) {
+            const int i = q & (kRB - 1), r = q >> 6;
+            acc[q] = i < nr ? X[c0 + r0 + i + r * ldx] : 0.0;
         }
         for (int k = 0; k < tk.blk; ++k) {
-            const int k0 = k * kRB;      // full block: k < blk
-            __syncthreads();
-            for (int q = tid; q < nr * kRB; q += kTriThreads) {
-                const int j = q / nr, i = q % nr;
-                tile[i * (kRB + 1) + j] = pan[int64_t(k0 + j) * ld + r0 + i];
-            }
+            const int k0 = k * kRB;                  // full block: k < blk
+            if (k + 1 < tk.blk)
+                stage_tile<T, TL>(tiles + ((k + 1) & 1) * kRB * TL, pan, ld, r0, nr, k0 + kRB, kRB, tid,
+                                  kTriThreads);
+            cpa_commit();
             wait_flag(flags + tk.flag_base + k, 1, err);
-            for (int q = tid; q < kRB * nrhs; q += kTriThreads) {
-                const int j = q / nrhs, r = q % nrhs;
+            for (int q = tid; q < nq; q += kTriThreads) {
+                const int j = q & (kRB - 1), r = q >> 6;
                 yk[q] = __ldcg(&X[c0 + k0 + j + r * ldx]);
             }
+            cpa_wait<1>();
             __syncthreads();
-            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-                const int i = q / nrhs, r = q % nrhs;
-                const T *trow = tile + i * (kRB + 1);
+            const T *tl = tiles + (k & 1) * kRB * TL;
+            for (int q = tid; q < nq; q += kTriThreads) {
+                const int i = q & (kRB - 1), r = q >> 6;
+                const double *yr = yk + r * kRB;
                 double a0 = 0.0, a1 = 0.0;
 #pragma unroll 8
                 for (int j = 0; j < kRB; j += 2) {
-                    a0 += double(trow[j]) * yk[j * nrhs + r];
-                    a1 += double(trow[j + 1]) * yk[(j + 1) * nrhs + r];
+                    a0 += double(tl[j * TL + i]) * yr[j];
+                    a1 += double(tl[(j + 1) * TL + i]) * yr[j + 1];
                 }
                 acc[q] -= a0 + a1;
             }
+            __syncthreads();                         // tile (k & 1) is refilled at k + 2
         }
+        cpa_wait<0>();
         __syncthreads();
         if (has_inv) {
             // y = inv(L(r, r)) acc, written straight to X
-            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-                const int i = q / nrhs, r = q % nrhs;
+            for (int q = tid; q < nq; q += kTriThreads) {
+                const int i = q & (kRB - 1), r = q >> 6;
+                if (i >= nr) continue;
                 const T *irow = dblk + i * (kRB + 1);
+                const double *ar = acc + r * kRB;
                 double a0 = 0.0, a1 = 0.0;
                 int j = 0;
                 for (; j + 1 <= i; j += 2) {
-                    a0 += double(irow[j]) * acc[j * nrhs + r];
-                    a1 += double(irow[j + 1]) * acc[(j + 1) * nrhs + r];
+                    a0 += double(irow[j]) * ar[j];
+                    a1 += double(irow[j + 1]) * ar[j + 1];
                 }
-                if (j == i) a0 += double(irow[j]) * acc[j * nrhs + r];
+                if (j == i) a0 += double(irow[j]) * ar[j];
                 X[c0 + r0 + i + r * ldx] = a0 + a1;
             }
         } else {
             if (tid < 32) {
                 for (int j = 0; j < nr; ++j) {
                     const double ljj = double(dblk[j * (kRB + 1) + j]);
-                    for (int r = tid; r < nrhs; r += 32) acc[j * nrhs + r] /= ljj;
+                    for (int r = tid; r < nrhs; r += 32) acc[r * kRB + j] /= ljj;
                     __syncwarp();
                     for (int i = j + 1 + tid; i < nr; i += 32) {
                         const double lij = double(dblk[i * (kRB + 1) + j]);
-                        for (int r = 0; r < nrhs; ++r) acc[i * nrhs + r] -= lij * acc[j * nrhs + r];
+                        for (int r = 0; r < nrhs; ++r) acc[r * kRB + i] -= lij * acc[r * kRB + j];
                     }
                     __syncwarp();
                 }
             }
             __syncthreads();
-            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-                const int i = q / nrhs, r = q % nrhs;
-                X[c0 + r0 + i + r * ldx] = acc[q];
+            for (int q = tid; q < nq; q += kTriThreads) {
+                const int i = q & (kRB - 1), r = q >> 6;
+                if (i < nr) X[c0 + r0 + i + r * ldx] = acc[q];
             }
         }
         __threadfence();
@@ -256,12 +320,14 @@ __global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *
                                                                SnDev sd, const T *__restrict__ factor,
                                                                double *__restrict__ X, int64_t ldx, int nrhs,
                                                                int *__restrict__ flags, int *__restrict__ err) {
+    constexpr int TL = TileLd<T>::v;
     extern __shared__ __align__(16) double smem_d[];
     double *acc = smem_d;
     double *xk = acc + kRB * nrhs;
-    T *tile = reinterpret_cast<T *>(xk + kRB * nrhs);   // tile[i * (kRB+1) + j] = L(i0+i, r0+j)
-    T *dblk = tile + kRB * (kRB + 1);
+    T *tiles = reinterpret_cast<T *>(xk + kRB * nrhs);   // two tiles: (i, j) = L(i0+i, r0+j) at [j * TL + i]
+    T *dblk = tiles + 2 * kRB * TL;
     const int tid = threadIdx.x;
+    const int nq = kRB * nrhs;
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SolveTask tk = tasks[t];
         const int s = tk.sn;
@@ -270,61 +336,78 @@ __global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *
         const int nbw = (w + kRB - 1) / kRB;
         const int r0 = tk.blk * kRB, nr = min(kRB, w - r0);
         const T *pan = factor + sd.pan_off[s];
+        __syncthreads();
+        const int kfirst = nbw - 1;
+        if (kfirst > tk.blk)
+            stage_tile<T, TL>(tiles, pan, ld, kfirst * kRB, min(kRB, w - kfirst * kRB), r0, nr, tid, kTriThreads);
+        cpa_commit();
         const bool has_inv = load_diag_block(dblk, factor, pan, sd.inv_off[s], ld, r0, nr, tk.blk);
-        for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-            const int j = q / nrhs, r = q % nrhs;
-            acc[q] = X[c0 + r0 + j + r * ldx];
+        for (int q = tid; q < nq; q += kTriThreads) {
+            const int j = q & (kRB - 1), r = q >> 6;
+            acc[q] = j < nr ? X[c0 + r0 + j + r * ldx] : 0.0;
         }
-        for (int k = nbw - 1; k > tk.blk; --k) {
+        int buf = 0;
+        for (int k = kfirst; k > tk.blk; --k, buf ^= 1) {
             const int i0 = k * kRB, ni = min(kRB, w - i0);
-            __syncthreads();
-            for (int q = tid; q < ni * nr; q += kTriThreads) {
-                const int j = q / ni, i = q % ni;
-                tile[i * (kRB + 1) + j] = pan[int64_t(r0 + j) * ld + i0 + i];
-            }
+            if (k - 1 > tk.blk)
+                stage_tile<T, TL>(tiles + (buf ^ 1) * kRB * TL, pan, ld, i0 - kRB, kRB, r0, nr, tid, kTriThreads);
+            cpa_commit();
             wait_flag(flags + tk.flag_base + k, 2, err);
-            for (int q = tid; q < ni * nrhs; q += kTriThreads) {
-                const int i = q / nrhs, r = q % nrhs;
-                xk[q] = __ldcg(&X[c0 + i0 + i + r * ldx]);
+            for (int q = tid; q < nq; q += kTriThreads) {
+                const int i = q & (kRB - 1), r = q >> 6;
+                xk[q] = i < ni ? __ldcg(&X[c0 + i0 + i + r * ldx]) : 0.0;
+            }
+            cpa_wait<1>();
+            __syncthreads();
+            const T *tl = tiles + buf * kRB * TL;
+            for (int q = tid; q < nq; q += kTriThreads) {
+                const int j = q & (kRB - 1), r = q >> 6;
+                const double *xr = xk + r * kRB;
+                double a0 = 0.0, a1 = 0.0;
+                // skewed order: the lanes of a warp read 32 different rows (distinct banks)
+#pragma unroll 8
+                for (int u = 0; u < kRB; u += 2) {
+                    const int i = (u + j) & (kRB - 1), i1 = (u + 1 + j) & (kRB - 1);
+                    a0 += (i < ni ? double(tl[j * TL + i]) : 0.0) * xr[i];
+                    a1 += (i1 < ni ? double(tl[j * TL + i1]) : 0.0) * xr[i1];
+                }
+                acc[q] -= a0 + a1;
             }
             __syncthreads();
-            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-                const int j = q / nrhs, r = q % nrhs;
-                double a = 0.0;
-                for (int i = 0; i < ni; ++i) a += double(tile[i * (kRB + 1) + j]) * xk[i * nrhs + r];
-                acc[q] -= a;
-            }
         }
+        cpa_wait<0>();
         __syncthreads();
         if (has_inv) {
             // x = inv(L(r, r))^T acc
-            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-                const int j = q / nrhs, r = q % nrhs;
+            for (int q = tid; q < nq; q += kTriThreads) {
+                const int j = q & (kRB - 1), r = q >> 6;
+                if (j >= nr) continue;
+                const double *ar = acc + r * kRB;
                 double a0 = 0.0, a1 = 0.0;
                 int i = j;
                 for (; i + 1 < nr; i += 2) {
-                    a0 += double(dblk[i * (kRB + 1) + j]) * acc[i * nrhs + r];
-                    a1 += double(dblk[(i + 1) * (kRB + 1) + j]) * acc[(i + 1) * nrhs + r];
+                    a0 += double(dblk[i * (kRB + 1) + j]) * ar[i];
+                    a1 += double(dblk[(i + 1) * (kRB + 1) + j]) * ar[i + 1];
                 }
-                if (i < nr) a0 += double(dblk[i * (kRB + 1) + j]) * acc[i * nrhs + r];
+                if (i < nr) a0 += double(dblk[i * (kRB + 1) + j]) * ar[i];
                 X[c0 + r0 + j + r * ldx] = a0 + a1;
             }
         } else {
             if (tid < 32) {
                 for (int j = nr - 1; j >= 0; --j) {
-                    for (int r = tid; r < nrhs; r += 32) acc[j * nrhs + r] /= double(dblk[j * (kRB + 1) + j]);
+                    for (int r = tid; r < nrhs; r += 32) acc[r * kRB + j] /= double(dblk[j * (kRB + 1) + j]);
                     __syncwarp();
                     for (int i = tid; i < j; i += 32) {
                         const double lji = double(dblk[j * (kRB + 1) + i]);
-                        for (int r = 0; r < nrhs; ++r) acc[i * nrhs + r] -= lji * acc[j * nrhs + r];
+                        for (int r = 0; r < nrhs; ++r) acc[r * kRB + i] -= lji * acc[r * kRB + j];
                     }
                     __syncwarp();
                 }
             }
             __syncthreads();
-            for (int q = tid; q < nr * nrhs; q += kTriThreads) {
-                const int j = q / nrhs, r = q % nrhs;
-                X[c0 + r0 + j + r * ldx] = acc[q];
+            for (int q = tid; q < nq; q += kTriThreads) {
+                const int j = q & (kRB - 1), r = q >> 6;
+                if (j < nr) X[c0 + r0 + j + r * ldx] = acc[q];
             }
         }
         __threadfence();
@@ -335,16 +418,19 @@ __global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *
 
 // Structure part, forward: P(task) = L21(rows, cols) y(cols); backward:
 // P(task) = L21(rows, cols)^T x(struct rows). One 64 x kStrChunk (or
-// kStrChunk x 64) slab of L21 per CTA, read as 64 x 64 tiles.
+// kStrChunk x 64) slab of L21 per CTA, streamed as 64 x 64 tiles with the next
+// tile and its vector slice in flight (cp.async) while the current one is used.
+// P slab layout: P[r * kRB + a].
 template <typename T, bool FWD>
 __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restrict__ tasks, SnDev sd,
                                                           const T *__restrict__ factor,
                                                           const double *__restrict__ X, int64_t ldx, int nrhs,
                                                           double *__restrict__ P) {
+    constexpr int TL = TileLd<T>::v;
     extern __shared__ __align__(16) double smem_d[];
     double *out = smem_d;                      // [kRB * nrhs]
-    double *vec = out + kRB * nrhs;            // [kRB * nrhs]
-    double *tile = vec + kRB * nrhs;           // [kRB][kRB + 1]
+    double *vecs = out + kRB * nrhs;           // [2][kRB * nrhs]
+    T *tiles = reinterpret_cast<T *>(vecs + 2 * kRB * nrhs);   // [2][kRB][TL]
     const StrTask tk = tasks[blockIdx.x];
     const int s = tk.sn;
     const int w = sd.w[s], d = sd.d[s], ld = sd.ld[s];
@@ -353,53 +439,74 @@ __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restr
     const T *pan = factor + sd.pan_off[s];
     const int32_t *rows = sd.struct_rows + sd.struct_ptr[s];
     const int tid = threadIdx.x, nt = blockDim.x;
-    // FWD: fixed 64 struct rows [a0, a0+na), loop over 64-col blocks of the chunk
-    // BWD: fixed 64 columns [a0, a0+na), loop over 64-row blocks of the chunk
+    const int nq = kRB * nrhs;
+    // FWD: fixed 64 struct rows [a0, a0+na), 64-column blocks of the chunk
+    // BWD: fixed 64 columns [a0, a0+na), 64-row blocks of the chunk
     const int a0 = tk.idx * kRB;
     const int na = FWD ? min(kRB, d - a0) : min(kRB, w - a0);
     const int lim = FWD ? w : d;
     const int b_begin = tk.chunk * kStrChunk, b_end = min(lim, b_begin + kStrChunk);
-    for (int q = tid; q < na * nrhs; q += nt) out[q] = 0.0;
-    for (int b0 = b_begin; b0 < b_end; b0 += kRB) {
-        const int nbk = min(kRB, b_end - b0);
-        __syncthreads();
+    const int nblk = (b_end - b_begin + kRB - 1) / kRB;
+    int sh = 0;
+    auto stage = [&](int b, int buf) {
+        const int b0 = b_begin + b * kRB, nbk = min(kRB, b_end - b0);
+        double *v = vecs + buf * nq;
         if (FWD) {
-            // tile[i][j] = L(w + a0 + i, b0 + j), vec[j] = y(b0 + j)
-            for (int q = tid; q < na * nbk; q += nt) {
-                const int j = q / na, i = q % na;
-                tile[i * (kRB + 1) + j] = double(pan[int64_t(b0 + j) * ld + w + a0 + i]);
-            }
-            for (int q = tid; q < nbk * nrhs; q += nt) {
-                const int j = q / nrhs, r = q % nrhs;
-                vec[q] = X[c0 + b0 + j + r * ldx];
+            sh = stage_tile<T, TL>(tiles + buf * kRB * TL, pan, ld, w + a0, na, b0, nbk, tid, nt);
+            for (int q = tid; q < nq; q += nt) {
+                const int j = q & (kRB - 1), r = q >> 6;
+                if (j < nbk) cpa8(v + q, X + c0 + b0 + j + r * ldx);
             }
         } else {
-            // tile[i][j] = L(w + b0 + i, a0 + j), vec[i] = x(struct row b0 + i)
-            for (int q = tid; q < nbk * na; q += nt) {
-                const int j = q / nbk, i = q % nbk;
-                tile[i * (kRB + 1) + j] = double(pan[int64_t(a0 + j) * ld + w + b0 + i]);
-            }
-            for (int q = tid; q < nbk * nrhs; q += nt) {
-                const int i = q / nrhs, r = q % nrhs;
+            sh = stage_tile<T, TL>(tiles + buf * kRB * TL, pan, ld, w + b0, nbk, a0, na, tid, nt);
+            for (int q = tid; q < nq; q += nt) {
+                const int i = q & (kRB - 1), r = q >> 6;
                 const int li = b0 + i;
-                const int64_t gi = int64_t(rows[li / vb]) * vb + li % vb;
-                vec[q] = X[gi + r * ldx];
+                if (i < nbk) cpa8(v + q, X + int64_t(rows[li / vb]) * vb + li % vb + r * ldx);
             }
         }
+        cpa_commit();
+    };
+    for (int q = tid; q < nq; q += nt) out[q] = 0.0;
+    stage(0, 0);
+    for (int b = 0; b < nblk; ++b) {
+        const int buf = b & 1;
+        const int nbk = min(kRB, b_end - (b_begin + b * kRB));
+        if (b + 1 < nblk) stage(b + 1, buf ^ 1);
+        else cpa_commit();
+        cpa_wait<1>();
         __syncthreads();
-        for (int q = tid; q < na * nrhs; q += nt) {
-            const int a = q / nrhs, r = q % nrhs;
-            double acc = 0.0;
-            if (FWD)
-                for (int j = 0; j < nbk; ++j) acc += tile[a * (kRB + 1) + j] * vec[j * nrhs + r];
-            else
-                for (int i = 0; i < nbk; ++i) acc += tile[i * (kRB + 1) + a] * vec[i * nrhs + r];
-            out[q] += acc;
+        const T *tl = tiles + buf * kRB * TL + sh;
+        const double *v = vecs + buf * nq;
+        for (int q = tid; q < nq; q += nt) {
+            const int a = q & (kRB - 1), r = q >> 6;
+            const double *vr = v + r * kRB;
+            double a0s = 0.0, a1s = 0.0;
+            if (FWD) {
+                // out(a) += sum_j L(w + a0 + a, b0 + j) y(b0 + j)
+                int j = 0;
+#pragma unroll 4
+                for (; j + 1 < nbk; j += 2) {
+                    a0s += double(tl[j * TL + a]) * vr[j];
+                    a1s += double(tl[(j + 1) * TL + a]) * vr[j + 1];
+                }
+                if (j < nbk) a0s += double(tl[j * TL + a]) * vr[j];
+            } else {
+                // out(a) += sum_i L(w + b0 + i, a0 + a) x(struct row b0 + i), rows in skewed order
+#pragma unroll 8
+                for (int u = 0; u < kRB; u += 2) {
+                    const int i = (u + a) & (kRB - 1), i1 = (u + 1 + a) & (kRB - 1);
+                    a0s += (i < nbk ? double(tl[a * TL + i]) * vr[i] : 0.0);
+                    a1s += (i1 < nbk ? double(tl[a * TL + i1]) * vr[i1] : 0.0);
+                }
+            }
+            out[q] += a0s + a1s;
         }
+        __syncthreads();                       // buffer `buf` is refilled at b + 2
     }
-    __syncthreads();
-    double *Pt = P + int64_t(blockIdx.x) * kRB * nrhs;
-    for (int q = tid; q < na * nrhs; q += nt) Pt[q] = out[q];
+    cpa_wait<0>();
+    double *Pt = P + int64_t(blockIdx.x) * nq;
+    for (int q = tid; q < nq; q += nt) Pt[q] = out[q];
 }
 
 // Subtract the chunk partials of one 64-row (FWD: of u_s) or 64-column (BWD: of x) slab, in chunk order.
@@ -413,9 +520,9 @@ __global__ void __launch_bounds__(256) str_reduce_kernel(const StrReduce *__rest
     const int a0 = rd.idx * kRB;
     const int na = FWD ? min(kRB, d - a0) : min(kRB, w - a0);
     for (int q = threadIdx.x; q < na * nrhs; q += blockDim.x) {
-        const int a = q / nrhs, r = q % nrhs;
+        const int a = q % na, r = q / na;
         double acc = 0.0;
-        for (int c = 0; c < rd.nchunks; ++c) acc += P[int64_t(rd.first + c) * kRB * nrhs + q];
+        for (int c = 0; c < rd.nchunks; ++c) acc += P[int64_t(rd.first + c) * kRB * nrhs + r * kRB + a];
         if (FWD) sol[sd.sol_off[s] * nrhs + (a0 + a) + int64_t(r) * d] -= acc;
         else X[sd.col0[s] + a0 + a + r * ldx] -= acc;
     }
@@ -477,12 +584,12 @@ void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce 
                 const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st) {
     if (ntasks <= 0) return;
     g_kernel_launches += 2;
-    const size_t smem = str_smem(nrhs);
+    const size_t smem = str_smem<T>(nrhs);
     static const bool attr_ok =
         (cudaFuncSetAttribute(str_partial_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(str_smem(kMaxSolveRhs))),
+                              int(str_smem<T>(kMaxSolveRhs))),
          cudaFuncSetAttribute(str_partial_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(str_smem(kMaxSolveRhs))),
+                              int(str_smem<T>(kMaxSolveRhs))),
          true);
     (void)attr_ok;
     if (forward) {
