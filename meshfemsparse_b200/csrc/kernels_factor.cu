@@ -153,7 +153,14 @@ __global__ void __launch_bounds__(256) small_factor_kernel(const int32_t *__rest
 
 // Large fronts: zero U_s and extend-add every child into the columns
 // [c0, c0 + kAsmCols) of the front (panel part or U_s part).
-template <typename T>
+// child_rel with the analysis block size known at compile time (1 or 3), else vb.
+template <int VB>
+__device__ __forceinline__ int child_rel_vb(const int32_t *rel, int i, int vb) {
+    if (VB > 0) return rel[i / VB] + i % VB;
+    return rel[i / vb] + i % vb;
+}
+
+template <typename T, int VB>
 __global__ void __launch_bounds__(256) assemble_large_kernel(const AssembleTask *__restrict__ tasks, int ntasks,
                                                              SnDev sd, T *__restrict__ factor,
                                                              T *__restrict__ upd) {
@@ -192,17 +199,34 @@ __global__ void __launch_bounds__(256) assemble_large_kernel(const AssembleTask 
         const int jc0 = a * vb, jc1 = e * vb;
         const int ncols = jc1 - jc0;
         if (ncols > 0) {
-            // pairs (jc, ic) with ic >= jc; iterate jc-major
-            for (int jj = 0; jj < ncols; ++jj) {
+            // One warp per child column (columns jc0 + warp, + 8, ...), lanes over the
+            // rows ic >= jc with 8 read-modify-writes in flight per lane. Targets are
+            // distinct (child_rel_indices is injective).
+            const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+            for (int jj = warp; jj < ncols; jj += nwarps) {
                 const int jc = jc0 + jj;
-                const int rj = child_rel(rel, jc, vb);
+                const int rj = child_rel_vb<VB>(rel, jc, vb);
                 if (rj < c0 || rj >= c1) continue;
                 const T *Ucol = U + int64_t(jc) * dc;
-                for (int ic = jc + tid; ic < dc; ic += nt) {
-                    const int ri = child_rel(rel, ic, vb);
-                    const T v = Ucol[ic];
-                    if (rj < w) pan[int64_t(rj) * ld + ri] += v;
-                    else Us[int64_t(rj - w) * d + (ri - w)] += v;
+                T *dcol = (rj < w) ? pan + int64_t(rj) * ld : Us + int64_t(rj - w) * d - w;
+                for (int ib = jc + lane; ib < dc; ib += 8 * 32) {
+                    T v[8], old[8];
+                    int ri[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const int ic = ib + 32 * u;
+                        ri[u] = -1;
+                        if (ic < dc) {
+                            ri[u] = child_rel_vb<VB>(rel, ic, vb);
+                            v[u] = Ucol[ic];
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (ri[u] >= 0) old[u] = dcol[ri[u]];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (ri[u] >= 0) dcol[ri[u]] = old[u] + v[u];
                 }
             }
         }
@@ -258,7 +282,9 @@ void launch_assemble_large(const AssembleTask *tasks, int ntasks, int ntiles, Sn
                            cudaStream_t st) {
     if (ntiles <= 0) return;
     ++g_kernel_launches;
-    assemble_large_kernel<T><<<ntiles, 256, 0, st>>>(tasks, ntasks, sd, factor, upd);
+    if (sd.vb == 3) assemble_large_kernel<T, 3><<<ntiles, 256, 0, st>>>(tasks, ntasks, sd, factor, upd);
+    else if (sd.vb == 1) assemble_large_kernel<T, 1><<<ntiles, 256, 0, st>>>(tasks, ntasks, sd, factor, upd);
+    else assemble_large_kernel<T, 0><<<ntiles, 256, 0, st>>>(tasks, ntasks, sd, factor, upd);
 }
 
 template <typename T>

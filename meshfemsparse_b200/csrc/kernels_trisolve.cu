@@ -118,13 +118,29 @@ __global__ void __launch_bounds__(256) fwd_asm_kernel(const SolveAsmTask *__rest
         int e = a;
         while (e < nblk && rel[e] < r1) ++e;
         const int i0 = a * vb, n = (e - a) * vb;
-        for (int q = tid; q < n * nrhs; q += nt) {
-            const int r = q / n, i = i0 + q % n;
-            const int ri = child_rel(rel, i, vb);
-            if (ri < r0 || ri >= r1) continue;
-            const double v = uc[i + r * dc];
-            if (ri < w) X[c0 + ri + r * ldx] += v;
-            else us[(ri - w) + r * d] += v;
+        // 4 independent read-modify-writes in flight per thread (targets are distinct)
+        for (int q0 = tid; q0 < n * nrhs; q0 += 4 * nt) {
+            double v[4], old[4];
+            double *dst[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                dst[u] = nullptr;
+                const int q = q0 + u * nt;
+                if (q < n * nrhs) {
+                    const int r = q / n, i = i0 + q % n;
+                    const int ri = child_rel(rel, i, vb);
+                    if (ri >= r0 && ri < r1) {
+                        v[u] = uc[i + r * dc];
+                        dst[u] = (ri < w) ? X + c0 + ri + r * ldx : us + (ri - w) + r * d;
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (dst[u]) old[u] = *dst[u];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (dst[u]) *dst[u] = old[u] + v[u];
         }
         __syncthreads();
     }
@@ -467,6 +483,18 @@ __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restr
         }
         cpa_commit();
     };
+    // Up to 4 right-hand sides (the common case) accumulate in registers:
+    //   FWD: thread = (row pair a, a + 32) x (8-column group of the tile), summed over
+    //        the groups at the end; BWD: lane = (row pair i, i + 32), warp = 8 columns,
+    //        summed over the lanes at the end.
+    // More right-hand sides take the generic per-(row, rhs) loop.
+    const bool fast = nrhs <= 4;
+    const int lane = tid & 31, wgrp = tid >> 5;
+    double racc[8][4];
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) racc[c][r] = 0.0;
     for (int q = tid; q < nq; q += nt) out[q] = 0.0;
     stage(0, 0);
     for (int b = 0; b < nblk; ++b) {
@@ -478,33 +506,97 @@ __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restr
         __syncthreads();
         const T *tl = tiles + buf * kRB * TL + sh;
         const double *v = vecs + buf * nq;
-        for (int q = tid; q < nq; q += nt) {
-            const int a = q & (kRB - 1), r = q >> 6;
-            const double *vr = v + r * kRB;
-            double a0s = 0.0, a1s = 0.0;
+        if (fast) {
             if (FWD) {
-                // out(a) += sum_j L(w + a0 + a, b0 + j) y(b0 + j)
-                int j = 0;
-#pragma unroll 4
-                for (; j + 1 < nbk; j += 2) {
-                    a0s += double(tl[j * TL + a]) * vr[j];
-                    a1s += double(tl[(j + 1) * TL + a]) * vr[j + 1];
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj) {
+                    const int j = 8 * wgrp + jj;
+                    if (j < nbk) {
+                        const double t0 = double(tl[j * TL + lane]), t1 = double(tl[j * TL + lane + 32]);
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            if (r < nrhs) {
+                                const double vv = v[r * kRB + j];
+                                racc[0][r] += t0 * vv;
+                                racc[1][r] += t1 * vv;
+                            }
+                    }
                 }
-                if (j < nbk) a0s += double(tl[j * TL + a]) * vr[j];
             } else {
-                // out(a) += sum_i L(w + b0 + i, a0 + a) x(struct row b0 + i), rows in skewed order
-#pragma unroll 8
-                for (int u = 0; u < kRB; u += 2) {
-                    const int i = (u + a) & (kRB - 1), i1 = (u + 1 + a) & (kRB - 1);
-                    a0s += (i < nbk ? double(tl[a * TL + i]) * vr[i] : 0.0);
-                    a1s += (i1 < nbk ? double(tl[a * TL + i1]) * vr[i1] : 0.0);
+                double x0[4], x1[4];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    x0[r] = (r < nrhs && lane < nbk) ? v[r * kRB + lane] : 0.0;
+                    x1[r] = (r < nrhs && lane + 32 < nbk) ? v[r * kRB + lane + 32] : 0.0;
+                }
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const int a = 8 * wgrp + c;
+                    const double t0 = lane < nbk ? double(tl[a * TL + lane]) : 0.0;
+                    const double t1 = lane + 32 < nbk ? double(tl[a * TL + lane + 32]) : 0.0;
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) racc[c][r] += t0 * x0[r] + t1 * x1[r];
                 }
             }
-            out[q] += a0s + a1s;
+        } else {
+            for (int q = tid; q < nq; q += nt) {
+                const int a = q & (kRB - 1), r = q >> 6;
+                const double *vr = v + r * kRB;
+                double a0s = 0.0, a1s = 0.0;
+                if (FWD) {
+                    // out(a) += sum_j L(w + a0 + a, b0 + j) y(b0 + j)
+                    int j = 0;
+#pragma unroll 4
+                    for (; j + 1 < nbk; j += 2) {
+                        a0s += double(tl[j * TL + a]) * vr[j];
+                        a1s += double(tl[(j + 1) * TL + a]) * vr[j + 1];
+                    }
+                    if (j < nbk) a0s += double(tl[j * TL + a]) * vr[j];
+                } else {
+                    // out(a) += sum_i L(w + b0 + i, a0 + a) x(struct row b0 + i), rows in skewed order
+#pragma unroll 8
+                    for (int u = 0; u < kRB; u += 2) {
+                        const int i = (u + a) & (kRB - 1), i1 = (u + 1 + a) & (kRB - 1);
+                        a0s += (i < nbk ? double(tl[a * TL + i]) * vr[i] : 0.0);
+                        a1s += (i1 < nbk ? double(tl[a * TL + i1]) * vr[i1] : 0.0);
+                    }
+                }
+                out[q] += a0s + a1s;
+            }
         }
         __syncthreads();                       // buffer `buf` is refilled at b + 2
     }
     cpa_wait<0>();
+    if (fast) {
+        if (FWD) {
+            // sum the 8 column groups: red[(group * 4 + r) * kRB + a] in the (now idle) tile buffers
+            double *red = reinterpret_cast<double *>(tiles);
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (r < nrhs) {
+                    red[(wgrp * 4 + r) * kRB + lane] = racc[0][r];
+                    red[(wgrp * 4 + r) * kRB + lane + 32] = racc[1][r];
+                }
+            __syncthreads();
+            for (int q = tid; q < nq; q += nt) {
+                const int a = q & (kRB - 1), r = q >> 6;
+                double sacc = 0.0;
+                for (int g = 0; g < 8; ++g) sacc += red[(g * 4 + r) * kRB + a];
+                out[q] = sacc;
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    double g = racc[c][r];
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) g += __shfl_down_sync(0xffffffffu, g, off);
+                    if (lane == 0 && r < nrhs) out[r * kRB + 8 * wgrp + c] = g;
+                }
+        }
+    }
+    __syncthreads();
     double *Pt = P + int64_t(blockIdx.x) * nq;
     for (int q = tid; q < nq; q += nt) Pt[q] = out[q];
 }
