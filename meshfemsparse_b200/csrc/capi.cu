@@ -84,9 +84,10 @@ struct LevelPlan {
     int large_count = 0;
     int asm_off = 0, asm_n = 0, asm_tiles = 0;
     struct Step {
+        int left_off, left_n, left_tiles;   // the block's columns updated by the earlier blocks of its group
         int potrf_off, potrf_n, potrf_maxnb;
         int trsm_off, trsm_n, trsm_tiles;   // X := X inv(L)^T of the rows below the block
-        int gemm_off, gemm_n, gemm_tiles;   // trailing update of the remaining panel columns
+        int gemm_off, gemm_n, gemm_tiles;   // trailing update of the columns after a finished group
     };
     std::vector<Step> steps;
     int syrk_off = 0, syrk_n = 0, syrk_tiles = 0;
@@ -352,8 +353,27 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             base += g.tiles_m * g.tiles_n;
             gemm_tasks.push_back(g);
         };
+        // Column blocks of NB are grouped by GB = 4 NB: inside a group the block
+        // columns are brought up to date left-looking (one GEMM with k = kb - group
+        // start), after a group the rest of the front gets one rank-GB update. The
+        // Schur updates so run with k up to GB instead of NB, reading and writing
+        // the trailing columns GB / NB times less often.
+        const idx GB = 4 * NB;
         for (idx kb = 0; kb < maxw; kb += NB) {
             LevelPlan::Step sp{};
+            const idx ko = kb - kb % GB;                // start of the block's group
+            sp.left_off = int(gemm_tasks.size());
+            int lb = 0;
+            if (kb > ko)
+                for (idx s : large) {
+                    const idx w = S.w[s], f = S.f[s], ld = dld[s], pan = dpan[s];
+                    if (w <= kb) continue;
+                    const int nb = int(std::min<idx>(NB, w - kb));
+                    const int64_t a = pan + ko * ld + kb;
+                    gemm(a, a, pan + kb * ld + kb, int(ld), int(ld), int(ld), f - kb, nb, kb - ko, 1, 0, lb);
+                }
+            sp.left_n = int(gemm_tasks.size()) - sp.left_off;
+            sp.left_tiles = lb;
             sp.potrf_off = int(potrf_tasks.size());
             int64_t dslot = 0;
             for (idx s : large) {
@@ -390,18 +410,16 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             }
             sp.trsm_n = int(gemm_tasks.size()) - sp.trsm_off;
             sp.trsm_tiles = tb;
-            // trailing update of the remaining panel columns
+            // after the last block of a group: update the columns after the group
             sp.gemm_off = int(gemm_tasks.size());
             int gb = 0;
             for (idx s : large) {
                 const idx w = S.w[s], f = S.f[s], ld = dld[s], pan = dpan[s];
                 if (w <= kb) continue;
-                const int nb = int(std::min<idx>(NB, w - kb));
-                const idx m = f - kb - nb, n = w - kb - nb;
-                if (n > 0) {
-                    const int64_t a = pan + kb * ld + kb + nb;
-                    gemm(a, a, pan + (kb + nb) * ld + kb + nb, int(ld), int(ld), int(ld), m, n, nb, 1, 0, gb);
-                }
+                const idx ke = std::min<idx>(kb + NB, w);          // end of this block
+                if (ke != std::min<idx>(ko + GB, w) || ke >= w) continue;
+                const int64_t a = pan + ko * ld + ke;
+                gemm(a, a, pan + ke * ld + ke, int(ld), int(ld), int(ld), f - ke, w - ke, ke - ko, 1, 0, gb);
             }
             sp.gemm_n = int(gemm_tasks.size()) - sp.gemm_off;
             sp.gemm_tiles = gb;
@@ -568,6 +586,9 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         launch_assemble_large<T>(ds.asm_tasks.p + L.asm_off, L.asm_n, L.asm_tiles, ds.sd, factor, upd, st);
         MFS_LAUNCHED();
         for (const auto &sp : L.steps) {
+            launch_gemm<T>(ds.gemm_tasks.p + sp.left_off, sp.left_n, sp.left_tiles, factor, factor, factor, split,
+                           h->gemm_err.p, st);
+            MFS_LAUNCHED();
             launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, dscr, pv, split == 1,
                             st);
             MFS_LAUNCHED();
