@@ -113,6 +113,8 @@ struct DevSym {
     DBuf<StrTask> fstr_tasks, bstr_tasks;
     DBuf<StrReduce> fred, bred;
     int max_str_tasks = 0;
+    DBuf<int2> subs;                     // subtree ranges solved one per CTA (levels <= solve_cut)
+    int nsub = 0, sub_fmax = 0, solve_cut = -1;
     DBuf<int> flags;                     // one per 64-row diagonal block of every front
     DBuf<int64_t> spmv_ptr, spmv_src;
     DBuf<int32_t> spmv_col, spmv_flag;
@@ -526,6 +528,14 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     up(ds->fred, fred);
     up(ds->bred, bred);
     ds->max_str_tasks = max_str;
+    {
+        std::vector<int2> sv(S.sub_lo.size());
+        for (size_t k = 0; k < sv.size(); ++k) sv[k] = make_int2(int(S.sub_lo[k]), int(S.sub_hi[k]));
+        up(ds->subs, sv);
+        ds->nsub = int(sv.size());
+        ds->sub_fmax = int(S.sub_fmax);
+        ds->solve_cut = int(S.solve_cut);
+    }
     ds->flags.ensure(size_t(std::max(nflags, 1)));
     MFS_CUDA(cudaMemsetAsync(ds->flags.p, 0, ds->flags.bytes(), st));
     MFS_CUDA(cudaStreamSynchronize(st));
@@ -617,7 +627,10 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
         const int nr = std::min(kMaxSolveRhs, nrhs - r0);
         double *Xc = X + int64_t(r0) * S.n;
         MFS_CUDA(cudaMemsetAsync(ds.flags.p, 0, ds.flags.bytes(), st));
-        for (size_t l = 0; l < ds.levels.size(); ++l) {
+        // levels <= solve_cut: whole subtrees, one per CTA
+        launch_subtree_solve<T>(true, ds.subs.p, ds.nsub, ds.sub_fmax, ds.sd, factor, Xc, S.n, nr, h->sol.p, st);
+        MFS_LAUNCHED();
+        for (size_t l = size_t(ds.solve_cut + 1); l < ds.levels.size(); ++l) {
             const LevelPlan &L = ds.levels[l];
             launch_fwd_asm(ds.sasm_tasks.p + L.sasm_off, L.sasm_n, L.sasm_tiles, ds.sd, Xc, S.n, nr, h->sol.p, st);
             MFS_LAUNCHED();
@@ -627,7 +640,7 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
                           factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
             MFS_LAUNCHED();
         }
-        for (size_t l = ds.levels.size(); l-- > 0;) {
+        for (size_t l = ds.levels.size(); l-- > size_t(ds.solve_cut + 1);) {
             const LevelPlan &L = ds.levels[l];
             launch_str<T>(false, ds.bstr_tasks.p + L.bstr_off, L.bstr_n, ds.bred.p + L.bred_off, L.bred_n, ds.sd,
                           factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
@@ -635,6 +648,8 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
             MFS_CUDA(launch_diag<T>(false, ds.btri_tasks.p + L.btri_off, L.btri_n, ds.sd, factor, Xc, S.n, nr,
                                     ds.flags.p, h->solve_err.p, st));
         }
+        launch_subtree_solve<T>(false, ds.subs.p, ds.nsub, ds.sub_fmax, ds.sd, factor, Xc, S.n, nr, h->sol.p, st);
+        MFS_LAUNCHED();
     }
 }
 

@@ -157,6 +157,11 @@ template <typename T>
 void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce *red, int nred, SnDev sd,
                 const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st);
 int solve_rows_per_task();
+// Forward / backward solve of whole subtrees (subs[k] = postorder range [x, y]),
+// one CTA per subtree, fronts of at most fmax rows.
+template <typename T>
+void launch_subtree_solve(bool forward, const int2 *subs, int nsub, int fmax, SnDev sd, const T *factor, double *X,
+                          int64_t ldx, int nrhs, double *sol, cudaStream_t st);
 
 // Symmetric block SpMV over permuted reduced rows: Y = A X (both ld = n).
 void launch_spmv(const int64_t *ptr, const int64_t *src, const int32_t *col, const int32_t *flag, int64_t nrows,

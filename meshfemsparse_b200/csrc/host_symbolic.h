@@ -133,10 +133,16 @@ struct Symbolic {
     // levels [level(s), level(parent(s))].
     std::vector<idx> upd_off;
     idx upd_size = 0;
-    // Forward-solve update vectors u_s (d x nrhs) use the same lifetimes with
-    // unit size d: offsets here are scaled by nrhs at solve time.
+    // Forward-solve update vectors u_s (d x nrhs), unit size d: offsets here are
+    // scaled by nrhs at solve time. Supernodes at levels <= solve_cut are solved
+    // by whole subtrees (contiguous postorder ranges [sub_lo, sub_hi], largest
+    // work first, fronts of at most sub_fmax rows), so their u_s live from the
+    // start of the solve until their parent's level.
     std::vector<idx> sol_off;
     idx sol_size = 0;
+    idx solve_cut = -1;
+    std::vector<idx> sub_lo, sub_hi;
+    idx sub_fmax = 0;
 
     // Conversion plan (CatamariConversionPlan.hh:402-541): entries grouped by
     // permuted analysis column, two buckets per column (transposed, copied).

@@ -550,7 +550,65 @@ std::string analyze(idx nblocks, const idx *Ap, const idx *Ai, int bs, const idx
         total = arena.top;
     };
     plan_arena(true, S.upd_off, S.upd_size);
-    plan_arena(false, S.sol_off, S.sol_size);
+
+    // ---- subtree solve cut: the highest level whose subtrees are still many
+    // (>= kMinSubtrees, to fill the GPU) and small (fronts <= kSubFmax rows)
+    {
+        constexpr idx kMinSubtrees = 148, kSubFmax = 2048;
+        S.solve_cut = -1;
+        std::vector<idx> fmax_le(S.nlevels, 0);           // max front at levels <= l
+        for (idx s = 0; s < nsn; ++s) fmax_le[S.level[s]] = std::max(fmax_le[S.level[s]], S.f[s]);
+        for (idx l = 1; l < S.nlevels; ++l) fmax_le[l] = std::max(fmax_le[l], fmax_le[l - 1]);
+        for (idx l = S.nlevels - 2; l >= 0; --l) {
+            if (fmax_le[l] > kSubFmax) continue;
+            idx roots = 0;
+            for (idx s = 0; s < nsn; ++s)
+                if (S.level[s] <= l && (S.sn_parent[s] < 0 || S.level[S.sn_parent[s]] > l)) ++roots;
+            if (roots >= kMinSubtrees) {
+                S.solve_cut = l;
+                S.sub_fmax = fmax_le[l];
+                break;
+            }
+        }
+        if (S.solve_cut >= 0) {
+            // subtree of root s = [s - size(s) + 1, s] in postorder
+            std::vector<idx> size(nsn, 1);
+            for (idx s = 0; s < nsn; ++s)
+                if (S.sn_parent[s] >= 0) size[S.sn_parent[s]] += size[s];
+            std::vector<std::pair<double, idx>> work;
+            for (idx s = 0; s < nsn; ++s) {
+                if (S.level[s] > S.solve_cut) continue;
+                if (S.sn_parent[s] >= 0 && S.level[S.sn_parent[s]] <= S.solve_cut) continue;
+                double wk = 0;
+                for (idx t = s - size[s] + 1; t <= s; ++t) wk += double(S.f[t]) * double(S.w[t]);
+                work.push_back({wk, s});
+            }
+            std::sort(work.begin(), work.end(), [](const auto &a, const auto &b) {
+                return a.first > b.first || (a.first == b.first && a.second < b.second);
+            });
+            for (const auto &pw : work) {
+                S.sub_lo.push_back(pw.second - size[pw.second] + 1);
+                S.sub_hi.push_back(pw.second);
+            }
+        }
+    }
+    // ---- solve arena: as the update arena, except that subtree supernodes are
+    // allocated up front and kept at least until the levels above the cut
+    {
+        S.sol_off.assign(nsn, -1);
+        Arena arena;
+        std::vector<std::vector<idx>> release_at(S.nlevels + 2);
+        auto alloc_level = [&](idx s) { return S.level[s] <= S.solve_cut ? 0 : idx(S.level[s]); };
+        for (idx l = 0; l < S.nlevels; ++l) {
+            for (idx s : release_at[l]) arena.release(S.sol_off[s], S.d[s]);
+            for (idx s = 0; s < nsn; ++s) {
+                if (alloc_level(s) != l || S.d[s] == 0 || S.sn_parent[s] < 0) continue;
+                S.sol_off[s] = arena.alloc(S.d[s]);
+                release_at[std::max<idx>(S.level[S.sn_parent[s]] + 1, S.solve_cut + 1)].push_back(s);
+            }
+        }
+        S.sol_size = arena.top;
+    }
 
     // ---- conversion plan
     S.plan_ptr.assign(2 * nv + 1, 0);
