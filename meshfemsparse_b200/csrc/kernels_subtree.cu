@@ -14,9 +14,12 @@
 //            by the level kernels above the cut);
 //   backward (reverse postorder) v = [x(cols); x(struct rows)] (ancestors are
 //            final); v[0:w] -= L21^T x_struct; x = L11^{-T} v[0:w].
-// Same arithmetic order as the level kernels within a front; nothing is shared
-// between CTAs, so no flags are needed. Subtrees are assigned round-robin in
-// order of decreasing work.
+// The next front's panel (ld x w, contiguous) is copied into shared memory with
+// cp.async while the current one is solved (panels up to kPanelStageBytes;
+// bigger ones are read from global memory). Fronts factored in shared memory
+// (no stored inverse) are substituted by one warp per right-hand side. Nothing
+// is shared between CTAs, so no flags are needed. Subtrees are assigned
+// round-robin in order of decreasing work.
 #include "device.h"
 
 #include <algorithm>
@@ -28,6 +31,26 @@ namespace {
 constexpr int kSubThreads = 256;
 constexpr int kSubRhs = 4;                 // right-hand sides per pass (more are looped)
 constexpr int kSubRed = 4 * kSubRhs * 64;  // split-k partials of a 64-row block
+constexpr int kPanelStageBytes = 8192;     // per staging buffer (two buffers); larger ones cost occupancy
+
+__device__ __forceinline__ void sub_cp16(void *dst_smem, const void *src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void sub_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void sub_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Panel of s staged into buf when it fits (ld x w elements are contiguous and
+// 16-byte aligned); returns whether it was staged.
+template <typename T>
+__device__ __forceinline__ bool stage_panel(int s, const SnDev &sd, const T *factor, T *buf) {
+    const int64_t n = int64_t(sd.ld[s]) * sd.w[s];
+    if (n * int64_t(sizeof(T)) > kPanelStageBytes) return false;
+    const T *src = factor + sd.pan_off[s];
+    constexpr int E = 16 / int(sizeof(T));
+    for (int q = threadIdx.x; q * E < n; q += blockDim.x) sub_cp16(buf + q * E, src + q * E);
+    return true;
+}
 
 template <int VB>
 __device__ __forceinline__ int crel(const int32_t *rel, int i, int vb) {
@@ -43,11 +66,11 @@ __device__ __forceinline__ double warp_sum(double x) {
 
 // ------------------------------------------------------------------ forward
 template <typename T, int VB>
-__device__ __forceinline__ void fwd_front(int s, const SnDev &sd, const T *__restrict__ factor, double *__restrict__ X, int64_t ldx,
-                          int nrhs, int rg, int nr, double *__restrict__ sol, double *v, double *red) {
-    const int tid = threadIdx.x, nt = blockDim.x;
+__device__ __forceinline__ void fwd_front(int s, const SnDev &sd, const T *__restrict__ factor, const T *pan,
+                                          double *__restrict__ X, int64_t ldx, int nrhs, int rg, int nr,
+                                          double *__restrict__ sol, double *v, double *red) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     const int w = sd.w[s], d = sd.d[s], f = w + d, c0 = sd.col0[s], ld = sd.ld[s];
-    const T *pan = factor + sd.pan_off[s];
     for (int q = tid; q < nr * f; q += nt) {
         const int r = q / f, i = q - r * f;
         v[q] = i < w ? X[c0 + i + int64_t(rg + r) * ldx] : 0.0;
@@ -128,17 +151,15 @@ __device__ __forceinline__ void fwd_front(int s, const SnDev &sd, const T *__res
             for (int r = 0; r < kSubRhs; ++r)
                 if (r < nr) v[r * f + w + k] -= acc[r];
         }
-    } else {
-        // column substitution over the whole front (y and u together)
+    } else if (warp < nr) {
+        // column substitution over the whole front (y and u together), warp r for rhs r
+        double *vr = v + warp * f;
         for (int j = 0; j < w; ++j) {
-            if (tid < nr) v[tid * f + j] /= double(pan[int64_t(j) * ld + j]);
-            __syncthreads();
-            const int m = f - j - 1;
-            for (int q = tid; q < nr * m; q += nt) {
-                const int r = q / m, i = j + 1 + (q - r * m);
-                v[r * f + i] -= double(pan[int64_t(j) * ld + i]) * v[r * f + j];
-            }
-            __syncthreads();
+            const double y = vr[j] / double(pan[int64_t(j) * ld + j]);
+            __syncwarp();
+            if (lane == 0) vr[j] = y;
+            for (int i = j + 1 + lane; i < f; i += 32) vr[i] -= double(pan[int64_t(j) * ld + i]) * y;
+            __syncwarp();
         }
     }
     __syncthreads();
@@ -153,11 +174,10 @@ __device__ __forceinline__ void fwd_front(int s, const SnDev &sd, const T *__res
 
 // ------------------------------------------------------------------ backward
 template <typename T, int VB>
-__device__ __forceinline__ void bwd_front(int s, const SnDev &sd, const T *__restrict__ factor, double *__restrict__ X, int64_t ldx,
-                          int rg, int nr, double *v) {
+__device__ __forceinline__ void bwd_front(int s, const SnDev &sd, const T *__restrict__ factor, const T *pan,
+                                          double *__restrict__ X, int64_t ldx, int rg, int nr, double *v) {
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     const int w = sd.w[s], d = sd.d[s], f = w + d, c0 = sd.col0[s], ld = sd.ld[s];
-    const T *pan = factor + sd.pan_off[s];
     const int32_t *rows = sd.struct_rows + sd.struct_ptr[s];
     const int vb = sd.vb;
     for (int q = tid; q < nr * f; q += nt) {
@@ -171,8 +191,10 @@ __device__ __forceinline__ void bwd_front(int s, const SnDev &sd, const T *__res
         v[q] = X[gi + int64_t(rg + r) * ldx];
     }
     __syncthreads();
-    // v[0:w] -= L21^T x_struct: one warp per column, lanes over rows
-    if (d > 0) {
+    const int64_t inv = sd.inv_off[s];
+    // v[0:w] -= L21^T x_struct: one warp per column, lanes over rows (fronts with
+    // inverses; the substitution below covers the struct rows otherwise)
+    if (d > 0 && inv >= 0) {
         for (int j = warp; j < w; j += nw) {
             double acc[kSubRhs] = {0.0, 0.0, 0.0, 0.0};
             for (int k = lane; k < d; k += 32) {
@@ -189,7 +211,6 @@ __device__ __forceinline__ void bwd_front(int s, const SnDev &sd, const T *__res
         }
         __syncthreads();
     }
-    const int64_t inv = sd.inv_off[s];
     if (inv >= 0) {
         const int nbw = (w + 63) / 64;
         for (int rb = nbw - 1; rb >= 0; --rb) {
@@ -242,18 +263,19 @@ __device__ __forceinline__ void bwd_front(int s, const SnDev &sd, const T *__res
                 __syncthreads();
             }
         }
-    } else {
-        // column-oriented backward substitution: x_j = v_j / L_jj, then v_i -= L(j, i) x_j (i < j)
+    } else if (warp < nr) {
+        // left-looking backward substitution, warp r for rhs r:
+        // x_j = (v_j - sum_{i > j} L(i, j) x_i) / L_jj over front rows i (struct rows included)
+        double *vr = v + warp * f;
         for (int j = w - 1; j >= 0; --j) {
-            if (tid < nr) v[tid * f + j] /= double(pan[int64_t(j) * ld + j]);
-            __syncthreads();
-            for (int q = tid; q < nr * j; q += nt) {
-                const int r = q / j, i = q - r * j;
-                v[r * f + i] -= double(pan[int64_t(i) * ld + j]) * v[r * f + j];
-            }
-            __syncthreads();
+            double acc = 0.0;
+            for (int i = j + 1 + lane; i < f; i += 32) acc += double(pan[int64_t(j) * ld + i]) * vr[i];
+            acc = warp_sum(acc);
+            if (lane == 0) vr[j] = (vr[j] - acc) / double(pan[int64_t(j) * ld + j]);
+            __syncwarp();
         }
     }
+    __syncthreads();
     for (int q = tid; q < nr * w; q += nt) {
         const int r = q / w, j = q - r * w;
         X[c0 + j + int64_t(rg + r) * ldx] = v[r * f + j];
@@ -266,13 +288,28 @@ __global__ void __launch_bounds__(kSubThreads) subtree_fwd_kernel(const int2 *__
                                                                   const T *__restrict__ factor, double *X, int64_t ldx,
                                                                   int nrhs, double *sol) {
     extern __shared__ __align__(16) double sub_smem[];
-    double *red = sub_smem;
-    double *v = sub_smem + kSubRed;
+    T *pbuf = reinterpret_cast<T *>(sub_smem);                       // 2 staging buffers
+    double *red = sub_smem + 2 * kPanelStageBytes / 8;
+    double *v = red + kSubRed;
     for (int k = blockIdx.x; k < nsub; k += gridDim.x) {
         const int2 sr = subs[k];
         for (int rg = 0; rg < nrhs; rg += kSubRhs) {
             const int nr = min(kSubRhs, nrhs - rg);
-            for (int s = sr.x; s <= sr.y; ++s) fwd_front<T, VB>(s, sd, factor, X, ldx, nrhs, rg, nr, sol, v, red);
+            constexpr int PB = kPanelStageBytes / int(sizeof(T));
+            bool staged = stage_panel(sr.x, sd, factor, pbuf);
+            sub_commit();
+            for (int s = sr.x; s <= sr.y; ++s) {
+                const int b = (s - sr.x) & 1;
+                const bool next = s < sr.y && stage_panel(s + 1, sd, factor, pbuf + (b ^ 1) * PB);
+                sub_commit();
+                sub_wait1();
+                __syncthreads();
+                const T *pan = staged ? pbuf + b * PB : factor + sd.pan_off[s];
+                fwd_front<T, VB>(s, sd, factor, pan, X, ldx, nrhs, rg, nr, sol, v, red);
+                staged = next;
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            __syncthreads();
         }
     }
 }
@@ -282,12 +319,27 @@ __global__ void __launch_bounds__(kSubThreads) subtree_bwd_kernel(const int2 *__
                                                                   const T *__restrict__ factor, double *X, int64_t ldx,
                                                                   int nrhs) {
     extern __shared__ __align__(16) double sub_smem[];
-    double *v = sub_smem + kSubRed;
+    T *pbuf = reinterpret_cast<T *>(sub_smem);
+    double *v = sub_smem + 2 * kPanelStageBytes / 8 + kSubRed;
     for (int k = blockIdx.x; k < nsub; k += gridDim.x) {
         const int2 sr = subs[k];
         for (int rg = 0; rg < nrhs; rg += kSubRhs) {
             const int nr = min(kSubRhs, nrhs - rg);
-            for (int s = sr.y; s >= sr.x; --s) bwd_front<T, VB>(s, sd, factor, X, ldx, rg, nr, v);
+            constexpr int PB = kPanelStageBytes / int(sizeof(T));
+            bool staged = stage_panel(sr.y, sd, factor, pbuf);
+            sub_commit();
+            for (int s = sr.y; s >= sr.x; --s) {
+                const int b = (sr.y - s) & 1;
+                const bool next = s > sr.x && stage_panel(s - 1, sd, factor, pbuf + (b ^ 1) * PB);
+                sub_commit();
+                sub_wait1();
+                __syncthreads();
+                const T *pan = staged ? pbuf + b * PB : factor + sd.pan_off[s];
+                bwd_front<T, VB>(s, sd, factor, pan, X, ldx, rg, nr, v);
+                staged = next;
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            __syncthreads();
         }
     }
 }
@@ -304,7 +356,9 @@ int sub_sm_count() {
 
 }  // namespace
 
-size_t subtree_smem_bytes(int fmax) { return (size_t(kSubRed) + size_t(kSubRhs) * fmax) * sizeof(double); }
+size_t subtree_smem_bytes(int fmax) {
+    return size_t(2) * kPanelStageBytes + (size_t(kSubRed) + size_t(kSubRhs) * fmax) * sizeof(double);
+}
 
 template <typename T>
 void launch_subtree_solve(bool forward, const int2 *subs, int nsub, int fmax, SnDev sd, const T *factor, double *X,
