@@ -194,7 +194,10 @@ typedef struct {
     int64_t kernel_launches;     /* kernels launched by the library since it was loaded */
     int32_t perturbed_pivots;    /* FP32 factor under refinement: non-positive pivots replaced by a
                                     floor relative to the injected diagonal (last numeric) */
+    int32_t pcg_iterations;      /* iterations of the last mfs_pcg_solve (max over RHS) */
+    int32_t pcg_fallback;        /* 1: the last mfs_pcg_solve missed the tolerance and used the factor */
     int32_t reserved_stats;
+    double pcg_ms;               /* device time of the last converged mfs_pcg_solve (inference + PCG) */
 } mfs_stats;
 mfs_status mfs_get_stats(const mfs_handle *h, mfs_stats *st);
 

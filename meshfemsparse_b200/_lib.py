@@ -25,7 +25,8 @@ EXPORTED = [
     "mfs_numeric", "mfs_solve", "mfs_assembly_setup", "mfs_assemble", "mfs_apply", "mfs_info",
     "mfs_inverse_permutation", "mfs_nd_ordering", "mfs_supernodes", "mfs_conversion_plan", "mfs_factor_values",
     "mfs_stash", "mfs_swap_stash", "mfs_clear_stash", "mfs_has_stash", "mfs_clear_factors", "mfs_get_stats",
-    "mfs_set_options", "mfs_apply_noalloc",
+    "mfs_set_options", "mfs_apply_noalloc", "mfs_lpc_param_count", "mfs_lpc_create", "mfs_lpc_destroy",
+    "mfs_lpc_get_weights", "mfs_lpc_set_weights", "mfs_lpc_loss_grad", "mfs_lpc_train_step", "mfs_pcg_solve",
 ]
 
 
@@ -44,7 +45,8 @@ class Stats(C.Structure):
         ("factor_ms", C.c_double), ("solve_ms", C.c_double), ("assemble_ms", C.c_double),
         ("refine_iterations", C.c_int32), ("failed_column", C.c_int32), ("residual", C.c_double),
         ("device_bytes", C.c_int64), ("num_levels", C.c_int32), ("num_large", C.c_int32),
-        ("kernel_launches", C.c_int64), ("perturbed_pivots", C.c_int32), ("reserved_stats", C.c_int32),
+        ("kernel_launches", C.c_int64), ("perturbed_pivots", C.c_int32), ("pcg_iterations", C.c_int32),
+        ("pcg_fallback", C.c_int32), ("reserved_stats", C.c_int32), ("pcg_ms", C.c_double),
     ]
 
 
@@ -84,6 +86,17 @@ def load() -> C.CDLL:
         getattr(lib, name).argtypes = [P]
     lib.mfs_has_stash.argtypes = [P, C.POINTER(C.c_int32)]
     lib.mfs_get_stats.argtypes = [P, C.POINTER(Stats)]
+    f32p = C.POINTER(C.c_float)
+    lib.mfs_lpc_param_count.argtypes = [i64p]
+    lib.mfs_lpc_create.argtypes = [C.POINTER(P), C.c_int32, C.c_uint64]
+    lib.mfs_lpc_destroy.argtypes = [P]
+    lib.mfs_lpc_get_weights.argtypes = [P, f32p, C.c_int64]
+    lib.mfs_lpc_set_weights.argtypes = [P, f32p, C.c_int64]
+    lib.mfs_lpc_loss_grad.argtypes = [P, P, P, P, P, C.c_int64, C.c_int64, C.c_int32, C.POINTER(C.c_double), f32p]
+    lib.mfs_lpc_train_step.argtypes = [P, P, P, P, P, C.c_int64, C.c_int64, C.c_int32, C.c_float,
+                                       C.POINTER(C.c_double)]
+    lib.mfs_pcg_solve.argtypes = [P, P, P, P, P, C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_double,
+                                  C.POINTER(C.c_int32)]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib

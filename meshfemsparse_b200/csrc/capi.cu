@@ -4,6 +4,7 @@
 // kernels_factor.cu / kernels_solve.cu.
 #include "../../include/mfs_b200.h"
 #include "device.h"
+#include "handle.h"
 #include "host_symbolic.h"
 
 #include <cuda_runtime.h>
@@ -21,196 +22,12 @@
 #include <vector>
 
 namespace mfs {
-
 long long g_kernel_launches = 0;
-
-struct CudaError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-struct StatusError : std::runtime_error {
-    mfs_status status;
-    StatusError(mfs_status s, const std::string &m) : std::runtime_error(m), status(s) {}
-};
-
-#define MFS_CUDA(call)                                                                                   \
-    do {                                                                                                 \
-        cudaError_t _e = (call);                                                                         \
-        if (_e != cudaSuccess)                                                                           \
-            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(_e));                         \
-    } while (0)
-
-#define MFS_LAUNCHED() MFS_CUDA(cudaGetLastError())
-
-template <typename T>
-struct DBuf {
-    T *p = nullptr;
-    size_t n = 0;
-    DBuf() = default;
-    DBuf(const DBuf &) = delete;
-    DBuf &operator=(const DBuf &) = delete;
-    ~DBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    void ensure(size_t count) {
-        if (count <= n && p) return;
-        release();
-        size_t c = std::max<size_t>(count, 1);
-        cudaError_t e = cudaMalloc(&p, c * sizeof(T));
-        if (e != cudaSuccess) {
-            p = nullptr;
-            throw StatusError(MFS_OOM, std::string("cudaMalloc of ") + std::to_string(c * sizeof(T)) +
-                                           " bytes failed: " + cudaGetErrorString(e));
-        }
-        n = c;
-    }
-    template <typename U>
-    void upload(const std::vector<U> &v, cudaStream_t st) {
-        ensure(v.size());
-        if (v.empty()) return;
-        std::vector<T> tmp(v.begin(), v.end());
-        MFS_CUDA(cudaMemcpyAsync(p, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-        MFS_CUDA(cudaStreamSynchronize(st));
-    }
-    size_t bytes() const { return n * sizeof(T); }
-};
-
-
-struct LevelPlan {
-    int small_off = 0, small_count = 0, small_max_front = 0;
-    int all_off = 0, all_count = 0, all_max_front = 0;
-    int large_count = 0;
-    int asm_off = 0, asm_n = 0, asm_tiles = 0;
-    struct Step {
-        int left_off, left_n, left_tiles;   // the block's columns updated by the earlier blocks of its group
-        int potrf_off, potrf_n, potrf_maxnb;
-        int trsm_off, trsm_n, trsm_tiles;   // X := X inv(L)^T of the rows below the block
-        int gemm_off, gemm_n, gemm_tiles;   // trailing update of the columns after a finished group
-    };
-    std::vector<Step> steps;
-    int syrk_off = 0, syrk_n = 0, syrk_tiles = 0;
-    // solve task lists of this level
-    int sasm_off = 0, sasm_n = 0, sasm_tiles = 0;
-    int ftri_off = 0, ftri_n = 0;
-    int btri_off = 0, btri_n = 0;
-    int fstr_off = 0, fstr_n = 0, fred_off = 0, fred_n = 0;
-    int bstr_off = 0, bstr_n = 0, bred_off = 0, bred_n = 0;
-};
-
-struct DevSym {
-    std::shared_ptr<Symbolic> S;
-    DBuf<int32_t> w, d, f, ld, col0, child_ptr, child_list, struct_rows, rel, small_list, all_list;
-    DBuf<int64_t> pan_off, upd_off, sol_off, struct_ptr, diag_off;
-    DBuf<int64_t> inv_off;               // 64 x 64 diagonal inverses of large fronts (-1: none)
-    DBuf<PlanEntryDev> plan;
-    DBuf<AssembleTask> asm_tasks;
-    DBuf<PanelTask> potrf_tasks;
-    DBuf<GemmTask> gemm_tasks;
-    DBuf<SolveAsmTask> sasm_tasks;
-    DBuf<SolveTask> ftri_tasks, btri_tasks;
-    DBuf<StrTask> fstr_tasks, bstr_tasks;
-    DBuf<StrReduce> fred, bred;
-    int max_str_tasks = 0;
-    DBuf<int2> subs;                     // subtree ranges solved one per CTA (levels <= solve_cut)
-    int nsub = 0, sub_fmax = 0, solve_cut = -1;
-    DBuf<int> flags;                     // one per 64-row diagonal block of every front
-    DBuf<int64_t> spmv_ptr, spmv_src;
-    DBuf<int32_t> spmv_col, spmv_flag;
-    DBuf<int64_t> prrfr, sperm;
-    std::vector<LevelPlan> levels;
-    SnDev sd{};
-    int64_t ax_len = 0;
-    std::vector<int64_t> Ap_full, Ai_full;   // caller's pattern (for the element slot map)
-    int num_large = 0;
-    int64_t inv_scratch = 0;             // elements of the block inverses of one column-block step
-    int64_t factor_alloc = 0;            // panels followed by the diagonal inverses
-    std::vector<int64_t> dpan;           // device panel offsets (leading dimension padded to 4)
-    std::vector<int32_t> dld;            // device panel leading dimensions
-    int64_t panel_alloc = 0;             // elements of the padded panels
-    size_t bytes() const {
-        return w.bytes() * 5 + col0.bytes() + child_ptr.bytes() + child_list.bytes() + struct_rows.bytes() +
-               rel.bytes() + small_list.bytes() + all_list.bytes() + pan_off.bytes() + upd_off.bytes() +
-               sol_off.bytes() + struct_ptr.bytes() + diag_off.bytes() + inv_off.bytes() + plan.bytes() + asm_tasks.bytes() +
-               potrf_tasks.bytes() + gemm_tasks.bytes() + spmv_ptr.bytes() +
-               spmv_src.bytes() + spmv_col.bytes() + spmv_flag.bytes() + prrfr.bytes() + sperm.bytes();
-    }
-};
-
-struct State {
-    std::shared_ptr<DevSym> sym;
-    std::shared_ptr<DBuf<double>> f64;
-    std::shared_ptr<DBuf<float>> f32;
-    std::shared_ptr<DBuf<double>> ax, bx;   // values the numeric factor was computed from
-    int type = 0;   // 0 none, 1 symbolic, 2 numeric
-    double sigma = 0.0;
-};
-
 }  // namespace mfs
 
 using namespace mfs;
 
-struct mfs_handle {
-    mfs_options opt{};
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    State cur, stash;
-    bool has_stash = false;
-    DBuf<double> upd64;            // update arena (multifrontal Schur complements)
-    DBuf<float> upd32;
-    DBuf<double> dscr64;           // inverses of the diagonal blocks of one column-block step
-    DBuf<float> dscr32;
-    DBuf<double> sol;
-    std::shared_ptr<DBuf<double>> asm_ax;   // output of the last mfs_assemble (device resident)
-    std::shared_ptr<DBuf<double>> asm_spare;   // an earlier assembly buffer, reused once nothing holds it
-    DBuf<double> rhs, work_r, work_z, work_p, work_ap, work_x, work_s, io;
-    DBuf<double> partials, dots;
-    DBuf<int> active;
-    DBuf<int> fail;
-    DBuf<int> perturbed;          // pivots perturbed in the last numeric factorization
-    DBuf<double> dorig;           // injected diagonal (perturbation reference)
-    DBuf<int> solve_err;          // set by a solve kernel whose dependency wait timed out
-    DBuf<int> gemm_err;           // set by a tensor-core GEMM whose pipeline wait timed out
-    DBuf<double> str_partials;    // chunk partial sums of the solve structure phases (scratch)
-    int *fail_host = nullptr;
-    double *dots_host = nullptr;
-    // assembly
-    DBuf<int64_t> slot_ptr, contrib;
-    int64_t nslots = 0, nelem = 0;
-    DBuf<double> ke;
-    std::string err;
-    mfs_stats stats{};
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-};
-
 namespace {
-
-void set_device(mfs_handle *h) {
-    if (h->opt.device < 0) throw StatusError(MFS_INVALID_ARG, "analysis-only handle (device -1) has no GPU state");
-    MFS_CUDA(cudaSetDevice(h->opt.device));
-}
-
-template <typename F>
-mfs_status guarded(mfs_handle *h, F &&fn) {
-    try {
-        fn();
-        if (h) h->err.clear();
-        return MFS_OK;
-    } catch (const StatusError &e) {
-        if (h) h->err = e.what();
-        return e.status;
-    } catch (const CudaError &e) {
-        if (h) h->err = e.what();
-        return MFS_CUDA_ERROR;
-    } catch (const std::bad_alloc &e) {
-        if (h) h->err = "host allocation failed";
-        return MFS_OOM;
-    } catch (const std::exception &e) {
-        if (h) h->err = e.what();
-        return MFS_INTERNAL;
-    }
-}
 
 int small_front_limit(const mfs_handle *h) {
     if (h->opt.small_front_max > 0) return h->opt.small_front_max;
