@@ -150,6 +150,39 @@ mfs_status mfs_apply(mfs_handle *h, const double *x, double *y, int64_t nrhs, in
  * that overlap on the GPU (other handles, other streams) race and must be
  * serialised by the caller. Returns after the result is written. */
 mfs_status mfs_apply_noalloc(mfs_handle *h, const double *x, double *y, int64_t nrhs, int64_t ld, int32_t flags);
+
+/* ---- Learned preconditioner (no counterpart in the reference). A 4-layer
+ * message-passing network (hidden 64, BF16 weights, FP32 accumulation) reads the
+ * Jacobi-scaled 3 x 3 blocks of H and emits a lower block-triangular G on H's
+ * pattern; mfs_pcg_solve runs PCG with M^{-1} = D^{-1/2} G^T G D^{-1/2}
+ * (D = diag H) and falls back to the Cholesky factor (mfs_numeric + mfs_solve on
+ * the same values) when PCG misses `tol` within `maxit` iterations. Needs a 3 x 3
+ * block analysis (block size 3, whole-block pins). A network lives on one device
+ * and may serve many handles on that device; it is not re-entrant. */
+typedef struct mfs_lpc mfs_lpc;
+mfs_status mfs_lpc_param_count(int64_t *count);
+/* Weights drawn from `seed`; the output head starts at zero, so G = I (Jacobi). */
+mfs_status mfs_lpc_create(mfs_lpc **net, int32_t device, uint64_t seed);
+mfs_status mfs_lpc_destroy(mfs_lpc *net);
+/* FP32 master weights (host arrays of mfs_lpc_param_count floats); setting them
+ * resets the optimizer state. */
+mfs_status mfs_lpc_get_weights(const mfs_lpc *net, float *w, int64_t count);
+mfs_status mfs_lpc_set_weights(mfs_lpc *net, const float *w, int64_t count);
+/* Loss mean_r ||M^{-1} b_r - x_r||_H^2 / (x_r^T b_r) of pairs (B, X = H^{-1} B) and
+ * its gradient (host, param_count floats; NULL to skip). Ax: matrix values in the
+ * caller's block-CSC layout, NULL = the last mfs_assemble; flags as mfs_solve
+ * (vector order | MFS_DEVICE_POINTERS, which also covers Ax). nrhs <= 64. */
+mfs_status mfs_lpc_loss_grad(mfs_handle *h, mfs_lpc *net, const double *Ax, const double *B, const double *X,
+                             int64_t nrhs, int64_t ld, int32_t flags, double *loss, float *grad);
+/* One Adam step (beta 0.9 / 0.999) of the loss above at learning rate lr. */
+mfs_status mfs_lpc_train_step(mfs_handle *h, mfs_lpc *net, const double *Ax, const double *B, const double *X,
+                              int64_t nrhs, int64_t ld, int32_t flags, float lr, double *loss);
+/* X = H^{-1} B by PCG to relative residual tol (per column) within maxit
+ * iterations (<= 0: 200); net NULL = Jacobi. On a miss the handle factors Ax and
+ * solves (its own precision and refinement options); mfs_stats.pcg_fallback says
+ * which ran. *iterations = PCG iterations taken. */
+mfs_status mfs_pcg_solve(mfs_handle *h, mfs_lpc *net, const double *Ax, const double *B, double *X, int64_t nrhs,
+                         int64_t ld, int32_t flags, int32_t maxit, double tol, int32_t *iterations);
 /* Conversion-plan entries are exported as 4 int64 each: (dst, src, ld, flags);
  * flags bit0 = source block transposed, bit1 = diagonal block (lower part only). */
 
