@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--tc", type=int, default=0, help="FP32 Schur updates: 0 auto, 1 TF32, 2 split 3xTF32")
     p.add_argument("--maxit", type=int, default=50, help="refinement iteration cap")
     p.add_argument("--cpu-budget", type=float, default=2.5e11, help="flops of the CPU factorization sample")
+    p.add_argument("--train-hessians", type=int, default=10, help="config 4: Hessians of the training set")
+    p.add_argument("--train-steps", type=int, default=300, help="config 4: Adam steps before timing")
     return p.parse_args()
 
 
@@ -261,6 +263,181 @@ def run_b200(args, rank, world, local, dist):
         print(json.dumps(result), flush=True)
 
 
+# ------------------------------------------------- config 4: learned PCG on a Newton sequence
+def run_newton_sequence(args, rank, world, local, dist):
+    """Learned-PCG form on the 30-step load ramp, beside FP32+refine and FP64 plain.
+
+    Untimed: the network is trained on `--train-hessians` Hessians at seeded random
+    loads (20 right-hand sides each, solutions from the FP64 factor). Timed: `--steps`
+    load steps of the ramp (each its own Hessian, resident on the device); one step =
+    assemble -> PCG with the learned G (cap 200, tolerance 1e-10) -> Cholesky fallback
+    (FP32 factor + FP64 refinement) when PCG misses."""
+    import torch
+    from meshfemsparse_b200 import B200Factorizer, _lib, workloads
+    from meshfemsparse_b200.learned import LearnedPreconditioner
+
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    lib = _lib.load()
+    D = _lib.MFS_DEVICE_POINTERS
+    FULL = _lib.MFS_SOLVE_FULL
+    t0 = time.time()
+    seq = workloads.newton_sequence(k=args.k or 48, final_hessians=False)
+    wl = seq.wl
+    n_full, nrhs = wl.n_full, wl.nrhs
+    stream = torch.cuda.current_stream()
+
+    def make(single):
+        f = B200Factorizer(single, refine=single, stream=stream.cuda_stream, device=local, refine_maxit=args.maxit)
+        f.factorizeSymbolic(wl.H, wl.pins)
+        f.setElements(wl.tets)
+        return f
+
+    f32, f64 = make(True), make(False)
+    rng = np.random.default_rng(44)
+    keep = np.ones(n_full, dtype=bool)
+    keep[wl.pins] = False
+    # ---- training data from the FP64 factor
+    train = []
+    for i in range(args.train_hessians):
+        Ke = torch.from_numpy(seq.hessians(float(rng.uniform(0.0, seq.max_strain)), seed=1000 + i,
+                                           device=dev).reshape(-1)).to(dev)
+        Ax = torch.empty(int(f64._axlen), dtype=torch.float64, device=dev)
+        _lib.check(lib.mfs_assemble(f64._h, C.c_void_p(Ke.data_ptr()), C.c_void_p(Ax.data_ptr()), D), f64._h, "asm")
+        _lib.check(lib.mfs_numeric(f64._h, None, None, 0.0, 0), f64._h, "numeric")
+        Bh = rng.normal(size=(20, n_full))
+        Bh[:, ~keep] = 0.0
+        B = torch.from_numpy(Bh).to(dev)
+        X = torch.empty_like(B)
+        _lib.check(lib.mfs_solve(f64._h, C.c_void_p(B.data_ptr()), C.c_void_p(X.data_ptr()), 20, n_full, FULL | D),
+                   f64._h, "solve")
+        train.append((Ax, B, X))
+        del Ke
+    t_data = time.time() - t0
+    net = LearnedPreconditioner(device=local, seed=4)
+    torch.cuda.synchronize()
+    t1 = time.time()
+    losses = []
+    for it in range(args.train_steps):
+        Ax, B, X = train[it % len(train)]
+        losses.append(net.train_step(f32, B.data_ptr(), X.data_ptr(), lr=2e-3, Ax=Ax.data_ptr(),
+                                     device_pointers=True, nrhs=20, ld=n_full))
+    torch.cuda.synchronize()
+    t_train = time.time() - t1
+    del train
+    # ---- the timed load steps (Hessians resident on the device)
+    K = args.steps
+    ts = [int(round(seq.steps * (i + 1) / K)) for i in range(K)]
+    Kes = [torch.from_numpy(seq.hessians(seq.strain(t), device=dev).reshape(-1)).to(dev) for t in ts]
+    B = torch.from_numpy(np.ascontiguousarray(wl.rhs.T)).to(dev)
+    X = torch.empty_like(B)
+    it_c = C.c_int32()
+
+    def step_pcg(f, Ke, netp, Bp, Xp, flags):
+        _lib.check(lib.mfs_assemble(f._h, Ke, None, flags), f._h, "assemble")
+        _lib.check(lib.mfs_pcg_solve(f._h, netp, None, Bp, Xp, nrhs, n_full, FULL | flags, 200, 1e-10,
+                                     C.byref(it_c)), f._h, "pcg")
+        st = f.stats()
+        return int(it_c.value), bool(st["pcg_fallback"])
+
+    def step_factor(f, Ke, Bp, Xp, flags):
+        _lib.check(lib.mfs_assemble(f._h, Ke, None, flags), f._h, "assemble")
+        _lib.check(lib.mfs_numeric(f._h, None, None, 0.0, 0), f._h, "numeric")
+        _lib.check(lib.mfs_solve(f._h, Bp, Xp, nrhs, n_full, FULL | flags), f._h, "solve")
+        return f.stats()["refine_iterations"], False
+
+    def run(fn, W, sample_clocks=False):
+        for i in range(W):
+            fn(i % K)
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        l0 = f32.stats()["kernel_launches"]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        info = [fn(i) for i in range(K)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = f32.stats()["kernel_launches"] - l0
+        clocks = sampler.stop() if sampler else None
+        total = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([total], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        return total / K, info, launches, clocks
+
+    pB, pX = C.c_void_p(B.data_ptr()), C.c_void_p(X.data_ptr())
+    ms_l, info_l, launches, clocks = run(lambda i: step_pcg(f32, C.c_void_p(Kes[i].data_ptr()), net._p, pB, pX, D),
+                                         args.warmup, sample_clocks=True)
+
+    def residual(f):
+        Y = torch.empty_like(X)
+        _lib.check(lib.mfs_apply(f._h, pX, C.c_void_p(Y.data_ptr()), nrhs, n_full, FULL | D), f._h, "apply")
+        m = torch.from_numpy(keep).to(dev)
+        R = (B - Y)[:, m]
+        return float((R.norm(dim=1) / B[:, m].norm(dim=1)).max().item())
+
+    res_l = residual(f32)
+    ms_j, info_j, _, _ = run(lambda i: step_pcg(f32, C.c_void_p(Kes[i].data_ptr()), None, pB, pX, D), 1)
+    ms_32, info_32, _, _ = run(lambda i: step_factor(f32, C.c_void_p(Kes[i].data_ptr()), pB, pX, D), 1)
+    res_32 = residual(f32)
+    ms_64, _, _, _ = run(lambda i: step_factor(f64, C.c_void_p(Kes[i].data_ptr()), pB, pX, D), 1)
+    res_64 = residual(f64)
+    # e2e of the learned form through host (pinned) buffers
+    Ke_h = [k.cpu().pin_memory() for k in Kes[:min(K, 3)]]
+    B_h = B.cpu().pin_memory()
+    X_h = torch.empty_like(B_h).pin_memory()
+    Ke_bytes = Kes[0].numel() * 8
+    del Kes
+    torch.cuda.empty_cache()
+    Ke2 = Ke_h
+    K2 = len(Ke2)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(K2):
+        step_pcg(f32, C.c_void_p(Ke2[i].data_ptr()), net._p, C.c_void_p(B_h.data_ptr()), C.c_void_p(X_h.data_ptr()), 0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / K2
+
+    peaks, peak_kind = measured_peaks()
+    result = {
+        "metric": METRIC, "value": world * 1000.0 / ms_l, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": ms_l, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 network / f64 PCG", "data": "synthetic",
+        "config": {"workload": f"config4:{wl.name}", "n_free_dofs": f32.n_reduced(), "tets": int(wl.tets.shape[0]),
+                   "nrhs": nrhs, "parallelism": f"replicas{world}", "load_steps_timed": ts,
+                   "l2": "inputs larger than L2 (element Hessians %.2f GB per step)" % (Ke_bytes / 1e9),
+                   **wl.info},
+        "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(Ke_bytes + B.numel() * 8),
+                "d2h_bytes_per_step": int(B.numel() * 8)},
+        "gpu_launches": int(launches), "clocks": clocks,
+        "roofline": None,
+        "residual": res_l,
+        "learned_pcg": {"iterations": [i for i, _ in info_l], "fallbacks": int(sum(fb for _, fb in info_l)),
+                        "cap": 200},
+        "jacobi_pcg": {"solves_per_s": 1000.0 / ms_j, "iterations": [i for i, _ in info_j],
+                       "fallbacks": int(sum(fb for _, fb in info_j))},
+        "fp32_refine": {"solves_per_s": 1000.0 / ms_32, "refine_iterations": [i for i, _ in info_32],
+                        "residual": res_32},
+        "fp64_plain_solves_per_s": world * 1000.0 / ms_64, "fp64_plain_ms_per_step": ms_64, "fp64_residual": res_64,
+        "speedup_learned_pcg_vs_fp64_plain": ms_64 / ms_l, "speedup_fp32_refine_vs_fp64_plain": ms_64 / ms_32,
+        "training": {"hessians": args.train_hessians, "pairs": 20 * args.train_hessians, "steps": args.train_steps,
+                     "seconds": t_train, "data_seconds": t_data, "loss_first": float(np.mean(losses[:10])),
+                     "loss_last": float(np.mean(losses[-10:]))},
+        "peaks": peak_kind,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        wl.Ke = Ke2[-1].numpy().reshape(-1, 12, 12)
+        result["cpu_baseline"] = cpu_baseline(wl, f32, args)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
 # -------------------------------------------------------------- CPU legs
 def cpu_baseline(wl, f, args):
     """Oracle port (FP64 multifrontal + OpenBLAS, all host threads) on a bounded sample:
@@ -350,6 +527,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world, dist)
+        elif args.config == 4:
+            run_newton_sequence(args, rank, world, local, dist)
         else:
             run_b200(args, rank, world, local, dist)
     finally:

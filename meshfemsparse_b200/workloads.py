@@ -106,6 +106,61 @@ def config3(count: int = 256, seed: int = 3, dof_range=(1000, 50000)) -> Workloa
                     dict(count=count, sides=ks.tolist(), tets=int(tets.shape[0])))
 
 
+def compression_displacement(nodes: np.ndarray, strain: float, nu: float = 0.4, seed: int = 0,
+                             amplitude: float = 0.01) -> np.ndarray:
+    """Top-face compression by `strain` (z=0 fixed): u = s [nu (x-1/2) z, nu (y-1/2) z, -z]
+    plus a seeded smooth perturbation that grows with the load and vanishes at z=0. A
+    stand-in for the equilibrium states of the load ramp (the Hessians are inputs)."""
+    z = nodes[:, 2]
+    u = np.zeros_like(nodes)
+    u[:, 0] = nu * strain * (nodes[:, 0] - 0.5) * z
+    u[:, 1] = nu * strain * (nodes[:, 1] - 0.5) * z
+    u[:, 2] = -strain * z
+    pert = fem.fourier_displacement(nodes, amplitude=amplitude, modes=3, seed=seed)
+    return u + (strain / 0.2) * pert * z[:, None]
+
+
+@dataclass
+class NewtonSequence:
+    """Config 4: one mesh and material, Hessians that drift with the load on a fixed pattern."""
+    wl: Workload
+    E: np.ndarray
+    nu: float
+    steps: int
+    max_strain: float
+    seed: int
+
+    def strain(self, t: int) -> float:
+        return self.max_strain * t / self.steps
+
+    def hessians(self, strain: float, seed: int | None = None, device: str | None = None) -> np.ndarray:
+        u = compression_displacement(self.wl.nodes, strain, 0.4, self.seed if seed is None else seed)
+        return fem.neo_hookean_hessians(self.wl.nodes, self.wl.tets, u, self.E, self.nu, clamp=1e-8, device=device)
+
+
+def newton_sequence(k: int = 48, seed: int = 4, steps: int = 30, device: str | None = None,
+                    final_hessians: bool = True) -> NewtonSequence:
+    """48^3 cube, Neo-Hookean E log-uniform [0.1, 10], nu = 0.4, `steps` load steps of a
+    top-face compression ramp to 20%; one right-hand side per Newton step."""
+    nodes, tets = fem.tet_cube(k, jitter=0.0, seed=seed)
+    rng = np.random.default_rng(seed)
+    E = np.exp(rng.uniform(math.log(0.1), math.log(10.0), size=tets.shape[0]))
+    pins = fem.bottom_pins(nodes)
+    H = SystemAssembler(nodes.shape[0]).blockSparsityPattern(tets)
+    wl = Workload(f"cube{k}_neo_hookean_compression", nodes, tets, np.zeros((0, 12, 12)), pins, 1, H,
+                  _rhs(3 * nodes.shape[0], pins, 1, seed + 100),
+                  dict(k=k, tets=int(tets.shape[0]), material="Neo-Hookean E~logU[0.1,10] nu=0.4",
+                       load_steps=steps, max_strain=0.2))
+    seq = NewtonSequence(wl, E, 0.4, steps, 0.2, seed)
+    if final_hessians:
+        wl.Ke = seq.hessians(seq.strain(steps), device=device)
+    return seq
+
+
+def config4(k: int = 48, seed: int = 4, device: str | None = None) -> Workload:
+    return newton_sequence(k, seed, device=device).wl
+
+
 def build(cfg: int, k: int | None = None, device: str | None = None) -> Workload:
     if cfg == 1:
         return config1(k or 20)
@@ -113,6 +168,8 @@ def build(cfg: int, k: int | None = None, device: str | None = None) -> Workload
         return config2(k or 64, device=device)
     if cfg == 3:
         return config3()
+    if cfg == 4:
+        return config4(k or 48, device=device)
     if cfg == 5:
         return config5(k or 96)
     raise ValueError(f"unknown configuration {cfg}")
