@@ -551,24 +551,29 @@ std::string analyze(idx nblocks, const idx *Ap, const idx *Ai, int bs, const idx
     };
     plan_arena(true, S.upd_off, S.upd_size);
 
-    // ---- subtree solve cut: the highest level whose subtrees are still many
-    // (>= kMinSubtrees, to fill the GPU) and small (fronts <= kSubFmax rows)
+    // ---- subtree solve cut: the highest level whose subtrees are many and small
+    // (fronts <= kSubFmax rows). One CTA walks a subtree sequentially, so the
+    // largest subtree bounds the phase: aim for kManySubtrees (16 per SM of a
+    // 148-SM B200, the measured optimum on the 811k-DOF cube), else settle for
+    // kMinSubtrees (one per SM).
     {
-        constexpr idx kMinSubtrees = 148, kSubFmax = 2048;
+        constexpr idx kManySubtrees = 2368, kMinSubtrees = 148, kSubFmax = 2048;
         S.solve_cut = -1;
         std::vector<idx> fmax_le(S.nlevels, 0);           // max front at levels <= l
         for (idx s = 0; s < nsn; ++s) fmax_le[S.level[s]] = std::max(fmax_le[S.level[s]], S.f[s]);
         for (idx l = 1; l < S.nlevels; ++l) fmax_le[l] = std::max(fmax_le[l], fmax_le[l - 1]);
-        for (idx l = S.nlevels - 2; l >= 0; --l) {
-            if (fmax_le[l] > kSubFmax) continue;
-            idx roots = 0;
-            for (idx s = 0; s < nsn; ++s)
-                if (S.level[s] <= l && (S.sn_parent[s] < 0 || S.level[S.sn_parent[s]] > l)) ++roots;
-            if (roots >= kMinSubtrees) {
+        std::vector<idx> roots_at(S.nlevels, 0);           // subtree count for a cut at level l
+        for (idx s = 0; s < nsn; ++s)
+            for (idx l = S.level[s]; l < (S.sn_parent[s] < 0 ? S.nlevels : S.level[S.sn_parent[s]]); ++l)
+                ++roots_at[l];
+        for (idx want : {kManySubtrees, kMinSubtrees}) {
+            for (idx l = S.nlevels - 2; l >= 0; --l) {
+                if (fmax_le[l] > kSubFmax || roots_at[l] < want) continue;
                 S.solve_cut = l;
                 S.sub_fmax = fmax_le[l];
                 break;
             }
+            if (S.solve_cut >= 0) break;
         }
         if (S.solve_cut >= 0) {
             // subtree of root s = [s - size(s) + 1, s] in postorder
