@@ -256,6 +256,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     }
     // ---- solve tasks (all supernodes, level by level)
     const int RB = solve_rows_per_task();
+    const int DG = diag_blocks_per_task();
     std::vector<int32_t> flag_base(nsn);
     int nflags = 0;
     for (idx s = 0; s < nsn; ++s) {
@@ -281,16 +282,17 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             }
             const int nbw = int((S.w[s] + RB - 1) / RB), nbd = int((S.d[s] + RB - 1) / RB);
             maxblk = std::max(maxblk, nbw + nbd);
-            maxnbw = std::max(maxnbw, nbw);
+            maxnbw = std::max(maxnbw, (nbw + DG - 1) / DG);
         }
         L.sasm_n = int(sasm.size()) - L.sasm_off;
         L.sasm_tiles = base;
-        // ascending block index across the level's fronts: every dependency precedes its task
+        // ascending task (block pair) index across the level's fronts: every dependency
+        // precedes its task
         for (int b = 0; b < maxnbw; ++b)
             for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
                 const idx s = S.level_list[k];
-                const int nbw = int((S.w[s] + RB - 1) / RB);
-                if (b < nbw) ftri.push_back({int32_t(s), b, flag_base[s], 0});
+                const int nlk = int((S.w[s] + RB * DG - 1) / (RB * DG));
+                if (b < nlk) ftri.push_back({int32_t(s), b, flag_base[s], 0});
             }
         // structure slabs: forward 64-row slabs x kStrChunk-column chunks, backward 64-column slabs x row chunks
         L.fstr_off = int(fstr.size());
@@ -319,8 +321,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         for (int p = 0; p < maxnbw; ++p)
             for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
                 const idx s = S.level_list[k];
-                const int nbw = int((S.w[s] + RB - 1) / RB);
-                if (p < nbw) btri.push_back({int32_t(s), nbw - 1 - p, flag_base[s], 0});
+                const int nlk = int((S.w[s] + RB * DG - 1) / (RB * DG));
+                if (p < nlk) btri.push_back({int32_t(s), nlk - 1 - p, flag_base[s], 0});
             }
         L.ftri_n = int(ftri.size()) - L.ftri_off;
         L.btri_n = int(btri.size()) - L.btri_off;

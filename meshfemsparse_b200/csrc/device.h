@@ -157,6 +157,7 @@ template <typename T>
 void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce *red, int nred, SnDev sd,
                 const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st);
 int solve_rows_per_task();
+int diag_blocks_per_task();             // 64-row blocks per diagonal-chain task (one flag each)
 // Forward / backward solve of whole subtrees (subs[k] = postorder range [x, y]),
 // one CTA per subtree, fronts of at most fmax rows.
 template <typename T>

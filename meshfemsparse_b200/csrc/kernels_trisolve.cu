@@ -9,16 +9,17 @@
 // A front of supernode s is [L11; L21] (w + d rows, w columns). Per level:
 //   forward   fwd_asm      zero u_s and pull every child's update vector u_c into the
 //                          front through child_rel_indices (children in order);
-//             fwd_diag     L11 y = v, one task per 64-row diagonal block; block r
-//                          subtracts L11(r, k) y_k for k < r (waiting on block k's
-//                          epoch flag) and solves its triangle;
+//             fwd_diag     L11 y = v, one task per pair of 64-row diagonal blocks; a
+//                          pair subtracts L11(rows, k) y_k for every earlier block k
+//                          (waiting on block k's epoch flag) and solves its two
+//                          triangles inside the CTA, publishing each block's flag;
 //             str_partial  P = L21(rows, chunk) y(chunk) for 64-row tiles of L21 and
 //                          512-column chunks (independent tasks);
 //             fwd_reduce   u_s(rows) -= sum over chunks of P, in chunk order.
 //   backward  str_partial  P = L21(chunk, cols)^T x_struct for 64-column blocks and
 //                          512-row chunks of L21 (ancestors are final);
 //             bwd_reduce   x(cols) -= sum over chunks of P, in chunk order;
-//             bwd_diag     L11^T x = y, blocks descending, waiting on flags.
+//             bwd_diag     L11^T x = y, pairs and blocks descending, waiting on flags.
 // Everything is summed in a fixed order: results are run-to-run identical.
 // The diag kernels are cooperative launches (all CTAs co-resident); every CTA
 // walks its tasks in ascending order and a task only waits on lower-numbered
@@ -36,7 +37,8 @@ namespace mfs {
 namespace {
 
 constexpr int kRB = 64;                     // rows / columns per task
-constexpr int kTriThreads = 128;
+constexpr int kDG = 2;                      // 64-row blocks per diagonal-chain task (one flag per task)
+constexpr int kDiagThreads = 256;
 constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s per wait at most
 
 __device__ __forceinline__ int child_rel(const int32_t *rel, int i, int vb) { return rel[i / vb] + i % vb; }
@@ -201,100 +203,88 @@ template <typename T>
 __host__ __device__ inline size_t str_smem(int nrhs) {
     return size_t(3) * kRB * nrhs * sizeof(double) + size_t(2) * kRB * TileLd<T>::v * sizeof(T);
 }
-// shared memory of the diag kernels: acc[kRB * nrhs] | vec[kRB * nrhs] (double) | tile[2][kRB][TL] |
-// dblk[kRB][kRB + 1] (factor type)
+// shared memory of the diag kernels: acc[kDG][kRB * nrhs] | vec[kRB * nrhs] (double) |
+// tile[3][kRB][TL] (ring of two, in-task tile) | dblk[kDG][kRB][kRB + 1] (factor type)
 template <typename T>
 __host__ __device__ inline size_t diag_smem(int nrhs) {
-    return size_t(2) * kRB * nrhs * sizeof(double) + size_t(2) * kRB * TileLd<T>::v * sizeof(T) +
-           size_t(kRB) * (kRB + 1) * sizeof(T);
+    return size_t(kDG + 1) * kRB * nrhs * sizeof(double) + size_t(3) * kRB * TileLd<T>::v * sizeof(T) +
+           size_t(kDG) * kRB * (kRB + 1) * sizeof(T);
 }
 
-// Diagonal block of the task into dblk (row-major, ld kRB + 1): the stored
+// Diagonal block `blk` of the front into dblk (row-major, ld kRB + 1): the stored
 // inverse of L(r, r) when the front has one, else the lower triangle of L(r, r).
 template <typename T>
 __device__ __forceinline__ bool load_diag_block(T *dblk, const T *factor, const T *pan, int64_t inv, int ld, int r0,
                                                 int nr, int blk) {
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, nt = blockDim.x;
     if (inv >= 0) {
         const T *src = factor + inv + int64_t(blk) * kRB * kRB;   // column-major 64 x 64
 #pragma unroll 8
-        for (int q = tid; q < kRB * kRB; q += kTriThreads) {
+        for (int q = tid; q < kRB * kRB; q += nt) {
             const int j = q >> 6, i = q & 63;
             dblk[i * (kRB + 1) + j] = src[q];
         }
         return true;
     }
-    for (int q = tid; q < nr * nr; q += kTriThreads) {
+    for (int q = tid; q < nr * nr; q += nt) {
         const int j = q / nr, i = q % nr;
         dblk[i * (kRB + 1) + j] = i >= j ? pan[int64_t(r0 + j) * ld + r0 + i] : T(0);
     }
     return false;
 }
 
-// Vectors in shared memory are column-major per right-hand side: v[r * kRB + i].
-template <typename T>
-__global__ void __launch_bounds__(kTriThreads) fwd_diag_kernel(const SolveTask *__restrict__ tasks, int ntasks,
-                                                               SnDev sd, const T *__restrict__ factor,
-                                                               double *__restrict__ X, int64_t ldx, int nrhs,
-                                                               int *__restrict__ flags, int *__restrict__ err) {
-    constexpr int TL = TileLd<T>::v;
-    extern __shared__ __align__(16) double smem_d[];
-    double *acc = smem_d;
-    double *yk = acc + kRB * nrhs;
-    T *tiles = reinterpret_cast<T *>(yk + kRB * nrhs);   // two tiles: (i, j) = L(r0+i, k0+j) at [j * TL + i]
-    T *dblk = tiles + 2 * kRB * TL;
-    const int tid = threadIdx.x;
+// acc -= tile * v (forward: acc(i) -= sum_j L(r0 + i, k0 + j) v(j)); tile (i, j) at [j * TL + i]
+template <typename T, int TL>
+__device__ __forceinline__ void tile_sub_fwd(double *acc, const T *tl, const double *v, int nrows, int nrhs) {
     const int nq = kRB * nrhs;
-    for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
-        const SolveTask tk = tasks[t];
-        const int s = tk.sn;
-        const int w = sd.w[s], ld = sd.ld[s];
-        const int c0 = sd.col0[s];
-        const int r0 = tk.blk * kRB, nr = min(kRB, w - r0);
-        const T *pan = factor + sd.pan_off[s];
-        __syncthreads();                             // previous task done with shared memory
-        // everything that does not depend on earlier blocks is requested before the first wait
-        if (tk.blk > 0) stage_tile<T, TL>(tiles, pan, ld, r0, nr, 0, kRB, tid, kTriThreads);
-        cpa_commit();
-        const bool has_inv = load_diag_block(dblk, factor, pan, sd.inv_off[s], ld, r0, nr, tk.blk);
-        for (int q = tid; q < nq; q += kTriThreads) {
-            const int i = q & (kRB - 1), r = q >> 6;
-            acc[q] = i < nr ? X[c0 + r0 + i + r * ldx] : 0.0;
-        }
-        for (int k = 0; k < tk.blk; ++k) {
-            const int k0 = k * kRB;                  // full block: k < blk
-            if (k + 1 < tk.blk)
-                stage_tile<T, TL>(tiles + ((k + 1) & 1) * kRB * TL, pan, ld, r0, nr, k0 + kRB, kRB, tid,
-                                  kTriThreads);
-            cpa_commit();
-            wait_flag(flags + tk.flag_base + k, 1, err);
-            for (int q = tid; q < nq; q += kTriThreads) {
-                const int j = q & (kRB - 1), r = q >> 6;
-                yk[q] = __ldcg(&X[c0 + k0 + j + r * ldx]);
-            }
-            cpa_wait<1>();
-            __syncthreads();
-            const T *tl = tiles + (k & 1) * kRB * TL;
-            for (int q = tid; q < nq; q += kTriThreads) {
-                const int i = q & (kRB - 1), r = q >> 6;
-                const double *yr = yk + r * kRB;
-                double a0 = 0.0, a1 = 0.0;
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        const int i = q & (kRB - 1), r = q >> 6;
+        if (i >= nrows) continue;
+        const double *vr = v + r * kRB;
+        double a0 = 0.0, a1 = 0.0;
 #pragma unroll 8
-                for (int j = 0; j < kRB; j += 2) {
-                    a0 += double(tl[j * TL + i]) * yr[j];
-                    a1 += double(tl[(j + 1) * TL + i]) * yr[j + 1];
-                }
-                acc[q] -= a0 + a1;
-            }
-            __syncthreads();                         // tile (k & 1) is refilled at k + 2
+        for (int j = 0; j < kRB; j += 2) {
+            a0 += double(tl[j * TL + i]) * vr[j];
+            a1 += double(tl[(j + 1) * TL + i]) * vr[j + 1];
         }
-        cpa_wait<0>();
-        __syncthreads();
-        if (has_inv) {
-            // y = inv(L(r, r)) acc, written straight to X
-            for (int q = tid; q < nq; q += kTriThreads) {
-                const int i = q & (kRB - 1), r = q >> 6;
-                if (i >= nr) continue;
+        acc[q] -= a0 + a1;
+    }
+}
+
+// acc -= tile^T * v (backward: acc(j) -= sum_i L(i0 + i, c0 + j) v(i), i < ni); rows in
+// skewed order so the lanes of a warp read 32 different rows (distinct banks)
+template <typename T, int TL>
+__device__ __forceinline__ void tile_sub_bwd(double *acc, const T *tl, const double *v, int ni, int ncols, int nrhs) {
+    const int nq = kRB * nrhs;
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        const int j = q & (kRB - 1), r = q >> 6;
+        if (j >= ncols) continue;
+        const double *xr = v + r * kRB;
+        double a0 = 0.0, a1 = 0.0;
+#pragma unroll 8
+        for (int u = 0; u < kRB; u += 2) {
+            const int i = (u + j) & (kRB - 1), i1 = (u + 1 + j) & (kRB - 1);
+            a0 += (i < ni ? double(tl[j * TL + i]) : 0.0) * xr[i];
+            a1 += (i1 < ni ? double(tl[j * TL + i1]) : 0.0) * xr[i1];
+        }
+        acc[q] -= a0 + a1;
+    }
+}
+
+// acc := L(b, b)^{-1} acc for one 64-row block, in place (rows >= nr zeroed): through
+// the stored inverse, or by substitution on the lower triangle (warp 0). The result
+// also goes to X.
+template <typename T>
+__device__ __forceinline__ void diag_apply_fwd(bool has_inv, const T *dblk, double *acc, int nr, int nrhs, double *X,
+                                               int64_t row0, int64_t ldx) {
+    const int tid = threadIdx.x, nt = blockDim.x, nq = kRB * nrhs;
+    if (has_inv) {
+        double out[kMaxSolveRhs * kRB / kDiagThreads];
+        int c = 0;
+        for (int q = tid; q < nq; q += nt, ++c) {
+            const int i = q & (kRB - 1), r = q >> 6;
+            double v = 0.0;
+            if (i < nr) {
                 const T *irow = dblk + i * (kRB + 1);
                 const double *ar = acc + r * kRB;
                 double a0 = 0.0, a1 = 0.0;
@@ -304,100 +294,52 @@ __global__ void __launch_bounds__(kTriThreads) fwd_diag_kernel(const SolveTask *
                     a1 += double(irow[j + 1]) * ar[j + 1];
                 }
                 if (j == i) a0 += double(irow[j]) * ar[j];
-                X[c0 + r0 + i + r * ldx] = a0 + a1;
+                v = a0 + a1;
             }
-        } else {
-            if (tid < 32) {
-                for (int j = 0; j < nr; ++j) {
-                    const double ljj = double(dblk[j * (kRB + 1) + j]);
-                    for (int r = tid; r < nrhs; r += 32) acc[r * kRB + j] /= ljj;
-                    __syncwarp();
-                    for (int i = j + 1 + tid; i < nr; i += 32) {
-                        const double lij = double(dblk[i * (kRB + 1) + j]);
-                        for (int r = 0; r < nrhs; ++r) acc[r * kRB + i] -= lij * acc[r * kRB + j];
-                    }
-                    __syncwarp();
+            out[c] = v;
+        }
+        __syncthreads();                                 // every read of acc is done
+        c = 0;
+        for (int q = tid; q < nq; q += nt, ++c) {
+            const int i = q & (kRB - 1), r = q >> 6;
+            acc[q] = out[c];
+            if (i < nr) X[row0 + i + r * ldx] = out[c];
+        }
+    } else {
+        if (tid < 32) {
+            for (int j = 0; j < nr; ++j) {
+                const double ljj = double(dblk[j * (kRB + 1) + j]);
+                for (int r = tid; r < nrhs; r += 32) acc[r * kRB + j] /= ljj;
+                __syncwarp();
+                for (int i = j + 1 + tid; i < nr; i += 32) {
+                    const double lij = double(dblk[i * (kRB + 1) + j]);
+                    for (int r = 0; r < nrhs; ++r) acc[r * kRB + i] -= lij * acc[r * kRB + j];
                 }
-            }
-            __syncthreads();
-            for (int q = tid; q < nq; q += kTriThreads) {
-                const int i = q & (kRB - 1), r = q >> 6;
-                if (i < nr) X[c0 + r0 + i + r * ldx] = acc[q];
+                __syncwarp();
             }
         }
-        __threadfence();
         __syncthreads();
-        if (tid == 0) st_release(flags + tk.flag_base + tk.blk, 1);
+        for (int q = tid; q < nq; q += nt) {
+            const int i = q & (kRB - 1), r = q >> 6;
+            if (i < nr) X[row0 + i + r * ldx] = acc[q];
+            else acc[q] = 0.0;
+        }
     }
 }
 
+// acc := L(b, b)^{-T} acc for one 64-column block, in place (stored inverse or
+// substitution); also to X.
 template <typename T>
-__global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *__restrict__ tasks, int ntasks,
-                                                               SnDev sd, const T *__restrict__ factor,
-                                                               double *__restrict__ X, int64_t ldx, int nrhs,
-                                                               int *__restrict__ flags, int *__restrict__ err) {
-    constexpr int TL = TileLd<T>::v;
-    extern __shared__ __align__(16) double smem_d[];
-    double *acc = smem_d;
-    double *xk = acc + kRB * nrhs;
-    T *tiles = reinterpret_cast<T *>(xk + kRB * nrhs);   // two tiles: (i, j) = L(i0+i, r0+j) at [j * TL + i]
-    T *dblk = tiles + 2 * kRB * TL;
-    const int tid = threadIdx.x;
-    const int nq = kRB * nrhs;
-    for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
-        const SolveTask tk = tasks[t];
-        const int s = tk.sn;
-        const int w = sd.w[s], ld = sd.ld[s];
-        const int c0 = sd.col0[s];
-        const int nbw = (w + kRB - 1) / kRB;
-        const int r0 = tk.blk * kRB, nr = min(kRB, w - r0);
-        const T *pan = factor + sd.pan_off[s];
-        __syncthreads();
-        const int kfirst = nbw - 1;
-        if (kfirst > tk.blk)
-            stage_tile<T, TL>(tiles, pan, ld, kfirst * kRB, min(kRB, w - kfirst * kRB), r0, nr, tid, kTriThreads);
-        cpa_commit();
-        const bool has_inv = load_diag_block(dblk, factor, pan, sd.inv_off[s], ld, r0, nr, tk.blk);
-        for (int q = tid; q < nq; q += kTriThreads) {
+__device__ __forceinline__ void diag_apply_bwd(bool has_inv, const T *dblk, double *acc, int nr, int nrhs, double *X,
+                                               int64_t row0, int64_t ldx) {
+    const int tid = threadIdx.x, nt = blockDim.x, nq = kRB * nrhs;
+    if (has_inv) {
+        double out[kMaxSolveRhs * kRB / kDiagThreads];
+        int c = 0;
+        for (int q = tid; q < nq; q += nt, ++c) {
             const int j = q & (kRB - 1), r = q >> 6;
-            acc[q] = j < nr ? X[c0 + r0 + j + r * ldx] : 0.0;
-        }
-        int buf = 0;
-        for (int k = kfirst; k > tk.blk; --k, buf ^= 1) {
-            const int i0 = k * kRB, ni = min(kRB, w - i0);
-            if (k - 1 > tk.blk)
-                stage_tile<T, TL>(tiles + (buf ^ 1) * kRB * TL, pan, ld, i0 - kRB, kRB, r0, nr, tid, kTriThreads);
-            cpa_commit();
-            wait_flag(flags + tk.flag_base + k, 2, err);
-            for (int q = tid; q < nq; q += kTriThreads) {
-                const int i = q & (kRB - 1), r = q >> 6;
-                xk[q] = i < ni ? __ldcg(&X[c0 + i0 + i + r * ldx]) : 0.0;
-            }
-            cpa_wait<1>();
-            __syncthreads();
-            const T *tl = tiles + buf * kRB * TL;
-            for (int q = tid; q < nq; q += kTriThreads) {
-                const int j = q & (kRB - 1), r = q >> 6;
-                const double *xr = xk + r * kRB;
-                double a0 = 0.0, a1 = 0.0;
-                // skewed order: the lanes of a warp read 32 different rows (distinct banks)
-#pragma unroll 8
-                for (int u = 0; u < kRB; u += 2) {
-                    const int i = (u + j) & (kRB - 1), i1 = (u + 1 + j) & (kRB - 1);
-                    a0 += (i < ni ? double(tl[j * TL + i]) : 0.0) * xr[i];
-                    a1 += (i1 < ni ? double(tl[j * TL + i1]) : 0.0) * xr[i1];
-                }
-                acc[q] -= a0 + a1;
-            }
-            __syncthreads();
-        }
-        cpa_wait<0>();
-        __syncthreads();
-        if (has_inv) {
-            // x = inv(L(r, r))^T acc
-            for (int q = tid; q < nq; q += kTriThreads) {
-                const int j = q & (kRB - 1), r = q >> 6;
-                if (j >= nr) continue;
+            double v = 0.0;
+            if (j < nr) {
                 const double *ar = acc + r * kRB;
                 double a0 = 0.0, a1 = 0.0;
                 int i = j;
@@ -406,29 +348,242 @@ __global__ void __launch_bounds__(kTriThreads) bwd_diag_kernel(const SolveTask *
                     a1 += double(dblk[(i + 1) * (kRB + 1) + j]) * ar[i + 1];
                 }
                 if (i < nr) a0 += double(dblk[i * (kRB + 1) + j]) * ar[i];
-                X[c0 + r0 + j + r * ldx] = a0 + a1;
+                v = a0 + a1;
             }
-        } else {
-            if (tid < 32) {
-                for (int j = nr - 1; j >= 0; --j) {
-                    for (int r = tid; r < nrhs; r += 32) acc[r * kRB + j] /= double(dblk[j * (kRB + 1) + j]);
-                    __syncwarp();
-                    for (int i = tid; i < j; i += 32) {
-                        const double lji = double(dblk[j * (kRB + 1) + i]);
-                        for (int r = 0; r < nrhs; ++r) acc[r * kRB + i] -= lji * acc[r * kRB + j];
-                    }
-                    __syncwarp();
+            out[c] = v;
+        }
+        __syncthreads();
+        c = 0;
+        for (int q = tid; q < nq; q += nt, ++c) {
+            const int j = q & (kRB - 1), r = q >> 6;
+            acc[q] = out[c];
+            if (j < nr) X[row0 + j + r * ldx] = out[c];
+        }
+    } else {
+        if (tid < 32) {
+            for (int j = nr - 1; j >= 0; --j) {
+                for (int r = tid; r < nrhs; r += 32) acc[r * kRB + j] /= double(dblk[j * (kRB + 1) + j]);
+                __syncwarp();
+                for (int i = tid; i < j; i += 32) {
+                    const double lji = double(dblk[j * (kRB + 1) + i]);
+                    for (int r = 0; r < nrhs; ++r) acc[r * kRB + i] -= lji * acc[r * kRB + j];
                 }
-            }
-            __syncthreads();
-            for (int q = tid; q < nq; q += kTriThreads) {
-                const int j = q & (kRB - 1), r = q >> 6;
-                if (j < nr) X[c0 + r0 + j + r * ldx] = acc[q];
+                __syncwarp();
             }
         }
-        __threadfence();
         __syncthreads();
-        if (tid == 0) st_release(flags + tk.flag_base + tk.blk, 2);
+        for (int q = tid; q < nq; q += nt) {
+            const int j = q & (kRB - 1), r = q >> 6;
+            if (j < nr) X[row0 + j + r * ldx] = acc[q];
+            else acc[q] = 0.0;
+        }
+    }
+}
+
+// Forward diagonal chain. A task is a pair of consecutive 64-row blocks b0, b0 + 1
+// of L11 (the last task of a front may hold one); every block has its own flag. The
+// task subtracts L11(block b0 + h, block k) y_k for every earlier block k as k's flag
+// arrives, finishes block b0 and publishes it before its last tile for block b0 + 1,
+// then applies the in-task tile L(b0 + 1, b0) (prefetched into its own buffer) and
+// finishes block b0 + 1. Tiles stream through a double-buffered cp.async ring;
+// vectors are column-major per RHS: v[r * kRB + i].
+template <typename T>
+__global__ void __launch_bounds__(kDiagThreads) fwd_diag_kernel(const SolveTask *__restrict__ tasks, int ntasks,
+                                                                SnDev sd, const T *__restrict__ factor,
+                                                                double *__restrict__ X, int64_t ldx, int nrhs,
+                                                                int *__restrict__ flags, int *__restrict__ err) {
+    constexpr int TL = TileLd<T>::v;
+    extern __shared__ __align__(16) double smem_d[];
+    const int nq = kRB * nrhs;
+    double *acc = smem_d;                               // [kDG][nq]: accumulators, then y in place
+    double *vec = acc + kDG * nq;                       // [nq]: y_k of the block being applied
+    T *tiles = reinterpret_cast<T *>(vec + nq);         // [3][kRB * TL]: ring of 2, in-task tile
+    T *tin = tiles + 2 * kRB * TL;
+    T *dblk = tiles + 3 * kRB * TL;                     // [kDG][kRB * (kRB + 1)]
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
+        const SolveTask tk = tasks[t];
+        const int s = tk.sn;
+        const int w = sd.w[s], ld = sd.ld[s];
+        const int c0 = sd.col0[s];
+        const int nbw = (w + kRB - 1) / kRB;
+        const int b0 = tk.blk * kDG, nb = min(kDG, nbw - b0);
+        const int nr0 = min(kRB, w - b0 * kRB), nr1 = nb == 2 ? min(kRB, w - (b0 + 1) * kRB) : 0;
+        const T *pan = factor + sd.pan_off[s];
+        const int64_t inv = sd.inv_off[s];
+        const int nseq = b0 * nb;                       // tiles (k, h), k < b0 ascending, h < nb
+        auto stage = [&](int q, int buf) {
+            const int k = q / nb, h = q - k * nb;
+            const int r0 = (b0 + h) * kRB;
+            stage_tile<T, TL>(tiles + buf * kRB * TL, pan, ld, r0, min(kRB, w - r0), k * kRB, kRB, tid, nt);
+        };
+        auto publish = [&](int blk) {
+            __syncthreads();
+            if (tid == 0) {
+                __threadfence();
+                st_release(flags + tk.flag_base + blk, 1);
+            }
+        };
+        __syncthreads();                                  // previous task done with shared memory
+        if (nb == 2) stage_tile<T, TL>(tin, pan, ld, (b0 + 1) * kRB, nr1, b0 * kRB, kRB, tid, nt);
+        if (nseq > 0) stage(0, 0);
+        cpa_commit();
+        bool has_inv[kDG];
+#pragma unroll
+        for (int h = 0; h < kDG; ++h) {
+            has_inv[h] = false;
+            if (h < nb)
+                has_inv[h] = load_diag_block(dblk + h * kRB * (kRB + 1), factor, pan, inv, ld, (b0 + h) * kRB,
+                                             h == 0 ? nr0 : nr1, b0 + h);
+        }
+        for (int q = tid; q < kDG * nq; q += nt) {
+            const int h = q / nq, i = q & (kRB - 1), r = (q - h * nq) >> 6;
+            const int row = (b0 + h) * kRB + i;
+            acc[q] = (h < nb && row < w) ? X[c0 + row + r * ldx] : 0.0;
+        }
+        bool done0 = false;
+        for (int q = 0; q < nseq; ++q) {
+            const int k = q / nb, h = q - k * nb;
+            if (q + 1 < nseq) stage(q + 1, (q + 1) & 1);
+            cpa_commit();
+            if (h == 0) {
+                wait_flag(flags + tk.flag_base + k, 1, err);
+                for (int e = tid; e < nq; e += nt) {
+                    const int j = e & (kRB - 1), r = e >> 6;
+                    vec[e] = __ldcg(&X[c0 + k * kRB + j + r * ldx]);
+                }
+            }
+            cpa_wait<1>();
+            __syncthreads();
+            if (h == 1 && k == b0 - 1) {
+                // every dependency of block b0 is in: finish and publish it first
+                diag_apply_fwd<T>(has_inv[0], dblk, acc, nr0, nrhs, X, c0 + b0 * kRB, ldx);
+                publish(b0);
+                done0 = true;
+            }
+            tile_sub_fwd<T, TL>(acc + h * nq, tiles + (q & 1) * kRB * TL, vec, h == 0 ? nr0 : nr1, nrhs);
+            __syncthreads();                              // the ring buffer is refilled two tiles later
+        }
+        cpa_wait<0>();
+        __syncthreads();
+        if (!done0) {
+            diag_apply_fwd<T>(has_inv[0], dblk, acc, nr0, nrhs, X, c0 + b0 * kRB, ldx);
+            publish(b0);
+        }
+        if (nb == 2) {
+            __syncthreads();
+            tile_sub_fwd<T, TL>(acc + nq, tin, acc, nr1, nrhs);
+            __syncthreads();
+            diag_apply_fwd<T>(has_inv[1], dblk + kRB * (kRB + 1), acc + nq, nr1, nrhs, X, c0 + (b0 + 1) * kRB, ldx);
+            publish(b0 + 1);
+        }
+    }
+}
+
+// Backward diagonal chain (L11^T x = y), blocks descending. A task (pair b0, b0 + 1)
+// subtracts L11(block k, block b0 + h)^T x_k for every later block k as k's flag
+// arrives, finishes block b0 + 1 and publishes it before its last tile for block b0,
+// then applies the in-task tile L(b0 + 1, b0)^T x_{b0+1} and finishes block b0.
+template <typename T>
+__global__ void __launch_bounds__(kDiagThreads) bwd_diag_kernel(const SolveTask *__restrict__ tasks, int ntasks,
+                                                                SnDev sd, const T *__restrict__ factor,
+                                                                double *__restrict__ X, int64_t ldx, int nrhs,
+                                                                int *__restrict__ flags, int *__restrict__ err) {
+    constexpr int TL = TileLd<T>::v;
+    extern __shared__ __align__(16) double smem_d[];
+    const int nq = kRB * nrhs;
+    double *acc = smem_d;                               // [kDG][nq]: accumulators, then x in place
+    double *vec = acc + kDG * nq;                       // [nq]: x_k of the block being applied
+    T *tiles = reinterpret_cast<T *>(vec + nq);
+    T *tin = tiles + 2 * kRB * TL;
+    T *dblk = tiles + 3 * kRB * TL;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
+        const SolveTask tk = tasks[t];
+        const int s = tk.sn;
+        const int w = sd.w[s], ld = sd.ld[s];
+        const int c0 = sd.col0[s];
+        const int nbw = (w + kRB - 1) / kRB;
+        const int b0 = tk.blk * kDG, nb = min(kDG, nbw - b0);
+        const int nr0 = min(kRB, w - b0 * kRB), nr1 = nb == 2 ? min(kRB, w - (b0 + 1) * kRB) : 0;
+        const T *pan = factor + sd.pan_off[s];
+        const int64_t inv = sd.inv_off[s];
+        const int nlater = nbw - (b0 + nb);
+        const int nseq = nlater * nb;                   // tiles (k, h): k descending, h descending
+        auto tile_of = [&](int q, int &k, int &h) {
+            k = nbw - 1 - q / nb;
+            h = nb - 1 - (q - (q / nb) * nb);
+        };
+        auto stage = [&](int q, int buf) {
+            int k, h;
+            tile_of(q, k, h);
+            const int i0 = k * kRB, cc = (b0 + h) * kRB;
+            stage_tile<T, TL>(tiles + buf * kRB * TL, pan, ld, i0, min(kRB, w - i0), cc, min(kRB, w - cc), tid, nt);
+        };
+        auto publish = [&](int blk) {
+            __syncthreads();
+            if (tid == 0) {
+                __threadfence();
+                st_release(flags + tk.flag_base + blk, 2);
+            }
+        };
+        __syncthreads();
+        if (nb == 2) stage_tile<T, TL>(tin, pan, ld, (b0 + 1) * kRB, nr1, b0 * kRB, kRB, tid, nt);
+        if (nseq > 0) stage(0, 0);
+        cpa_commit();
+        bool has_inv[kDG];
+#pragma unroll
+        for (int h = 0; h < kDG; ++h) {
+            has_inv[h] = false;
+            if (h < nb)
+                has_inv[h] = load_diag_block(dblk + h * kRB * (kRB + 1), factor, pan, inv, ld, (b0 + h) * kRB,
+                                             h == 0 ? nr0 : nr1, b0 + h);
+        }
+        for (int q = tid; q < kDG * nq; q += nt) {
+            const int h = q / nq, j = q & (kRB - 1), r = (q - h * nq) >> 6;
+            const int row = (b0 + h) * kRB + j;
+            acc[q] = (h < nb && row < w) ? X[c0 + row + r * ldx] : 0.0;
+        }
+        bool done1 = false;
+        for (int q = 0; q < nseq; ++q) {
+            int k, h;
+            tile_of(q, k, h);
+            if (q + 1 < nseq) stage(q + 1, (q + 1) & 1);
+            cpa_commit();
+            const int ni = min(kRB, w - k * kRB);
+            if (h == nb - 1) {
+                wait_flag(flags + tk.flag_base + k, 2, err);
+                for (int e = tid; e < nq; e += nt) {
+                    const int i = e & (kRB - 1), r = e >> 6;
+                    vec[e] = i < ni ? __ldcg(&X[c0 + k * kRB + i + r * ldx]) : 0.0;
+                }
+            }
+            cpa_wait<1>();
+            __syncthreads();
+            if (nb == 2 && h == 0 && k == b0 + 2) {
+                // every dependency of block b0 + 1 is in: finish and publish it first
+                diag_apply_bwd<T>(has_inv[1], dblk + kRB * (kRB + 1), acc + nq, nr1, nrhs, X, c0 + (b0 + 1) * kRB,
+                                  ldx);
+                publish(b0 + 1);
+                done1 = true;
+            }
+            tile_sub_bwd<T, TL>(acc + h * nq, tiles + (q & 1) * kRB * TL, vec, ni, h == 0 ? nr0 : nr1, nrhs);
+            __syncthreads();
+        }
+        cpa_wait<0>();
+        __syncthreads();
+        if (nb == 2) {
+            if (!done1) {
+                diag_apply_bwd<T>(has_inv[1], dblk + kRB * (kRB + 1), acc + nq, nr1, nrhs, X, c0 + (b0 + 1) * kRB,
+                                  ldx);
+                publish(b0 + 1);
+            }
+            __syncthreads();
+            tile_sub_bwd<T, TL>(acc, tin, acc + nq, nr1, kRB, nrhs);
+            __syncthreads();
+        }
+        diag_apply_bwd<T>(has_inv[0], dblk, acc, nr0, nrhs, X, c0 + b0 * kRB, ldx);
+        publish(b0);
     }
 }
 
@@ -633,7 +788,7 @@ int sm_count() {
 template <typename K>
 int coop_grid(K kernel, size_t smem, int ntasks) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTriThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kDiagThreads, smem);
     const int g = std::max(1, per_sm) * sm_count();
     return std::min(g, std::max(1, ntasks));
 }
@@ -668,7 +823,7 @@ cudaError_t launch_diag(bool forward, const SolveTask *tasks, int ntasks, SnDev 
     void *args[] = {(void *)&tasks, (void *)&ntasks, (void *)&sd, (void *)&factor, (void *)&X, (void *)&ldx,
                     (void *)&nrhs, (void *)&flags, (void *)&err};
     ++g_kernel_launches;
-    return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kTriThreads), args, smem, st);
+    return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kDiagThreads), args, smem, st);
 }
 
 template <typename T>
@@ -702,5 +857,6 @@ MFS_TRI_INSTANTIATE(double)
 MFS_TRI_INSTANTIATE(float)
 
 int solve_rows_per_task() { return kRB; }
+int diag_blocks_per_task() { return kDG; }
 
 }  // namespace mfs
