@@ -31,6 +31,7 @@
 #include "device.h"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace mfs {
 
@@ -198,10 +199,12 @@ __device__ __forceinline__ int stage_tile(T *dst, const T *pan, int64_t ld, int 
     return sh;
 }
 
-// shared memory of the structure kernels: out[kRB * nrhs] | vec[2][kRB * nrhs] (double) | tile[2][kRB][TL]
+// shared memory of the structure kernels: out[kRB * nrhs] | vec[2][kRB * nrhs] (double) | tile[2][kRB][TL] |
+// FP32 copy of a vector slice (kRB * 4, FP32 factors)
 template <typename T>
 __host__ __device__ inline size_t str_smem(int nrhs) {
-    return size_t(3) * kRB * nrhs * sizeof(double) + size_t(2) * kRB * TileLd<T>::v * sizeof(T);
+    return size_t(3) * kRB * nrhs * sizeof(double) + size_t(2) * kRB * TileLd<T>::v * sizeof(T) +
+           size_t(kRB) * 4 * sizeof(double);
 }
 // shared memory of the diag kernels: acc[kDG][kRB * nrhs] | vec[kRB * nrhs] (double) |
 // tile[3][kRB][TL] (ring of two, in-task tile) | dblk[kDG][kRB][kRB + 1] (factor type)
@@ -593,7 +596,7 @@ __global__ void __launch_bounds__(kDiagThreads) bwd_diag_kernel(const SolveTask 
 // tile and its vector slice in flight (cp.async) while the current one is used.
 // P slab layout: P[r * kRB + a].
 template <typename T, bool FWD>
-__global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restrict__ tasks, SnDev sd,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) str_partial_kernel(const StrTask *__restrict__ tasks, SnDev sd,
                                                           const T *__restrict__ factor,
                                                           const double *__restrict__ X, int64_t ldx, int nrhs,
                                                           double *__restrict__ P) {
@@ -642,14 +645,20 @@ __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restr
     //   FWD: thread = (row pair a, a + 32) x (8-column group of the tile), summed over
     //        the groups at the end; BWD: lane = (row pair i, i + 32), warp = 8 columns,
     //        summed over the lanes at the end.
+    // With an FP32 factor (the preconditioner of FP64 refinement) the products and the
+    // chunk's partial sums are FP32: each tile's vector slice is rounded to FP32 once;
+    // chunk partials are reduced in FP64. An FP64 factor keeps FP64 throughout.
     // More right-hand sides take the generic per-(row, rhs) loop.
+    using Acc = std::conditional_t<sizeof(T) == 4, float, double>;
+    constexpr bool kF32 = sizeof(T) == 4;
+    Acc *vf = reinterpret_cast<Acc *>(tiles + 2 * kRB * TL);   // [kRB * 4] FP32 copy of the slice
     const bool fast = nrhs <= 4;
     const int lane = tid & 31, wgrp = tid >> 5;
-    double racc[8][4];
+    Acc racc[FWD ? 2 : 8][4];
 #pragma unroll
-    for (int c = 0; c < 8; ++c)
+    for (int c = 0; c < (FWD ? 2 : 8); ++c)
 #pragma unroll
-        for (int r = 0; r < 4; ++r) racc[c][r] = 0.0;
+        for (int r = 0; r < 4; ++r) racc[c][r] = Acc(0);
     for (int q = tid; q < nq; q += nt) out[q] = 0.0;
     stage(0, 0);
     for (int b = 0; b < nblk; ++b) {
@@ -662,33 +671,41 @@ __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restr
         const T *tl = tiles + buf * kRB * TL + sh;
         const double *v = vecs + buf * nq;
         if (fast) {
+            const Acc *va;
+            if constexpr (kF32) {
+                for (int q = tid; q < nq; q += nt) vf[q] = Acc(v[q]);
+                __syncthreads();
+                va = vf;
+            } else {
+                va = v;
+            }
             if (FWD) {
 #pragma unroll
                 for (int jj = 0; jj < 8; ++jj) {
                     const int j = 8 * wgrp + jj;
                     if (j < nbk) {
-                        const double t0 = double(tl[j * TL + lane]), t1 = double(tl[j * TL + lane + 32]);
+                        const Acc t0 = Acc(tl[j * TL + lane]), t1 = Acc(tl[j * TL + lane + 32]);
 #pragma unroll
                         for (int r = 0; r < 4; ++r)
                             if (r < nrhs) {
-                                const double vv = v[r * kRB + j];
+                                const Acc vv = va[r * kRB + j];
                                 racc[0][r] += t0 * vv;
                                 racc[1][r] += t1 * vv;
                             }
                     }
                 }
             } else {
-                double x0[4], x1[4];
+                Acc x0[4], x1[4];
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
-                    x0[r] = (r < nrhs && lane < nbk) ? v[r * kRB + lane] : 0.0;
-                    x1[r] = (r < nrhs && lane + 32 < nbk) ? v[r * kRB + lane + 32] : 0.0;
+                    x0[r] = (r < nrhs && lane < nbk) ? va[r * kRB + lane] : Acc(0);
+                    x1[r] = (r < nrhs && lane + 32 < nbk) ? va[r * kRB + lane + 32] : Acc(0);
                 }
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
+                for (int c = 0; c < (FWD ? 2 : 8); ++c) {
                     const int a = 8 * wgrp + c;
-                    const double t0 = lane < nbk ? double(tl[a * TL + lane]) : 0.0;
-                    const double t1 = lane + 32 < nbk ? double(tl[a * TL + lane + 32]) : 0.0;
+                    const Acc t0 = lane < nbk ? Acc(tl[a * TL + lane]) : Acc(0);
+                    const Acc t1 = lane + 32 < nbk ? Acc(tl[a * TL + lane + 32]) : Acc(0);
 #pragma unroll
                     for (int r = 0; r < 4; ++r) racc[c][r] += t0 * x0[r] + t1 * x1[r];
                 }
@@ -729,8 +746,8 @@ __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restr
 #pragma unroll
             for (int r = 0; r < 4; ++r)
                 if (r < nrhs) {
-                    red[(wgrp * 4 + r) * kRB + lane] = racc[0][r];
-                    red[(wgrp * 4 + r) * kRB + lane + 32] = racc[1][r];
+                    red[(wgrp * 4 + r) * kRB + lane] = double(racc[0][r]);
+                    red[(wgrp * 4 + r) * kRB + lane + 32] = double(racc[1][r]);
                 }
             __syncthreads();
             for (int q = tid; q < nq; q += nt) {
@@ -741,10 +758,10 @@ __global__ void __launch_bounds__(256) str_partial_kernel(const StrTask *__restr
             }
         } else {
 #pragma unroll
-            for (int c = 0; c < 8; ++c)
+            for (int c = 0; c < (FWD ? 2 : 8); ++c)
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
-                    double g = racc[c][r];
+                    double g = double(racc[c][r]);
 #pragma unroll
                     for (int off = 16; off > 0; off >>= 1) g += __shfl_down_sync(0xffffffffu, g, off);
                     if (lane == 0 && r < nrhs) out[r * kRB + 8 * wgrp + c] = g;
