@@ -229,19 +229,34 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             }
             sp.trsm_n = int(gemm_tasks.size()) - sp.trsm_off;
             sp.trsm_tiles = tb;
-            // after the last block of a group: update the columns after the group
+            // after the last block of a group: update the columns after the group, the next
+            // group's GB columns apart from the rest, so that the next group's panels can
+            // start while the rest is updated (one-group look-ahead)
             sp.gemm_off = int(gemm_tasks.size());
             int gb = 0;
+            std::vector<idx> rest_fronts;
             for (idx s : large) {
                 const idx w = S.w[s], f = S.f[s], ld = dld[s], pan = dpan[s];
                 if (w <= kb) continue;
                 const idx ke = std::min<idx>(kb + NB, w);          // end of this block
                 if (ke != std::min<idx>(ko + GB, w) || ke >= w) continue;
                 const int64_t a = pan + ko * ld + ke;
-                gemm(a, a, pan + ke * ld + ke, int(ld), int(ld), int(ld), f - ke, w - ke, ke - ko, 1, 0, gb);
+                gemm(a, a, pan + ke * ld + ke, int(ld), int(ld), int(ld), f - ke, std::min<idx>(GB, w - ke), ke - ko,
+                     1, 0, gb);
+                if (ke + GB < w) rest_fronts.push_back(s);
             }
             sp.gemm_n = int(gemm_tasks.size()) - sp.gemm_off;
             sp.gemm_tiles = gb;
+            sp.rest_off = int(gemm_tasks.size());
+            int rb = 0;
+            for (idx s : rest_fronts) {
+                const idx w = S.w[s], f = S.f[s], ld = dld[s], pan = dpan[s];
+                const idx ke = std::min<idx>(kb + NB, w), kr = ke + GB;
+                const int64_t a = pan + ko * ld + kr;
+                gemm(a, a, pan + kr * ld + kr, int(ld), int(ld), int(ld), f - kr, w - kr, ke - ko, 1, 0, rb);
+            }
+            sp.rest_n = int(gemm_tasks.size()) - sp.rest_off;
+            sp.rest_tiles = rb;
             L.steps.push_back(sp);
         }
         L.syrk_off = int(gemm_tasks.size());
@@ -388,6 +403,14 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
     // 1: single-pass TF32 on tcgen05, 3: split 3xTF32 (mma.sync), 0: single-pass TF32 on mma.sync
     const int tc = h->opt.tensor_cores;
     const int split = tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : (h->opt.refine ? 1 : 3);
+    if (!h->side) {
+        int least = 0, greatest = 0;
+        MFS_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        MFS_CUDA(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, greatest));
+        MFS_CUDA(cudaEventCreateWithFlags(&h->ev_ready, cudaEventDisableTiming));
+        MFS_CUDA(cudaEventCreateWithFlags(&h->ev_rest, cudaEventDisableTiming));
+        MFS_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    }
     launch_zero<T>(factor, ds.panel_alloc, st);
     MFS_LAUNCHED();
     launch_inject<T>(ds.plan.p, int64_t(S.plan.size()), S.vb, S.src_ld, Ax, Bx, Bx ? sigma : 0.0, factor, st);
@@ -414,20 +437,45 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         if (L.large_count == 0) continue;
         launch_assemble_large<T>(ds.asm_tasks.p + L.asm_off, L.asm_n, L.asm_tiles, ds.sd, factor, upd, st);
         MFS_LAUNCHED();
+        // One-group look-ahead: the column-block chain (left-looking update, panel, row
+        // solve) and the update of the next group's columns run on a high-priority
+        // stream, so their CTAs take the next free SMs; the update of the columns after
+        // the next group runs meanwhile on the handle's stream. The next such update
+        // overlaps that region and waits for it; the level's SYRK waits for both.
+        cudaStream_t hs = h->side;
+        MFS_CUDA(cudaEventRecord(h->ev_join, st));
+        MFS_CUDA(cudaStreamWaitEvent(hs, h->ev_join, 0));
+        bool rest_pending = false;
         for (const auto &sp : L.steps) {
             launch_gemm<T>(ds.gemm_tasks.p + sp.left_off, sp.left_n, sp.left_tiles, factor, factor, factor, split,
-                           h->gemm_err.p, st);
+                           h->gemm_err.p, hs);
             MFS_LAUNCHED();
             launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, dscr, pv, split == 1,
-                            st);
+                            hs);
             MFS_LAUNCHED();
             launch_gemm<T>(ds.gemm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, factor, dscr, factor, split,
-                           h->gemm_err.p, st);
+                           h->gemm_err.p, hs);
             MFS_LAUNCHED();
+            if (sp.gemm_n == 0) continue;
+            if (sp.rest_n > 0) MFS_CUDA(cudaEventRecord(h->ev_ready, hs));
+            if (rest_pending) {
+                MFS_CUDA(cudaStreamWaitEvent(hs, h->ev_rest, 0));
+                rest_pending = false;
+            }
             launch_gemm<T>(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor, factor, split,
-                           h->gemm_err.p, st);
+                           h->gemm_err.p, hs);
             MFS_LAUNCHED();
+            if (sp.rest_n > 0) {
+                MFS_CUDA(cudaStreamWaitEvent(st, h->ev_ready, 0));
+                launch_gemm<T>(ds.gemm_tasks.p + sp.rest_off, sp.rest_n, sp.rest_tiles, factor, factor, factor, split,
+                               h->gemm_err.p, st);
+                MFS_LAUNCHED();
+                MFS_CUDA(cudaEventRecord(h->ev_rest, st));
+                rest_pending = true;
+            }
         }
+        MFS_CUDA(cudaEventRecord(h->ev_join, hs));
+        MFS_CUDA(cudaStreamWaitEvent(st, h->ev_join, 0));
         if (L.syrk_n > 0) {
             launch_gemm<T>(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, factor, upd, split, h->gemm_err.p, st);
             MFS_LAUNCHED();
@@ -714,6 +762,13 @@ mfs_status mfs_destroy(mfs_handle *h) {
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->side) {
+        cudaStreamSynchronize(h->side);
+        cudaStreamDestroy(h->side);
+    }
+    if (h->ev_ready) cudaEventDestroy(h->ev_ready);
+    if (h->ev_rest) cudaEventDestroy(h->ev_rest);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
     if (h->fail_host) cudaFreeHost(h->fail_host);
     if (h->dots_host) cudaFreeHost(h->dots_host);
     delete h;

@@ -78,7 +78,8 @@ struct LevelPlan {
         int left_off, left_n, left_tiles;   // the block's columns updated by the earlier blocks of its group
         int potrf_off, potrf_n, potrf_maxnb;
         int trsm_off, trsm_n, trsm_tiles;   // X := X inv(L)^T of the rows below the block
-        int gemm_off, gemm_n, gemm_tiles;   // trailing update of the columns after a finished group
+        int gemm_off, gemm_n, gemm_tiles;   // after a finished group: update of the next group's columns
+        int rest_off, rest_n, rest_tiles;   // ... and of the columns after it (overlaps the next group)
     };
     std::vector<Step> steps;
     int syrk_off = 0, syrk_n = 0, syrk_tiles = 0;
@@ -175,6 +176,8 @@ struct mfs_handle {
     mfs_stats stats{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::shared_ptr<void> lpc_work;      // learned preconditioner: work buffers (built on first use)
+    cudaStream_t side = nullptr;         // high-priority stream of the factorization's column-block chain
+    cudaEvent_t ev_ready = nullptr, ev_rest = nullptr, ev_join = nullptr;
 };
 
 inline void set_device(mfs_handle *h) {

@@ -32,6 +32,18 @@ namespace mfs {
 namespace {
 
 constexpr int kPanelThreads = 256;
+constexpr int kPanelLoadVecs = 16;                 // 16-byte loads per thread and batch
+
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    using type = float4;
+};
+template <>
+struct Vec16<double> {
+    using type = double2;
+};
 
 template <typename T>
 __device__ __forceinline__ T recip_sqrt(T x);
@@ -173,15 +185,39 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask
     T *rdiag = P + 6 * 32 * 33;                      // reciprocal diagonal of L
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     T *blk = factor + tk.off;
-    // unrolled so that many global loads are in flight per thread
-#pragma unroll 8
-    for (int q = tid; q < NBP * NBP; q += nt) {
-        const int j = q / NBP, i = q - j * NBP;
-        T v = T(0);
-        if (i < nb && j < nb) v = i >= j ? blk[int64_t(j) * ld + i] : T(0);
-        else if (i == j) v = T(1);
-        D[j * LDD + i] = v;
-        Iv[j * LDD + i] = T(0);
+    // Load with 16-byte vectors (panel columns, the block's first row and ld are 16-byte
+    // aligned), every load of a batch issued before the first shared-memory store.
+    {
+        using V = typename Vec16<T>::type;
+        constexpr int E = 16 / int(sizeof(T));
+        const int nvec = NBP / E, tot = NBP * nvec;
+        for (int base = 0; base < tot; base += kPanelLoadVecs * nt) {
+            V buf[kPanelLoadVecs];
+#pragma unroll
+            for (int u = 0; u < kPanelLoadVecs; ++u) {
+                const int q = base + tid + u * nt;
+                const int j = q / nvec, i0 = (q - j * nvec) * E;
+                if (q < tot && j < nb && i0 + E <= nb)
+                    buf[u] = *reinterpret_cast<const V *>(blk + int64_t(j) * ld + i0);
+            }
+#pragma unroll
+            for (int u = 0; u < kPanelLoadVecs; ++u) {
+                const int q = base + tid + u * nt;
+                if (q >= tot) continue;
+                const int j = q / nvec, i0 = (q - j * nvec) * E;
+                const T *bv = reinterpret_cast<const T *>(&buf[u]);
+                const bool full = j < nb && i0 + E <= nb;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int i = i0 + e;
+                    T v;
+                    if (i < nb && j < nb) v = i >= j ? (full ? bv[e] : blk[int64_t(j) * ld + i]) : T(0);
+                    else v = (i == j) ? T(1) : T(0);
+                    D[j * LDD + i] = v;
+                    Iv[j * LDD + i] = T(0);
+                }
+            }
+        }
     }
     __syncthreads();
     if (warp == 0) warp_diag_tile(D, Iv, rdiag, LDD, 0, nb, lane, tk.col, pv.fail_col, pv.perturbed, pv.dorig);
@@ -256,13 +292,37 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask
         }
         __syncthreads();
     }
-#pragma unroll 4
-    for (int q = tid; q < nb * nb; q += nt) {
-        const int j = q / nb, i = q - j * nb;
-        if (i >= j) blk[int64_t(j) * ld + i] = D[j * LDD + i];
-        T v = i >= j ? Iv[j * LDD + i] : T(0);
-        if (round_inv) v = round_operand(v);
-        inv_scratch[tk.inv_full + int64_t(j) * tk.ldi + i] = v;
+    // L (lower triangle only: the strict upper part keeps its stored values) and inv(L)
+    // (zeros above the diagonal) with 16-byte vector stores where a vector is whole
+    {
+        using V = typename Vec16<T>::type;
+        constexpr int E = 16 / int(sizeof(T));
+        const int nvec = (nb + E - 1) / E, tot = nb * nvec;
+        for (int q = tid; q < tot; q += nt) {
+            const int j = q / nvec, i0 = (q - j * nvec) * E;
+            V lv, iv;
+            T *l = reinterpret_cast<T *>(&lv), *ivp = reinterpret_cast<T *>(&iv);
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int i = i0 + e;
+                l[e] = D[j * LDD + i];
+                const T v = i >= j ? Iv[j * LDD + i] : T(0);
+                ivp[e] = round_inv ? round_operand(v) : v;
+            }
+            T *dl = blk + int64_t(j) * ld + i0;
+            T *di = inv_scratch + tk.inv_full + int64_t(j) * tk.ldi + i0;
+            if (i0 + E <= nb) {
+                *reinterpret_cast<V *>(di) = iv;
+                if (i0 >= j) {
+                    *reinterpret_cast<V *>(dl) = lv;
+                    continue;
+                }
+            } else {
+                for (int e = 0; e < E && i0 + e < nb; ++e) di[e] = ivp[e];
+            }
+            for (int e = 0; e < E && i0 + e < nb; ++e)
+                if (i0 + e >= j) dl[e] = l[e];
+        }
     }
     if (tk.inv_out >= 0) {
         // 64 x 64 diagonal blocks of inv(L) (the inverses of L's 64 x 64 diagonal blocks)
