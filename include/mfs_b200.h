@@ -76,7 +76,9 @@ typedef struct {
     int32_t tensor_cores;       /* FP32 Schur updates: 0 auto (TF32 with refinement, else split 3xTF32),
                                    1 TF32 on tcgen05, 2 split 3xTF32 (FP32-level products, mma.sync),
                                    3 TF32 on mma.sync (the pre-Blackwell tensor-core path) */
-    int32_t reserved[7];
+    int32_t time_kernels;       /* 1: mfs_numeric times each tensor-core GEMM launch with CUDA events on its
+                                   stream (mfs_stats.gemm_ms / gemm_flops); adds event records, off by default */
+    int32_t reserved[6];
 } mfs_options;
 
 typedef struct mfs_handle mfs_handle;
@@ -231,6 +233,9 @@ typedef struct {
     int32_t pcg_fallback;        /* 1: the last mfs_pcg_solve missed the tolerance and used the factor */
     int32_t reserved_stats;
     double pcg_ms;               /* device time of the last converged mfs_pcg_solve (inference + PCG) */
+    double gemm_ms;              /* time_kernels: summed device time of the last mfs_numeric's GEMM launches */
+    double gemm_flops;           /* algorithmic flops of those launches (2mnk, triangle-aware; m n k per row solve) */
+    int64_t gemm_launches;       /* GEMM launches timed */
 } mfs_stats;
 mfs_status mfs_get_stats(const mfs_handle *h, mfs_stats *st);
 

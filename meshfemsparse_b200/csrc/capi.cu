@@ -354,6 +354,16 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     up(ds->asm_tasks, asm_tasks);
     up(ds->potrf_tasks, potrf_tasks);
     up(ds->gemm_tasks, gemm_tasks);
+    // algorithmic flops per task: 2 m n k for an update (the lower triangle only for
+    // lower tasks, whose block starts on the diagonal), m n k for a row solve by inv(L)
+    ds->gemm_flops_prefix.assign(gemm_tasks.size() + 1, 0.0);
+    for (size_t t = 0; t < gemm_tasks.size(); ++t) {
+        const GemmTask &g = gemm_tasks[t];
+        const double m = g.m, n = g.n, k = g.k;
+        double fl = g.mode == 1 ? m * n * k : 2.0 * m * n * k;
+        if (g.lower && g.mode == 0) fl = 2.0 * k * (m * n - std::min(m, n) * (std::min(m, n) - 1.0) / 2.0);
+        ds->gemm_flops_prefix[t + 1] = ds->gemm_flops_prefix[t] + fl;
+    }
     up(ds->sasm_tasks, sasm);
     up(ds->ftri_tasks, ftri);
     up(ds->btri_tasks, btri);
@@ -403,6 +413,31 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
     // 1: single-pass TF32 on tcgen05, 3: split 3xTF32 (mma.sync), 0: single-pass TF32 on mma.sync
     const int tc = h->opt.tensor_cores;
     const int split = tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : (h->opt.refine ? 1 : 3);
+    // GEMM launch, bracketed by CUDA events on its stream when kernel timing is on
+    const bool timing = h->opt.time_kernels != 0;
+    h->gemm_events_used = 0;
+    h->gemm_flops_timed = 0.0;
+    auto tgemm = [&](const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int sp, int *err,
+                     cudaStream_t s) {
+        if (ntasks <= 0) return;
+        if (!timing) {
+            launch_gemm<T>(tasks, ntasks, ntiles, A, B, C, sp, err, s);
+            return;
+        }
+        if (h->gemm_events_used + 2 > h->gemm_events.size()) {
+            cudaEvent_t e0, e1;
+            MFS_CUDA(cudaEventCreate(&e0));
+            MFS_CUDA(cudaEventCreate(&e1));
+            h->gemm_events.push_back(e0);
+            h->gemm_events.push_back(e1);
+        }
+        const size_t t0 = size_t(tasks - ds.gemm_tasks.p);
+        h->gemm_flops_timed += ds.gemm_flops_prefix[t0 + ntasks] - ds.gemm_flops_prefix[t0];
+        MFS_CUDA(cudaEventRecord(h->gemm_events[h->gemm_events_used], s));
+        launch_gemm<T>(tasks, ntasks, ntiles, A, B, C, sp, err, s);
+        MFS_CUDA(cudaEventRecord(h->gemm_events[h->gemm_events_used + 1], s));
+        h->gemm_events_used += 2;
+    };
     if (!h->side) {
         int least = 0, greatest = 0;
         MFS_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -447,13 +482,13 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         MFS_CUDA(cudaStreamWaitEvent(hs, h->ev_join, 0));
         bool rest_pending = false;
         for (const auto &sp : L.steps) {
-            launch_gemm<T>(ds.gemm_tasks.p + sp.left_off, sp.left_n, sp.left_tiles, factor, factor, factor, split,
+            tgemm(ds.gemm_tasks.p + sp.left_off, sp.left_n, sp.left_tiles, factor, factor, factor, split,
                            h->gemm_err.p, hs);
             MFS_LAUNCHED();
             launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, dscr, pv, split == 1,
                             hs);
             MFS_LAUNCHED();
-            launch_gemm<T>(ds.gemm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, factor, dscr, factor, split,
+            tgemm(ds.gemm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, factor, dscr, factor, split,
                            h->gemm_err.p, hs);
             MFS_LAUNCHED();
             if (sp.gemm_n == 0) continue;
@@ -462,12 +497,12 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
                 MFS_CUDA(cudaStreamWaitEvent(hs, h->ev_rest, 0));
                 rest_pending = false;
             }
-            launch_gemm<T>(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor, factor, split,
+            tgemm(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor, factor, split,
                            h->gemm_err.p, hs);
             MFS_LAUNCHED();
             if (sp.rest_n > 0) {
                 MFS_CUDA(cudaStreamWaitEvent(st, h->ev_ready, 0));
-                launch_gemm<T>(ds.gemm_tasks.p + sp.rest_off, sp.rest_n, sp.rest_tiles, factor, factor, factor, split,
+                tgemm(ds.gemm_tasks.p + sp.rest_off, sp.rest_n, sp.rest_tiles, factor, factor, factor, split,
                                h->gemm_err.p, st);
                 MFS_LAUNCHED();
                 MFS_CUDA(cudaEventRecord(h->ev_rest, st));
@@ -477,7 +512,7 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         MFS_CUDA(cudaEventRecord(h->ev_join, hs));
         MFS_CUDA(cudaStreamWaitEvent(st, h->ev_join, 0));
         if (L.syrk_n > 0) {
-            launch_gemm<T>(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, factor, upd, split, h->gemm_err.p, st);
+            tgemm(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, factor, upd, split, h->gemm_err.p, st);
             MFS_LAUNCHED();
         }
     }
@@ -699,6 +734,7 @@ mfs_status mfs_default_options(mfs_options *opt) {
     opt->refine_maxit = 50;
     opt->use_graphs = 0;
     opt->tensor_cores = 0;
+    opt->time_kernels = 0;
     return MFS_OK;
 }
 
@@ -769,6 +805,7 @@ mfs_status mfs_destroy(mfs_handle *h) {
     if (h->ev_ready) cudaEventDestroy(h->ev_ready);
     if (h->ev_rest) cudaEventDestroy(h->ev_rest);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
+    for (cudaEvent_t e : h->gemm_events) cudaEventDestroy(e);
     if (h->fail_host) cudaFreeHost(h->fail_host);
     if (h->dots_host) cudaFreeHost(h->dots_host);
     delete h;
@@ -903,6 +940,14 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
         cudaEventElapsedTime(&ms, h->ev0, h->ev1);
         h->stats.factor_ms = ms;
         h->stats.perturbed_pivots = h->fail_host[1];
+        h->stats.gemm_ms = 0.0;
+        h->stats.gemm_flops = h->gemm_flops_timed;
+        h->stats.gemm_launches = int64_t(h->gemm_events_used / 2);
+        for (size_t e = 0; e + 1 < h->gemm_events_used; e += 2) {
+            float g = 0;
+            MFS_CUDA(cudaEventElapsedTime(&g, h->gemm_events[e], h->gemm_events[e + 1]));
+            h->stats.gemm_ms += g;
+        }
         h->cur.sigma = sigma;
         if (h->fail_host[2]) {
             MFS_CUDA(cudaMemset(h->gemm_err.p, 0, sizeof(int)));

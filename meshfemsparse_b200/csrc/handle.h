@@ -122,6 +122,7 @@ struct DevSym {
     std::vector<int32_t> dld;            // device panel leading dimensions
     int64_t panel_alloc = 0;             // elements of the padded panels
     std::shared_ptr<void> lpc_graph;     // learned preconditioner: graph arrays (built on first use)
+    std::vector<double> gemm_flops_prefix;   // prefix sums of the GEMM tasks' algorithmic flops
     size_t bytes() const {
         return w.bytes() * 5 + col0.bytes() + child_ptr.bytes() + child_list.bytes() + struct_rows.bytes() +
                rel.bytes() + small_list.bytes() + all_list.bytes() + pan_off.bytes() + upd_off.bytes() +
@@ -178,6 +179,9 @@ struct mfs_handle {
     std::shared_ptr<void> lpc_work;      // learned preconditioner: work buffers (built on first use)
     cudaStream_t side = nullptr;         // high-priority stream of the factorization's column-block chain
     cudaEvent_t ev_ready = nullptr, ev_rest = nullptr, ev_join = nullptr;
+    std::vector<cudaEvent_t> gemm_events;    // time_kernels: (start, end) per GEMM launch
+    size_t gemm_events_used = 0;
+    double gemm_flops_timed = 0.0;
 };
 
 inline void set_device(mfs_handle *h) {
