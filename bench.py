@@ -68,6 +68,17 @@ def dist_setup(args):
     return rank, world, local, pg
 
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest of every rank's value (a timed region's device time): replicas report
+    the slowest rank. Every rank must call it at the same point."""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -181,10 +192,7 @@ def run_b200(args, rank, world, local, dist):
         launches = f.stats()["kernel_launches"] - l0
         clocks = sampler.stop() if sampler else None
         total = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([total], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total = float(t.item())
+        total = max_over_ranks(total, dist, dev)
         if dist:
             dist.barrier()
         return total, launches, clocks
@@ -378,10 +386,7 @@ def run_newton_sequence(args, rank, world, local, dist):
         launches = f32.stats()["kernel_launches"] - l0
         clocks = sampler.stop() if sampler else None
         total = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([total], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total = float(t.item())
+        total = max_over_ranks(total, dist, dev)
         return total / K, info, launches, clocks
 
     pB, pX = C.c_void_p(B.data_ptr()), C.c_void_p(X.data_ptr())
