@@ -29,7 +29,13 @@ using namespace mfs;
 
 namespace {
 
+// Fronts up to this size are factored whole in one CTA's shared memory (f x f entries).
 int small_front_limit(const mfs_handle *h) {
+    const int el = h->opt.precision == MFS_PREC_FP32 ? 4 : 8;
+    const int cap = int(std::sqrt(double(kMaxSmemOptin) / el));
+    if (h->opt.small_front_max > cap)
+        throw StatusError(MFS_INVALID_ARG, "small_front_max above " + std::to_string(cap) +
+                                               " (a front must fit one CTA's shared memory)");
     if (h->opt.small_front_max > 0) return h->opt.small_front_max;
     return h->opt.precision == MFS_PREC_FP32 ? 160 : 128;
 }
@@ -403,6 +409,22 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     return ds;
 }
 
+void ensure_side_stream(mfs_handle *h) {
+    if (h->side) return;
+    int least = 0, greatest = 0;
+    MFS_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    MFS_CUDA(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, greatest));
+    MFS_CUDA(cudaEventCreateWithFlags(&h->ev_ready, cudaEventDisableTiming));
+    MFS_CUDA(cudaEventCreateWithFlags(&h->ev_rest, cudaEventDisableTiming));
+    MFS_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+}
+
+void clear_factor_graphs(mfs_handle *h) {
+    for (auto &g : h->factor_graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    h->factor_graphs.clear();
+}
+
 template <typename T>
 void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const double *Ax, const double *Bx,
                 double sigma) {
@@ -438,14 +460,6 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         MFS_CUDA(cudaEventRecord(h->gemm_events[h->gemm_events_used + 1], s));
         h->gemm_events_used += 2;
     };
-    if (!h->side) {
-        int least = 0, greatest = 0;
-        MFS_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        MFS_CUDA(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, greatest));
-        MFS_CUDA(cudaEventCreateWithFlags(&h->ev_ready, cudaEventDisableTiming));
-        MFS_CUDA(cudaEventCreateWithFlags(&h->ev_rest, cudaEventDisableTiming));
-        MFS_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
-    }
     launch_zero<T>(factor, ds.panel_alloc, st);
     MFS_LAUNCHED();
     launch_inject<T>(ds.plan.p, int64_t(S.plan.size()), S.vb, S.src_ld, Ax, Bx, Bx ? sigma : 0.0, factor, st);
@@ -516,6 +530,62 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
             MFS_LAUNCHED();
         }
     }
+}
+
+// The factorization's launch sequence, replayed from an instantiated CUDA graph when
+// use_graphs is on: the first call with a new key runs directly (it also makes the
+// one-time allocations and kernel attribute settings), the second captures the
+// sequence from the handle's stream (the look-ahead stream joins the capture through
+// its events) and later calls launch the graph. Kernel timing runs directly.
+template <typename T>
+void factor_sequence(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const double *Ax, const double *Bx,
+                     double sigma) {
+    ensure_side_stream(h);
+    const int tc = h->opt.tensor_cores;
+    const int split = tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : (h->opt.refine ? 1 : 3);
+    // (the legacy default stream cannot be captured: graphs need a handle or caller stream)
+    if (!h->opt.use_graphs || h->opt.time_kernels || h->stream == nullptr) {
+        run_factor<T>(h, ds, factor, upd, dscr, Ax, Bx, sigma);
+        return;
+    }
+    const void *dorig = h->dorig.p;
+    mfs_handle::FactorGraph key{&ds, factor, upd, dscr, Ax, Bx, dorig, sigma, split, nullptr};
+    auto same = [&](const mfs_handle::FactorGraph &g) {
+        return g.ds == key.ds && g.factor == key.factor && g.upd == key.upd && g.dscr == key.dscr &&
+               g.ax == key.ax && g.bx == key.bx && g.dorig == key.dorig && g.sigma == key.sigma &&
+               g.split == key.split;
+    };
+    auto it = std::find_if(h->factor_graphs.begin(), h->factor_graphs.end(), same);
+    if (it != h->factor_graphs.end() && it->exec) {
+        MFS_CUDA(cudaGraphLaunch(it->exec, h->stream));
+        return;
+    }
+    if (it == h->factor_graphs.end()) {
+        run_factor<T>(h, ds, factor, upd, dscr, Ax, Bx, sigma);
+        if (h->factor_graphs.size() >= 4) {
+            if (h->factor_graphs.front().exec) cudaGraphExecDestroy(h->factor_graphs.front().exec);
+            h->factor_graphs.erase(h->factor_graphs.begin());
+        }
+        h->factor_graphs.push_back(key);
+        return;
+    }
+    cudaStream_t st = h->stream;
+    MFS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    try {
+        run_factor<T>(h, ds, factor, upd, dscr, Ax, Bx, sigma);
+    } catch (...) {
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    MFS_CUDA(cudaStreamEndCapture(st, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    MFS_CUDA(e);
+    it->exec = exec;
+    MFS_CUDA(cudaGraphLaunch(exec, st));
 }
 
 template <typename T>
@@ -806,6 +876,7 @@ mfs_status mfs_destroy(mfs_handle *h) {
     if (h->ev_rest) cudaEventDestroy(h->ev_rest);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
     for (cudaEvent_t e : h->gemm_events) cudaEventDestroy(e);
+    clear_factor_graphs(h);
     if (h->fail_host) cudaFreeHost(h->fail_host);
     if (h->dots_host) cudaFreeHost(h->dots_host);
     delete h;
@@ -872,6 +943,7 @@ mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, cons
             h->stats.num_levels = int(Sp->nlevels);
             return;
         }
+        clear_factor_graphs(h);
         auto ds = upload_symbolic(h, Sp);
         ds->ax_len = Ap[n_blocks] * int64_t(block_size) * block_size;
         ds->Ap_full.assign(Ap, Ap + n_blocks + 1);
@@ -923,13 +995,13 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
             h->cur.f32->ensure(size_t(ds.factor_alloc));
             h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
             h->dscr32.ensure(size_t(std::max<int64_t>(ds.inv_scratch, 1)));
-            run_factor<float>(h, ds, h->cur.f32->p, h->upd32.p, h->dscr32.p, h->cur.ax->p, dBx, sigma);
+            factor_sequence<float>(h, ds, h->cur.f32->p, h->upd32.p, h->dscr32.p, h->cur.ax->p, dBx, sigma);
         } else {
             if (!h->cur.f64 || h->cur.f64.use_count() > 1) h->cur.f64 = std::make_shared<DBuf<double>>();
             h->cur.f64->ensure(size_t(ds.factor_alloc));
             h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
             h->dscr64.ensure(size_t(std::max<int64_t>(ds.inv_scratch, 1)));
-            run_factor<double>(h, ds, h->cur.f64->p, h->upd64.p, h->dscr64.p, h->cur.ax->p, dBx, sigma);
+            factor_sequence<double>(h, ds, h->cur.f64->p, h->upd64.p, h->dscr64.p, h->cur.ax->p, dBx, sigma);
         }
         MFS_CUDA(cudaEventRecord(h->ev1, st));
         MFS_CUDA(cudaMemcpyAsync(h->fail_host, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1279,6 +1351,7 @@ mfs_status mfs_swap_stash(mfs_handle *h) {
     if (!h) return MFS_INVALID_ARG;
     return guarded(h, [&] {
         if (!h->has_stash) throw StatusError(MFS_NO_FACTOR, "No stashed factorization");
+        clear_factor_graphs(h);
         std::swap(h->cur, h->stash);
         if (h->cur.sym) {
             const Symbolic &S = *h->cur.sym->S;
@@ -1290,6 +1363,7 @@ mfs_status mfs_swap_stash(mfs_handle *h) {
 
 mfs_status mfs_clear_stash(mfs_handle *h) {
     if (!h) return MFS_INVALID_ARG;
+    clear_factor_graphs(h);
     h->stash = State();
     h->has_stash = false;
     return MFS_OK;
@@ -1303,6 +1377,7 @@ mfs_status mfs_has_stash(const mfs_handle *h, int32_t *has) {
 
 mfs_status mfs_clear_factors(mfs_handle *h) {
     if (!h) return MFS_INVALID_ARG;
+    clear_factor_graphs(h);
     h->cur = State();
     h->asm_ax.reset();
     h->asm_spare.reset();

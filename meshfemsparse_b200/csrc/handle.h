@@ -179,6 +179,15 @@ struct mfs_handle {
     std::shared_ptr<void> lpc_work;      // learned preconditioner: work buffers (built on first use)
     cudaStream_t side = nullptr;         // high-priority stream of the factorization's column-block chain
     cudaEvent_t ev_ready = nullptr, ev_rest = nullptr, ev_join = nullptr;
+    // use_graphs: instantiated graphs of the factorization's launch sequence, keyed by
+    // everything the launches bake in (symbolic data, buffers, values, shift)
+    struct FactorGraph {
+        const void *ds, *factor, *upd, *dscr, *ax, *bx, *dorig;
+        double sigma;
+        int split;
+        cudaGraphExec_t exec;
+    };
+    std::vector<FactorGraph> factor_graphs;
     std::vector<cudaEvent_t> gemm_events;    // time_kernels: (start, end) per GEMM launch
     size_t gemm_events_used = 0;
     double gemm_flops_timed = 0.0;

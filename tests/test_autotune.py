@@ -1,0 +1,26 @@
+"""Autotuner selection and on-disk cache (no GPU: the timing is injected)."""
+from meshfemsparse_b200 import autotune
+
+from helpers import grid_forest
+
+
+def test_picks_fastest_and_caches(tmp_path):
+    H = grid_forest(6)
+    pins = [0, 1, 2]
+    calls = []
+
+    def fake(cut, tc):
+        calls.append((cut, tc))
+        return abs(cut - 128) + (0.5 if tc == 2 else 0.0)
+
+    cache = tmp_path / "tune.json"
+    r = autotune.tune(H, pins, None, None, None, single=True, refine=True, cache=cache, measure=fake)
+    assert (r["small_front_max"], r["tensor_cores"]) == (128, 1) and not r["cached"]
+    assert len(calls) == len(autotune.CUTOFFS_FP32) * 2
+    r2 = autotune.tune(H, pins, None, None, None, single=True, refine=True, cache=cache, measure=fake)
+    assert r2["cached"] and r2["small_front_max"] == 128 and len(calls) == len(autotune.CUTOFFS_FP32) * 2
+    # another precision or other pins is another key
+    r3 = autotune.tune(H, pins, None, None, None, single=False, refine=False, cache=cache, measure=fake)
+    assert not r3["cached"] and r3["tensor_cores"] == 0
+    r4 = autotune.tune(H, [3, 4, 5], None, None, None, single=True, refine=True, cache=cache, measure=fake)
+    assert not r4["cached"]
