@@ -166,6 +166,92 @@ class BlockCSCHessian:
                         offs.append(bs * bs * k + c * bs + r)
         return np.asarray(offs, dtype=np.int64)
 
+    # ------------------------------------------------------- binary format
+    # The reference's on-disk format (BlockCSCHessian.cc:11-100), always written in
+    # the non-contiguous block layout: header size_t blockSize, size_t numBlocks,
+    # int64 m, n (= numBlocks), nz (blocks), snz (scalars in Ax, 0 when sparsity
+    # only), uint32 symmetry mode (1 = upper triangle); then Ap (n + 1), Ai (nz)
+    # as int64 and Ax (snz) as double. In that layout each scalar column of a block
+    # column lists the bs rows of every off-diagonal block, then rows 0..c of the
+    # diagonal block (upper triangle only): the scalar upper-CSC value order.
+    _SYM_UPPER = 1
+
+    def _noncontiguous_offsets(self) -> np.ndarray:
+        """Offset in this (contiguous) Ax of every value of the non-contiguous layout, in order."""
+        bs, nb, nz = self.bs, self.numBlocks, self.nz
+        bj = np.repeat(np.arange(nb, dtype=np.int64), np.diff(self.Ap))
+        last = self.Ap[1:] - 1
+        if nb and (np.any(np.diff(self.Ap) <= 0) or np.any(self.Ai[last] != np.arange(nb))):
+            raise ValueError("every block column must end with its diagonal block")
+        diag = self.Ai == bj
+        K = np.repeat(np.arange(nz, dtype=np.int64), bs * bs)
+        C = np.tile(np.repeat(np.arange(bs, dtype=np.int64), bs), nz)
+        R = np.tile(np.tile(np.arange(bs, dtype=np.int64), bs), nz)
+        keep = ~diag[K] | (R <= C)
+        K, C, R = K[keep], C[keep], R[keep]
+        order = np.lexsort((R, K, C, bj[K]))
+        return (bs * bs * K + C * bs + R)[order]
+
+    def dumpBinaryToStream(self, f) -> None:
+        """BlockCSCHessianBase::dumpBinaryToStream (BlockCSCHessian.cc:11-40)."""
+        offs = self._noncontiguous_offsets()
+        snz = 0 if self.Ax is None else int(offs.size)
+        f.write(struct.pack("<QQ", self.bs, self.numBlocks))
+        f.write(struct.pack("<qqqqI", self.numBlocks, self.numBlocks, self.nz, snz, self._SYM_UPPER))
+        f.write(self.Ap.astype("<i8").tobytes())
+        f.write(self.Ai.astype("<i8").tobytes())
+        if snz:
+            f.write(self.Ax[offs].astype("<f8").tobytes())
+
+    def dumpBinaryToFile(self, path) -> None:
+        with open(path, "wb") as f:
+            self.dumpBinaryToStream(f)
+
+    dumpBinary = dumpBinaryToFile
+
+    @staticmethod
+    def constructFromBinaryStream(f) -> "BlockCSCHessian":
+        """BlockCSCHessianBase::constructFromBinaryStream / readBinaryFromStream
+        (BlockCSCHessian.cc:42-100): returns the contiguous-block form; the strict
+        lower triangle of each diagonal block (not stored) mirrors its upper triangle."""
+        def read(nbytes):
+            b = f.read(nbytes)
+            if len(b) != nbytes:
+                raise ValueError("truncated BlockCSC binary stream")
+            return b
+        bs, nb = struct.unpack("<QQ", read(16))
+        if bs not in (1, 2, 3):
+            raise ValueError("constructFromBinaryStream: uninstantiated block size")
+        m, n, nz, snz, sym = struct.unpack("<qqqqI", read(36))
+        if sym not in (0, 1, 2):
+            raise ValueError(f"Invalid symmetry_mode: {sym}")
+        if m != nb or n != nb:
+            raise ValueError("block counts in the header disagree")
+        Ap = np.frombuffer(read(8 * (n + 1)), dtype="<i8").astype(np.int64)
+        Ai = np.frombuffer(read(8 * nz), dtype="<i8").astype(np.int64)
+        H = BlockCSCHessian(int(nb), Ap, Ai, int(bs))
+        if snz:
+            vals = np.frombuffer(read(8 * snz), dtype="<f8").astype(np.float64)
+            offs = H._noncontiguous_offsets()
+            if offs.size != snz:
+                raise ValueError("constructFromBinaryStream: scalarNNZ mismatch")
+            Ax = np.zeros(H.scalarNNZ())
+            Ax[offs] = vals
+            bj = np.repeat(np.arange(H.numBlocks), np.diff(H.Ap))
+            dk = np.nonzero(H.Ai == bj)[0]
+            blocks = Ax.reshape(-1, bs, bs)                   # [k][c][r]: column-major blocks
+            d = blocks[dk]
+            lower = np.tril_indices(bs, -1)                    # (c, r) with r < c ... mirrored below
+            d[:, lower[1], lower[0]] = d[:, lower[0], lower[1]]
+            blocks[dk] = d
+            H.Ax = Ax
+        return H
+
+    @staticmethod
+    def constructFromBinaryFile(path) -> "BlockCSCHessian":
+        with open(path, "rb") as f:
+            return BlockCSCHessian.constructFromBinaryStream(f)
+
     def toScalar(self, sparsityOnly: bool = False) -> ScalarCSC:
         bs = self.bs
         n = self.n
