@@ -107,3 +107,23 @@ def tune(H, pins, tets, Ke, rhs, single: bool = True, refine: bool = True, devic
     tmp.write_text(json.dumps(store, indent=1))
     os.replace(tmp, cache)
     return {**choice, "cached": False}
+
+
+def choose_form(H, pins, tets, Ke, rhs, device: int = 0, cache: Path | str | None = None,
+                measure: Callable | None = None, **kw) -> dict:
+    """Tune both forms and keep the faster one: FP32 factor + FP64 refinement wins
+    on large fronts (tensor-core Schur updates), plain FP64 can win on batches of
+    small fronts, where the factor is cheap and the refinement's solves dominate.
+    Returns the B200Factorizer arguments (singlePrecision, refine, small_front_max,
+    tensor_cores) and the measured ms. `measure(single, cut, tc) -> ms` replaces the
+    GPU timing (tests)."""
+    res = {}
+    for single in (True, False):
+        m = None if measure is None else (lambda cut, tc, s=single: measure(s, cut, tc))
+        res[single] = tune(H, pins, tets, Ke, rhs, single=single, refine=single, device=device, cache=cache,
+                           measure=m, **kw)
+    single = res[True]["ms"] <= res[False]["ms"]
+    r = res[single]
+    return {"singlePrecision": single, "refine": single, "small_front_max": r["small_front_max"],
+            "tensor_cores": r["tensor_cores"], "ms": r["ms"],
+            "fp32_refine_ms": res[True]["ms"], "fp64_ms": res[False]["ms"]}

@@ -24,3 +24,13 @@ def test_picks_fastest_and_caches(tmp_path):
     assert not r3["cached"] and r3["tensor_cores"] == 0
     r4 = autotune.tune(H, [3, 4, 5], None, None, None, single=True, refine=True, cache=cache, measure=fake)
     assert not r4["cached"]
+
+
+def test_choose_form_keeps_the_faster_precision(tmp_path):
+    H = grid_forest(5)
+    fast64 = lambda single, cut, tc: (10.0 if single else 5.0) + cut / 1000.0
+    r = autotune.choose_form(H, [0], None, None, None, cache=tmp_path / "a.json", measure=fast64)
+    assert not r["singlePrecision"] and not r["refine"] and r["small_front_max"] == 64
+    fast32 = lambda single, cut, tc: (3.0 if single else 5.0) + tc
+    r = autotune.choose_form(H, [1], None, None, None, cache=tmp_path / "b.json", measure=fast32)
+    assert r["singlePrecision"] and r["refine"] and r["tensor_cores"] == 1
