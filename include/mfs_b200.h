@@ -78,7 +78,11 @@ typedef struct {
                                    3 TF32 on mma.sync (the pre-Blackwell tensor-core path) */
     int32_t time_kernels;       /* 1: mfs_numeric times each tensor-core GEMM launch with CUDA events on its
                                    stream (mfs_stats.gemm_ms / gemm_flops); adds event records, off by default */
-    int32_t reserved[6];
+    int32_t nd_reuse_period;    /* > 0: a nested-dissection analysis of a changed pattern on the same variables
+                                   reuses the previous separator tree, re-dissecting only the subtrees that a
+                                   new edge violates (PARTH-style temporal reuse, ParallelNestedDissection/
+                                   README.md:86-127); a full dissection every nd_reuse_period analyses */
+    int32_t reserved[5];
 } mfs_options;
 
 typedef struct mfs_handle mfs_handle;
@@ -231,11 +235,12 @@ typedef struct {
                                     floor relative to the injected diagonal (last numeric) */
     int32_t pcg_iterations;      /* iterations of the last mfs_pcg_solve (max over RHS) */
     int32_t pcg_fallback;        /* 1: the last mfs_pcg_solve missed the tolerance and used the factor */
-    int32_t reserved_stats;
+    int32_t nd_reused;           /* 1: the last symbolic analysis reused the previous separator tree */
     double pcg_ms;               /* device time of the last converged mfs_pcg_solve (inference + PCG) */
     double gemm_ms;              /* time_kernels: summed device time of the last mfs_numeric's GEMM launches */
     double gemm_flops;           /* algorithmic flops of those launches (2mnk, triangle-aware; m n k per row solve) */
     int64_t gemm_launches;       /* GEMM launches timed */
+    int64_t nd_rebuilt_vertices; /* nd_reused: analysis variables re-dissected */
 } mfs_stats;
 mfs_status mfs_get_stats(const mfs_handle *h, mfs_stats *st);
 

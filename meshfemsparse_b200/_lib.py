@@ -36,7 +36,8 @@ class Options(C.Structure):
         ("relax_zeros", C.c_int64), ("relax_ratio", C.c_double), ("nd_leaf_size", C.c_int64),
         ("seed", C.c_uint64), ("stream", C.c_void_p), ("small_front_max", C.c_int32), ("refine", C.c_int32),
         ("refine_tol", C.c_double), ("refine_maxit", C.c_int32), ("use_graphs", C.c_int32),
-        ("tensor_cores", C.c_int32), ("time_kernels", C.c_int32), ("reserved", C.c_int32 * 6),
+        ("tensor_cores", C.c_int32), ("time_kernels", C.c_int32), ("nd_reuse_period", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -46,8 +47,9 @@ class Stats(C.Structure):
         ("refine_iterations", C.c_int32), ("failed_column", C.c_int32), ("residual", C.c_double),
         ("device_bytes", C.c_int64), ("num_levels", C.c_int32), ("num_large", C.c_int32),
         ("kernel_launches", C.c_int64), ("perturbed_pivots", C.c_int32), ("pcg_iterations", C.c_int32),
-        ("pcg_fallback", C.c_int32), ("reserved_stats", C.c_int32), ("pcg_ms", C.c_double),
+        ("pcg_fallback", C.c_int32), ("nd_reused", C.c_int32), ("pcg_ms", C.c_double),
         ("gemm_ms", C.c_double), ("gemm_flops", C.c_double), ("gemm_launches", C.c_int64),
+        ("nd_rebuilt_vertices", C.c_int64),
     ]
 
 

@@ -929,11 +929,24 @@ mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, cons
         so.relax_ratio = h->opt.relax_ratio;
         so.nd.leaf_size = h->opt.nd_leaf_size > 0 ? h->opt.nd_leaf_size : 120;
         so.nd.seed = h->opt.seed;
+        const bool reuse = h->opt.nd_reuse_period > 0 && h->nd_prev && h->nd_reuse_count < h->opt.nd_reuse_period;
+        if (reuse) so.nd_prev = h->nd_prev.get();
         std::string e = analyze(n_blocks, Ap, Ai, block_size, pinned, n_pinned, so, user_perm, *Sp, supernode_sizes,
                                 supernode_sizes ? num_supernodes : 0);
         if (!e.empty())
             throw StatusError(e.rfind("Fixed variable index out of range", 0) == 0 ? MFS_SIZE_MISMATCH : MFS_INVALID_ARG,
                               e);
+        // keep this dissection's separator tree for the next analysis
+        h->stats.nd_reused = Sp->nd_rebuilt >= 0 ? 1 : 0;
+        h->stats.nd_rebuilt_vertices = Sp->nd_rebuilt >= 0 ? Sp->nd_rebuilt : Sp->nv;
+        if (!Sp->nd_cmember.empty()) {
+            auto nd = std::make_shared<NDResult>();
+            nd->cparent = Sp->nd_cparent;
+            nd->cmember = Sp->nd_cmember;
+            nd->ncomp = Sp->nd_ncomp;
+            h->nd_prev = nd;
+            h->nd_reuse_count = Sp->nd_rebuilt >= 0 ? h->nd_reuse_count + 1 : 0;
+        }
         if (host_only) {
             auto ds = std::make_shared<DevSym>();
             ds->S = Sp;

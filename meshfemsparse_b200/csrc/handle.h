@@ -188,6 +188,8 @@ struct mfs_handle {
         cudaGraphExec_t exec;
     };
     std::vector<FactorGraph> factor_graphs;
+    std::shared_ptr<NDResult> nd_prev;       // last nested dissection (temporal reuse)
+    int nd_reuse_count = 0;                  // analyses since the last full dissection
     std::vector<cudaEvent_t> gemm_events;    // time_kernels: (start, end) per GEMM launch
     size_t gemm_events_used = 0;
     double gemm_flops_timed = 0.0;

@@ -47,6 +47,15 @@ struct NDResult {
 NDResult nested_dissection(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
                            const OrderingOptions &opt);
 
+// Temporal reuse of a previous dissection of a graph on the same vertices (the
+// PARTH idea): the previous separator tree is kept, and only the subtrees whose
+// components an edge of the new graph joins (their lowest common ancestor) are
+// dissected afresh; leaves are reordered by minimum degree as usual. Falls back to
+// a full dissection when `prev` does not match. *rebuilt_vertices = vertices
+// re-dissected.
+NDResult nested_dissection_reuse(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
+                                 const NDResult &prev, const OrderingOptions &opt, idx *rebuilt_vertices);
+
 // Minimum-degree order of the whole graph (used for the AMD-style mode and for
 // nested-dissection leaves).
 std::vector<idx> minimum_degree(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj);
@@ -65,6 +74,7 @@ struct SymbolicOptions {
     idx relax_zeros = 128;           // allowable explicit zeros per relaxed supernode
     double relax_ratio = 0.01;       // alternative allowance: zeros / stored entries
     OrderingOptions nd;
+    const NDResult *nd_prev = nullptr;   // reuse this dissection's separator tree (same vertices)
 };
 
 // One conversion-plan entry: copy a vb x vb block of the user's value array
@@ -103,6 +113,8 @@ struct Symbolic {
 
     // ND separator tree snapshot (CholeskyFactorizerBase.hh:55-59).
     std::vector<idx> nd_cparent, nd_cmember;
+    idx nd_ncomp = 0;
+    idx nd_rebuilt = -1;                    // reused dissection: vertices re-dissected (-1: full dissection)
 
     // Supernodes (postordered; children precede parents).
     idx nsn = 0;

@@ -500,17 +500,34 @@ struct NDState {
         for (idx v : S) { iperm.push_back(v); member_node[v] = snode; placed[v] = 1; }
         finish(snode);
     }
+
+    // Temporal reuse: replay the previous separator tree, re-dissecting only the
+    // subtrees whose components an edge of the new graph now joins. `first[c]` is
+    // the first postorder index in c's subtree; `rebuild[c]` marks a subtree to
+    // dissect afresh; `members[c]` are c's own vertices.
+    void replay(idx c, idx parent, const std::vector<std::vector<idx>> &children,
+                const std::vector<std::vector<idx>> &members, const std::vector<idx> &first,
+                const std::vector<char> &rebuild, const std::vector<idx> &cmember, idx &rebuilt) {
+        if (rebuild[c]) {
+            std::vector<idx> verts;
+            for (idx v = 0; v < idx(cmember.size()); ++v)
+                if (cmember[v] >= first[c] && cmember[v] <= c) verts.push_back(v);
+            rebuilt += idx(verts.size());
+            recurse(verts, parent);
+            return;
+        }
+        if (children[c].empty()) {
+            order_leaf(members[c], parent);
+            return;
+        }
+        idx node = new_node(parent);
+        for (idx ch : children[c]) replay(ch, node, children, members, first, rebuild, cmember, rebuilt);
+        for (idx v : members[c]) { iperm.push_back(v); member_node[v] = node; placed[v] = 1; }
+        finish(node);
+    }
 };
 
-}  // namespace
-
-NDResult nested_dissection(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
-                           const OrderingOptions &opt) {
-    NDState st(xadj, adj, opt, n);
-    st.iperm.reserve(n);
-    std::vector<idx> all(n);
-    std::iota(all.begin(), all.end(), 0);
-    st.recurse(all, -1);
+NDResult finish_result(NDState &st, idx n) {
     if (idx(st.iperm.size()) != n) throw std::logic_error("nested dissection lost vertices");
     NDResult r;
     r.iperm = std::move(st.iperm);
@@ -524,6 +541,50 @@ NDResult nested_dissection(idx n, const std::vector<idx> &xadj, const std::vecto
     r.cmember.resize(n);
     for (idx v = 0; v < n; ++v) r.cmember[v] = st.node_post[st.member_node[v]];
     return r;
+}
+
+}  // namespace
+
+NDResult nested_dissection_reuse(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
+                                 const NDResult &prev, const OrderingOptions &opt, idx *rebuilt_vertices) {
+    if (idx(prev.cmember.size()) != n || prev.ncomp <= 0) return nested_dissection(n, xadj, adj, opt);
+    const idx nc = prev.ncomp;
+    std::vector<std::vector<idx>> children(nc), members(nc);
+    std::vector<idx> first(nc);
+    for (idx c = 0; c < nc; ++c) first[c] = c;
+    for (idx c = 0; c < nc; ++c)               // postorder: children precede parents
+        if (prev.cparent[c] >= 0) {
+            children[prev.cparent[c]].push_back(c);
+            first[prev.cparent[c]] = std::min(first[prev.cparent[c]], first[c]);
+        }
+    for (idx v = 0; v < n; ++v) members[prev.cmember[v]].push_back(v);
+    auto is_anc = [&](idx a, idx d) { return first[a] <= d && d <= a; };
+    std::vector<char> rebuild(nc, 0);
+    for (idx u = 0; u < n; ++u)
+        for (idx e = xadj[u]; e < xadj[u + 1]; ++e) {
+            idx a = prev.cmember[u], b = prev.cmember[adj[e]];
+            if (a == b || is_anc(a, b) || is_anc(b, a)) continue;
+            idx c = a;                            // lowest common ancestor: climb until it covers b
+            while (!is_anc(c, b)) c = prev.cparent[c];
+            rebuild[c] = 1;
+        }
+    NDState st(xadj, adj, opt, n);
+    st.iperm.reserve(n);
+    idx rebuilt = 0;
+    for (idx c = 0; c < nc; ++c)
+        if (prev.cparent[c] < 0) st.replay(c, -1, children, members, first, rebuild, prev.cmember, rebuilt);
+    if (rebuilt_vertices) *rebuilt_vertices = rebuilt;
+    return finish_result(st, n);
+}
+
+NDResult nested_dissection(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
+                           const OrderingOptions &opt) {
+    NDState st(xadj, adj, opt, n);
+    st.iperm.reserve(n);
+    std::vector<idx> all(n);
+    std::iota(all.begin(), all.end(), 0);
+    st.recurse(all, -1);
+    return finish_result(st, n);
 }
 
 std::vector<idx> minimum_degree(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj) {

@@ -271,10 +271,14 @@ std::string analyze(idx nblocks, const idx *Ap, const idx *Ai, int bs, const idx
     } else if (opt.ordering == ORDER_MD) {
         iperm = minimum_degree(nv, gx, ga);
     } else {
-        NDResult nd = nested_dissection(nv, gx, ga, opt.nd);
+        idx rebuilt = -1;
+        NDResult nd = opt.nd_prev ? nested_dissection_reuse(nv, gx, ga, *opt.nd_prev, opt.nd, &rebuilt)
+                                  : nested_dissection(nv, gx, ga, opt.nd);
         iperm = nd.iperm;
         S.nd_cparent = nd.cparent;
         S.nd_cmember = nd.cmember;
+        S.nd_ncomp = nd.ncomp;
+        S.nd_rebuilt = rebuilt;
     }
     std::vector<idx> perm(nv);
     for (idx k = 0; k < nv; ++k) perm[iperm[k]] = k;

@@ -89,7 +89,7 @@ class B200Factorizer:
     def __init__(self, singlePrecision: bool = False, *, refine: bool = False, device: int = 0,
                  orderingMethod: OrderingMethod = OrderingMethod.CholmodNesdisParallel, refine_tol: float = 1e-10,
                  refine_maxit: int = 50, small_front_max: int = 0, tensor_cores: int = 0, relax: bool = True,
-                 use_graphs: bool = False,
+                 use_graphs: bool = False, nd_reuse_period: int = 0,
                  relax_zeros: int = 128, relax_ratio: float = 0.01, nd_leaf_size: int = 120, seed: int = 12345,
                  stream: int | None = None):
         self._lib = _lib.load()
@@ -98,7 +98,7 @@ class B200Factorizer:
         self._base_opts = dict(
             precision=_lib.MFS_PREC_FP32 if singlePrecision else _lib.MFS_PREC_FP64, device=device,
             refine=int(refine), refine_tol=refine_tol, refine_maxit=refine_maxit, small_front_max=small_front_max,
-            use_graphs=int(use_graphs),
+            use_graphs=int(use_graphs), nd_reuse_period=int(nd_reuse_period),
             tensor_cores=tensor_cores, relax=int(relax), relax_zeros=relax_zeros, relax_ratio=relax_ratio,
             nd_leaf_size=nd_leaf_size, seed=seed)
         opts = _lib.default_options(**self._base_opts)
