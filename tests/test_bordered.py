@@ -85,3 +85,21 @@ def test_no_border_is_the_sparse_solve():
     F = BorderedSparseFactorization(H, f, [])
     b = np.arange(H.numVars(), dtype=float)
     assert np.allclose(F.solve(b), f.solve(b))
+
+
+def test_equality_constraints_match_dense_kkt():
+    H = bordered(8, nd=2, rank=1)
+    rng = np.random.default_rng(3)
+    m = 3
+    C = rng.normal(size=(m, H.numVars()))
+    H.setConstraints(C)
+    F = BorderedSparseFactorization(H, DenseFactorizer(), [])
+    b = rng.normal(size=H.numVars())
+    r = rng.normal(size=m)
+    x, lam = F.solve(b, r, return_multipliers=True)
+    M = dense(H)
+    K = np.block([[M, C.T], [C, np.zeros((m, m))]])
+    ref = np.linalg.solve(K, np.concatenate([b, r]))
+    assert np.allclose(x, ref[:H.numVars()], rtol=1e-8, atol=1e-9)
+    assert np.allclose(lam, ref[H.numVars():], rtol=1e-8, atol=1e-9)
+    assert np.allclose(C @ x, r)
