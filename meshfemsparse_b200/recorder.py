@@ -116,9 +116,12 @@ def recorded_sequence(directory) -> list[tuple[str, int, Path]]:
     return sorted(events, key=lambda e: e[1])
 
 
-def replay(directory, factorizer, solve: bool = True, seed: int = 0) -> list[dict]:
+def replay(directory, factorizer, solve: bool = True, seed: int = 0, shift_ratio: float | None = None) -> list[dict]:
     """Run a recorded sequence through `factorizer` (a B200Factorizer). Each numeric
-    step returns its relative residual when `solve` is set (a seeded N(0,1) RHS, pins zero)."""
+    step returns its relative residual when `solve` is set (a seeded N(0,1) RHS, pins
+    zero). With `shift_ratio`, each numeric step factors H + (shift_ratio * trace(H) / n) I,
+    as the reference's benchmark driver does with 1e-8 (benchmark_linear_systems.cc:298-302);
+    the residual is then against H + shift I."""
     out = []
     pins = np.zeros(0, dtype=np.int64)
     rng = np.random.default_rng(seed)
@@ -131,15 +134,20 @@ def replay(directory, factorizer, solve: bool = True, seed: int = 0) -> list[dic
             factorizer.factorizeSymbolic(H, pins)
             out.append({"id": i, "kind": kind, "n": H.n, "blocks": H.nz})
             continue
-        factorizer.factorizeNumeric(H)
-        rec = {"id": i, "kind": kind, "n": H.n}
+        sigma = 0.0
+        if shift_ratio is not None:
+            sigma = float(shift_ratio) * H.trace() / H.n
+            factorizer.factorizeNumericWithShift(H, sigma)
+        else:
+            factorizer.factorizeNumeric(H)
+        rec = {"id": i, "kind": kind, "n": H.n, "shift": sigma}
         if solve:
             b = rng.normal(size=H.n)
             b[pins] = 0.0
             x = factorizer.solve(b)
             keep = np.ones(H.n, dtype=bool)
             keep[pins] = False
-            r = (b - H.apply(x))[keep]
+            r = (b - H.apply(x) - sigma * x)[keep]
             rec["residual"] = float(np.linalg.norm(r) / np.linalg.norm(b[keep]))
         out.append(rec)
     return out

@@ -61,6 +61,9 @@ class _Recording:
     def factorizeNumeric(self, H):
         self.calls.append(("numeric", float(H.Ax.sum())))
 
+    def factorizeNumericWithShift(self, H, sigma):
+        self.calls.append(("shifted", float(sigma)))
+
 
 def test_recorder_names_and_replay_order(tmp_path):
     rec = MatrixRecorder()
@@ -80,6 +83,10 @@ def test_recorder_names_and_replay_order(tmp_path):
     replay(tmp_path, f, solve=False)
     assert f.calls[0] == ("symbolic", H.nz, [0, 1, 2])
     assert f.calls[1][0] == "numeric" and f.calls[2][1] == pytest.approx(2.0 * f.calls[1][1])
+    g = _Recording()
+    out = replay(tmp_path, g, solve=False, shift_ratio=1e-8)
+    assert g.calls[1][0] == "shifted" and g.calls[1][1] == pytest.approx(1e-8 * H.trace() / H.n)
+    assert out[1]["shift"] == g.calls[1][1]
     rec.stopRecordingMatrices()
     rec.recordNumeric(H)                   # not recording: nothing written
     assert len(list(tmp_path.iterdir())) == 4
