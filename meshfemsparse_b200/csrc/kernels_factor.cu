@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(256) small_factor_kernel(const int32_t *__rest
 // child_rel with the analysis block size known at compile time (1 or 3), else vb.
 template <int VB>
 __device__ __forceinline__ int child_rel_vb(const int32_t *rel, int i, int vb) {
-    if (VB > 0) return rel[i / VB] + i % VB;
+    if constexpr (VB > 0) return rel[i / VB] + i % VB;
     return rel[i / vb] + i % vb;
 }
 

@@ -42,12 +42,6 @@ int lgrid(int64_t work, int per_block = kT) {
 
 __device__ __forceinline__ int64_t lmin64(int64_t a, int64_t b) { return a < b ? a : b; }
 
-__device__ __forceinline__ float warp_sum_f(float x) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
-    return x;
-}
-
 // Block (r, c) of H(i, j) for SpMV entry e (orientation row i, column j).
 __device__ __forceinline__ double hblock(const double *Ax, int64_t so, int fl, int r, int c) {
     if (fl & 2) return (r <= c) ? Ax[so + c * 3 + r] : Ax[so + r * 3 + c];

@@ -54,7 +54,7 @@ __device__ __forceinline__ bool stage_panel(int s, const SnDev &sd, const T *fac
 
 template <int VB>
 __device__ __forceinline__ int crel(const int32_t *rel, int i, int vb) {
-    if (VB > 0) return rel[i / VB] + i % VB;
+    if constexpr (VB > 0) return rel[i / VB] + i % VB;
     return rel[i / vb] + i % vb;
 }
 

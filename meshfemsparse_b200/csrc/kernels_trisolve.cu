@@ -75,15 +75,6 @@ __device__ __forceinline__ void wait_flag(const int *flag, int epoch, int *err) 
     __syncthreads();
 }
 
-__device__ __forceinline__ int find_base(const int32_t *base, int n, int t) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (base[mid] <= t) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
 __global__ void __launch_bounds__(256) fwd_asm_kernel(const SolveAsmTask *__restrict__ tasks, int ntasks, SnDev sd,
                                                       double *__restrict__ X, int64_t ldx, int nrhs,
                                                       double *__restrict__ sol) {
