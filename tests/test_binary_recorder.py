@@ -90,24 +90,3 @@ def test_recorder_names_and_replay_order(tmp_path):
     rec.stopRecordingMatrices()
     rec.recordNumeric(H)                   # not recording: nothing written
     assert len(list(tmp_path.iterdir())) == 4
-
-
-@pytest.mark.gpu
-def test_replay_recorded_newton_steps_on_gpu(tmp_path):
-    """A recorded sequence (one pattern, three value sets) replayed through the GPU factorizer."""
-    from meshfemsparse_b200 import B200Factorizer, SystemAssembler, fem
-    from oracle import pyoracle
-    nodes, tets = fem.tet_cube(3, jitter=0.1, seed=2)
-    H = SystemAssembler(nodes.shape[0]).blockSparsityPattern(tets)
-    pins = fem.bottom_pins(nodes)
-    rec = MatrixRecorder()
-    rec.recordMatrices(str(tmp_path))
-    rec.countSparsityUpdateCall()
-    rec.recordSymbolic(H, pins)
-    for scale in (1.0, 2.0, 0.5):
-        Ke = fem.linear_elastic_hessians(nodes, tets, scale, 0.3)
-        H.Ax = pyoracle.assemble(H.numBlocks, H.Ap, H.Ai, tets, Ke)
-        rec.recordNumeric(H)
-    out = replay(tmp_path, B200Factorizer())
-    assert [o["kind"] for o in out] == ["symbolic", "numeric", "numeric", "numeric"]
-    assert max(o["residual"] for o in out[1:]) <= 1e-10

@@ -36,16 +36,3 @@ def test_cpp_adapter_matches_python(tmp_path):
     # solve without a factor -> runtime_error; numeric on an analysis-only handle and a
     # non-upper pattern -> invalid_argument
     assert out[2] == "caught 7"
-
-
-@pytest.mark.gpu
-@pytest.mark.skipif(shutil.which("g++") is None, reason="g++ not available")
-def test_cpp_adapter_factor_and_solve_on_gpu(tmp_path):
-    exe = tmp_path / "adapter_solve"
-    lib_dir = _lib.LIB_PATH.parent
-    cmd = ["g++", "-std=c++17", "-O1", "-I", str(ROOT / "include"), str(ROOT / "tests/cpp/adapter_solve.cpp"),
-           "-L", str(lib_dir), "-lmfs_b200", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)]
-    subprocess.run(cmd, check=True, capture_output=True, text=True)
-    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, timeout=300).stdout.splitlines()
-    res = {ln.split()[0]: float(ln.split()[2]) for ln in out}
-    assert res["fp64"] <= 1e-12 and res["fp32+refine"] <= 1e-10

@@ -61,15 +61,3 @@ def test_spsd_system_with_fixed_values():
     assert np.allclose(u[fixed], vals)
     free = np.setdiff1d(np.arange(15), fixed)
     assert np.allclose((K @ u)[free], f[free])
-
-
-@pytest.mark.gpu
-def test_cli_on_gpu(tmp_path):
-    K, I, J, V = spd_triplets(40, 2)
-    write_triplet_binary(tmp_path / "m.bin", I, J, V)
-    b = np.linspace(-1, 1, 40)
-    np.savetxt(tmp_path / "rhs.txt", b)
-    out = subprocess.run([sys.executable, "-m", "meshfemsparse_b200.solve_system", str(tmp_path / "m.bin"),
-                          str(tmp_path / "rhs.txt")], capture_output=True, text=True, cwd=ROOT, check=True)
-    u = np.array([float(v) for v in out.stdout.split()])
-    assert np.linalg.norm(K @ u - b) <= 1e-12 * np.linalg.norm(b)
