@@ -160,7 +160,13 @@ public:
         m_nr = size_t(nr);
     }
     void clearStashedFactorization() { check(mfs_clear_stash(m_h)); }
-    void clearFactors() { check(mfs_clear_factors(m_h)); }
+    // The sizes follow the factorization state, as in the reference: after
+    // clearFactors() a solve fails its size check until the next factorizeSymbolic.
+    void clearFactors() {
+        check(mfs_clear_factors(m_h));
+        m_n = 0;
+        m_nr = 0;
+    }
 
     mfs_handle *handle() const { return m_h; }
 

@@ -1,0 +1,42 @@
+/* Test hooks of libmfs_b200.so.
+ *
+ * These entry points have no counterpart in the reference: they expose single
+ * kernels of the numeric factorization so that tests can check them against a
+ * host computation on crafted inputs (edge tiles, operand alignment shifts,
+ * lower-triangle masks), the way tests/test_catamari_solve_kernels.cc checks
+ * catamari's dense kernels against dense references. They are not part of the
+ * factorizer interface and are not needed by callers of it.
+ */
+#ifndef MFS_B200_TESTING_H
+#define MFS_B200_TESTING_H
+
+#include "mfs_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Fields of one Schur-update GEMM task, in this order (int64 each). */
+#define MFS_GEMM_TASK_FIELDS 11
+/* a_off, b_off, c_off, lda, ldb, ldc, m, n, k, lower, mode:
+ *   mode 0:  C(i,j) -= sum_k A(i,k) B(j,k)     mode 1:  C(i,j) = sum_k A(i,k) B(j,k)
+ *   for i < m, j < n (lower = 1: only i >= j), A, B, C column-major at the given
+ *   offsets (elements) of the arrays A, B, C of a_len, b_len, c_len elements.
+ *
+ * Runs one launch of the factorization's GEMM kernel over all tasks on `device`
+ * (device pointers; the call synchronizes the device). precision MFS_PREC_FP32:
+ * float arrays, `kernel` 1 = single-pass TF32 on the 5th-generation tensor cores
+ * (tcgen05), 3 = split 3xTF32 (mma.sync), 0 = single-pass TF32 (mma.sync);
+ * MFS_PREC_FP64: double arrays on the FP64 tensor cores (kernel ignored).
+ * FP32 leading dimensions must be multiples of 4 (16-byte aligned columns, as
+ * the factor's panels are). Every access is checked against the array lengths
+ * before the launch (MFS_INVALID_ARG otherwise). */
+mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t kernel, int64_t ntasks,
+                          const int64_t *tasks, const void *A, int64_t a_len, const void *B, int64_t b_len,
+                          void *C, int64_t c_len, char *err_buf, size_t err_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MFS_B200_TESTING_H */

@@ -27,7 +27,9 @@ EXPORTED = [
     "mfs_stash", "mfs_swap_stash", "mfs_clear_stash", "mfs_has_stash", "mfs_clear_factors", "mfs_get_stats",
     "mfs_set_options", "mfs_apply_noalloc", "mfs_lpc_param_count", "mfs_lpc_create", "mfs_lpc_destroy",
     "mfs_lpc_get_weights", "mfs_lpc_set_weights", "mfs_lpc_loss_grad", "mfs_lpc_train_step", "mfs_pcg_solve",
+    "mfs_debug_gemm",
 ]
+GEMM_TASK_FIELDS = 11
 
 
 class Options(C.Structure):
@@ -100,6 +102,8 @@ def load() -> C.CDLL:
                                        C.POINTER(C.c_double)]
     lib.mfs_pcg_solve.argtypes = [P, P, P, P, P, C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_double,
                                   C.POINTER(C.c_int32)]
+    lib.mfs_debug_gemm.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, i64p, P, C.c_int64, P, C.c_int64,
+                                   P, C.c_int64, C.c_char_p, C.c_size_t]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -161,6 +165,21 @@ def build_pattern(nvars: int, conn: np.ndarray):
     check(lib.mfs_build_pattern(nvars, nelem, npe, i64ptr(conn), i64ptr(Ap), i64ptr(Ai), C.byref(nnz)),
           what="pattern")
     return Ap, Ai
+
+
+def debug_gemm(device: int, precision: int, kernel: int, tasks: np.ndarray, A: int, a_len: int, B: int,
+               b_len: int, Cp: int, c_len: int):
+    """Test hook: one launch of the factorization's GEMM kernel over `tasks`
+    (ntasks x GEMM_TASK_FIELDS int64) on device arrays given by address."""
+    tasks = np.ascontiguousarray(tasks, dtype=np.int64).reshape(-1, GEMM_TASK_FIELDS)
+    buf = C.create_string_buffer(512)
+    st = load().mfs_debug_gemm(device, precision, kernel, tasks.shape[0], i64ptr(tasks), C.c_void_p(A), a_len,
+                               C.c_void_p(B), b_len, C.c_void_p(Cp), c_len, buf, 512)
+    if st != MFS_OK:
+        msg = buf.value.decode(errors="replace") or f"mfs status {st}"
+        if st == MFS_INVALID_ARG:
+            raise ValueError(msg)
+        raise MFSError(st, msg)
 
 
 def library_present() -> bool:

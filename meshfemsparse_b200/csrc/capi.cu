@@ -23,6 +23,25 @@
 
 namespace mfs {
 long long g_kernel_launches = 0;
+
+int current_device() {
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) return 0;
+    return d;
+}
+
+int device_sm_count() {
+    static int sms[kMaxDevices] = {};
+    static PerDeviceOnce once;
+    const int d = current_device();
+    if (d < 0 || d >= kMaxDevices) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+        return v;
+    }
+    once([&] { cudaDeviceGetAttribute(&sms[d], cudaDevAttrMultiProcessorCount, d); });
+    return sms[d];
+}
 }  // namespace mfs
 
 using namespace mfs;

@@ -1,0 +1,127 @@
+// Test hooks (include/mfs_b200_testing.h): single kernels of the numeric
+// factorization on caller device arrays, with every access bounds-checked on the
+// host before the launch.
+#include "../../include/mfs_b200_testing.h"
+#include "device.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace mfs;
+
+namespace {
+
+void put_error(char *buf, size_t len, const std::string &msg) {
+    if (buf && len > 0) {
+        std::snprintf(buf, len, "%s", msg.c_str());
+    }
+}
+
+}  // namespace
+
+extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t kernel, int64_t ntasks,
+                                     const int64_t *tasks, const void *A, int64_t a_len, const void *B,
+                                     int64_t b_len, void *C, int64_t c_len, char *err_buf, size_t err_len) {
+    const bool f64 = precision == MFS_PREC_FP64;
+    if (precision != MFS_PREC_FP64 && precision != MFS_PREC_FP32) {
+        put_error(err_buf, err_len, "unknown precision");
+        return MFS_INVALID_ARG;
+    }
+    if (ntasks <= 0 || !tasks || !A || !B || !C) {
+        put_error(err_buf, err_len, "empty task list or null array");
+        return MFS_INVALID_ARG;
+    }
+    if (!f64 && kernel != 0 && kernel != 1 && kernel != 3) {
+        put_error(err_buf, err_len, "kernel must be 0, 1 or 3");
+        return MFS_INVALID_ARG;
+    }
+    const int TM = gemm_tile_m(f64), TN = gemm_tile_n(f64);
+    std::vector<GemmTask> gt(static_cast<size_t>(ntasks));
+    int base = 0;
+    for (int64_t t = 0; t < ntasks; ++t) {
+        const int64_t *q = tasks + t * MFS_GEMM_TASK_FIELDS;
+        const int64_t a_off = q[0], b_off = q[1], c_off = q[2], lda = q[3], ldb = q[4], ldc = q[5];
+        const int64_t m = q[6], n = q[7], k = q[8], lower = q[9], mode = q[10];
+        const std::string id = "task " + std::to_string(t) + ": ";
+        if (m <= 0 || n <= 0 || k <= 0 || m > (1 << 30) || n > (1 << 30) || k > (1 << 30)) {
+            put_error(err_buf, err_len, id + "m, n, k must be positive");
+            return MFS_INVALID_ARG;
+        }
+        if ((mode != 0 && mode != 1) || (lower != 0 && lower != 1)) {
+            put_error(err_buf, err_len, id + "mode and lower must be 0 or 1");
+            return MFS_INVALID_ARG;
+        }
+        if (lda < m || ldb < n || ldc < m || lda > INT32_MAX || ldb > INT32_MAX || ldc > INT32_MAX) {
+            put_error(err_buf, err_len, id + "leading dimension below the extent");
+            return MFS_INVALID_ARG;
+        }
+        int da = 0, db = 0;
+        if (!f64) {
+            if ((lda & 3) || (ldb & 3)) {
+                put_error(err_buf, err_len, id + "FP32 leading dimensions must be multiples of 4");
+                return MFS_INVALID_ARG;
+            }
+            da = int(a_off & 3);
+            db = int(b_off & 3);
+        }
+        // the kernels read A rows [a_off - da, a_off + m) of columns 0..k-1, B likewise,
+        // and write C rows [0, m) of columns 0..n-1
+        if (a_off - da < 0 || b_off - db < 0 || c_off < 0 || a_off + (k - 1) * lda + m > a_len ||
+            b_off + (k - 1) * ldb + n > b_len || c_off + (n - 1) * ldc + m > c_len) {
+            put_error(err_buf, err_len, id + "an access falls outside the arrays");
+            return MFS_INVALID_ARG;
+        }
+        GemmTask &g = gt[size_t(t)];
+        g.a_off = a_off; g.b_off = b_off; g.c_off = c_off;
+        g.lda = int32_t(lda); g.ldb = int32_t(ldb); g.ldc = int32_t(ldc);
+        g.m = int32_t(m); g.n = int32_t(n); g.k = int32_t(k);
+        g.shift = da | (db << 8);
+        g.tiles_m = int32_t((m + da + TM - 1) / TM);
+        g.tiles_n = int32_t((n + db + TN - 1) / TN);
+        g.tile_base = base;
+        g.lower = int32_t(lower);
+        g.mode = int32_t(mode);
+        if (int64_t(base) + int64_t(g.tiles_m) * g.tiles_n > INT32_MAX / 2) {
+            put_error(err_buf, err_len, "too many tiles");
+            return MFS_INVALID_ARG;
+        }
+        base += g.tiles_m * g.tiles_n;
+    }
+    GemmTask *dt = nullptr;
+    int *derr = nullptr;
+    auto fail = [&](cudaError_t e) {
+        put_error(err_buf, err_len, cudaGetErrorString(e));
+        if (dt) cudaFree(dt);
+        if (derr) cudaFree(derr);
+        return MFS_CUDA_ERROR;
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&dt, gt.size() * sizeof(GemmTask))) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&derr, sizeof(int))) != cudaSuccess) return fail(e);
+    if ((e = cudaMemcpy(dt, gt.data(), gt.size() * sizeof(GemmTask), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e);
+    if ((e = cudaMemset(derr, 0, sizeof(int))) != cudaSuccess) return fail(e);
+    if (f64)
+        launch_gemm<double>(dt, int(ntasks), base, static_cast<const double *>(A), static_cast<const double *>(B),
+                            static_cast<double *>(C), 0, derr, nullptr);
+    else
+        launch_gemm<float>(dt, int(ntasks), base, static_cast<const float *>(A), static_cast<const float *>(B),
+                           static_cast<float *>(C), kernel, derr, nullptr);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e);
+    int herr = 0;
+    if ((e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return fail(e);
+    cudaFree(dt);
+    cudaFree(derr);
+    if (herr) {
+        put_error(err_buf, err_len, "a tensor-core pipeline wait timed out");
+        return MFS_TIMEOUT;
+    }
+    return MFS_OK;
+}

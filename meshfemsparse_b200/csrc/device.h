@@ -17,7 +17,29 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <utility>
+
 namespace mfs {
+
+// One-time host set-up per device. Kernel attributes (the dynamic shared-memory
+// opt-in) and occupancy figures belong to the device that is current when they
+// are set or measured, so every such set-up is keyed by the current device.
+constexpr int kMaxDevices = 64;
+int current_device();                   // the calling thread's current device (0 if the query fails)
+int device_sm_count();                  // SM count of the current device (cached per device)
+struct PerDeviceOnce {
+    std::once_flag flag[kMaxDevices];
+    template <typename F>
+    void operator()(F &&fn) {
+        const int d = current_device();
+        if (d < 0 || d >= kMaxDevices) {
+            fn();
+            return;
+        }
+        std::call_once(flag[d], std::forward<F>(fn));
+    }
+};
 
 // Kernels launched by this library since load (every launcher increments it).
 extern long long g_kernel_launches;

@@ -271,8 +271,8 @@ void launch_small_factor(const int32_t *list, int count, int max_front, SnDev sd
                          cudaStream_t st) {
     if (count <= 0) return;
     const size_t smem = size_t(max_front) * max_front * sizeof(T);
-    static const bool smem_ok = (cudaFuncSetAttribute(small_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin), true);
-    (void)smem_ok;
+    static PerDeviceOnce once;
+    once([] { cudaFuncSetAttribute(small_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin); });
     ++g_kernel_launches;
     small_factor_kernel<T><<<count, 256, smem, st>>>(list, sd, factor, upd, pv);
 }

@@ -309,12 +309,12 @@ void launch_gemm<float>(const GemmTask *tasks, int ntasks, int ntiles, const flo
     }
     ++g_kernel_launches;
     if (split == 3) {
-        static const bool ok3 = (cudaFuncSetAttribute(gemm_tf32_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTF32Smem), true);
-        (void)ok3;
+        static PerDeviceOnce once3;
+        once3([] { cudaFuncSetAttribute(gemm_tf32_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTF32Smem); });
         gemm_tf32_kernel<3><<<ntiles, 256, kTF32Smem, st>>>(tasks, ntasks, A, B, C);
     } else {
-        static const bool ok1 = (cudaFuncSetAttribute(gemm_tf32_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTF32Smem), true);
-        (void)ok1;
+        static PerDeviceOnce once1;
+        once1([] { cudaFuncSetAttribute(gemm_tf32_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTF32Smem); });
         gemm_tf32_kernel<1><<<ntiles, 256, kTF32Smem, st>>>(tasks, ntasks, A, B, C);
     }
 }
@@ -326,8 +326,8 @@ void launch_gemm<double>(const GemmTask *tasks, int ntasks, int ntiles, const do
     (void)err;
     if (ntiles <= 0) return;
     ++g_kernel_launches;
-    static const bool ok = (cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kF64Smem), true);
-    (void)ok;
+    static PerDeviceOnce once;
+    once([] { cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kF64Smem); });
     gemm_f64_kernel<<<ntiles, 256, kF64Smem, st>>>(tasks, ntasks, A, B, C);
 }
 

@@ -106,6 +106,13 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *er
         }
     }
 }
+// Bounded wait that ignores the error flag: after a timeout the MMA issuer still
+// lets the MMAs it has issued retire before the CTA frees TMEM and exits.
+__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity) {
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try(bar, parity))
+        if (global_ns() - t0 > kPipeWaitNs) return;
+}
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -326,9 +333,13 @@ __global__ void __launch_bounds__(kUThreads, 1) gemm_tc_kernel(const GemmTask *_
     } else if (lane == 0) {
         // ---------------- MMA issuer
         const uint32_t idesc = umma_idesc(bn);
+        bool broke = false;
         for (int kb = 0; kb < nk; ++kb) {
             const int s = kb % STAGES;
-            if (!mbar_wait(full0 + 8 * s, uint32_t(kb / STAGES) & 1u, err)) break;
+            if (!mbar_wait(full0 + 8 * s, uint32_t(kb / STAGES) & 1u, err)) {
+                broke = true;
+                break;
+            }
             tc_fence_after();
             const uint32_t sa = sbase + uint32_t(s) * kUStage;
             const uint32_t sb = sa + kUStageA;
@@ -341,6 +352,7 @@ __global__ void __launch_bounds__(kUThreads, 1) gemm_tc_kernel(const GemmTask *_
             umma_commit(empty0 + 8 * s);
         }
         umma_commit(done);
+        if (broke) mbar_drain(done, 0u);
     }
     tc_fence_before();
     __syncthreads();
@@ -358,9 +370,8 @@ constexpr int kTcSmem = kTcStages * kUStage + 1024;
 void launch_gemm_tc(const GemmTask *tasks, int ntasks, int ntiles, const float *A, const float *B, float *C, int *err,
                     cudaStream_t st) {
     if (ntiles <= 0) return;
-    static const bool ok =
-        (cudaFuncSetAttribute(gemm_tc_kernel<kTcStages>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem), true);
-    (void)ok;
+    static PerDeviceOnce once;
+    once([] { cudaFuncSetAttribute(gemm_tc_kernel<kTcStages>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem); });
     ++g_kernel_launches;
     gemm_tc_kernel<kTcStages><<<ntiles, kUThreads, kTcSmem, st>>>(tasks, ntasks, A, B, C, err);
 }

@@ -516,12 +516,11 @@ void lpc_features(const LGraph &g, const double *Ax, LWork &w, cudaStream_t st) 
 }
 
 void lpc_forward(const LGraph &g, const __nv_bfloat16 *wb, LWork &w, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce once;
+    once([] {
         cudaFuncSetAttribute(dense_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin);
         cudaFuncSetAttribute(dense_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin);
-        attr = true;
-    }
+    });
     const LParamLayout L = lpc_layout();
     const int grid = lpc_dense_parts();
     for (int l = 0; l < kLLayers; ++l) {

@@ -350,9 +350,8 @@ void launch_panel(const PanelTask *tasks, int ntasks, int max_nb, T *factor, T *
                   bool round_inv, cudaStream_t st) {
     if (ntasks <= 0) return;
     const size_t smem = panel_smem_bytes(max_nb, sizeof(T) == 8);
-    static const bool smem_ok =
-        (cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin), true);
-    (void)smem_ok;
+    static PerDeviceOnce once;
+    once([] { cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin); });
     ++g_kernel_launches;
     panel_kernel<T><<<ntasks, kPanelThreads, smem, st>>>(tasks, factor, inv_scratch, pv, round_inv);
 }

@@ -344,15 +344,7 @@ __global__ void __launch_bounds__(kSubThreads) subtree_bwd_kernel(const int2 *__
     }
 }
 
-int sub_sm_count() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
-    return sms;
-}
+int sub_sm_count() { return device_sm_count(); }
 
 }  // namespace
 
@@ -365,15 +357,15 @@ void launch_subtree_solve(bool forward, const int2 *subs, int nsub, int fmax, Sn
                           int64_t ldx, int nrhs, double *sol, cudaStream_t st) {
     if (nsub <= 0) return;
     const size_t smem = subtree_smem_bytes(fmax);
-    static const bool attr_ok =
-        (cudaFuncSetAttribute(subtree_fwd_kernel<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin),
-         cudaFuncSetAttribute(subtree_fwd_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin),
-         cudaFuncSetAttribute(subtree_fwd_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin),
-         cudaFuncSetAttribute(subtree_bwd_kernel<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin),
-         cudaFuncSetAttribute(subtree_bwd_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin),
-         cudaFuncSetAttribute(subtree_bwd_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin),
-         true);
-    (void)attr_ok;
+    static PerDeviceOnce once;
+    once([] {
+        cudaFuncSetAttribute(subtree_fwd_kernel<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin);
+        cudaFuncSetAttribute(subtree_fwd_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin);
+        cudaFuncSetAttribute(subtree_fwd_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin);
+        cudaFuncSetAttribute(subtree_bwd_kernel<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin);
+        cudaFuncSetAttribute(subtree_bwd_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin);
+        cudaFuncSetAttribute(subtree_bwd_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin);
+    });
     const int grid = std::min(nsub, 8 * sub_sm_count());
     ++g_kernel_launches;
     const int vb = sd.vb;

@@ -783,15 +783,7 @@ __global__ void __launch_bounds__(256) str_reduce_kernel(const StrReduce *__rest
     }
 }
 
-int sm_count() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
-    return sms;
-}
+int sm_count() { return device_sm_count(); }
 
 template <typename K>
 int coop_grid(K kernel, size_t smem, int ntasks) {
@@ -816,16 +808,18 @@ cudaError_t launch_diag(bool forward, const SolveTask *tasks, int ntasks, SnDev 
     if (ntasks <= 0) return cudaSuccess;
     void *kern = forward ? (void *)fwd_diag_kernel<T> : (void *)bwd_diag_kernel<T>;
     const size_t smem = diag_smem<T>(nrhs);
-    // one-time per kernel: shared-memory opt-in and co-resident grid per RHS count
-    static const bool attr_ok =
-        (cudaFuncSetAttribute(fwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(diag_smem<T>(kMaxSolveRhs))),
-         cudaFuncSetAttribute(bwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(diag_smem<T>(kMaxSolveRhs))),
-         true);
-    (void)attr_ok;
-    static int grid_cache[2][kMaxSolveRhs + 1] = {};
-    int &gmax = grid_cache[forward ? 0 : 1][nrhs];
+    // one-time per kernel and device: shared-memory opt-in and co-resident grid per RHS count
+    static PerDeviceOnce once;
+    once([] {
+        cudaFuncSetAttribute(fwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(diag_smem<T>(kMaxSolveRhs)));
+        cudaFuncSetAttribute(bwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(diag_smem<T>(kMaxSolveRhs)));
+    });
+    static int grid_cache[kMaxDevices][2][kMaxSolveRhs + 1] = {};
+    const int dev = current_device();
+    int gtmp = 0;
+    int &gmax = (dev >= 0 && dev < kMaxDevices) ? grid_cache[dev][forward ? 0 : 1][nrhs] : gtmp;
     if (!gmax) gmax = forward ? coop_grid(fwd_diag_kernel<T>, smem, 1 << 30) : coop_grid(bwd_diag_kernel<T>, smem, 1 << 30);
     const int grid = std::min(gmax, ntasks);
     void *args[] = {(void *)&tasks, (void *)&ntasks, (void *)&sd, (void *)&factor, (void *)&X, (void *)&ldx,
@@ -840,13 +834,13 @@ void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce 
     if (ntasks <= 0) return;
     g_kernel_launches += 2;
     const size_t smem = str_smem<T>(nrhs);
-    static const bool attr_ok =
-        (cudaFuncSetAttribute(str_partial_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(str_smem<T>(kMaxSolveRhs))),
-         cudaFuncSetAttribute(str_partial_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(str_smem<T>(kMaxSolveRhs))),
-         true);
-    (void)attr_ok;
+    static PerDeviceOnce once;
+    once([] {
+        cudaFuncSetAttribute(str_partial_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(str_smem<T>(kMaxSolveRhs)));
+        cudaFuncSetAttribute(str_partial_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(str_smem<T>(kMaxSolveRhs)));
+    });
     if (forward) {
         str_partial_kernel<T, true><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
         str_reduce_kernel<true><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);

@@ -20,7 +20,8 @@
  *                       given supernode partition (SparseLDL::RefactorWithFixedSparsityPattern,
  *                       called at CatamariFactorizer.cc:660; failure rule :701-705)
  *   orc_mf_solve        forward / backward substitution, multi-RHS column-major
- *                       (SparseLDL::Solve, CatamariFactorizer.cc:54,70)
+ *                       (SparseLDL::Solve, CatamariFactorizer.cc:54,70); plain loops
+ *                       for the checker, per-supernode TRSM / GEMM for the timed baseline
  *
  * Dense kernels optionally go through OpenBLAS (the copy bundled with scipy,
  * loaded with dlopen) so the oracle can double as the timed CPU baseline;
@@ -431,9 +432,18 @@ i64 orc_mf_factor(i64 nsn, int vb, const i64 *sn_start, const i64 *parent, const
     double **U = calloc((size_t)nsn + 1, sizeof(double *));
     i64 fail = -1;
     const int use_blas = threads > 0 && p_dpotrf != 0;
-    for (i64 l = 0; l < T.nlevels; ++l) {
+    /* one dense front buffer per host thread, reused across fronts (grown on demand) */
+    const int nbuf = threads > 0 ? threads : 1;
+    double **ws = calloc((size_t)nbuf, sizeof(double *));
+    size_t *wcap = calloc((size_t)nbuf, sizeof(size_t));
+    /* Per level, two passes: fronts with more than kBigFront dense flops one after
+     * another with all BLAS threads, then the rest concurrently with one BLAS thread
+     * each (a large front on one thread would stall its level). */
+    const double kBigFront = 2e9;
+    for (i64 l = 0; l < T.nlevels; ++l)
+    for (int pass = 0; pass < 2; ++pass) {
         i64 lo = T.level_ptr[l], hi = T.level_ptr[l + 1];
-        int par = use_blas && (hi - lo) >= 8;
+        int par = use_blas && pass == 1 && (hi - lo) >= 2;
         if (use_blas && p_setthreads) p_setthreads(par ? 1 : threads);
 #ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 1) num_threads(par ? threads : 1) if (par)
@@ -441,15 +451,39 @@ i64 orc_mf_factor(i64 nsn, int vb, const i64 *sn_start, const i64 *parent, const
         for (i64 q = lo; q < hi; ++q) {
             i64 s = T.level_list[q];
             if (s < g_range_lo || (g_range_hi >= 0 && s > g_range_hi)) continue;
+            {
+                double fw = (double)T.w[s], fd = (double)T.d[s];
+                int big = use_blas && (fw * fw * fw / 3 + fw * fw * fd + fw * fd * fd) > kBigFront;
+                if (big != (pass == 0)) continue;
+                if (!use_blas && pass == 1) continue;
+            }
             i64 w = T.w[s], d = T.d[s], f = T.f[s];
-            double *F = calloc((size_t)(f * f), sizeof(double));
+#ifdef _OPENMP
+            int tid = par ? omp_get_thread_num() : 0;
+#else
+            int tid = 0;
+#endif
+            if ((size_t)(f * f) > wcap[tid]) {
+                free(ws[tid]);
+                ws[tid] = malloc((size_t)(f * f) * sizeof(double));
+                wcap[tid] = (size_t)(f * f);
+            }
+            double *F = ws[tid];
             double *pan = factor + T.pan_off[s];
+            /* the panel's w columns, then the lower triangle of the update block zeroed
+             * (the only part the extend-add, SYRK and the update copy touch) */
             memcpy(F, pan, (size_t)(f * w) * sizeof(double));
+            for (i64 j = w; j < f; ++j) memset(F + j * f + j, 0, (size_t)(f - j) * sizeof(double));
             for (i64 k = T.child_ptr[s]; k < T.child_ptr[s + 1]; ++k) {
                 i64 c = T.child_list[k];
                 i64 dc = T.d[c];
                 i64 *pos = malloc((size_t)(dc + 1) * sizeof(i64));
                 for (i64 i = 0; i < dc; ++i) pos[i] = front_pos(&T, s, struct_scalar(&T, c, i));
+                /* columns of one child go to distinct front columns: with one front per
+                 * level (the top of the tree) the host threads split them */
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads) if (use_blas && !par && dc > 512)
+#endif
                 for (i64 j = 0; j < dc; ++j)
                     for (i64 i = j; i < dc; ++i) F[pos[j] * f + pos[i]] += U[c][j * dc + i];
                 free(pos);
@@ -469,25 +503,73 @@ i64 orc_mf_factor(i64 nsn, int vb, const i64 *sn_start, const i64 *parent, const
             memcpy(pan, F, (size_t)(f * w) * sizeof(double));
             if (d > 0 && parent[s] >= 0) {
                 U[s] = malloc((size_t)(d * d) * sizeof(double));
-                for (i64 j = 0; j < d; ++j) memcpy(U[s] + j * d, F + (w + j) * f + w, (size_t)d * sizeof(double));
+                for (i64 j = 0; j < d; ++j)
+                    memcpy(U[s] + j * d + j, F + (w + j) * f + w + j, (size_t)(d - j) * sizeof(double));
             }
-            free(F);
         }
     }
+    for (int t = 0; t < nbuf; ++t) free(ws[t]);
+    free(ws);
+    free(wcap);
     for (i64 s = 0; s < nsn; ++s) free(U[s]);
     free(U);
     tree_free(&T);
     return fail;
 }
 
-/* Forward then backward substitution on X (n x nrhs, ld n, permuted order). */
+/* Supernodal substitution with dense BLAS kernels per supernode (the timed CPU
+ * baseline): forward  X[cols] = L11^{-1} X[cols], X[struct] -= L21 X[cols];
+ * backward X[cols] -= L21^T X[struct], X[cols] = L11^{-T} X[cols]. */
+static void mf_solve_blas(const Tree *T, const double *factor, double *X, i64 n, int nrhs, int threads) {
+    if (p_setthreads) p_setthreads(threads);
+    i64 dmax = 0;
+    for (i64 s = 0; s < T->nsn; ++s) if (T->d[s] > dmax) dmax = T->d[s];
+    double *tmp = malloc((size_t)(dmax * nrhs + 1) * sizeof(double));
+    i64 *rows = malloc((size_t)(dmax + 1) * sizeof(i64));
+    for (i64 s = 0; s < T->nsn; ++s) {
+        if (s < g_range_lo || (g_range_hi >= 0 && s > g_range_hi)) continue;
+        i64 w = T->w[s], d = T->d[s], f = T->f[s], c0 = T->col0[s];
+        const double *pan = factor + T->pan_off[s];
+        p_dtrsm(ColMajor, Left, Lower, NoTrans, NonUnit, (int)w, nrhs, 1.0, pan, (int)f, X + c0, (int)n);
+        if (d > 0) {
+            p_dgemm(ColMajor, NoTrans, NoTrans, (int)d, nrhs, (int)w, 1.0, pan + w, (int)f, X + c0, (int)n, 0.0, tmp,
+                    (int)d);
+            for (i64 i = 0; i < d; ++i) rows[i] = struct_scalar(T, s, i);
+            for (int r = 0; r < nrhs; ++r)
+                for (i64 i = 0; i < d; ++i) X[rows[i] + (i64)r * n] -= tmp[i + (i64)r * d];
+        }
+    }
+    for (i64 s = T->nsn - 1; s >= 0; --s) {
+        if (s < g_range_lo || (g_range_hi >= 0 && s > g_range_hi)) continue;
+        i64 w = T->w[s], d = T->d[s], f = T->f[s], c0 = T->col0[s];
+        const double *pan = factor + T->pan_off[s];
+        if (d > 0) {
+            for (i64 i = 0; i < d; ++i) rows[i] = struct_scalar(T, s, i);
+            for (int r = 0; r < nrhs; ++r)
+                for (i64 i = 0; i < d; ++i) tmp[i + (i64)r * d] = X[rows[i] + (i64)r * n];
+            p_dgemm(ColMajor, Trans, NoTrans, (int)w, nrhs, (int)d, -1.0, pan + w, (int)f, tmp, (int)d, 1.0, X + c0,
+                    (int)n);
+        }
+        p_dtrsm(ColMajor, Left, Lower, Trans, NonUnit, (int)w, nrhs, 1.0, pan, (int)f, X + c0, (int)n);
+    }
+    free(tmp);
+    free(rows);
+}
+
+/* Forward then backward substitution on X (n x nrhs, ld n, permuted order).
+ * threads > 0 with OpenBLAS loaded: the dense per-supernode form above;
+ * otherwise plain loops (the checker). */
 void orc_mf_solve(i64 nsn, int vb, const i64 *sn_start, const i64 *parent, const i64 *struct_ptr,
                   const i64 *struct_rows, const double *factor, double *X, i64 n, int nrhs, int threads) {
     Tree T = {0};
     T.nsn = nsn; T.vb = vb; T.sn_start = sn_start; T.parent = parent; T.struct_ptr = struct_ptr;
     T.struct_rows = struct_rows;
     tree_build(&T);
-    (void)threads;
+    if (threads > 0 && p_dpotrf) {
+        mf_solve_blas(&T, factor, X, n, nrhs, threads);
+        tree_free(&T);
+        return;
+    }
     /* forward: X[cols] = L11^{-1} X[cols]; X[struct] -= L21 X[cols] (sequential column order) */
     for (i64 s = 0; s < nsn; ++s) {
         if (s < g_range_lo || (g_range_hi >= 0 && s > g_range_hi)) continue;

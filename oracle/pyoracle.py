@@ -180,3 +180,24 @@ def scalar_perm_map(n_full: int, pins, iperm_scalar):
     perm = np.empty_like(iperm_scalar)
     perm[iperm_scalar] = np.arange(iperm_scalar.size)
     return np.where(rr >= 0, perm[np.maximum(rr, 0)], -1)
+
+
+def panels_to_csc(sn: dict, factor: np.ndarray, n: int):
+    """The lower-triangular factor (or injected lower triangle) stored in catamari panels
+    as an n x n scipy CSC matrix in the permuted reduced order."""
+    import scipy.sparse as sp
+    vb = sn["vb"]
+    w, d, f, pan, col0 = panel_layout(sn)
+    rows_all, cols_all, vals_all = [], [], []
+    for s in range(len(w)):
+        P = factor[pan[s]:pan[s + 1]].reshape(w[s], f[s]).T      # f x w, column-major panel
+        srows = sn["struct_rows"][sn["struct_ptr"][s]:sn["struct_ptr"][s + 1]]
+        rows = np.concatenate([col0[s] + np.arange(w[s]), (srows[:, None] * vb + np.arange(vb)[None, :]).reshape(-1)])
+        ii, jj = np.nonzero(np.arange(f[s])[:, None] >= np.arange(w[s])[None, :])
+        rows_all.append(rows[ii])
+        cols_all.append(col0[s] + jj)
+        vals_all.append(P[ii, jj])
+    r = np.concatenate(rows_all)
+    c = np.concatenate(cols_all)
+    v = np.concatenate(vals_all)
+    return sp.csc_matrix((v, (r, c)), shape=(n, n))

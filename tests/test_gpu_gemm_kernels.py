@@ -1,0 +1,226 @@
+"""The factorization's Schur-update GEMM kernels against a host FP64 product.
+
+Crafted operands go through the test hook ``mfs_debug_gemm`` (one launch of the
+kernel the factorization uses), the way ``tests/test_catamari_solve_kernels.cc``
+checks catamari's dense kernels against dense references. Cases cover edge tiles
+(m, n, k not multiples of the 128 x 256 x 32 tile), both tcgen05 tile widths
+(bn = 128 when at most 128 columns are left, 256 otherwise), every 16-byte
+alignment shift of the A and B operands, the lower-triangle mask, several tasks in
+one launch, and the row solve's (mode 1) rounding of its A operand and result.
+
+Tolerances:
+* tcgen05 single-pass TF32, mode 0 (C -= A B^T on TF32-exact operands, as the
+  factorization's L21 blocks are): the product of two TF32 values is exact in FP32,
+  so the only error is FP32 accumulation: elementwise within (k + 2) 2^-21 times
+  S = |C| + |A||B|^T (the standard bound with 4x room for the tensor cores'
+  accumulation order), and normwise within 1e-6 of ||S||. A misplaced row, column
+  or k index moves an element by about S / k, far above both.
+* mode 1 (C = A B^T, A rounded to TF32 in the kernel, result stored rounded to
+  TF32): within 2^-11 relative per element plus the accumulation bound, and every
+  output is a TF32 value.
+* split 3xTF32 (mma.sync): FP32-level, 1e-5 normwise on arbitrary FP32 operands.
+* FP64 (DMMA): 1e-13 normwise.
+Elements outside the written block (guard rows and columns, the strict upper
+triangle of lower tasks) must be unchanged.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from meshfemsparse_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def tf32_rna(x: np.ndarray) -> np.ndarray:
+    """Round FP32 values to TF32 (10 explicit mantissa bits), nearest, ties away from zero."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32)
+    r = ((u.astype(np.uint64) + 0x1000) & 0xFFFFE000).astype(np.uint32)
+    return r.view(np.float32)
+
+
+def column_block(arr, off, ld, rows, cols):
+    """View of the column-major block (rows x cols) at element offset `off` with leading dimension `ld`."""
+    idx = off + np.arange(rows)[:, None] + ld * np.arange(cols)[None, :]
+    return arr[idx]
+
+
+def run_case(tasks, a_len, b_len, c_len, dtype, kernel, seed, tf32_exact=True):
+    """tasks: list of dicts with a_off b_off c_off lda ldb ldc m n k lower mode.
+    Returns (A, B, C_before, C_after) host arrays."""
+    rng = np.random.default_rng(seed)
+    A = rng.uniform(-1, 1, a_len).astype(dtype)
+    B = rng.uniform(-1, 1, b_len).astype(dtype)
+    C0 = rng.uniform(-1, 1, c_len).astype(dtype)
+    if dtype == np.float32 and tf32_exact:
+        A, B = tf32_rna(A), tf32_rna(B)
+    dev = "cuda:0"
+    tA, tB, tC = (torch.from_numpy(v.copy()).to(dev) for v in (A, B, C0))
+    fields = ["a_off", "b_off", "c_off", "lda", "ldb", "ldc", "m", "n", "k", "lower", "mode"]
+    tk = np.array([[t[f] for f in fields] for t in tasks], dtype=np.int64)
+    prec = _lib.MFS_PREC_FP32 if dtype == np.float32 else _lib.MFS_PREC_FP64
+    _lib.debug_gemm(0, prec, kernel, tk, tA.data_ptr(), a_len, tB.data_ptr(), b_len, tC.data_ptr(), c_len)
+    torch.cuda.synchronize()
+    return A, B, C0, tC.cpu().numpy()
+
+
+def expected(tasks, A, B, C0, a_round=None):
+    """FP64 reference of every task applied to C0 (tasks write disjoint blocks), the
+    elementwise accumulation scale, and the mask of written elements."""
+    ref = C0.astype(np.float64).copy()
+    scale = np.abs(C0.astype(np.float64))
+    written = np.zeros(C0.shape, dtype=bool)
+    for t in tasks:
+        m, n, k = t["m"], t["n"], t["k"]
+        Ab = column_block(A, t["a_off"], t["lda"], m, k).astype(np.float64)
+        if a_round is not None:
+            Ab = a_round(Ab.astype(np.float32)).astype(np.float64)
+        Bb = column_block(B, t["b_off"], t["ldb"], n, k).astype(np.float64)
+        P = Ab @ Bb.T
+        S = np.abs(Ab) @ np.abs(Bb).T
+        idx = t["c_off"] + np.arange(m)[:, None] + t["ldc"] * np.arange(n)[None, :]
+        mask = np.ones((m, n), dtype=bool)
+        if t["lower"]:
+            mask = np.arange(m)[:, None] >= np.arange(n)[None, :]
+        cur = ref[idx]
+        new = cur - P if t["mode"] == 0 else P
+        ref[idx[mask]] = new[mask]
+        sc = scale[idx]
+        sc = sc + S if t["mode"] == 0 else S
+        scale[idx[mask]] = sc[mask]
+        written[idx[mask]] = True
+    return ref, scale, written
+
+
+def task(a_off, b_off, c_off, lda, ldb, ldc, m, n, k, lower=0, mode=0):
+    return dict(a_off=a_off, b_off=b_off, c_off=c_off, lda=lda, ldb=ldb, ldc=ldc, m=m, n=n, k=k, lower=lower,
+                mode=mode)
+
+
+def lens(tasks):
+    a = max(t["a_off"] + (t["k"] - 1) * t["lda"] + t["m"] for t in tasks)
+    b = max(t["b_off"] + (t["k"] - 1) * t["ldb"] + t["n"] for t in tasks)
+    c = max(t["c_off"] + (t["n"] - 1) * t["ldc"] + t["m"] for t in tasks)
+    return a + 64, b + 64, c + 4 * max(t["ldc"] for t in tasks)
+
+
+def check_mode0(tasks, A, B, C0, C, k_max):
+    ref, scale, written = expected(tasks, A, B, C0)
+    err = np.abs(C.astype(np.float64) - ref)
+    bound = (k_max + 2) * 2.0 ** -21 * scale
+    assert np.all(err[written] <= bound[written]), float(np.max(err[written] / np.maximum(bound[written], 1e-300)))
+    assert np.linalg.norm(err[written]) <= 1e-6 * np.linalg.norm(scale[written])
+    assert np.array_equal(C[~written], C0[~written]), "an element outside the task blocks changed"
+
+
+SHIFTS = [(0, 0), (1, 3), (2, 1), (3, 2)]
+
+
+@pytest.mark.parametrize("da,db", SHIFTS)
+@pytest.mark.parametrize("m,n,k", [(300, 200, 77), (129, 100, 512), (37, 300, 1), (520, 129, 96)])
+def test_tcgen05_update_edges_and_shifts(m, n, k, da, db):
+    """mode 0, rectangular: edge tiles in m, n and k; n + db <= 128 takes the 128-wide
+    tile, wider blocks the 256-wide one; every operand shift."""
+    lda = (m + da + 3) // 4 * 4 + 8
+    ldb = (n + db + 3) // 4 * 4 + 4
+    ldc = m + 5
+    t = [task(16 + da, 8 + db, 3, lda, ldb, ldc, m, n, k)]
+    a_len, b_len, c_len = lens(t)
+    A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float32, 1, seed=m * 7 + n + k + da * 3 + db)
+    check_mode0(t, A, B, C0, C, k)
+
+
+@pytest.mark.parametrize("n,da", [(333, 0), (333, 2), (100, 1), (256, 3)])
+def test_tcgen05_syrk_lower(n, da):
+    """SYRK of a diagonal block (A and B the same panel rows): only the lower
+    triangle is written, tiles above the diagonal exit early."""
+    k = 200
+    ld = (n + da + 3) // 4 * 4
+    t = [task(4 + da, 4 + da, 0, ld, ld, n + 2, n, n, k, lower=1)]
+    a_len, _, c_len = lens(t)
+    rng = np.random.default_rng(n + da)
+    A = tf32_rna(rng.uniform(-1, 1, a_len).astype(np.float32))
+    C0 = rng.uniform(-1, 1, c_len).astype(np.float32)
+    dev = "cuda:0"
+    tA, tC = torch.from_numpy(A.copy()).to(dev), torch.from_numpy(C0.copy()).to(dev)
+    fields = ["a_off", "b_off", "c_off", "lda", "ldb", "ldc", "m", "n", "k", "lower", "mode"]
+    tk = np.array([[t[0][f] for f in fields]], dtype=np.int64)
+    _lib.debug_gemm(0, _lib.MFS_PREC_FP32, 1, tk, tA.data_ptr(), a_len, tA.data_ptr(), a_len, tC.data_ptr(), c_len)
+    C = tC.cpu().numpy()
+    check_mode0(t, A, A, C0, C, k)
+
+
+@pytest.mark.parametrize("m,n,da", [(700, 300, 1), (1000, 512, 0), (257, 129, 3)])
+def test_tcgen05_trailing_update_lower(m, n, da):
+    """A front's trailing update: rows below the block (m > n), lower mask, the
+    operand rows start db = da rows into their 16-byte chunk."""
+    k = 128
+    ld = 1024 + 4
+    t = [task(8 + da, 8 + da, 11, ld, ld, ld, m, n, k, lower=1)]
+    a_len, b_len, c_len = lens(t)
+    A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float32, 1, seed=m + n + da)
+    check_mode0(t, A, B, C0, C, k)
+
+
+def test_tcgen05_several_tasks_one_launch():
+    """Tasks of different shapes in one launch (the tile prefix and the task search)."""
+    ts = [task(0, 0, 0, 512, 512, 400, 300, 250, 64),
+          task(2, 1, 400 * 250, 512, 512, 200, 150, 90, 33, lower=0),
+          task(3, 3, 400 * 250 + 200 * 90, 512, 512, 520, 520, 260, 130, lower=1)]
+    a_len, b_len, c_len = lens(ts)
+    a_len = max(a_len, 130 * 512 + 600)
+    b_len = max(b_len, 130 * 512 + 600)
+    A, B, C0, C = run_case(ts, a_len, b_len, c_len, np.float32, 1, seed=5)
+    check_mode0(ts, A, B, C0, C, 130)
+
+
+@pytest.mark.parametrize("m,n,da", [(500, 128, 0), (333, 128, 3), (61, 72, 2), (1024, 100, 1)])
+def test_tcgen05_row_solve_rounding(m, n, da):
+    """mode 1 (the row solve X := X inv(L)^T): the FP32 A operand is rounded to TF32
+    in the kernel, B (the stored inverse) is TF32-exact, the result is stored rounded
+    to TF32."""
+    k = n
+    lda = (m + da + 3) // 4 * 4
+    ldb = (n + 3) // 4 * 4
+    t = [task(da, 0, 7, lda, ldb, m + 9, m, n, k, mode=1)]
+    a_len, b_len, c_len = lens(t)
+    rng = np.random.default_rng(m + n)
+    A = rng.uniform(-1, 1, a_len).astype(np.float32)              # arbitrary FP32
+    B = tf32_rna(rng.uniform(-1, 1, b_len).astype(np.float32))
+    C0 = rng.uniform(-1, 1, c_len).astype(np.float32)
+    dev = "cuda:0"
+    tA, tB, tC = (torch.from_numpy(v.copy()).to(dev) for v in (A, B, C0))
+    fields = ["a_off", "b_off", "c_off", "lda", "ldb", "ldc", "m", "n", "k", "lower", "mode"]
+    tk = np.array([[t[0][f] for f in fields]], dtype=np.int64)
+    _lib.debug_gemm(0, _lib.MFS_PREC_FP32, 1, tk, tA.data_ptr(), a_len, tB.data_ptr(), b_len, tC.data_ptr(), c_len)
+    C = tC.cpu().numpy()
+    ref, scale, written = expected(t, A, B, C0, a_round=tf32_rna)
+    got = C.astype(np.float64)
+    err = np.abs(got - ref)
+    bound = 2.0 ** -11 * np.abs(ref) + (k + 2) * 2.0 ** -21 * scale
+    assert np.all(err[written] <= bound[written])
+    assert np.array_equal(tf32_rna(C[written]), C[written]), "row-solve output is not TF32-exact"
+    assert np.array_equal(C[~written], C0[~written])
+
+
+def test_mma_split3_fp32_accuracy():
+    """The split 3xTF32 kernel keeps FP32-level accuracy on arbitrary FP32 operands."""
+    t = [task(1, 2, 0, 404, 260, 310, 300, 250, 200)]
+    a_len, b_len, c_len = lens(t)
+    A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float32, 3, seed=11, tf32_exact=False)
+    ref, scale, written = expected(t, A, B, C0)
+    prod = (ref - C0.astype(np.float64))[written]
+    assert np.linalg.norm((C.astype(np.float64) - ref)[written]) <= 1e-5 * np.linalg.norm(prod)
+    assert np.array_equal(C[~written], C0[~written])
+
+
+@pytest.mark.parametrize("lower", [0, 1])
+def test_dmma_fp64(lower):
+    t = [task(3, 5, 1, 301, 299, 305, 290, 290 if lower else 170, 75, lower=lower)]
+    a_len, b_len, c_len = lens(t)
+    A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float64, 0, seed=12 + lower)
+    ref, scale, written = expected(t, A, B, C0)
+    prod = (ref - C0)[written]
+    assert np.linalg.norm((C - ref)[written]) <= 1e-13 * np.linalg.norm(prod)
+    assert np.array_equal(C[~written], C0[~written])

@@ -165,3 +165,84 @@ def test_fp32_refined_reaches_1e_minus_10():
     r = A @ x[keep] - b[keep]
     assert np.max(np.linalg.norm(r, axis=0) / np.linalg.norm(b[keep], axis=0)) <= 1e-10
     assert f.stats()["refine_iterations"] >= 1
+
+
+@pytest.mark.parametrize("tc", [0, 1])
+def test_bench_path_tcgen05_factor_k24(tc):
+    """The benchmark's own FP32 path at k = 24 (45,000 DOFs): refined FP32 with
+    tensor_cores 0 (automatic: tcgen05 TF32 under refinement) and 1 (tcgen05 TF32).
+    * every panel entry within 3e-2 of the FP64 oracle factor, relative to its
+      largest entry (single-pass TF32 Schur updates);
+    * backward error of the TF32 factor ||L L^T x - A x|| / ||A x|| <= 1e-2 for a
+      random x (an indexing error in a Schur-update tile gives O(1));
+    * refinement reaches 1e-10 within 12 iterations with no perturbed pivot."""
+    H, tets, Ke, pins, nodes = cube_problem(24)
+    f = B200Factorizer(True, refine=True, tensor_cores=tc)
+    f.factorizeSymbolic(H, pins)
+    f.factorizeNumeric(H)
+    sn = f.supernodes()
+    plan = f.conversionPlan()
+    w, d, fr, pan, col0 = pyoracle.panel_layout(sn)
+    injected = pyoracle.inject(plan["entries"], sn["vb"], H.bs, H.Ax, int(pan[-1]))
+    ref = injected.copy()
+    pyoracle.load_blas()
+    assert pyoracle.mf_factor(sn, ref, 8) == -1
+    got = f.factorValues()
+    assert rel_err(got, ref) <= 3e-2
+    n = f.n_reduced()
+    L = pyoracle.panels_to_csc(sn, got, n)
+    Al = pyoracle.panels_to_csc(sn, injected, n)
+    import scipy.sparse as sp
+    A = Al + Al.T - sp.diags(Al.diagonal())
+    x = np.random.default_rng(24).normal(size=n)
+    Ax = A @ x
+    assert np.linalg.norm(L @ (L.T @ x) - Ax) <= 1e-2 * np.linalg.norm(Ax)
+    assert f.stats()["perturbed_pivots"] == 0
+    rng = np.random.default_rng(5)
+    b = rng.normal(size=(H.n, 4))
+    b[pins] = 0
+    X = f.solveMultiRHS(b)
+    keep = np.ones(H.n, bool)
+    keep[pins] = False
+    Af = H.to_scipy_full()[keep][:, keep]
+    r = Af @ X[keep] - b[keep]
+    assert np.max(np.linalg.norm(r, axis=0) / np.linalg.norm(b[keep], axis=0)) <= 1e-10
+    assert f.stats()["refine_iterations"] <= 12
+
+
+def test_config1_exact():
+    """The plain FP64 parity case as stated: 20^3 hexes -> 48,000 jittered tets,
+    linear elastic E = 1, nu = 0.3, z = 0 pinned, one N(0,1) right-hand side.
+    GPU assembly bit-exact with the oracle, the FP64 factor entrywise within 1e-11
+    of the oracle's, the solve within 1e-11 of the oracle's solve, and the relative
+    residual within 1e-10."""
+    from meshfemsparse_b200 import workloads
+    wl = workloads.config1()
+    assert wl.tets.shape[0] == 48000 and wl.nodes.shape[0] == 9261
+    f = B200Factorizer(False)
+    f.factorizeSymbolic(wl.H, wl.pins)
+    assert f.n_reduced() == 26460
+    f.setElements(wl.tets)
+    Ax = f.assemble(wl.Ke)
+    Ax_ref = pyoracle.assemble(wl.H.numBlocks, wl.H.Ap, wl.H.Ai, wl.tets, wl.Ke)
+    assert np.array_equal(Ax, Ax_ref)
+    f.factorizeAssembled()
+    sn = f.supernodes()
+    plan = f.conversionPlan()
+    w, d, fr, pan, col0 = pyoracle.panel_layout(sn)
+    ref = pyoracle.inject(plan["entries"], sn["vb"], 3, Ax_ref, int(pan[-1]))
+    pyoracle.load_blas()
+    assert pyoracle.mf_factor(sn, ref, 8) == -1
+    got = f.factorValues()
+    assert rel_err(got, ref) <= 1e-11
+    b = wl.rhs[:, 0]
+    x = f.solve(b)
+    bp = f.removeFixedEntries(b, permute=True)
+    x_ref = f.extractFullSolution(pyoracle.mf_solve(sn, ref, bp), permute=True)
+    assert np.linalg.norm(x - x_ref) <= 1e-11 * np.linalg.norm(x_ref)
+    wl.H.Ax = Ax_ref
+    keep = np.ones(wl.H.n, bool)
+    keep[wl.pins] = False
+    A = wl.H.to_scipy_full()[keep][:, keep]
+    assert np.linalg.norm(A @ x[keep] - b[keep]) <= 1e-10 * np.linalg.norm(b[keep])
+    assert np.all(x[wl.pins] == 0.0)
