@@ -75,7 +75,11 @@ typedef struct {
     int32_t use_graphs;         /* capture the factorization / solve launch sequence in CUDA graphs */
     int32_t tensor_cores;       /* FP32 Schur updates: 0 auto (TF32 with refinement, else split 3xTF32),
                                    1 TF32 on tcgen05, 2 split 3xTF32 (FP32-level products, mma.sync),
-                                   3 TF32 on mma.sync (the pre-Blackwell tensor-core path) */
+                                   3 TF32 on mma.sync (the pre-Blackwell tensor-core path),
+                                   4 TF32 on tcgen05 with TMA-fed operands for the Schur updates,
+                                   5 FP16 operands on tcgen05 (kind::f16, TMA-fed): the row solves
+                                     write a copy of the panels scaled by a power of two per front;
+                                     needs refine = 1 (without it: as 2) */
     int32_t time_kernels;       /* 1: mfs_numeric times each tensor-core GEMM launch with CUDA events on its
                                    stream (mfs_stats.gemm_ms / gemm_flops); adds event records, off by default */
     int32_t nd_reuse_period;    /* > 0: a nested-dissection analysis of a changed pattern on the same variables
@@ -231,8 +235,9 @@ typedef struct {
     int32_t num_levels;          /* levels of the assembly tree */
     int32_t num_large;           /* supernodes on the tiled large-front path */
     int64_t kernel_launches;     /* kernels launched by the library since it was loaded */
-    int32_t perturbed_pivots;    /* FP32 factor under refinement: non-positive pivots replaced by a
-                                    floor relative to the injected diagonal (last numeric) */
+    int32_t perturbed_pivots;    /* FP32 factor under refinement: non-positive pivots (after the FP64
+                                    re-factor, for large fronts) replaced by a floor relative to the
+                                    injected diagonal (last numeric) */
     int32_t pcg_iterations;      /* iterations of the last mfs_pcg_solve (max over RHS) */
     int32_t pcg_fallback;        /* 1: the last mfs_pcg_solve missed the tolerance and used the factor */
     int32_t nd_reused;           /* 1: the last symbolic analysis reused the previous separator tree */
@@ -241,6 +246,10 @@ typedef struct {
     double gemm_flops;           /* algorithmic flops of those launches (2mnk, triangle-aware; m n k per row solve) */
     int64_t gemm_launches;       /* GEMM launches timed */
     int64_t nd_rebuilt_vertices; /* nd_reused: analysis variables re-dissected */
+    int32_t refactored_blocks;   /* FP32 factor under refinement: large-front diagonal blocks whose FP32
+                                    factorization met a pivot <= 1e-5 x the injected diagonal and were
+                                    factored again in FP64 (last numeric) */
+    int32_t reserved_stats;
 } mfs_stats;
 mfs_status mfs_get_stats(const mfs_handle *h, mfs_stats *st);
 

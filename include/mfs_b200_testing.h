@@ -17,20 +17,23 @@ extern "C" {
 #endif
 
 /* Fields of one Schur-update GEMM task, in this order (int64 each). */
-#define MFS_GEMM_TASK_FIELDS 11
-/* a_off, b_off, c_off, lda, ldb, ldc, m, n, k, lower, mode:
- *   mode 0:  C(i,j) -= sum_k A(i,k) B(j,k)     mode 1:  C(i,j) = sum_k A(i,k) B(j,k)
+#define MFS_GEMM_TASK_FIELDS 12
+/* a_off, b_off, c_off, lda, ldb, ldc, m, n, k, lower, mode, scale_exp:
+ *   mode 0:  C(i,j) -= 2^scale_exp sum_k A(i,k) B(j,k)     mode 1:  C(i,j) = sum_k A(i,k) B(j,k)
  *   for i < m, j < n (lower = 1: only i >= j), A, B, C column-major at the given
  *   offsets (elements) of the arrays A, B, C of a_len, b_len, c_len elements.
  *
  * Runs one launch of the factorization's GEMM kernel over all tasks on `device`
  * (device pointers; the call synchronizes the device). precision MFS_PREC_FP32:
  * float arrays, `kernel` 1 = single-pass TF32 on the 5th-generation tensor cores
- * (tcgen05), 3 = split 3xTF32 (mma.sync), 0 = single-pass TF32 (mma.sync);
+ * (tcgen05), 4 = the same with TMA-fed operands (mode 0 only; arrays 16-byte
+ * aligned), 5 = FP16 A and B (IEEE half arrays, leading dimensions multiples of 8)
+ * with FP32 C on tcgen05 with TMA (mode 0 only; scale_exp is used by this kernel
+ * only), 3 = split 3xTF32 (mma.sync), 0 = single-pass TF32 (mma.sync);
  * MFS_PREC_FP64: double arrays on the FP64 tensor cores (kernel ignored).
  * FP32 leading dimensions must be multiples of 4 (16-byte aligned columns, as
  * the factor's panels are). Every access is checked against the array lengths
- * before the launch (MFS_INVALID_ARG otherwise). */
+ * (elements of each array's type) before the launch (MFS_INVALID_ARG otherwise). */
 mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t kernel, int64_t ntasks,
                           const int64_t *tasks, const void *A, int64_t a_len, const void *B, int64_t b_len,
                           void *C, int64_t c_len, char *err_buf, size_t err_len);

@@ -29,7 +29,7 @@ EXPORTED = [
     "mfs_lpc_get_weights", "mfs_lpc_set_weights", "mfs_lpc_loss_grad", "mfs_lpc_train_step", "mfs_pcg_solve",
     "mfs_debug_gemm",
 ]
-GEMM_TASK_FIELDS = 11
+GEMM_TASK_FIELDS = 12
 
 
 class Options(C.Structure):
@@ -51,7 +51,7 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_int64), ("perturbed_pivots", C.c_int32), ("pcg_iterations", C.c_int32),
         ("pcg_fallback", C.c_int32), ("nd_reused", C.c_int32), ("pcg_ms", C.c_double),
         ("gemm_ms", C.c_double), ("gemm_flops", C.c_double), ("gemm_launches", C.c_int64),
-        ("nd_rebuilt_vertices", C.c_int64),
+        ("nd_rebuilt_vertices", C.c_int64), ("refactored_blocks", C.c_int32), ("reserved_stats", C.c_int32),
     ]
 
 

@@ -73,11 +73,12 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         f32v[s] = int32_t(S.f[s]);
     }
     // Device panel layout: the catamari panel with its leading dimension rounded up
-    // to a multiple of 4, so every column starts 16-byte aligned.
+    // to a multiple of 8, so every column starts 16-byte aligned, in the factor and in
+    // the half-precision operand copy of an FP32 factor alike.
     ds->dpan.assign(nsn + 1, 0);
     ds->dld.assign(nsn, 0);
     for (idx s = 0; s < nsn; ++s) {
-        ds->dld[s] = int32_t((S.f[s] + 3) & ~idx(3));
+        ds->dld[s] = int32_t((S.f[s] + 7) & ~idx(7));
         ds->dpan[s + 1] = ds->dpan[s] + int64_t(ds->dld[s]) * S.w[s];
     }
     ds->panel_alloc = ds->dpan[nsn];
@@ -159,6 +160,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         int base = 0;
         idx maxw = 0;
         for (idx s : large) {
+            ds->large_fronts.push_back(int32_t(s));
             inv_off[s] = inv_end;
             inv_end += ((S.w[s] + 63) / 64) * 4096;
             asm_tasks.push_back({int32_t(s), base});
@@ -172,21 +174,24 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         const int TM = gemm_tile_m(f64), TN = gemm_tile_n(f64);
         // The in-place row solve needs every CTA tile to span the block's columns
         // (with the FP32 tiles' alignment shift of up to 3 columns).
-        if (NB + (f64 ? 0 : 3) > TN) throw StatusError(MFS_INTERNAL, "column block wider than the GEMM tile");
+        if (NB + (f64 ? 0 : 7) > TN) throw StatusError(MFS_INTERNAL, "column block wider than the GEMM tile");
+        // sn: the front of the task; for a mode-0 task its panel holds A and B, which the
+        // TMA-fed kernel reads through the panel's tensor map
         auto gemm = [&](int64_t a_off, int64_t b_off, int64_t c_off, int lda, int ldb, int ldc, idx m, idx n, idx k,
-                        int lower, int mode, int &base) {
+                        int lower, int mode, int &base, idx sn) {
             GemmTask g{};
             g.a_off = a_off; g.b_off = b_off; g.c_off = c_off;
             g.lda = lda; g.ldb = ldb; g.ldc = ldc;
             g.m = int32_t(m); g.n = int32_t(n); g.k = int32_t(k);
-            // FP32 operands are staged in 16-byte chunks: a tile starts at the
-            // aligned element at or before the operand (leading dimensions are
-            // multiples of 4, so the shift is the same for every column).
+            // FP32 operands (and their FP16 copies) are staged in 16-byte chunks: a
+            // tile starts at the 8-element aligned element at or before the operand
+            // (panel leading dimensions are multiples of 8, so the shift is the same
+            // for every column).
             int da = 0, db = 0;
             if (!f64) {
                 if ((lda & 3) || (ldb & 3)) throw StatusError(MFS_INTERNAL, "unaligned GEMM operand");
-                da = int(a_off & 3);
-                db = int(b_off & 3);
+                da = int(a_off & 7);
+                db = int(b_off & 7);
             }
             g.shift = da | (db << 8);
             g.tiles_m = int32_t((m + da + TM - 1) / TM);
@@ -194,6 +199,16 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             g.tile_base = base;
             g.lower = lower;
             g.mode = mode;
+            g.amap = g.bmap = -1;
+            g.sn = int32_t(sn);
+            if (!f64 && mode == 0 && sn >= 0) {
+                const int64_t ra = a_off - dpan[sn], rb = b_off - dpan[sn];
+                g.amap = g.bmap = int32_t(sn);
+                g.ax = int32_t(ra % dld[sn]) - da;
+                g.ay = int32_t(ra / dld[sn]);
+                g.bx = int32_t(rb % dld[sn]) - db;
+                g.by = int32_t(rb / dld[sn]);
+            }
             base += g.tiles_m * g.tiles_n;
             gemm_tasks.push_back(g);
         };
@@ -214,7 +229,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
                     if (w <= kb) continue;
                     const int nb = int(std::min<idx>(NB, w - kb));
                     const int64_t a = pan + ko * ld + kb;
-                    gemm(a, a, pan + kb * ld + kb, int(ld), int(ld), int(ld), f - kb, nb, kb - ko, 1, 0, lb);
+                    gemm(a, a, pan + kb * ld + kb, int(ld), int(ld), int(ld), f - kb, nb, kb - ko, 1, 0, lb, s);
                 }
             sp.left_n = int(gemm_tasks.size()) - sp.left_off;
             sp.left_tiles = lb;
@@ -249,7 +264,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
                     const idx m = S.f[s] - (kb + pt.nb);   // rows of the front below the block
                     if (m > 0)
                         gemm(pt.off + pt.nb, pt.inv_full, pt.off + pt.nb, pt.ld, pt.ldi, pt.ld, m, pt.nb, pt.nb, 0, 1,
-                             tb);
+                             tb, s);
                 }
             }
             sp.trsm_n = int(gemm_tasks.size()) - sp.trsm_off;
@@ -267,7 +282,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
                 if (ke != std::min<idx>(ko + GB, w) || ke >= w) continue;
                 const int64_t a = pan + ko * ld + ke;
                 gemm(a, a, pan + ke * ld + ke, int(ld), int(ld), int(ld), f - ke, std::min<idx>(GB, w - ke), ke - ko,
-                     1, 0, gb);
+                     1, 0, gb, s);
                 if (ke + GB < w) rest_fronts.push_back(s);
             }
             sp.gemm_n = int(gemm_tasks.size()) - sp.gemm_off;
@@ -278,7 +293,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
                 const idx w = S.w[s], f = S.f[s], ld = dld[s], pan = dpan[s];
                 const idx ke = std::min<idx>(kb + NB, w), kr = ke + GB;
                 const int64_t a = pan + ko * ld + kr;
-                gemm(a, a, pan + kr * ld + kr, int(ld), int(ld), int(ld), f - kr, w - kr, ke - ko, 1, 0, rb);
+                gemm(a, a, pan + kr * ld + kr, int(ld), int(ld), int(ld), f - kr, w - kr, ke - ko, 1, 0, rb, s);
             }
             sp.rest_n = int(gemm_tasks.size()) - sp.rest_off;
             sp.rest_tiles = rb;
@@ -289,7 +304,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         for (idx s : large) {
             if (S.d[s] == 0 || S.upd_off[s] < 0) continue;
             const int64_t a = dpan[s] + S.w[s];
-            gemm(a, a, S.upd_off[s], dld[s], dld[s], int(S.d[s]), S.d[s], S.d[s], S.w[s], 1, 0, sb);
+            gemm(a, a, S.upd_off[s], dld[s], dld[s], int(S.d[s]), S.d[s], S.d[s], S.w[s], 1, 0, sb, s);
         }
         L.syrk_n = int(gemm_tasks.size()) - L.syrk_off;
         L.syrk_tiles = sb;
@@ -303,6 +318,28 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         flag_base[s] = nflags;
         nflags += int((S.w[s] + RB - 1) / RB);
     }
+    // Superblock diagonal solves of the levels above the solve cut: one flag and one
+    // stored inverse (nrp x nrp, after the 64 x 64 diagonal inverses) per superblock.
+    std::vector<SbTask> fsb, bsb, isb;
+    std::vector<int32_t> sb_flag(nsn, -1);
+    std::vector<int64_t> sb_inv(nsn, -1);
+    int nsbflags = 0;
+    const idx SBk = kSuperBlock;
+    for (idx l = S.solve_cut + 1; l < S.nlevels; ++l)
+        for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
+            const idx s = S.level_list[k];
+            const idx nsb = (S.w[s] + SBk - 1) / SBk;
+            sb_flag[s] = nsbflags;
+            nsbflags += int(nsb);
+            sb_inv[s] = inv_end;
+            for (idx K = 0; K < nsb; ++K) {
+                const idx nr = std::min(SBk, S.w[s] - K * SBk), nrp = (nr + 63) & ~idx(63);
+                isb.push_back({int32_t(s), int32_t(K), sb_flag[s], 0, inv_end});
+                inv_end += nrp * nrp;
+            }
+        }
+    // every superblock before a front's last is full (SB x SB)
+    auto sb_task = [&](idx s, idx K) { return SbTask{int32_t(s), int32_t(K), sb_flag[s], 0, sb_inv[s] + K * SBk * SBk}; };
     std::vector<SolveAsmTask> sasm;
     std::vector<SolveTask> ftri, btri;
     std::vector<StrTask> fstr, bstr;
@@ -366,8 +403,31 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             }
         L.ftri_n = int(ftri.size()) - L.ftri_off;
         L.btri_n = int(btri.size()) - L.btri_off;
+        // superblock tasks: ascending superblock index across the level's fronts (forward),
+        // descending (backward); every dependency precedes its task
+        L.fsb_off = int(fsb.size());
+        L.bsb_off = int(bsb.size());
+        if (l > S.solve_cut) {
+            idx maxnsb = 0;
+            for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k)
+                maxnsb = std::max<idx>(maxnsb, (S.w[S.level_list[k]] + SBk - 1) / SBk);
+            for (idx K = 0; K < maxnsb; ++K)
+                for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
+                    const idx s = S.level_list[k];
+                    if (K < (S.w[s] + SBk - 1) / SBk) fsb.push_back(sb_task(s, K));
+                }
+            for (idx p = 0; p < maxnsb; ++p)
+                for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
+                    const idx s = S.level_list[k];
+                    const idx nsb = (S.w[s] + SBk - 1) / SBk;
+                    if (p < nsb) bsb.push_back(sb_task(s, nsb - 1 - p));
+                }
+        }
+        L.fsb_n = int(fsb.size()) - L.fsb_off;
+        L.bsb_n = int(bsb.size()) - L.bsb_off;
     }
     ds->small_list.upload(small_list, st);
+    ds->large_dev.upload(ds->large_fronts, st);
     ds->all_list.upload(all_list, st);
     ds->inv_off.upload(inv_off, st);
     ds->factor_alloc = std::max<int64_t>(inv_end, 1);
@@ -396,6 +456,10 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     up(ds->bstr_tasks, bstr);
     up(ds->fred, fred);
     up(ds->bred, bred);
+    up(ds->fsb_tasks, fsb);
+    up(ds->bsb_tasks, bsb);
+    up(ds->isb_tasks, isb);
+    ds->nsb_inv = int(isb.size());
     ds->max_str_tasks = max_str;
     {
         std::vector<int2> sv(S.sub_lo.size());
@@ -405,7 +469,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         ds->sub_fmax = int(S.sub_fmax);
         ds->solve_cut = int(S.solve_cut);
     }
-    ds->flags.ensure(size_t(std::max(nflags, 1)));
+    ds->flags.ensure(size_t(std::max(std::max(nflags, nsbflags), 1)));
     MFS_CUDA(cudaMemsetAsync(ds->flags.p, 0, ds->flags.bytes(), st));
     MFS_CUDA(cudaStreamSynchronize(st));
 
@@ -444,6 +508,39 @@ void clear_factor_graphs(mfs_handle *h) {
     h->factor_graphs.clear();
 }
 
+// FP32 Schur updates: 1 = single-pass TF32 on tcgen05 (cp.async operands), 4 = the same
+// with TMA-fed operands for the updates (mode 0) and cp.async for the row solves,
+// 5 = FP16 operands (a per-front power-of-two scaled half copy of the panels, written
+// by the row solves) on tcgen05 kind::f16 with TMA for the updates, 3 = split 3xTF32
+// (mma.sync), 0 = single-pass TF32 on mma.sync. Option values: tensor_cores 0 (auto: 1
+// with refinement, else 3), 1, 2 (-> 3), 3 (-> 0), 4, 5 (with refinement, else 3).
+int fp32_split(const mfs_handle *h) {
+    const int tc = h->opt.tensor_cores;
+    if (tc == 5) return h->opt.refine ? 5 : 3;
+    return tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : tc == 4 ? 4 : (h->opt.refine ? 1 : 3);
+}
+
+// Tensor maps of the large fronts' panels in `base` (the FP32 factor, or its FP16
+// copy) for the TMA-fed GEMM (built on the host once per symbolic analysis and
+// array; not during graph capture).
+void ensure_panel_maps(mfs_handle *h, DevSym &ds, const void *base, bool half) {
+    if (h->tmaps_base == base && h->tmaps_sym == &ds) return;
+    const Symbolic &S = *ds.S;
+    const size_t es = half ? 2 : 4;
+    std::vector<TensorMapBlob> maps(size_t(std::max<idx>(S.nsn, 1)));
+    std::memset(maps.data(), 0, maps.size() * sizeof(TensorMapBlob));
+    for (int32_t s : ds.large_fronts)
+        if (!encode_operand_map(&maps[size_t(s)], static_cast<const char *>(base) + size_t(ds.dpan[s]) * es, half,
+                                uint64_t(S.f[s]), uint64_t(S.w[s]), uint64_t(ds.dld[s])))
+            throw StatusError(MFS_INTERNAL, "cuTensorMapEncodeTiled refused a panel tensor map");
+    h->tmaps.ensure(maps.size());
+    MFS_CUDA(cudaMemcpyAsync(h->tmaps.p, maps.data(), maps.size() * sizeof(TensorMapBlob), cudaMemcpyHostToDevice,
+                             h->stream));
+    MFS_CUDA(cudaStreamSynchronize(h->stream));
+    h->tmaps_base = base;
+    h->tmaps_sym = &ds;
+}
+
 template <typename T>
 void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const double *Ax, const double *Bx,
                 double sigma) {
@@ -452,17 +549,30 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
     // FP32 factors: single-pass TF32 when FP64 refinement recovers the accuracy,
     // split 3xTF32 (FP32-level products) otherwise or when asked for.
     // 1: single-pass TF32 on tcgen05, 3: split 3xTF32 (mma.sync), 0: single-pass TF32 on mma.sync
-    const int tc = h->opt.tensor_cores;
-    const int split = tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : (h->opt.refine ? 1 : 3);
+    const int split = fp32_split(h);
     // GEMM launch, bracketed by CUDA events on its stream when kernel timing is on
     const bool timing = h->opt.time_kernels != 0;
     h->gemm_events_used = 0;
     h->gemm_flops_timed = 0.0;
+    auto launch = [&](const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int sp, int *err,
+                      cudaStream_t s, bool mode0) {
+        if constexpr (std::is_same<T, float>::value) {
+            if ((sp == 4 || sp == 5) && mode0) {
+                launch_gemm_tma(sp == 5, tasks, ntasks, ntiles, h->tmaps.p, C, sp == 5 ? h->sexp.p : nullptr, err, s);
+                return;
+            }
+            if (sp == 5) {
+                launch_gemm_tc(tasks, ntasks, ntiles, A, B, C, err, s, h->h16.p, h->sexp.p);
+                return;
+            }
+        }
+        launch_gemm<T>(tasks, ntasks, ntiles, A, B, C, sp >= 4 ? 1 : sp, err, s);
+    };
     auto tgemm = [&](const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int sp, int *err,
-                     cudaStream_t s) {
+                     cudaStream_t s, bool mode0 = true) {
         if (ntasks <= 0) return;
         if (!timing) {
-            launch_gemm<T>(tasks, ntasks, ntiles, A, B, C, sp, err, s);
+            launch(tasks, ntasks, ntiles, A, B, C, sp, err, s, mode0);
             return;
         }
         if (h->gemm_events_used + 2 > h->gemm_events.size()) {
@@ -475,7 +585,7 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         const size_t t0 = size_t(tasks - ds.gemm_tasks.p);
         h->gemm_flops_timed += ds.gemm_flops_prefix[t0 + ntasks] - ds.gemm_flops_prefix[t0];
         MFS_CUDA(cudaEventRecord(h->gemm_events[h->gemm_events_used], s));
-        launch_gemm<T>(tasks, ntasks, ntiles, A, B, C, sp, err, s);
+        launch(tasks, ntasks, ntiles, A, B, C, sp, err, s, mode0);
         MFS_CUDA(cudaEventRecord(h->gemm_events[h->gemm_events_used + 1], s));
         h->gemm_events_used += 2;
     };
@@ -487,12 +597,18 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         launch_diag_shift<T>(ds.diag_off.p, S.n, sigma, factor, st);
         MFS_LAUNCHED();
     }
-    // The FP32 factor preconditions FP64 refinement: non-positive pivots are
-    // perturbed (relative to the injected diagonal) instead of failing.
-    PivotCtl pv{h->fail.p, h->perturbed.p, nullptr};
+    // The FP32 factor preconditions FP64 refinement: a large front's diagonal block
+    // whose FP32 factorization meets a non-positive or tiny pivot is factored again
+    // in FP64 (mfs_stats.refactored_blocks); pivots that stay non-positive there, and
+    // non-positive pivots of fronts factored whole in shared memory, are perturbed
+    // (relative to the injected diagonal) instead of failing.
+    PivotCtl pv{h->fail.p, h->perturbed.p, nullptr, nullptr};
     if (h->opt.precision == MFS_PREC_FP32 && h->opt.refine) {
         h->dorig.ensure(size_t(std::max<idx>(S.n, 1)));
+        pv.refactored = h->refactored.p;
         launch_extract_diag<T>(ds.diag_off.p, S.n, factor, h->dorig.p, st);
+        if (split == 5)
+            launch_front_scale(ds.large_dev.p, int(ds.large_fronts.size()), ds.sd, h->dorig.p, h->sexp.p, st);
         MFS_LAUNCHED();
         pv.dorig = h->dorig.p;
     }
@@ -518,11 +634,11 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
             tgemm(ds.gemm_tasks.p + sp.left_off, sp.left_n, sp.left_tiles, factor, factor, factor, split,
                            h->gemm_err.p, hs);
             MFS_LAUNCHED();
-            launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, dscr, pv, split == 1,
+            launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, dscr, pv, split == 1 || split >= 4,
                             hs);
             MFS_LAUNCHED();
             tgemm(ds.gemm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, factor, dscr, factor, split,
-                           h->gemm_err.p, hs);
+                           h->gemm_err.p, hs, false);
             MFS_LAUNCHED();
             if (sp.gemm_n == 0) continue;
             if (sp.rest_n > 0) MFS_CUDA(cudaEventRecord(h->ev_ready, hs));
@@ -549,6 +665,9 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
             MFS_LAUNCHED();
         }
     }
+    // inverses of the superblocks of L11 that the diagonal solves apply
+    launch_sb_inverse<T>(ds.isb_tasks.p, ds.nsb_inv, ds.sd, factor, st);
+    MFS_LAUNCHED();
 }
 
 // The factorization's launch sequence, replayed from an instantiated CUDA graph when
@@ -560,18 +679,26 @@ template <typename T>
 void factor_sequence(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const double *Ax, const double *Bx,
                      double sigma) {
     ensure_side_stream(h);
-    const int tc = h->opt.tensor_cores;
-    const int split = tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : (h->opt.refine ? 1 : 3);
+    const int split = fp32_split(h);
+    if constexpr (std::is_same<T, float>::value) {
+        if (split == 4) ensure_panel_maps(h, ds, factor, false);
+        if (split == 5) {
+            h->h16.ensure(size_t(std::max<int64_t>(ds.panel_alloc, 1)));
+            h->sexp.ensure(size_t(std::max<idx>(ds.S->nsn, 1)));
+            ensure_panel_maps(h, ds, h->h16.p, true);
+        }
+    }
     // (the legacy default stream cannot be captured: graphs need a handle or caller stream)
     if (!h->opt.use_graphs || h->opt.time_kernels || h->stream == nullptr) {
         run_factor<T>(h, ds, factor, upd, dscr, Ax, Bx, sigma);
         return;
     }
     const void *dorig = h->dorig.p;
-    mfs_handle::FactorGraph key{&ds, factor, upd, dscr, Ax, Bx, dorig, sigma, split, nullptr};
+    mfs_handle::FactorGraph key{&ds, factor, upd, dscr, Ax, Bx, dorig, h->h16.p, h->tmaps.p, sigma, split, nullptr};
     auto same = [&](const mfs_handle::FactorGraph &g) {
         return g.ds == key.ds && g.factor == key.factor && g.upd == key.upd && g.dscr == key.dscr &&
-               g.ax == key.ax && g.bx == key.bx && g.dorig == key.dorig && g.sigma == key.sigma &&
+               g.ax == key.ax && g.bx == key.bx && g.dorig == key.dorig && g.h16 == key.h16 &&
+               g.tmaps == key.tmaps && g.sigma == key.sigma &&
                g.split == key.split;
     };
     auto it = std::find_if(h->factor_graphs.begin(), h->factor_graphs.end(), same);
@@ -625,8 +752,8 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
             const LevelPlan &L = ds.levels[l];
             launch_fwd_asm(ds.sasm_tasks.p + L.sasm_off, L.sasm_n, L.sasm_tiles, ds.sd, Xc, S.n, nr, h->sol.p, st);
             MFS_LAUNCHED();
-            MFS_CUDA(launch_diag<T>(true, ds.ftri_tasks.p + L.ftri_off, L.ftri_n, ds.sd, factor, Xc, S.n, nr,
-                                    ds.flags.p, h->solve_err.p, st));
+            MFS_CUDA(launch_sb_solve<T>(true, ds.fsb_tasks.p + L.fsb_off, L.fsb_n, ds.sd, factor, Xc, S.n, nr,
+                                        ds.flags.p, h->solve_err.p, st));
             launch_str<T>(true, ds.fstr_tasks.p + L.fstr_off, L.fstr_n, ds.fred.p + L.fred_off, L.fred_n, ds.sd,
                           factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
             MFS_LAUNCHED();
@@ -636,8 +763,8 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
             launch_str<T>(false, ds.bstr_tasks.p + L.bstr_off, L.bstr_n, ds.bred.p + L.bred_off, L.bred_n, ds.sd,
                           factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
             MFS_LAUNCHED();
-            MFS_CUDA(launch_diag<T>(false, ds.btri_tasks.p + L.btri_off, L.btri_n, ds.sd, factor, Xc, S.n, nr,
-                                    ds.flags.p, h->solve_err.p, st));
+            MFS_CUDA(launch_sb_solve<T>(false, ds.bsb_tasks.p + L.bsb_off, L.bsb_n, ds.sd, factor, Xc, S.n, nr,
+                                        ds.flags.p, h->solve_err.p, st));
         }
         launch_subtree_solve<T>(false, ds.subs.p, ds.nsub, ds.sub_fmax, ds.sd, factor, Xc, S.n, nr, h->sol.p, st);
         MFS_LAUNCHED();
@@ -849,10 +976,11 @@ mfs_status mfs_create(mfs_handle **out, const mfs_options *opt) {
         }
         MFS_CUDA(cudaEventCreate(&h->ev0));
         MFS_CUDA(cudaEventCreate(&h->ev1));
-        MFS_CUDA(cudaMallocHost(&h->fail_host, 3 * sizeof(int)));
+        MFS_CUDA(cudaMallocHost(&h->fail_host, 4 * sizeof(int)));
         MFS_CUDA(cudaMallocHost(&h->dots_host, 64 * sizeof(double)));
         h->fail.ensure(1);
         h->perturbed.ensure(1);
+        h->refactored.ensure(1);
         h->solve_err.ensure(1);
         MFS_CUDA(cudaMemset(h->solve_err.p, 0, sizeof(int)));
         h->gemm_err.ensure(1);
@@ -1021,6 +1149,7 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
         const int big = INT_MAX;
         MFS_CUDA(cudaMemcpyAsync(h->fail.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
         MFS_CUDA(cudaMemsetAsync(h->perturbed.p, 0, sizeof(int), st));
+        MFS_CUDA(cudaMemsetAsync(h->refactored.p, 0, sizeof(int), st));
         MFS_CUDA(cudaEventRecord(h->ev0, st));
         if (h->opt.precision == MFS_PREC_FP32) {
             if (!h->cur.f32 || h->cur.f32.use_count() > 1) h->cur.f32 = std::make_shared<DBuf<float>>();
@@ -1039,11 +1168,13 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
         MFS_CUDA(cudaMemcpyAsync(h->fail_host, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         MFS_CUDA(cudaMemcpyAsync(h->fail_host + 1, h->perturbed.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         MFS_CUDA(cudaMemcpyAsync(h->fail_host + 2, h->gemm_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        MFS_CUDA(cudaMemcpyAsync(h->fail_host + 3, h->refactored.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         MFS_CUDA(cudaStreamSynchronize(st));
         float ms = 0;
         cudaEventElapsedTime(&ms, h->ev0, h->ev1);
         h->stats.factor_ms = ms;
         h->stats.perturbed_pivots = h->fail_host[1];
+        h->stats.refactored_blocks = h->fail_host[3];
         h->stats.gemm_ms = 0.0;
         h->stats.gemm_flops = h->gemm_flops_timed;
         h->stats.gemm_launches = int64_t(h->gemm_events_used / 2);

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -36,17 +37,20 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
         put_error(err_buf, err_len, "empty task list or null array");
         return MFS_INVALID_ARG;
     }
-    if (!f64 && kernel != 0 && kernel != 1 && kernel != 3) {
-        put_error(err_buf, err_len, "kernel must be 0, 1 or 3");
+    if (!f64 && kernel != 0 && kernel != 1 && kernel != 3 && kernel != 4 && kernel != 5) {
+        put_error(err_buf, err_len, "kernel must be 0, 1, 3, 4 or 5");
         return MFS_INVALID_ARG;
     }
+    const bool tma = !f64 && (kernel == 4 || kernel == 5);
+    const bool half = !f64 && kernel == 5;              // A and B are FP16
+    std::vector<TensorMapBlob> maps;
     const int TM = gemm_tile_m(f64), TN = gemm_tile_n(f64);
     std::vector<GemmTask> gt(static_cast<size_t>(ntasks));
     int base = 0;
     for (int64_t t = 0; t < ntasks; ++t) {
         const int64_t *q = tasks + t * MFS_GEMM_TASK_FIELDS;
         const int64_t a_off = q[0], b_off = q[1], c_off = q[2], lda = q[3], ldb = q[4], ldc = q[5];
-        const int64_t m = q[6], n = q[7], k = q[8], lower = q[9], mode = q[10];
+        const int64_t m = q[6], n = q[7], k = q[8], lower = q[9], mode = q[10], scale_exp = q[11];
         const std::string id = "task " + std::to_string(t) + ": ";
         if (m <= 0 || n <= 0 || k <= 0 || m > (1 << 30) || n > (1 << 30) || k > (1 << 30)) {
             put_error(err_buf, err_len, id + "m, n, k must be positive");
@@ -62,12 +66,19 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
         }
         int da = 0, db = 0;
         if (!f64) {
-            if ((lda & 3) || (ldb & 3)) {
-                put_error(err_buf, err_len, id + "FP32 leading dimensions must be multiples of 4");
+            // 16-byte aligned columns; tiles start at the 8-element boundary at or before
+            // the operand, as in the factorization
+            const int64_t al = half ? 7 : 3;
+            if ((lda & al) || (ldb & al)) {
+                put_error(err_buf, err_len, id + "leading dimensions must span whole 16-byte units");
                 return MFS_INVALID_ARG;
             }
-            da = int(a_off & 3);
-            db = int(b_off & 3);
+            da = int(a_off & 7);
+            db = int(b_off & 7);
+        }
+        if (scale_exp < -60 || scale_exp > 60 || (scale_exp != 0 && !half)) {
+            put_error(err_buf, err_len, id + "scale_exp applies to FP16 operands only (|scale_exp| <= 60)");
+            return MFS_INVALID_ARG;
         }
         // the kernels read A rows [a_off - da, a_off + m) of columns 0..k-1, B likewise,
         // and write C rows [0, m) of columns 0..n-1
@@ -86,6 +97,33 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
         g.tile_base = base;
         g.lower = int32_t(lower);
         g.mode = int32_t(mode);
+        g.amap = g.bmap = -1;
+        g.ax = g.ay = g.bx = g.by = 0;
+        g.scale_exp = int32_t(scale_exp);
+        g.sn = -1;
+        if (tma) {
+            // one tensor map per operand, starting at the shifted (16-byte aligned) operand
+            if (mode != 0) {
+                put_error(err_buf, err_len, id + "the TMA-fed kernel runs mode 0 only");
+                return MFS_INVALID_ARG;
+            }
+            maps.resize(maps.size() + 2);
+            TensorMapBlob *ma = &maps[maps.size() - 2], *mb = &maps[maps.size() - 1];
+            const size_t es = half ? 2 : 4;
+            const char *Af = static_cast<const char *>(A) + size_t(a_off - da) * es;
+            const char *Bf = static_cast<const char *>(B) + size_t(b_off - db) * es;
+            if ((reinterpret_cast<uintptr_t>(Af) & 15) || (reinterpret_cast<uintptr_t>(Bf) & 15)) {
+                put_error(err_buf, err_len, id + "arrays must be 16-byte aligned");
+                return MFS_INVALID_ARG;
+            }
+            if (!encode_operand_map(ma, Af, half, uint64_t(m + da), uint64_t(k), uint64_t(lda)) ||
+                !encode_operand_map(mb, Bf, half, uint64_t(n + db), uint64_t(k), uint64_t(ldb))) {
+                put_error(err_buf, err_len, id + "tensor map refused by the driver");
+                return MFS_INVALID_ARG;
+            }
+            g.amap = int32_t(maps.size() - 2);
+            g.bmap = int32_t(maps.size() - 1);
+        }
         if (int64_t(base) + int64_t(g.tiles_m) * g.tiles_n > INT32_MAX / 2) {
             put_error(err_buf, err_len, "too many tiles");
             return MFS_INVALID_ARG;
@@ -94,10 +132,12 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
     }
     GemmTask *dt = nullptr;
     int *derr = nullptr;
+    TensorMapBlob *dmaps = nullptr;
     auto fail = [&](cudaError_t e) {
         put_error(err_buf, err_len, cudaGetErrorString(e));
         if (dt) cudaFree(dt);
         if (derr) cudaFree(derr);
+        if (dmaps) cudaFree(dmaps);
         return MFS_CUDA_ERROR;
     };
     cudaError_t e = cudaSetDevice(device);
@@ -107,7 +147,13 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
     if ((e = cudaMemcpy(dt, gt.data(), gt.size() * sizeof(GemmTask), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(e);
     if ((e = cudaMemset(derr, 0, sizeof(int))) != cudaSuccess) return fail(e);
-    if (f64)
+    if (tma) {
+        if ((e = cudaMalloc(&dmaps, maps.size() * sizeof(TensorMapBlob))) != cudaSuccess) return fail(e);
+        if ((e = cudaMemcpy(dmaps, maps.data(), maps.size() * sizeof(TensorMapBlob), cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return fail(e);
+        launch_gemm_tma(half, dt, int(ntasks), base, dmaps, static_cast<float *>(C), nullptr, derr, nullptr);
+    } else if (f64)
         launch_gemm<double>(dt, int(ntasks), base, static_cast<const double *>(A), static_cast<const double *>(B),
                             static_cast<double *>(C), 0, derr, nullptr);
     else
@@ -119,6 +165,7 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
     if ((e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return fail(e);
     cudaFree(dt);
     cudaFree(derr);
+    if (dmaps) cudaFree(dmaps);
     if (herr) {
         put_error(err_buf, err_len, "a tensor-core pipeline wait timed out");
         return MFS_TIMEOUT;

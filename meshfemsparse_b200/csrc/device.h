@@ -2,12 +2,14 @@
 //
 // Storage in HBM (all column-major):
 //   factor values  : one panel per supernode, (w+d) x w with ld = w+d rounded up to a
-//                    multiple of 4 (16-byte aligned columns for the tensor-core
-//                    GEMM loads), panels back to back; the catamari layout
+//                    multiple of 8 (16-byte aligned columns for the tensor-core
+//                    GEMM loads, FP32 and FP16), panels back to back; the catamari layout
 //                    (CatamariConversionPlan.hh:366, ld = w+d) is produced on export;
 //                    followed by the
 //                    64 x 64 inverses of the diagonal blocks of every large front's L11
-//                    (written by the panel kernel, read by the triangular solves)
+//                    (written by the panel kernel) and the inverses of the 256-row
+//                    superblocks of L11 of the fronts above the solve cut (written
+//                    after the factorization, read by the triangular solves)
 //   update arena   : U_s (d x d, ld d) of the multifrontal assembly tree; offsets from
 //                    the static level-lifetime plan built on the host
 //   solve arena    : u_s (d x nrhs, ld d) forward-substitution update vectors; offsets
@@ -46,9 +48,9 @@ extern long long g_kernel_launches;
 
 struct SnDev {
     const int32_t *w, *d, *f;           // scalar width / degree / front size
-    const int32_t *ld;                  // panel leading dimension: f rounded up to a multiple of 4
+    const int32_t *ld;                  // panel leading dimension: f rounded up to a multiple of 8
     const int32_t *col0;                // first scalar column of the supernode
-    const int64_t *pan_off;             // panel offset in the factor array (a multiple of 4)
+    const int64_t *pan_off;             // panel offset in the factor array (a multiple of 8)
     const int64_t *upd_off;             // U_s offset in the update arena (-1: none)
     const int64_t *sol_off;             // u_s offset (units of one RHS) in the solve arena
     const int64_t *inv_off;             // factor-array offset of the 64 x 64 inverses of L11's
@@ -66,7 +68,11 @@ struct PivotCtl {
     int *fail_col;
     int *perturbed;
     const double *dorig;                // nullptr: no perturbation, failures are reported
+    int *refactored;                    // FP32 panels under refinement: a diagonal block with a
+                                        // pivot <= kRefactorTiny * injected diagonal is factored
+                                        // again in FP64 (count of such blocks); nullptr: off
 };
+constexpr double kRefactorTiny = 1e-5;
 
 // Plan entry mirror of host_symbolic.h PlanEntry.
 struct PlanEntryDev {
@@ -88,8 +94,20 @@ struct GemmTask {
     int32_t lower;                      // 1: only i >= j is touched
     int32_t mode;
     int32_t shift;                      // FP32: tiles start da = shift & 255 rows before A and
-                                        // db = shift >> 8 rows before B (16-byte aligned starts);
+                                        // db = shift >> 8 rows before B (8-element aligned starts);
                                         // tiles_m / tiles_n cover m + da / n + db
+    // TMA-fed kernel (mode 0): tensor maps of A and B (indices into the launch's map
+    // array) and the map coordinates (row, column) of the shifted operand starts
+    // (A(-da, 0) and B(-db, 0)); C -= 2^scale_exp * A B^T.
+    int32_t amap, bmap;
+    int32_t ax, ay, bx, by;
+    int32_t scale_exp;
+    int32_t sn;                         // front of the task (-1: none); FP16 operands of a front
+                                        // are scaled by 2^-sexp[sn]
+};
+constexpr int kTensorMapBytes = 128;    // CUtensorMap (64-byte aligned in device memory)
+struct alignas(64) TensorMapBlob {
+    unsigned char bytes[kTensorMapBytes];
 };
 
 // One column block of a large front: factor its nb x nb diagonal block in
@@ -132,9 +150,18 @@ struct StrTask {
 struct StrReduce {
     int32_t sn, idx, first, nchunks;
 };
+// One superblock of a front's L11 in the diagonal-block solves: a CTA task of the
+// forward / backward chains and of the inverse kernel. inv: factor-array offset of
+// inv(L_KK) (nrp x nrp column-major, nrp = 64 * ceil(rows / 64)); flag0: the front's
+// first superblock flag.
+struct SbTask {
+    int32_t sn, K, flag0, pad;
+    int64_t inv;
+};
+constexpr int kSuperBlock = 256;        // rows per superblock
 constexpr int kStrChunk = 512;
 constexpr int kSolveAsmRows = 256;      // front rows per forward extend-add CTA
-constexpr int kMaxSolveRhs = 32;        // right-hand sides per solve pass (more are chunked)
+constexpr int kMaxSolveRhs = 16;        // right-hand sides per solve pass (more are chunked)
 
 constexpr int kAsmCols = 32;            // front columns per assemble CTA
 constexpr int kMaxSmemOptin = 232448;   // opt-in dynamic shared memory per CTA (227 KB)
@@ -164,8 +191,25 @@ void launch_panel(const PanelTask *tasks, int ntasks, int max_nb, T *factor, T *
 template <typename T>
 void launch_gemm(const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int split, int *err,
                  cudaStream_t st);
+// h16 (row solves, mode 1): also store each result as FP16 scaled by 2^-sexp[task.sn]
+// at the same offset of the half-precision copy, and store the FP32 result as that
+// FP16 value scaled back (nullptr: the result is stored rounded to TF32).
 void launch_gemm_tc(const GemmTask *tasks, int ntasks, int ntiles, const float *A, const float *B, float *C, int *err,
-                    cudaStream_t st);
+                    cudaStream_t st, void *h16 = nullptr, const int32_t *sexp = nullptr);
+// TMA-fed tcgen05 GEMM (mode 0 tasks only): FP32 operands as TF32, or FP16 operands
+// (kind::f16). C -= 2^e A B^T with e = 2 sexp[task.amap] when sexp is given (the
+// operands of a front's panel carry the front's scale), else e = task.scale_exp.
+void launch_gemm_tma(bool half, const GemmTask *tasks, int ntasks, int ntiles, const void *maps, float *C,
+                     const int32_t *sexp, int *err, cudaStream_t st);
+// Tensor map of a column-major operand (rows x cols, leading dimension ld elements,
+// base 16-byte aligned, ld * element size a multiple of 16) in the box and swizzle
+// form of the TMA-fed GEMM; false if the driver refuses it.
+bool encode_operand_map(void *out, const void *base, bool half, uint64_t rows, uint64_t cols, uint64_t ld);
+// Power-of-two scale exponent of each listed front's FP16 operand copy, from the
+// injected diagonal d: sexp[s] = e with max over the front's rows of sqrt(d) < 2^(e + 12),
+// so |L| 2^-e < 2^12 (|L(i, j)| <= sqrt(A(i, i)) for a Cholesky factor).
+void launch_front_scale(const int32_t *fronts, int nfronts, SnDev sd, const double *diag, int32_t *sexp,
+                        cudaStream_t st);
 int gemm_tile_m(bool fp64);
 int gemm_tile_n(bool fp64);
 
@@ -178,6 +222,12 @@ cudaError_t launch_diag(bool forward, const SolveTask *tasks, int ntasks, SnDev 
 template <typename T>
 void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce *red, int nred, SnDev sd,
                 const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st);
+// Superblock diagonal solves (cooperative launch) and the superblock inverses they apply.
+template <typename T>
+cudaError_t launch_sb_solve(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
+                            int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st);
+template <typename T>
+void launch_sb_inverse(const SbTask *tasks, int ntasks, SnDev sd, T *factor, cudaStream_t st);
 int solve_rows_per_task();
 int diag_blocks_per_task();             // 64-row blocks per diagonal-chain task (one flag each)
 // Forward / backward solve of whole subtrees (subs[k] = postorder range [x, y]),

@@ -87,6 +87,7 @@ struct LevelPlan {
     int sasm_off = 0, sasm_n = 0, sasm_tiles = 0;
     int ftri_off = 0, ftri_n = 0;
     int btri_off = 0, btri_n = 0;
+    int fsb_off = 0, fsb_n = 0, bsb_off = 0, bsb_n = 0;   // superblock diagonal solves (above the cut)
     int fstr_off = 0, fstr_n = 0, fred_off = 0, fred_n = 0;
     int bstr_off = 0, bstr_n = 0, bred_off = 0, bred_n = 0;
 };
@@ -104,6 +105,8 @@ struct DevSym {
     DBuf<SolveTask> ftri_tasks, btri_tasks;
     DBuf<StrTask> fstr_tasks, bstr_tasks;
     DBuf<StrReduce> fred, bred;
+    DBuf<SbTask> fsb_tasks, bsb_tasks, isb_tasks;   // superblock solves (forward, backward) and inverses
+    int nsb_inv = 0;
     int max_str_tasks = 0;
     DBuf<int2> subs;                     // subtree ranges solved one per CTA (levels <= solve_cut)
     int nsub = 0, sub_fmax = 0, solve_cut = -1;
@@ -123,6 +126,8 @@ struct DevSym {
     int64_t panel_alloc = 0;             // elements of the padded panels
     std::shared_ptr<void> lpc_graph;     // learned preconditioner: graph arrays (built on first use)
     std::vector<double> gemm_flops_prefix;   // prefix sums of the GEMM tasks' algorithmic flops
+    std::vector<int32_t> large_fronts;       // fronts factored by the tiled (GEMM) path
+    DBuf<int32_t> large_dev;                 // the same list on the device
     size_t bytes() const {
         return w.bytes() * 5 + col0.bytes() + child_ptr.bytes() + child_list.bytes() + struct_rows.bytes() +
                rel.bytes() + small_list.bytes() + all_list.bytes() + pan_off.bytes() + upd_off.bytes() +
@@ -163,6 +168,7 @@ struct mfs_handle {
     DBuf<int> active;
     DBuf<int> fail;
     DBuf<int> perturbed;          // pivots perturbed in the last numeric factorization
+    DBuf<int> refactored;         // FP32 diagonal blocks factored again in FP64 (last numeric)
     DBuf<double> dorig;           // injected diagonal (perturbation reference)
     DBuf<int> solve_err;          // set by a solve kernel whose dependency wait timed out
     DBuf<int> gemm_err;           // set by a tensor-core GEMM whose pipeline wait timed out
@@ -182,7 +188,7 @@ struct mfs_handle {
     // use_graphs: instantiated graphs of the factorization's launch sequence, keyed by
     // everything the launches bake in (symbolic data, buffers, values, shift)
     struct FactorGraph {
-        const void *ds, *factor, *upd, *dscr, *ax, *bx, *dorig;
+        const void *ds, *factor, *upd, *dscr, *ax, *bx, *dorig, *h16, *tmaps;
         double sigma;
         int split;
         cudaGraphExec_t exec;
@@ -190,6 +196,14 @@ struct mfs_handle {
     std::vector<FactorGraph> factor_graphs;
     std::shared_ptr<NDResult> nd_prev;       // last nested dissection (temporal reuse)
     int nd_reuse_count = 0;                  // analyses since the last full dissection
+    // TMA-fed GEMM: one tensor map per large front's panel (indexed by supernode),
+    // built for the array `tmaps_base` (the FP32 factor or its FP16 copy) of the
+    // symbolic data `tmaps_sym`
+    DBuf<TensorMapBlob> tmaps;
+    const void *tmaps_base = nullptr;
+    const void *tmaps_sym = nullptr;
+    DBuf<uint16_t> h16;                      // FP16 operand copy of the panels (tensor_cores 5)
+    DBuf<int32_t> sexp;                      // per front: power-of-two scale exponent of that copy
     std::vector<cudaEvent_t> gemm_events;    // time_kernels: (start, end) per GEMM launch
     size_t gemm_events_used = 0;
     double gemm_flops_timed = 0.0;

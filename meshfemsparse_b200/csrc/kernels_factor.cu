@@ -306,4 +306,40 @@ void launch_extract_diag(const int64_t *diag_off, int64_t n, const T *factor, do
 MFS_INSTANTIATE(double)
 MFS_INSTANTIATE(float)
 
+
+namespace {
+// One CTA per front: the largest injected diagonal over the front's rows (its own
+// columns and its structure rows), then the exponent that keeps its square root
+// below 2^12.
+__global__ void __launch_bounds__(256) front_scale_kernel(const int32_t *__restrict__ fronts, SnDev sd,
+                                                          const double *__restrict__ diag, int32_t *__restrict__ sexp) {
+    const int s = fronts[blockIdx.x];
+    const int w = sd.w[s], d = sd.d[s], c0 = sd.col0[s], vb = sd.vb;
+    const int32_t *rows = sd.struct_rows + sd.struct_ptr[s];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < w + d; i += blockDim.x) {
+        const int r = i < w ? c0 + i : rows[(i - w) / vb] * vb + (i - w) % vb;
+        m = fmax(m, fabs(diag[r]));
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double mx = red[0];
+        sexp[s] = (mx > 0.0 && isfinite(mx)) ? ilogb(sqrt(mx)) + 1 - 12 : 0;
+    }
+}
+}  // namespace
+
+void launch_front_scale(const int32_t *fronts, int nfronts, SnDev sd, const double *diag, int32_t *sexp,
+                        cudaStream_t st) {
+    if (nfronts <= 0) return;
+    ++g_kernel_launches;
+    front_scale_kernel<<<nfronts, 256, 0, st>>>(fronts, sd, diag, sexp);
+}
+
 }  // namespace mfs

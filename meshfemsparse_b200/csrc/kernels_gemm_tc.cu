@@ -3,6 +3,10 @@
 //     mode 0:  C(i,j) -= sum_k A(i,k) B(j,k)      (SYRK / trailing update)
 //     mode 1:  C(i,j)  = sum_k A(i,k) B(j,k)      (panel rows times inv(L_kk)^T)
 //
+// With FP16 Schur-update operands the row solve also writes each result, scaled
+// by its front's power of two, as FP16 into the half copy of the panels, and
+// stores the FP32 factor value as that FP16 value scaled back.
+//
 // The tensor cores read FP32 operands as TF32 by dropping mantissa bits. The
 // factorization therefore keeps every Schur-update operand TF32-exact: the row
 // solve (mode 1) rounds its A operand in shared memory and its result to
@@ -38,6 +42,8 @@
 // the kernel records an error in *err, stops issuing, drains its own copies,
 // frees TMEM and returns, and the host reports MFS_TIMEOUT.
 #include "device.h"
+
+#include <cuda_fp16.h>
 
 #include <cstdint>
 
@@ -190,7 +196,8 @@ __device__ __forceinline__ int find_gemm_task(const GemmTask *tasks, int ntasks,
 template <int STAGES>
 __global__ void __launch_bounds__(kUThreads, 1) gemm_tc_kernel(const GemmTask *__restrict__ tasks, int ntasks,
                                                                const float *Abase, const float *__restrict__ Bbase,
-                                                               float *Cbase, int *err) {
+                                                               float *Cbase, int *err, __half *h16,
+                                                               const int32_t *__restrict__ sexp) {
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
     __shared__ __align__(8) uint64_t bars[2 * STAGES + 1];
     __shared__ uint32_t tmem_holder;
@@ -320,12 +327,27 @@ __global__ void __launch_bounds__(kUThreads, 1) gemm_tc_kernel(const GemmTask *_
 #pragma unroll
                         for (int e = 0; e < 32; ++e)
                             if (e >= e_lo && e < e_hi) p[int64_t(e) * tk.ldc] = cv[e] - v[e];
-                    } else {
+                    } else if (!h16) {
                         // the solved rows become Schur-update operands: store them
                         // TF32-exact (rounded to nearest)
 #pragma unroll
                         for (int e = 0; e < 32; ++e)
                             if (e >= e_lo && e < e_hi) p[int64_t(e) * tk.ldc] = tf32_round(v[e]);
+                    } else {
+                        // FP16 Schur-update operands: the row scaled by the front's power of
+                        // two, rounded to FP16 (saturated) into the half copy; the factor
+                        // keeps exactly that value scaled back
+                        const int se = sexp[tk.sn];
+                        const float down = ldexpf(1.0f, -se), up = ldexpf(1.0f, se);
+                        __half *ph = h16 + tk.c_off + int64_t(jb) * tk.ldc + row;
+#pragma unroll
+                        for (int e = 0; e < 32; ++e)
+                            if (e >= e_lo && e < e_hi) {
+                                const float sv = fminf(fmaxf(v[e] * down, -65504.0f), 65504.0f);
+                                const __half hv = __float2half_rn(sv);
+                                ph[int64_t(e) * tk.ldc] = hv;
+                                p[int64_t(e) * tk.ldc] = __half2float(hv) * up;
+                            }
                     }
                 }
             }
@@ -368,12 +390,13 @@ constexpr int kTcSmem = kTcStages * kUStage + 1024;
 }  // namespace
 
 void launch_gemm_tc(const GemmTask *tasks, int ntasks, int ntiles, const float *A, const float *B, float *C, int *err,
-                    cudaStream_t st) {
+                    cudaStream_t st, void *h16, const int32_t *sexp) {
     if (ntiles <= 0) return;
     static PerDeviceOnce once;
     once([] { cudaFuncSetAttribute(gemm_tc_kernel<kTcStages>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem); });
     ++g_kernel_launches;
-    gemm_tc_kernel<kTcStages><<<ntiles, kUThreads, kTcSmem, st>>>(tasks, ntasks, A, B, C, err);
+    gemm_tc_kernel<kTcStages><<<ntiles, kUThreads, kTcSmem, st>>>(tasks, ntasks, A, B, C, err,
+                                                                    static_cast<__half *>(h16), sexp);
 }
 
 }  // namespace mfs

@@ -27,6 +27,8 @@
 // instructions.
 #include "device.h"
 
+#include <type_traits>
+
 namespace mfs {
 
 namespace {
@@ -66,9 +68,17 @@ __device__ __forceinline__ float round_operand<float>(float x) {
 // Same rule as the small-front kernel: report (plain) or perturb (refined FP32).
 // Kept out of line: it is rare, and inlined into the unrolled pivot loop it
 // stops that loop from being unrolled.
+// With an FP64 re-factor pending (sflag), a bad pivot only marks the block: the
+// FP32 pass still finishes on a floor value and the block is factored again in FP64.
 template <typename T>
-__device__ __noinline__ T panel_bad_pivot(T a, int col, PivotCtl pv) {
+__device__ __noinline__ T panel_bad_pivot(T a, int col, PivotCtl pv, int *sflag) {
     if (col < 0) return T(1);
+    if (sflag) {
+        *sflag = 1;
+        const T floor_v = T(1e-3 * fabs(pv.dorig[col]));
+        const T m = fabs(a);
+        return (m > floor_v) ? m : (floor_v > T(0) ? floor_v : T(1));
+    }
     if (pv.dorig) {
         const T floor_v = T(1e-3 * fabs(pv.dorig[col]));
         const T m = fabs(a);
@@ -133,8 +143,8 @@ __device__ __forceinline__ void tile_store(T *M, int ldm, const T (&c)[4][8], T 
 //            y[i] -= L(k + i, k) y_k (L read from shared memory, broadcast).
 template <typename T>
 __device__ __noinline__ void warp_diag_tile(T *D, T *Iv, T *rdiag, int LDD, int c0, int nb, int lane, int col_base,
-                                            int *fail_col, int *perturbed, const double *dorig) {
-    const PivotCtl pv{fail_col, perturbed, dorig};
+                                            int *fail_col, int *perturbed, const double *dorig, int *sflag) {
+    const PivotCtl pv{fail_col, perturbed, dorig, nullptr};
     T *Dt = D + c0 * LDD + c0;                       // tile element (i, j) at Dt[j * LDD + i]
     T r[32];
 #pragma unroll
@@ -142,7 +152,9 @@ __device__ __noinline__ void warp_diag_tile(T *D, T *Iv, T *rdiag, int LDD, int 
 #pragma unroll 1
     for (int k = 0; k < 32; ++k) {
         T piv = __shfl_sync(0xffffffffu, r[0], k);
-        if (!(piv > T(0))) piv = panel_bad_pivot(piv, c0 + k < nb ? col_base + c0 + k : -1, pv);
+        const int gcol = c0 + k < nb ? col_base + c0 + k : -1;
+        const bool bad = sflag ? (gcol >= 0 && !(double(piv) > kRefactorTiny * fabs(dorig[gcol]))) : !(piv > T(0));
+        if (bad) piv = panel_bad_pivot(piv, gcol, pv, sflag);
         const T rs = recip_sqrt(piv);
         const T lik = (lane == k) ? piv * rs : r[0] * rs;
         if (lane >= k) Dt[k * LDD + lane] = lik;
@@ -170,6 +182,86 @@ __device__ __noinline__ void warp_diag_tile(T *D, T *Iv, T *rdiag, int LDD, int 
     __syncwarp();
 }
 
+// FP64 re-factor of one FP32 diagonal block whose FP32 factorization met a
+// non-positive or tiny pivot (pivot <= kRefactorTiny * injected diagonal): the
+// block's stored (assembled and updated) values are factored by right-looking
+// Cholesky in FP64 and inverted in place (lower-triangular inverse, columns from
+// the last), then L, inv(L) (rounded for the tensor-core row solve when asked) and
+// the 64 x 64 diagonal inverses are written as the FP32 pass would have. A pivot
+// that stays non-positive in FP64 takes the refinement floor and is counted.
+// Shared memory: the block as doubles (ld nb + 1) and one column of scratch.
+template <typename T>
+__device__ __noinline__ void refactor_block_fp64(const PanelTask &tk, T *blk, T *inv_scratch, T *factor,
+                                                 const PivotCtl &pv, bool round_inv, unsigned char *smem) {
+    const int nb = tk.nb, ld = tk.ld, LD = nb + 1;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    double *F = reinterpret_cast<double *>(smem);          // (i, j) at F[j * LD + i]
+    double *tmp = F + nb * LD;
+    __shared__ double pivot;
+    for (int q = tid; q < nb * nb; q += nt) {
+        const int j = q / nb, i = q - j * nb;
+        F[j * LD + i] = i >= j ? double(blk[int64_t(j) * ld + i]) : 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < nb; ++k) {
+        if (tid == 0) {
+            double p = F[k * LD + k];
+            if (!(p > 0.0)) {
+                const double fl = 1e-3 * fabs(pv.dorig[tk.col + k]);
+                p = fabs(p) > fl ? fabs(p) : (fl > 0.0 ? fl : 1.0);
+                atomicAdd(pv.perturbed, 1);
+            }
+            pivot = sqrt(p);
+            F[k * LD + k] = pivot;
+        }
+        __syncthreads();
+        const double rp = 1.0 / pivot;
+        for (int i = k + 1 + tid; i < nb; i += nt) F[k * LD + i] *= rp;
+        __syncthreads();
+        const int m = nb - k - 1;
+        for (int q = tid; q < m * m; q += nt) {
+            const int j = k + 1 + q / m, i = k + 1 + q % m;
+            if (i >= j) F[j * LD + i] -= F[k * LD + i] * F[k * LD + j];
+        }
+        __syncthreads();
+    }
+    for (int q = tid; q < nb * nb; q += nt) {
+        const int j = q / nb, i = q - j * nb;
+        if (i >= j) blk[int64_t(j) * ld + i] = T(F[j * LD + i]);
+    }
+    __syncthreads();
+    // inv(L) in place: column j below the diagonal = -(1 / L_jj) inv(L_22) L(j+1:, j)
+    for (int j = nb - 1; j >= 0; --j) {
+        if (tid == 0) F[j * LD + j] = 1.0 / F[j * LD + j];
+        __syncthreads();
+        const double ajj = -F[j * LD + j];
+        for (int i = j + 1 + tid; i < nb; i += nt) {
+            double acc = 0.0;
+            for (int k = j + 1; k <= i; ++k) acc += F[k * LD + i] * F[j * LD + k];
+            tmp[i] = acc;
+        }
+        __syncthreads();
+        for (int i = j + 1 + tid; i < nb; i += nt) F[j * LD + i] = tmp[i] * ajj;
+        __syncthreads();
+    }
+    for (int q = tid; q < nb * nb; q += nt) {
+        const int j = q / nb, i = q - j * nb;
+        const T v = i >= j ? T(F[j * LD + i]) : T(0);
+        inv_scratch[tk.inv_full + int64_t(j) * tk.ldi + i] = round_inv ? round_operand(v) : v;
+    }
+    if (tk.inv_out >= 0) {
+        const int nb64 = (nb + 63) / 64;
+        T *inv = factor + tk.inv_out;
+        for (int q = tid; q < nb64 * 4096; q += nt) {
+            const int b = q >> 12, e = q & 4095;
+            const int j = e >> 6, i = e & 63;
+            const int gi = b * 64 + i, gj = b * 64 + j;
+            inv[q] = (gi < nb && gj < nb && gi >= gj) ? T(F[gj * LD + gi]) : T(0);
+        }
+    }
+    if (tid == 0) atomicAdd(pv.refactored, 1);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask *__restrict__ tasks,
                                                                  T *__restrict__ factor, T *__restrict__ inv_scratch,
@@ -185,6 +277,9 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask
     T *rdiag = P + 6 * 32 * 33;                      // reciprocal diagonal of L
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     T *blk = factor + tk.off;
+    __shared__ int refactor_flag;
+    int *sflag = (std::is_same<T, float>::value && pv.refactored && pv.dorig) ? &refactor_flag : nullptr;
+    if (tid == 0) refactor_flag = 0;
     // Load with 16-byte vectors (panel columns, the block's first row and ld are 16-byte
     // aligned), every load of a batch issued before the first shared-memory store.
     {
@@ -220,7 +315,8 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask
         }
     }
     __syncthreads();
-    if (warp == 0) warp_diag_tile(D, Iv, rdiag, LDD, 0, nb, lane, tk.col, pv.fail_col, pv.perturbed, pv.dorig);
+    if (warp == 0)
+        warp_diag_tile(D, Iv, rdiag, LDD, 0, nb, lane, tk.col, pv.fail_col, pv.perturbed, pv.dorig, sflag);
     __syncthreads();
     for (int I = 0; I < nblk; ++I) {
         const int c0 = 32 * I;
@@ -265,7 +361,8 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask
                 tile_mma(c, D + c0 * LDD + 32 * R, LDD, D + c0 * LDD + 32 * R, 1, LDD, lane);
                 tile_store(D + (32 * R) * LDD + 32 * R, LDD, c, T(-1), true, lane);
                 __syncwarp();
-                warp_diag_tile(D, Iv, rdiag, LDD, 32 * R, nb, lane, tk.col, pv.fail_col, pv.perturbed, pv.dorig);
+                warp_diag_tile(D, Iv, rdiag, LDD, 32 * R, nb, lane, tk.col, pv.fail_col, pv.perturbed, pv.dorig,
+                               sflag);
             } else {
                 for (int u = warp; u < ntrail + nterm; u += 7) {
                     T c[4][8];
@@ -291,6 +388,14 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask
             }
         }
         __syncthreads();
+    }
+    if (sflag) {
+        __syncthreads();
+        if (refactor_flag) {
+            // the block has not been written back: factor its stored values again in FP64
+            refactor_block_fp64(tk, blk, inv_scratch, factor, pv, round_inv, smem_raw);
+            return;
+        }
     }
     // L (lower triangle only: the strict upper part keeps its stored values) and inv(L)
     // (zeros above the diagonal) with 16-byte vector stores where a vector is whole

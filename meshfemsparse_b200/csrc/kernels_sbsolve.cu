@@ -1,0 +1,502 @@
+// Diagonal-block solves of the level-scheduled triangular solves (K6) through
+// explicit inverses of 256-row superblocks of L11.
+//
+// Reference: SparseLDL::Solve (forward L y = b, backward L^T x = y; called at
+// Solvers/CatamariFactorizer.cc:54,70) and its per-supernode kernels
+// (trs_kernels::SolveLowerTri, tests/test_catamari_solve_kernels.cc). The
+// dependency chain of a front's L11 solve is what bounds the solve: a block of y
+// cannot start before every earlier block is known. Here the chain runs over
+// superblocks of SB = 256 rows: after the numeric factorization,
+// sb_inverse_kernel writes inv(L_KK) of every superblock K of every front above
+// the solve cut (dense, column-major, nrp x nrp with nrp = 64 * ceil(rows / 64),
+// zeros above the diagonal), built from the 64 x 64 diagonal inverses by block
+// forward substitution. A solve task is one superblock of one front, run by one
+// CTA:
+//   forward   acc = b_K - sum_{J < K} L_KJ y_J   (waiting on superblock J's flag,
+//             L_KJ streamed in 256 x CW chunks), y_K = inv(L_KK) acc, publish;
+//   backward  acc = y_K - sum_{J > K} L_JK^T x_J (J descending),
+//             x_K = inv(L_KK)^T acc, publish.
+// The chain thus takes one flag hop, one superblock-wide product and one
+// inverse product per 256 rows. Launches are cooperative (all CTAs co-resident);
+// every CTA walks its tasks in ascending order and a task waits only on
+// lower-numbered tasks of its front, so the lowest unfinished task can always
+// proceed. Waits are bounded in time: on expiry the kernel records an error and
+// stops waiting; the host reports MFS_TIMEOUT. Sums run in a fixed order, so
+// results are run-to-run identical. With an FP32 factor (the preconditioner of
+// FP64 refinement) the chunk products are FP32 and chunk results are
+// accumulated in FP64; an FP64 factor keeps FP64 throughout.
+#include "device.h"
+
+#include <algorithm>
+#include <type_traits>
+
+namespace mfs {
+
+namespace {
+
+constexpr int SB = kSuperBlock;
+constexpr int kSbThreads = 256;
+constexpr int kRG = 8;                                    // right-hand sides per register group
+constexpr unsigned long long kWaitNs = 2000000000ull;    // 2 s per wait at most
+static_assert(SB == kSbThreads, "one thread per superblock row");
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// thread 0 waits for flag == epoch (bounded), then the whole block proceeds
+__device__ __forceinline__ void wait_flag(const int *flag, int epoch, int *err) {
+    if (threadIdx.x == 0) {
+        if (ld_acquire(flag) != epoch) {
+            const unsigned long long t0 = gtimer();
+            while (ld_acquire(flag) != epoch) {
+                if (*(volatile int *)err) break;
+                if (gtimer() - t0 > kWaitNs) {
+                    atomicExch(err, 1);
+                    break;
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ void cpa16(void *dst_smem, const void *src, int bytes) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Stage `ncols` columns of a column-major source (leading dimension lds), rows
+// [row0, row0 + ncopy) of each (ncopy a multiple of 16 bytes), into dst with
+// element (i, j) at dst[j * ldd + i]; rows at or past row0 + nvalid are zero-filled.
+template <typename T>
+__device__ __forceinline__ void stage_cols(T *dst, int ldd, const T *src, int64_t lds, int row0, int nvalid,
+                                           int ncopy, int ncols) {
+    constexpr int E = 16 / int(sizeof(T));
+    const int nch = ncopy / E;
+    const int tot = nch * ncols;
+    for (int q = threadIdx.x; q < tot; q += blockDim.x) {
+        const int j = q / nch, c = q - j * nch;
+        const int i = c * E;
+        const int nv = max(0, min(E, nvalid - i));
+        const T *s = src + int64_t(j) * lds + row0 + i;
+        cpa16(dst + j * ldd + i, nv ? s : src, nv * int(sizeof(T)));
+    }
+}
+
+// Product type of the chunk sums: FP32 for an FP32 factor, FP64 otherwise.
+template <typename T>
+using PT = std::conditional_t<sizeof(T) == 4, float, double>;
+
+template <typename T, int CW>
+struct SbLayout {
+    // doubles: acc[nrhs][SB] | out[nrhs][SB] | vec[nrhs][SB]; PT copy of vec [nrhs][SB]; ring
+    static __host__ __device__ constexpr size_t ring_off(int nrhs) {
+        return (size_t(3) * nrhs * SB * sizeof(double) + size_t(nrhs) * SB * sizeof(PT<T>) + 15) & ~size_t(15);
+    }
+    static constexpr int FWD_LD = SB;                          // forward chunk: (row i, column j) at j * SB + i
+    static constexpr int BWD_LD = CW + 16 / int(sizeof(T));    // backward chunk: (row i, column j) at j * BWD_LD + i
+    static __host__ __device__ constexpr size_t bytes(int nrhs, bool fwd) {
+        return ring_off(nrhs) + 2 * (fwd ? size_t(CW) * FWD_LD : size_t(SB) * BWD_LD) * sizeof(T);
+    }
+};
+
+// Rows of superblock K of a front with w columns, and its 64-rounded extent.
+__device__ __forceinline__ int sb_rows(int w, int K) { return min(SB, w - K * SB); }
+__device__ __forceinline__ int sb_pad(int nr) { return (nr + 63) & ~63; }
+
+template <typename T, int CW>
+__global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
+                                                               SnDev sd, const T *__restrict__ factor,
+                                                               double *__restrict__ X, int64_t ldx, int nrhs,
+                                                               int *__restrict__ flags, int *__restrict__ err) {
+    using L = SbLayout<T, CW>;
+    using P = PT<T>;
+    extern __shared__ __align__(16) double sb_smem[];
+    double *acc = sb_smem;
+    double *out = acc + nrhs * SB;
+    double *vec = out + nrhs * SB;
+    P *vp = reinterpret_cast<P *>(vec + nrhs * SB);
+    T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sb_smem) + L::ring_off(nrhs));
+    constexpr int BUF = CW * L::FWD_LD;
+    const int tid = threadIdx.x;
+    for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
+        const SbTask tk = tasks[t];
+        const int s = tk.sn, K = tk.K;
+        const int w = sd.w[s], ld = sd.ld[s], c0 = sd.col0[s];
+        const T *pan = factor + sd.pan_off[s];
+        const T *inv = factor + tk.inv;
+        const int nr = sb_rows(w, K), nrp = sb_pad(nr);
+        const int r0 = K * SB;
+        constexpr int per = SB / CW;                     // chunks per earlier superblock
+        const int ninv = (nrp + CW - 1) / CW;            // chunks of the inverse
+        const int nq = K * per + ninv;
+        auto stage = [&](int q) {
+            T *dst = ring + (q & 1) * BUF;
+            if (q < K * per) {
+                const int J = q / per, c = q - J * per;
+                stage_cols<T>(dst, L::FWD_LD, pan + int64_t(J * SB + c * CW) * ld, ld, r0, nr, nrp, CW);
+            } else {
+                const int c = q - K * per;
+                const int nc = min(CW, nrp - c * CW);
+                stage_cols<T>(dst, L::FWD_LD, inv + int64_t(c * CW) * nrp, nrp, 0, nrp, nrp, nc);
+            }
+            cpa_commit();
+        };
+        __syncthreads();                                 // the previous task is done with shared memory
+        stage(0);
+        for (int r = 0; r < nrhs; ++r) {
+            acc[r * SB + tid] = tid < nr ? X[c0 + r0 + tid + r * ldx] : 0.0;
+            out[r * SB + tid] = 0.0;
+        }
+        for (int q = 0; q < nq; ++q) {
+            if (q + 1 < nq) stage(q + 1);
+            else cpa_commit();
+            const bool lpart = q < K * per;
+            const int J = lpart ? q / per : K, c = lpart ? q - J * per : q - K * per;
+            if (lpart && c == 0) {
+                // y_J: wait for its superblock, then load it (written by another CTA: through L2)
+                wait_flag(flags + tk.flag0 + J, 1, err);
+                for (int r = 0; r < nrhs; ++r) {
+                    const double v = __ldcg(&X[c0 + J * SB + tid + r * ldx]);
+                    vec[r * SB + tid] = v;
+                    vp[r * SB + tid] = P(v);
+                }
+            } else if (!lpart && c == 0) {
+                // every earlier superblock is in: acc is the right-hand side of y_K = inv(L_KK) acc
+                __syncthreads();
+                for (int r = 0; r < nrhs; ++r) vp[r * SB + tid] = P(acc[r * SB + tid]);
+            }
+            cpa_wait<1>();
+            __syncthreads();
+            const T *tl = ring + (q & 1) * BUF;
+            if (tid < nr) {
+                const int ncol = lpart ? CW : min(CW, nrp - c * CW);
+                const int j0 = c * CW;                    // first vector entry of the chunk
+                for (int rg = 0; rg < nrhs; rg += kRG) {
+                    P p[kRG];
+#pragma unroll
+                    for (int u = 0; u < kRG; ++u) p[u] = P(0);
+#pragma unroll 8
+                    for (int j = 0; j < ncol; ++j) {
+                        const P a = P(tl[j * L::FWD_LD + tid]);
+#pragma unroll
+                        for (int u = 0; u < kRG; ++u)
+                            if (rg + u < nrhs) p[u] += a * vp[(rg + u) * SB + j0 + j];
+                    }
+#pragma unroll
+                    for (int u = 0; u < kRG; ++u)
+                        if (rg + u < nrhs) {
+                            if (lpart) acc[(rg + u) * SB + tid] -= double(p[u]);
+                            else out[(rg + u) * SB + tid] += double(p[u]);
+                        }
+                }
+            }
+            __syncthreads();                             // the ring slot is refilled at q + 2
+        }
+        cpa_wait<0>();
+        if (tid < nr)
+            for (int r = 0; r < nrhs; ++r) X[c0 + r0 + tid + r * ldx] = out[r * SB + tid];
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release(flags + tk.flag0 + K, 1);
+        }
+    }
+}
+
+template <typename T, int CW>
+__global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
+                                                               SnDev sd, const T *__restrict__ factor,
+                                                               double *__restrict__ X, int64_t ldx, int nrhs,
+                                                               int *__restrict__ flags, int *__restrict__ err) {
+    using L = SbLayout<T, CW>;
+    using P = PT<T>;
+    extern __shared__ __align__(16) double sb_smem[];
+    double *acc = sb_smem;
+    double *out = acc + nrhs * SB;
+    double *vec = out + nrhs * SB;
+    P *vp = reinterpret_cast<P *>(vec + nrhs * SB);
+    T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sb_smem) + L::ring_off(nrhs));
+    constexpr int LDB = L::BWD_LD;
+    constexpr int BUF = SB * LDB;
+    constexpr int per = SB / CW;                         // row chunks per later superblock
+    const int tid = threadIdx.x;
+    for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
+        const SbTask tk = tasks[t];
+        const int s = tk.sn, K = tk.K;
+        const int w = sd.w[s], ld = sd.ld[s], c0 = sd.col0[s];
+        const T *pan = factor + sd.pan_off[s];
+        const T *inv = factor + tk.inv;
+        const int nr = sb_rows(w, K), nrp = sb_pad(nr);
+        const int r0 = K * SB;
+        const int nsb = (w + SB - 1) / SB;
+        // chunks: for J = nsb - 1 down to K + 1 the rows of J in chunks of CW, then the
+        // inverse (rows in chunks of CW); chunk (row i, column j) at j * LDB + i
+        const int nql = (nsb - 1 - K) * per;
+        const int ninv = (nrp + CW - 1) / CW;
+        const int nq = nql + ninv;
+        auto jinfo = [&](int q, int &J, int &c, int &nrJ) {
+            const int m = q / per;
+            J = nsb - 1 - m;
+            c = q - m * per;
+            nrJ = sb_rows(w, J);
+        };
+        auto stage = [&](int q) {
+            T *dst = ring + (q & 1) * BUF;
+            if (q < nql) {
+                int J, c, nrJ;
+                jinfo(q, J, c, nrJ);
+                // rows [J SB + c CW, + CW) of columns [r0, r0 + nr) (nr = SB: K is not the last)
+                stage_cols<T>(dst, LDB, pan + int64_t(r0) * ld, ld, J * SB + c * CW, max(0, nrJ - c * CW), CW, nr);
+            } else {
+                const int c = q - nql;
+                const int nrow = min(CW, nrp - c * CW);
+                stage_cols<T>(dst, LDB, inv, nrp, c * CW, nrow, CW, nrp);
+            }
+            cpa_commit();
+        };
+        __syncthreads();
+        stage(0);
+        for (int r = 0; r < nrhs; ++r) {
+            acc[r * SB + tid] = tid < nr ? X[c0 + r0 + tid + r * ldx] : 0.0;
+            out[r * SB + tid] = 0.0;
+        }
+        for (int q = 0; q < nq; ++q) {
+            if (q + 1 < nq) stage(q + 1);
+            else cpa_commit();
+            const bool lpart = q < nql;
+            int J = K, c = q - nql, nrJ = 0;
+            if (lpart) jinfo(q, J, c, nrJ);
+            if (lpart && c == 0) {
+                wait_flag(flags + tk.flag0 + J, 2, err);
+                for (int r = 0; r < nrhs; ++r) {
+                    const double v = tid < nrJ ? __ldcg(&X[c0 + J * SB + tid + r * ldx]) : 0.0;
+                    vec[r * SB + tid] = v;
+                    vp[r * SB + tid] = P(v);
+                }
+            } else if (!lpart && c == 0) {
+                __syncthreads();
+                for (int r = 0; r < nrhs; ++r) vp[r * SB + tid] = P(acc[r * SB + tid]);
+            }
+            cpa_wait<1>();
+            __syncthreads();
+            const T *tl = ring + (q & 1) * BUF + tid * LDB;   // this thread's column
+            if (tid < nr) {
+                const int i0 = c * CW;                        // first vector entry of the chunk
+                const int nrow = lpart ? min(CW, max(0, nrJ - i0)) : min(CW, nrp - i0);
+                for (int rg = 0; rg < nrhs; rg += kRG) {
+                    P p[kRG];
+#pragma unroll
+                    for (int u = 0; u < kRG; ++u) p[u] = P(0);
+                    // rows in skewed order: the lanes of a warp read different banks
+#pragma unroll 8
+                    for (int v = 0; v < CW; ++v) {
+                        const int i = (v + tid) & (CW - 1);
+                        if (i < nrow) {
+                            const P a = P(tl[i]);
+#pragma unroll
+                            for (int u = 0; u < kRG; ++u)
+                                if (rg + u < nrhs) p[u] += a * vp[(rg + u) * SB + i0 + i];
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kRG; ++u)
+                        if (rg + u < nrhs) {
+                            if (lpart) acc[(rg + u) * SB + tid] -= double(p[u]);
+                            else out[(rg + u) * SB + tid] += double(p[u]);
+                        }
+                }
+            }
+            __syncthreads();
+        }
+        cpa_wait<0>();
+        if (tid < nr)
+            for (int r = 0; r < nrhs; ++r) X[c0 + r0 + tid + r * ldx] = out[r * SB + tid];
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release(flags + tk.flag0 + K, 2);
+        }
+    }
+}
+
+// inv(L_KK) of superblock K of front s (nr rows), nrp x nrp column-major at
+// factor + tk.inv. The 64 x 64 diagonal inverses D_b come from the panel kernel's
+// stored inverses when the front has them, else by column-wise substitution on
+// L_bb (one thread per column); then X_ab = -D_a sum_{c=b}^{a-1} L_ac X_cb.
+template <typename T>
+__global__ void __launch_bounds__(256) sb_inverse_kernel(const SbTask *__restrict__ tasks, SnDev sd, T *factor) {
+    constexpr int LD = 65;
+    constexpr int DPAR = sizeof(T) == 4 ? 4 : 2;          // diagonal blocks inverted at once
+    extern __shared__ __align__(16) double inv_smem[];
+    T *Ls = reinterpret_cast<T *>(inv_smem);              // [DPAR][64 * LD] diagonal blocks of L
+    T *Xs = Ls + DPAR * 64 * LD;                          // [DPAR][64 * LD] their inverses / a product tile
+    const SbTask tk = tasks[blockIdx.x];
+    const int s = tk.sn, K = tk.K;
+    const int w = sd.w[s], ld = sd.ld[s];
+    const T *pan = factor + sd.pan_off[s];
+    T *out = factor + tk.inv;
+    const int nr = sb_rows(w, K), nrp = sb_pad(nr), nbk = nrp / 64;
+    const int r0 = K * SB;
+    const int tid = threadIdx.x;
+    const int64_t dinv = sd.inv_off[s];
+    auto Lv = [&](int i, int j) -> T {                     // superblock-local L(i, j), 0 outside
+        return (i < nr && j < nr) ? pan[int64_t(r0 + j) * ld + r0 + i] : T(0);
+    };
+    // zero the strict upper block triangle of the output
+    for (int q = tid; q < nrp * nrp; q += blockDim.x) {
+        const int j = q / nrp, i = q - j * nrp;
+        if ((i >> 6) < (j >> 6)) out[q] = T(0);
+    }
+    // 1. diagonal inverses
+    for (int b0 = 0; b0 < nbk; b0 += DPAR) {
+        const int g = tid >> 6, j = tid & 63, b = b0 + g;
+        if (dinv >= 0) {
+            for (int q = tid; q < min(DPAR, nbk - b0) * 4096; q += blockDim.x) {
+                const int bb = b0 + (q >> 12), e = q & 4095, jj = e >> 6, ii = e & 63;
+                const T v = factor[dinv + int64_t(K * (SB / 64) + bb) * 4096 + e];
+                out[int64_t(bb * 64 + jj) * nrp + bb * 64 + ii] = (bb * 64 + ii < nr && bb * 64 + jj < nr) ? v : T(0);
+            }
+            continue;
+        }
+        __syncthreads();
+        if (g < DPAR && b < nbk)
+            for (int q = j; q < 64 * 64; q += 64) {
+                const int jj = q >> 6, ii = q & 63;
+                Ls[g * 64 * LD + jj * LD + ii] = Lv(b * 64 + ii, b * 64 + jj);
+            }
+        __syncthreads();
+        if (g < DPAR && b < nbk) {
+            const T *Lb = Ls + g * 64 * LD;
+            T *Xb = Xs + g * 64 * LD;
+            const int nb = min(64, nr - b * 64);
+            for (int k = 0; k < 64; ++k) {
+                T v = T(0);
+                if (k >= j && k < nb && j < nb) {
+                    v = k == j ? T(1) : T(0);
+                    for (int m = j; m < k; ++m) v -= Lb[m * LD + k] * Xb[j * LD + m];
+                    v /= Lb[k * LD + k];
+                }
+                Xb[j * LD + k] = v;
+            }
+            for (int k = 0; k < 64; ++k) out[int64_t(b * 64 + j) * nrp + b * 64 + k] = Xb[j * LD + k];
+        }
+    }
+    __syncthreads();
+    // 2. off-diagonal blocks, column block by column block
+    T *Ts = Xs;                                           // 64 x 64 product tile (ld LD)
+    const int i = tid & 63, jg = tid >> 6;                // row, 16-column group
+    for (int b = 0; b + 1 < nbk; ++b)
+        for (int a = b + 1; a < nbk; ++a) {
+            T acc[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) acc[u] = T(0);
+            for (int c = b; c < a; ++c)
+                for (int m = 0; m < 64; ++m) {
+                    const T l = Lv(a * 64 + i, c * 64 + m);
+#pragma unroll
+                    for (int u = 0; u < 16; ++u)
+                        acc[u] += l * __ldcg(&out[int64_t(b * 64 + jg * 16 + u) * nrp + c * 64 + m]);
+                }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < 16; ++u) Ts[(jg * 16 + u) * LD + i] = acc[u];
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < 16; ++u) acc[u] = T(0);
+            for (int m = 0; m < 64; ++m) {
+                const T dv = __ldcg(&out[int64_t(a * 64 + m) * nrp + a * 64 + i]);
+#pragma unroll
+                for (int u = 0; u < 16; ++u) acc[u] -= dv * Ts[(jg * 16 + u) * LD + m];
+            }
+#pragma unroll
+            for (int u = 0; u < 16; ++u) out[int64_t(b * 64 + jg * 16 + u) * nrp + a * 64 + i] = acc[u];
+            __syncthreads();
+        }
+}
+
+template <typename K>
+int coop_grid(K kernel, size_t smem, int ntasks) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kSbThreads, smem);
+    const int g = std::max(1, per_sm) * device_sm_count();
+    return std::min(g, std::max(1, ntasks));
+}
+
+// MAXR: the most right-hand sides this chunk width is launched with
+template <typename T, int CW, int MAXR>
+cudaError_t launch_sb_impl(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
+                           int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st) {
+    using L = SbLayout<T, CW>;
+    static_assert(SbLayout<T, CW>::bytes(MAXR, true) <= size_t(kMaxSmemOptin) &&
+                      SbLayout<T, CW>::bytes(MAXR, false) <= size_t(kMaxSmemOptin),
+                  "superblock solve shared memory");
+    void *kern = forward ? (void *)sb_fwd_kernel<T, CW> : (void *)sb_bwd_kernel<T, CW>;
+    const size_t smem = L::bytes(nrhs, forward);
+    static PerDeviceOnce once;
+    once([] {
+        cudaFuncSetAttribute(sb_fwd_kernel<T, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(L::bytes(MAXR, true)));
+        cudaFuncSetAttribute(sb_bwd_kernel<T, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(L::bytes(MAXR, false)));
+    });
+    const int grid = forward ? coop_grid(sb_fwd_kernel<T, CW>, smem, ntasks)
+                             : coop_grid(sb_bwd_kernel<T, CW>, smem, ntasks);
+    void *args[] = {(void *)&tasks, (void *)&ntasks, (void *)&sd, (void *)&factor, (void *)&X, (void *)&ldx,
+                    (void *)&nrhs, (void *)&flags, (void *)&err};
+    ++g_kernel_launches;
+    return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kSbThreads), args, smem, st);
+}
+
+}  // namespace
+
+template <typename T>
+cudaError_t launch_sb_solve(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
+                            int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st) {
+    if (ntasks <= 0) return cudaSuccess;
+    if (nrhs > kMaxSolveRhs) return cudaErrorInvalidValue;
+    // chunk width: the widest whose ring fits beside the vectors of nrhs right-hand sides
+    if constexpr (sizeof(T) == 4) {
+        if (nrhs <= 8)
+            return launch_sb_impl<T, 64, 8>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
+        return launch_sb_impl<T, 32, kMaxSolveRhs>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
+    } else {
+        if (nrhs <= 8)
+            return launch_sb_impl<T, 32, 8>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
+        return launch_sb_impl<T, 16, kMaxSolveRhs>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
+    }
+}
+
+template <typename T>
+void launch_sb_inverse(const SbTask *tasks, int ntasks, SnDev sd, T *factor, cudaStream_t st) {
+    if (ntasks <= 0) return;
+    constexpr int DPAR = sizeof(T) == 4 ? 4 : 2;
+    const size_t smem = size_t(2) * DPAR * 64 * 65 * sizeof(T);
+    static PerDeviceOnce once;
+    once([smem] { cudaFuncSetAttribute(sb_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); });
+    ++g_kernel_launches;
+    sb_inverse_kernel<T><<<ntasks, 256, smem, st>>>(tasks, sd, factor);
+}
+
+template cudaError_t launch_sb_solve<float>(bool, const SbTask *, int, SnDev, const float *, double *, int64_t, int,
+                                            int *, int *, cudaStream_t);
+template cudaError_t launch_sb_solve<double>(bool, const SbTask *, int, SnDev, const double *, double *, int64_t,
+                                             int, int *, int *, cudaStream_t);
+template void launch_sb_inverse<float>(const SbTask *, int, SnDev, float *, cudaStream_t);
+template void launch_sb_inverse<double>(const SbTask *, int, SnDev, double *, cudaStream_t);
+
+}  // namespace mfs

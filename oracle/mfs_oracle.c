@@ -453,9 +453,12 @@ i64 orc_mf_factor(i64 nsn, int vb, const i64 *sn_start, const i64 *parent, const
             if (s < g_range_lo || (g_range_hi >= 0 && s > g_range_hi)) continue;
             {
                 double fw = (double)T.w[s], fd = (double)T.d[s];
-                int big = use_blas && (fw * fw * fw / 3 + fw * fw * fd + fw * fd * fd) > kBigFront;
-                if (big != (pass == 0)) continue;
-                if (!use_blas && pass == 1) continue;
+                if (use_blas) {
+                    int big = (fw * fw * fw / 3 + fw * fw * fd + fw * fd * fd) > kBigFront;
+                    if (big != (pass == 0)) continue;
+                } else if (pass == 1) {
+                    continue;                      /* the checker: one pass in level order */
+                }
             }
             i64 w = T.w[s], d = T.d[s], f = T.f[s];
 #ifdef _OPENMP

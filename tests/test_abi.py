@@ -47,10 +47,10 @@ def test_gemm_hook_checks_accesses_before_launch():
     """The GEMM test hook validates every access against the array lengths on the
     host and refuses before touching a device (so this runs without a GPU)."""
     import numpy as np
-    t = np.array([[0, 0, 0, 128, 128, 128, 128, 128, 64, 0, 0]], dtype=np.int64)
+    t = np.array([[0, 0, 0, 128, 128, 128, 128, 128, 64, 0, 0, 0]], dtype=np.int64)
     import pytest
     with pytest.raises(ValueError):
         _lib.debug_gemm(0, _lib.MFS_PREC_FP32, 1, t, 1, 100, 1, 100, 1, 100)
-    bad_ld = np.array([[0, 0, 0, 130, 128, 128, 128, 128, 64, 0, 0]], dtype=np.int64)
+    bad_ld = np.array([[0, 0, 0, 130, 128, 128, 128, 128, 64, 0, 0, 0]], dtype=np.int64)
     with pytest.raises(ValueError):
         _lib.debug_gemm(0, _lib.MFS_PREC_FP32, 1, bad_ld, 1, 1 << 20, 1, 1 << 20, 1, 1 << 20)

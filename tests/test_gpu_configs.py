@@ -21,8 +21,8 @@ def residual(wl, X):
     return (np.linalg.norm(R, axis=0) / np.linalg.norm(wl.rhs[keep], axis=0)).max()
 
 
-def assembled(wl, single=False, refine=False):
-    f = B200Factorizer(single, refine=refine)
+def assembled(wl, single=False, refine=False, tc=0):
+    f = B200Factorizer(single, refine=refine, tensor_cores=tc)
     f.factorizeSymbolic(wl.H, wl.pins)
     f.setElements(wl.tets)
     wl.Ax = f.assemble(wl.Ke)
@@ -69,10 +69,13 @@ def test_batch_instances_are_independent():
         node0 += nn
 
 
-def test_two_material_contrast_32_rhs():
+@pytest.mark.parametrize("tc", [0, 5])
+def test_two_material_contrast_32_rhs(tc):
+    """1e3 stiffness contrast, 32 right-hand sides: FP32 + refinement with TF32 Schur
+    updates (tc 0) and with FP16 operands scaled per front (tc 5) reach 1e-10."""
     wl = workloads.config5(k=10, seed=5)
     assert wl.nrhs == 32
-    f32 = assembled(wl, single=True, refine=True)
+    f32 = assembled(wl, single=True, refine=True, tc=tc)
     X = f32.solveMultiRHS(wl.rhs)
     st = f32.stats()
     assert residual(wl, X) <= 1e-10

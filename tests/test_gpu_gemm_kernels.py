@@ -7,6 +7,9 @@ checks catamari's dense kernels against dense references. Cases cover edge tiles
 (bn = 128 when at most 128 columns are left, 256 otherwise), every 16-byte
 alignment shift of the A and B operands, the lower-triangle mask, several tasks in
 one launch, and the row solve's (mode 1) rounding of its A operand and result.
+The mode-0 cases run on both tcgen05 kernels: operands staged by cp.async
+(kernel 1) and by TMA through tensor maps (kernel 4); FP16 operands (kernel 5)
+have their own cases.
 
 Tolerances:
 * tcgen05 single-pass TF32, mode 0 (C -= A B^T on TF32-exact operands, as the
@@ -46,19 +49,22 @@ def column_block(arr, off, ld, rows, cols):
     return arr[idx]
 
 
+FIELDS = ["a_off", "b_off", "c_off", "lda", "ldb", "ldc", "m", "n", "k", "lower", "mode", "scale_exp"]
+
+
 def run_case(tasks, a_len, b_len, c_len, dtype, kernel, seed, tf32_exact=True):
-    """tasks: list of dicts with a_off b_off c_off lda ldb ldc m n k lower mode.
-    Returns (A, B, C_before, C_after) host arrays."""
+    """tasks: list of dicts with a_off b_off c_off lda ldb ldc m n k lower mode scale_exp.
+    Returns (A, B, C_before, C_after) host arrays (A and B FP16 for kernel 5)."""
     rng = np.random.default_rng(seed)
-    A = rng.uniform(-1, 1, a_len).astype(dtype)
-    B = rng.uniform(-1, 1, b_len).astype(dtype)
+    op = np.float16 if kernel == 5 else dtype
+    A = rng.uniform(-1, 1, a_len).astype(op)
+    B = rng.uniform(-1, 1, b_len).astype(op)
     C0 = rng.uniform(-1, 1, c_len).astype(dtype)
-    if dtype == np.float32 and tf32_exact:
+    if op == np.float32 and tf32_exact:
         A, B = tf32_rna(A), tf32_rna(B)
     dev = "cuda:0"
     tA, tB, tC = (torch.from_numpy(v.copy()).to(dev) for v in (A, B, C0))
-    fields = ["a_off", "b_off", "c_off", "lda", "ldb", "ldc", "m", "n", "k", "lower", "mode"]
-    tk = np.array([[t[f] for f in fields] for t in tasks], dtype=np.int64)
+    tk = np.array([[t[f] for f in FIELDS] for t in tasks], dtype=np.int64)
     prec = _lib.MFS_PREC_FP32 if dtype == np.float32 else _lib.MFS_PREC_FP64
     _lib.debug_gemm(0, prec, kernel, tk, tA.data_ptr(), a_len, tB.data_ptr(), b_len, tC.data_ptr(), c_len)
     torch.cuda.synchronize()
@@ -77,8 +83,9 @@ def expected(tasks, A, B, C0, a_round=None):
         if a_round is not None:
             Ab = a_round(Ab.astype(np.float32)).astype(np.float64)
         Bb = column_block(B, t["b_off"], t["ldb"], n, k).astype(np.float64)
-        P = Ab @ Bb.T
-        S = np.abs(Ab) @ np.abs(Bb).T
+        sc = 2.0 ** t.get("scale_exp", 0)
+        P = sc * (Ab @ Bb.T)
+        S = sc * (np.abs(Ab) @ np.abs(Bb).T)
         idx = t["c_off"] + np.arange(m)[:, None] + t["ldc"] * np.arange(n)[None, :]
         mask = np.ones((m, n), dtype=bool)
         if t["lower"]:
@@ -93,9 +100,9 @@ def expected(tasks, A, B, C0, a_round=None):
     return ref, scale, written
 
 
-def task(a_off, b_off, c_off, lda, ldb, ldc, m, n, k, lower=0, mode=0):
+def task(a_off, b_off, c_off, lda, ldb, ldc, m, n, k, lower=0, mode=0, scale_exp=0):
     return dict(a_off=a_off, b_off=b_off, c_off=c_off, lda=lda, ldb=ldb, ldc=ldc, m=m, n=n, k=k, lower=lower,
-                mode=mode)
+                mode=mode, scale_exp=scale_exp)
 
 
 def lens(tasks):
@@ -114,74 +121,80 @@ def check_mode0(tasks, A, B, C0, C, k_max):
     assert np.array_equal(C[~written], C0[~written]), "an element outside the task blocks changed"
 
 
-SHIFTS = [(0, 0), (1, 3), (2, 1), (3, 2)]
+SHIFTS = [(0, 0), (1, 3), (2, 1), (3, 2), (5, 7), (7, 4)]
+TCGEN05 = [1, 4]
 
 
+@pytest.mark.parametrize("kernel", TCGEN05)
 @pytest.mark.parametrize("da,db", SHIFTS)
 @pytest.mark.parametrize("m,n,k", [(300, 200, 77), (129, 100, 512), (37, 300, 1), (520, 129, 96)])
-def test_tcgen05_update_edges_and_shifts(m, n, k, da, db):
+def test_tcgen05_update_edges_and_shifts(m, n, k, da, db, kernel):
     """mode 0, rectangular: edge tiles in m, n and k; n + db <= 128 takes the 128-wide
     tile, wider blocks the 256-wide one; every operand shift."""
-    lda = (m + da + 3) // 4 * 4 + 8
-    ldb = (n + db + 3) // 4 * 4 + 4
+    lda = (m + da + 7) // 8 * 8 + 8
+    ldb = (n + db + 7) // 8 * 8 + 8
     ldc = m + 5
     t = [task(16 + da, 8 + db, 3, lda, ldb, ldc, m, n, k)]
     a_len, b_len, c_len = lens(t)
-    A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float32, 1, seed=m * 7 + n + k + da * 3 + db)
+    A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float32, kernel, seed=m * 7 + n + k + da * 3 + db)
     check_mode0(t, A, B, C0, C, k)
 
 
-@pytest.mark.parametrize("n,da", [(333, 0), (333, 2), (100, 1), (256, 3)])
-def test_tcgen05_syrk_lower(n, da):
+@pytest.mark.parametrize("kernel", TCGEN05)
+@pytest.mark.parametrize("n,da", [(333, 0), (333, 2), (100, 1), (256, 3), (300, 6)])
+def test_tcgen05_syrk_lower(n, da, kernel):
     """SYRK of a diagonal block (A and B the same panel rows): only the lower
     triangle is written, tiles above the diagonal exit early."""
     k = 200
-    ld = (n + da + 3) // 4 * 4
-    t = [task(4 + da, 4 + da, 0, ld, ld, n + 2, n, n, k, lower=1)]
+    ld = (n + da + 7) // 8 * 8
+    t = [task(8 + da, 8 + da, 0, ld, ld, n + 2, n, n, k, lower=1)]
     a_len, _, c_len = lens(t)
     rng = np.random.default_rng(n + da)
     A = tf32_rna(rng.uniform(-1, 1, a_len).astype(np.float32))
     C0 = rng.uniform(-1, 1, c_len).astype(np.float32)
     dev = "cuda:0"
     tA, tC = torch.from_numpy(A.copy()).to(dev), torch.from_numpy(C0.copy()).to(dev)
-    fields = ["a_off", "b_off", "c_off", "lda", "ldb", "ldc", "m", "n", "k", "lower", "mode"]
-    tk = np.array([[t[0][f] for f in fields]], dtype=np.int64)
-    _lib.debug_gemm(0, _lib.MFS_PREC_FP32, 1, tk, tA.data_ptr(), a_len, tA.data_ptr(), a_len, tC.data_ptr(), c_len)
+    tk = np.array([[t[0][f] for f in FIELDS]], dtype=np.int64)
+    _lib.debug_gemm(0, _lib.MFS_PREC_FP32, kernel, tk, tA.data_ptr(), a_len, tA.data_ptr(), a_len, tC.data_ptr(),
+                    c_len)
     C = tC.cpu().numpy()
     check_mode0(t, A, A, C0, C, k)
 
 
-@pytest.mark.parametrize("m,n,da", [(700, 300, 1), (1000, 512, 0), (257, 129, 3)])
-def test_tcgen05_trailing_update_lower(m, n, da):
+@pytest.mark.parametrize("kernel", TCGEN05)
+@pytest.mark.parametrize("m,n,da", [(700, 300, 1), (1000, 512, 0), (257, 129, 3), (500, 250, 7)])
+def test_tcgen05_trailing_update_lower(m, n, da, kernel):
     """A front's trailing update: rows below the block (m > n), lower mask, the
     operand rows start db = da rows into their 16-byte chunk."""
     k = 128
     ld = 1024 + 4
     t = [task(8 + da, 8 + da, 11, ld, ld, ld, m, n, k, lower=1)]
     a_len, b_len, c_len = lens(t)
-    A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float32, 1, seed=m + n + da)
+    A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float32, kernel, seed=m + n + da)
     check_mode0(t, A, B, C0, C, k)
 
 
-def test_tcgen05_several_tasks_one_launch():
+@pytest.mark.parametrize("kernel", TCGEN05)
+def test_tcgen05_several_tasks_one_launch(kernel):
     """Tasks of different shapes in one launch (the tile prefix and the task search)."""
     ts = [task(0, 0, 0, 512, 512, 400, 300, 250, 64),
           task(2, 1, 400 * 250, 512, 512, 200, 150, 90, 33, lower=0),
-          task(3, 3, 400 * 250 + 200 * 90, 512, 512, 520, 520, 260, 130, lower=1)]
+          task(3, 3, 400 * 250 + 200 * 90, 512, 512, 520, 520, 260, 130, lower=1),
+          task(6, 5, 400 * 250 + 200 * 90 + 520 * 260, 512, 512, 100, 77, 60, 17, lower=0)]
     a_len, b_len, c_len = lens(ts)
     a_len = max(a_len, 130 * 512 + 600)
     b_len = max(b_len, 130 * 512 + 600)
-    A, B, C0, C = run_case(ts, a_len, b_len, c_len, np.float32, 1, seed=5)
+    A, B, C0, C = run_case(ts, a_len, b_len, c_len, np.float32, kernel, seed=5)
     check_mode0(ts, A, B, C0, C, 130)
 
 
-@pytest.mark.parametrize("m,n,da", [(500, 128, 0), (333, 128, 3), (61, 72, 2), (1024, 100, 1)])
+@pytest.mark.parametrize("m,n,da", [(500, 128, 0), (333, 128, 3), (61, 72, 2), (1024, 100, 1), (400, 128, 6)])
 def test_tcgen05_row_solve_rounding(m, n, da):
     """mode 1 (the row solve X := X inv(L)^T): the FP32 A operand is rounded to TF32
     in the kernel, B (the stored inverse) is TF32-exact, the result is stored rounded
     to TF32."""
     k = n
-    lda = (m + da + 3) // 4 * 4
+    lda = (m + da + 7) // 8 * 8
     ldb = (n + 3) // 4 * 4
     t = [task(da, 0, 7, lda, ldb, m + 9, m, n, k, mode=1)]
     a_len, b_len, c_len = lens(t)
@@ -191,8 +204,7 @@ def test_tcgen05_row_solve_rounding(m, n, da):
     C0 = rng.uniform(-1, 1, c_len).astype(np.float32)
     dev = "cuda:0"
     tA, tB, tC = (torch.from_numpy(v.copy()).to(dev) for v in (A, B, C0))
-    fields = ["a_off", "b_off", "c_off", "lda", "ldb", "ldc", "m", "n", "k", "lower", "mode"]
-    tk = np.array([[t[0][f] for f in fields]], dtype=np.int64)
+    tk = np.array([[t[0][f] for f in FIELDS]], dtype=np.int64)
     _lib.debug_gemm(0, _lib.MFS_PREC_FP32, 1, tk, tA.data_ptr(), a_len, tB.data_ptr(), b_len, tC.data_ptr(), c_len)
     C = tC.cpu().numpy()
     ref, scale, written = expected(t, A, B, C0, a_round=tf32_rna)
@@ -224,3 +236,19 @@ def test_dmma_fp64(lower):
     prod = (ref - C0)[written]
     assert np.linalg.norm((C - ref)[written]) <= 1e-13 * np.linalg.norm(prod)
     assert np.array_equal(C[~written], C0[~written])
+
+
+@pytest.mark.parametrize("lower", [0, 1])
+@pytest.mark.parametrize("m,n,k,da,db,e", [(300, 200, 77, 3, 5, 0), (520, 256, 512, 7, 7, 6), (129, 100, 64, 0, 2, -9)])
+def test_tcgen05_fp16_operands(m, n, k, da, db, e, lower):
+    """kind::f16 with TMA (kernel 5): FP16 A and B, FP32 C, C -= 2^e A B^T. The product
+    of two FP16 values is exact in FP32; the error is FP32 accumulation only."""
+    if lower:
+        n = min(n, m)
+        db = da
+    lda = (m + da + 7) // 8 * 8 + 8
+    ldb = (n + db + 7) // 8 * 8
+    t = [task(8 + da, 16 + db, 5, lda, ldb, m + 3, m, n, k, lower=lower, scale_exp=e)]
+    a_len, b_len, c_len = lens(t)
+    A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float32, 5, seed=m + n + k + lower)
+    check_mode0(t, A, B, C0, C, k)

@@ -55,12 +55,12 @@ def test_factor_panels_cube(k, small):
 
 
 @pytest.mark.parametrize("small", [0, 16])
-@pytest.mark.parametrize("tc,tol", [(2, 1e-4), (1, 3e-2), (3, 3e-2)])
+@pytest.mark.parametrize("tc,tol", [(2, 1e-4), (1, 3e-2), (3, 3e-2), (4, 3e-2), (5, 3e-2)])
 def test_factor_panels_single_precision(small, tc, tol):
     """FP32 factor: split 3xTF32 Schur updates keep FP32-level error; single-pass TF32
     (tcgen05: tc=1, mma.sync: tc=3) is looser."""
     H, tets, Ke, pins, nodes = cube_problem(5)
-    f, sn, ref, got = gpu_and_oracle(H, pins, single=True, small_front_max=small, tensor_cores=tc)
+    f, sn, ref, got = gpu_and_oracle(H, pins, single=True, small_front_max=small, tensor_cores=tc, refine=tc == 5)
     assert rel_err(got, ref) <= tol
 
 
@@ -167,10 +167,11 @@ def test_fp32_refined_reaches_1e_minus_10():
     assert f.stats()["refine_iterations"] >= 1
 
 
-@pytest.mark.parametrize("tc", [0, 1])
+@pytest.mark.parametrize("tc", [0, 1, 4, 5])
 def test_bench_path_tcgen05_factor_k24(tc):
     """The benchmark's own FP32 path at k = 24 (45,000 DOFs): refined FP32 with
-    tensor_cores 0 (automatic: tcgen05 TF32 under refinement) and 1 (tcgen05 TF32).
+    tensor_cores 0 (automatic), 1 (tcgen05 TF32, cp.async operands), 4 (tcgen05
+    TF32, TMA-fed Schur updates) and 5 (tcgen05 FP16 operands scaled per front).
     * every panel entry within 3e-2 of the FP64 oracle factor, relative to its
       largest entry (single-pass TF32 Schur updates);
     * backward error of the TF32 factor ||L L^T x - A x|| / ||A x|| <= 1e-2 for a
