@@ -111,6 +111,13 @@ mfs_status mfs_last_error(const mfs_handle *h, char *buf, size_t len);
  *           Ap (nvars+1) and *nnz are produced; call again with Ai of size *nnz. */
 mfs_status mfs_build_pattern(int64_t nvars, int64_t nelem, int32_t npe, const int64_t *conn, int64_t *Ap,
                              int64_t *Ai, int64_t *nnz);
+/* Replaces: SystemAssembler<N>::blockSparsityPattern (SystemAssembler.hh:252-465),
+ *           built on the GPU: conn (nelem x npe, npe <= 32), Ap (nvars+1) and Ai are
+ *           device pointers on `device`, stream a cudaStream_t (NULL: the legacy
+ *           stream); *nnz is host memory. Same two-phase protocol and the same
+ *           result, entry for entry, as mfs_build_pattern. Synchronizes the stream. */
+mfs_status mfs_build_pattern_device(int32_t device, int64_t nvars, int64_t nelem, int32_t npe,
+                                    const int64_t *conn, int64_t *Ap, int64_t *Ai, int64_t *nnz, void *stream);
 
 /* Replaces: CatamariFactorizer::factorizeSymbolic(const BlockCSCHessianBase&, pinnedVars)
  *           (Solvers/CatamariFactorizer.cc:136-161, 177-616).
@@ -213,6 +220,11 @@ mfs_status mfs_supernodes(const mfs_handle *h, int64_t *nsn, int64_t *nstruct, i
  * entries (4 int64 each, see above). Sizes first with NULL outputs. */
 mfs_status mfs_conversion_plan(const mfs_handle *h, int64_t *nv, int64_t *nentries, int64_t *column_offsets,
                                int64_t *entries);
+/* The same conversion plan as built on the GPU for the numeric factorization
+ * (CatamariConversionPlan.hh:402-541, catamari layout), copied to host memory in
+ * the format of mfs_conversion_plan; equal to it entry for entry. */
+mfs_status mfs_conversion_plan_device(const mfs_handle *h, int64_t *nv, int64_t *nentries, int64_t *column_offsets,
+                                      int64_t *entries);
 /* Copies the factor values (factor_size entries as double) to host memory. */
 mfs_status mfs_factor_values(const mfs_handle *h, int64_t *factor_size, double *out);
 

@@ -27,7 +27,7 @@ EXPORTED = [
     "mfs_stash", "mfs_swap_stash", "mfs_clear_stash", "mfs_has_stash", "mfs_clear_factors", "mfs_get_stats",
     "mfs_set_options", "mfs_apply_noalloc", "mfs_lpc_param_count", "mfs_lpc_create", "mfs_lpc_destroy",
     "mfs_lpc_get_weights", "mfs_lpc_set_weights", "mfs_lpc_loss_grad", "mfs_lpc_train_step", "mfs_pcg_solve",
-    "mfs_debug_gemm",
+    "mfs_debug_gemm", "mfs_build_pattern_device", "mfs_conversion_plan_device",
 ]
 GEMM_TASK_FIELDS = 12
 
@@ -86,6 +86,8 @@ def load() -> C.CDLL:
     lib.mfs_nd_ordering.argtypes = [P, i64p, i64p, i64p, i64p]
     lib.mfs_supernodes.argtypes = [P, i64p, i64p, C.POINTER(C.c_int32), i64p, i64p, i64p, i64p, i64p]
     lib.mfs_conversion_plan.argtypes = [P, i64p, i64p, i64p, i64p]
+    lib.mfs_conversion_plan_device.argtypes = [P, i64p, i64p, i64p, i64p]
+    lib.mfs_build_pattern_device.argtypes = [C.c_int32, C.c_int64, C.c_int64, C.c_int32, P, P, P, i64p, P]
     lib.mfs_factor_values.argtypes = [P, i64p, P]
     for name in ("mfs_stash", "mfs_swap_stash", "mfs_clear_stash", "mfs_clear_factors"):
         getattr(lib, name).argtypes = [P]
@@ -180,6 +182,18 @@ def debug_gemm(device: int, precision: int, kernel: int, tasks: np.ndarray, A: i
         if st == MFS_INVALID_ARG:
             raise ValueError(msg)
         raise MFSError(st, msg)
+
+
+def build_pattern_device(nvars: int, conn_ptr: int, nelem: int, npe: int, Ap_ptr: int, Ai_ptr: int | None,
+                         device: int = 0, stream: int | None = None) -> int:
+    """SystemAssembler::blockSparsityPattern on the GPU (device pointers by address);
+    returns nnz (fills Ai when given)."""
+    nnz = C.c_int64(0)
+    st = load().mfs_build_pattern_device(device, nvars, nelem, npe, C.c_void_p(conn_ptr), C.c_void_p(Ap_ptr),
+                                         C.c_void_p(Ai_ptr) if Ai_ptr else None, C.byref(nnz),
+                                         C.c_void_p(stream) if stream else None)
+    check(st, what="GPU pattern")
+    return nnz.value
 
 
 def library_present() -> bool:

@@ -102,23 +102,10 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         for (idx k = 0; k < S.w[s]; ++k) diag[S.vb * S.sn_start[s] + k] = dpan[s] + k * dld[s] + k;
     ds->diag_off.upload(diag, st);
     {
-        // plan destinations move from the catamari layout to the padded device layout
-        std::vector<PlanEntryDev> pl(S.plan.size());
-        for (size_t k = 0; k < pl.size(); ++k) {
-            const idx dst = S.plan[k].dst;
-            const idx s = idx(std::upper_bound(S.pan_off.begin(), S.pan_off.begin() + nsn + 1, dst) -
-                              S.pan_off.begin()) - 1;
-            const idx rel = dst - S.pan_off[s];
-            pl[k].dst = dpan[s] + (rel / S.f[s]) * dld[s] + rel % S.f[s];
-            pl[k].src = S.plan[k].src;
-            pl[k].ld = dld[s];
-            pl[k].flags = S.plan[k].flags;
-        }
-        ds->plan.ensure(pl.size());
-        if (!pl.empty())
-            MFS_CUDA(cudaMemcpyAsync(ds->plan.p, pl.data(), pl.size() * sizeof(PlanEntryDev),
-                                     cudaMemcpyHostToDevice, st));
-        MFS_CUDA(cudaStreamSynchronize(st));
+        // the block conversion plan, built on the GPU from the reduced pattern, the
+        // ordering and the supernodes, in the padded device layout (and the catamari
+        // layout, exported by mfs_conversion_plan_device)
+        gpu_build_plan(S, dpan, dld, ds->plan, ds->plan_cat, ds->plan_ptr_dev, st);
     }
     ds->spmv_ptr.upload(S.spmv_ptr, st);
     ds->spmv_src.upload(S.spmv_src, st);
@@ -1053,6 +1040,15 @@ mfs_status mfs_build_pattern(int64_t nvars, int64_t nelem, int32_t npe, const in
     }
 }
 
+mfs_status mfs_build_pattern_device(int32_t device, int64_t nvars, int64_t nelem, int32_t npe,
+                                    const int64_t *conn, int64_t *Ap, int64_t *Ai, int64_t *nnz, void *stream) {
+    if (nvars < 0 || nelem < 0 || npe <= 0 || !Ap || !nnz || (nelem > 0 && !conn)) return MFS_INVALID_ARG;
+    return guarded(nullptr, [&] {
+        MFS_CUDA(cudaSetDevice(device));
+        *nnz = gpu_build_pattern(nvars, nelem, npe, conn, Ap, Ai, static_cast<cudaStream_t>(stream));
+    });
+}
+
 mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, const int64_t *Ai, int32_t block_size,
                         const int64_t *pinned, int64_t n_pinned, const int64_t *user_perm,
                         const int64_t *supernode_sizes, int64_t num_supernodes) {
@@ -1294,56 +1290,27 @@ mfs_status mfs_assembly_setup(mfs_handle *h, int64_t nelem, const int64_t *conn)
         if (nelem < 0 || (nelem > 0 && !conn)) throw StatusError(MFS_INVALID_ARG, "bad connectivity");
         const int64_t nb = int64_t(ds.Ap_full.size()) - 1;
         const int64_t nslots = ds.Ap_full[nb];
-        // Per element, in the reference's order (SystemAssembler.hh:60-98): columns by
-        // sorted global index; an upper block (bi, bj) takes He(i_loc, j_loc) when the
-        // local order agrees with the global one, else the transpose of He(j_loc, i_loc);
-        // the diagonal block adds its upper triangle only.
-        std::vector<int64_t> cnt(nslots + 1, 0);
-        auto find_slot = [&](int64_t bi, int64_t bj) -> int64_t {
-            const int64_t *b = ds.Ai_full.data() + ds.Ap_full[bj];
-            const int64_t *e = ds.Ai_full.data() + ds.Ap_full[bj + 1];
-            const int64_t *it = std::lower_bound(b, e, bi);
-            if (it == e || *it != bi) throw StatusError(MFS_INVALID_ARG, "element block not in the pattern");
-            return it - ds.Ai_full.data();
-        };
-        std::vector<int64_t> slots(size_t(nelem) * 10), codes(size_t(nelem) * 10);
-        for (int64_t e = 0; e < nelem; ++e) {
-            const int64_t *v = conn + 4 * e;
-            int order[4] = {0, 1, 2, 3};
-            for (int k = 0; k < 4; ++k) {
-                if (v[k] < 0 || v[k] >= nb) throw StatusError(MFS_INVALID_ARG, "element node out of range");
+        {
+            // the element -> slot map, built on the GPU. Per element, in the reference's
+            // order (SystemAssembler.hh:60-98): columns by sorted global index; an upper
+            // block (bi, bj) takes He(i_loc, j_loc) when the local order agrees with the
+            // global one, else the transpose of He(j_loc, i_loc); the diagonal block adds
+            // its upper triangle only; each slot sums its contributions in element order.
+            cudaStream_t st = h->stream;
+            if (!ds.Ap_full_dev.p || ds.Ap_full_dev.n < ds.Ap_full.size()) {
+                ds.Ap_full_dev.upload(ds.Ap_full, st);
+                ds.Ai_full_dev.upload(ds.Ai_full, st);
             }
-            std::stable_sort(order, order + 4, [&](int a, int b) { return v[a] < v[b]; });
-            int q = 0;
-            for (int jj = 0; jj < 4; ++jj) {
-                const int lj = order[jj];
-                const int64_t bj = v[lj];
-                for (int ii = 0; ii < jj; ++ii) {
-                    const int li = order[ii];
-                    const int64_t bi = v[li];
-                    const int64_t slot = find_slot(bi, bj);
-                    int64_t code;
-                    if (li < lj) code = ((e * 144 + (3 * li) * 12 + 3 * lj) << 2) | 0;
-                    else code = ((e * 144 + (3 * lj) * 12 + 3 * li) << 2) | 1;
-                    slots[e * 10 + q] = slot;
-                    codes[e * 10 + q] = code;
-                    ++q;
-                }
-                const int64_t slot = find_slot(bj, bj);
-                slots[e * 10 + q] = slot;
-                codes[e * 10 + q] = ((e * 144 + (3 * lj) * 12 + 3 * lj) << 2) | 2;
-                ++q;
+            DBuf<int64_t> cd;
+            if (nelem > 0) {
+                cd.ensure(size_t(nelem) * 4);
+                MFS_CUDA(cudaMemcpyAsync(cd.p, conn, size_t(nelem) * 4 * sizeof(int64_t), cudaMemcpyHostToDevice, st));
             }
+            gpu_build_slot_map(nelem, cd.p, nb, ds.Ap_full_dev.p, ds.Ai_full_dev.p, nslots, h->slot_ptr, h->contrib,
+                               st);
+            h->nslots = nslots;
+            h->nelem = nelem;
         }
-        for (size_t k = 0; k < slots.size(); ++k) cnt[slots[k] + 1]++;
-        for (int64_t s = 0; s < nslots; ++s) cnt[s + 1] += cnt[s];
-        std::vector<int64_t> contrib(slots.size());
-        std::vector<int64_t> back(cnt.begin(), cnt.end() - 1);
-        for (size_t k = 0; k < slots.size(); ++k) contrib[back[slots[k]]++] = codes[k];
-        h->slot_ptr.upload(cnt, h->stream);
-        h->contrib.upload(contrib, h->stream);
-        h->nslots = nslots;
-        h->nelem = nelem;
     });
 }
 
@@ -1450,6 +1417,34 @@ mfs_status mfs_conversion_plan(const mfs_handle *h, int64_t *nv, int64_t *nentri
             entries[4 * k + 2] = S.plan[k].ld;
             entries[4 * k + 3] = S.plan[k].flags;
         }
+    return MFS_OK;
+}
+
+mfs_status mfs_conversion_plan_device(const mfs_handle *h, int64_t *nv, int64_t *nentries, int64_t *column_offsets,
+                                      int64_t *entries) {
+    if (!h || !nv || !nentries) return MFS_INVALID_ARG;
+    if (!h->cur.sym || h->cur.type < 1) return MFS_NO_FACTOR;
+    if (h->opt.device < 0) return MFS_INVALID_ARG;
+    const DevSym &ds = *h->cur.sym;
+    const Symbolic &S = *ds.S;
+    *nv = S.nv;
+    *nentries = int64_t(S.plan.size());
+    if (cudaSetDevice(h->opt.device) != cudaSuccess) return MFS_CUDA_ERROR;
+    if (column_offsets && cudaMemcpy(column_offsets, ds.plan_ptr_dev.p, size_t(2 * S.nv + 1) * sizeof(int64_t),
+                                     cudaMemcpyDeviceToHost) != cudaSuccess)
+        return MFS_CUDA_ERROR;
+    if (entries && !S.plan.empty()) {
+        std::vector<PlanEntryDev> pe(S.plan.size());
+        if (cudaMemcpy(pe.data(), ds.plan_cat.p, pe.size() * sizeof(PlanEntryDev), cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+            return MFS_CUDA_ERROR;
+        for (size_t k = 0; k < pe.size(); ++k) {
+            entries[4 * k] = pe[k].dst;
+            entries[4 * k + 1] = pe[k].src;
+            entries[4 * k + 2] = pe[k].ld;
+            entries[4 * k + 3] = pe[k].flags;
+        }
+    }
     return MFS_OK;
 }
 

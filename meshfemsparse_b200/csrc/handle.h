@@ -98,6 +98,8 @@ struct DevSym {
     DBuf<int64_t> pan_off, upd_off, sol_off, struct_ptr, diag_off;
     DBuf<int64_t> inv_off;               // 64 x 64 diagonal inverses of large fronts (-1: none)
     DBuf<PlanEntryDev> plan;
+    DBuf<PlanEntryDev> plan_cat;         // the same plan in the catamari layout (built on the GPU)
+    DBuf<int64_t> plan_ptr_dev;          // its bucket offsets
     DBuf<AssembleTask> asm_tasks;
     DBuf<PanelTask> potrf_tasks;
     DBuf<GemmTask> gemm_tasks;
@@ -118,6 +120,7 @@ struct DevSym {
     SnDev sd{};
     int64_t ax_len = 0;
     std::vector<int64_t> Ap_full, Ai_full;   // caller's pattern (for the element slot map)
+    DBuf<int64_t> Ap_full_dev, Ai_full_dev;  // the same on the device
     int num_large = 0;
     int64_t inv_scratch = 0;             // elements of the block inverses of one column-block step
     int64_t factor_alloc = 0;            // panels followed by the diagonal inverses
@@ -208,6 +211,23 @@ struct mfs_handle {
     size_t gemm_events_used = 0;
     double gemm_flops_timed = 0.0;
 };
+
+namespace mfs {
+// GPU construction of the pattern-dependent structures (kernels_pattern.cu).
+// Block pattern from element stencils (device connectivity, npe <= 32): fills Ap
+// (device, nvars + 1) and, when Ai is non-null, Ai (device); returns nnz.
+int64_t gpu_build_pattern(int64_t nvars, int64_t nelem, int npe, const int64_t *conn, int64_t *Ap, int64_t *Ai,
+                          cudaStream_t st);
+// Element -> slot map of the assembly (device connectivity of 4-node elements and
+// device full pattern): slot_ptr (nslots + 1) and contrib, as the host map.
+void gpu_build_slot_map(int64_t nelem, const int64_t *conn, int64_t nb, const int64_t *Ap, const int64_t *Ai,
+                        int64_t nslots, DBuf<int64_t> &slot_ptr, DBuf<int64_t> &contrib, cudaStream_t st);
+// Block conversion plan of the analysis, in the device panel layout (plan_dev) and
+// in the catamari layout (plan_cat), with its bucket offsets (2 nv + 1).
+void gpu_build_plan(const Symbolic &S, const std::vector<int64_t> &dpan, const std::vector<int32_t> &dld,
+                    DBuf<PlanEntryDev> &plan_dev, DBuf<PlanEntryDev> &plan_cat, DBuf<int64_t> &plan_ptr,
+                    cudaStream_t st);
+}  // namespace mfs
 
 inline void set_device(mfs_handle *h) {
     if (h->opt.device < 0) throw StatusError(MFS_INVALID_ARG, "analysis-only handle (device -1) has no GPU state");

@@ -391,12 +391,15 @@ class B200Factorizer:
         out["vb"] = int(vb.value)
         return out
 
-    def conversionPlan(self) -> dict:
+    def conversionPlan(self, device_built: bool = False) -> dict:
+        """The block conversion plan (CatamariConversionPlan.hh:402-541); device_built:
+        the copy built on the GPU for the numeric factorization."""
+        fn = self._lib.mfs_conversion_plan_device if device_built else self._lib.mfs_conversion_plan
         nv, ne = C.c_int64(), C.c_int64()
-        _lib.check(self._lib.mfs_conversion_plan(self._h, C.byref(nv), C.byref(ne), None, None), self._h)
+        _lib.check(fn(self._h, C.byref(nv), C.byref(ne), None, None), self._h)
         offs = np.zeros(2 * nv.value + 1, dtype=np.int64)
         ent = np.zeros(4 * ne.value, dtype=np.int64)
-        self._lib.mfs_conversion_plan(self._h, C.byref(nv), C.byref(ne), _lib.i64ptr(offs), _lib.i64ptr(ent))
+        _lib.check(fn(self._h, C.byref(nv), C.byref(ne), _lib.i64ptr(offs), _lib.i64ptr(ent)), self._h)
         return {"columnOffsets": offs, "entries": ent.reshape(-1, 4)}
 
     def factorValues(self) -> np.ndarray:
