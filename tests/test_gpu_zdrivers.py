@@ -69,3 +69,68 @@ def test_cli_on_gpu(tmp_path):
                           str(tmp_path / "rhs.txt")], capture_output=True, text=True, cwd=ROOT, check=True)
     u = np.array([float(v) for v in out.stdout.split()])
     assert np.linalg.norm(K @ u - b) <= 1e-12 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("single", [False, True])
+@pytest.mark.parametrize("rank", [0, 2])
+def test_bordered_solve_through_gpu_factorizer(single, rank):
+    """BorderedSparseHessian (BorderedSparseHessian.hh:56-75): the sparse block factored
+    and solved on the GPU (one multi-RHS solve for the border columns), against the
+    dense solve of the whole system; FP32 + refinement as well as FP64."""
+    from meshfemsparse_b200 import B200Factorizer
+    from meshfemsparse_b200.bordered import BorderedSparseFactorization, BorderedSparseHessian
+    from helpers import random_stencil_hessian
+    rng = np.random.default_rng(7 + rank)
+    Hs = random_stencil_hessian(5)
+    ns, nd = Hs.n, 3
+    H = BorderedSparseHessian(Hs, rng.normal(size=(ns, nd)) * 0.3, np.diag(rng.uniform(1, 2, nd)) * 50.0)
+    if rank:
+        H.addLowRank(rng.normal(size=(ns + nd, rank)), 0.5)
+    M = np.zeros((ns + nd, ns + nd))
+    M[:ns, :ns] = H.H_ss.to_scipy_full().toarray()
+    M[:ns, ns:] = H.H_sd
+    M[ns:, :ns] = H.H_sd.T
+    M[ns:, ns:] = H.H_dd
+    V = np.vstack([H.V_s, H.V_d])
+    M = M + V @ V.T
+    pins = np.array([0, 1, 2])
+    F = BorderedSparseFactorization(H, B200Factorizer(single, refine=single), pins)
+    x = rng.normal(size=ns + nd)
+    b = M @ x
+    keep = np.ones(ns + nd, dtype=bool)
+    keep[pins] = False
+    xr = np.zeros_like(x)
+    xr[keep] = np.linalg.solve(M[np.ix_(keep, keep)], b[keep])
+    got = F.solve(b)
+    assert np.linalg.norm(got - xr) <= 1e-9 * np.linalg.norm(xr)
+    assert np.all(got[pins] == 0.0)
+
+
+def test_bordered_equality_constraints_through_gpu_factorizer():
+    """Equality constraints through Lagrange multipliers over the GPU factorization,
+    against the dense KKT solve."""
+    from meshfemsparse_b200 import B200Factorizer
+    from meshfemsparse_b200.bordered import BorderedSparseFactorization, BorderedSparseHessian
+    from helpers import random_stencil_hessian
+    rng = np.random.default_rng(11)
+    Hs = random_stencil_hessian(8)
+    ns, nd, m = Hs.n, 2, 3
+    H = BorderedSparseHessian(Hs, rng.normal(size=(ns, nd)) * 0.3, np.diag(rng.uniform(1, 2, nd)) * 50.0)
+    H.addLowRank(rng.normal(size=(ns + nd, 1)), 0.5)
+    C = rng.normal(size=(m, ns + nd))
+    H.setConstraints(C)
+    F = BorderedSparseFactorization(H, B200Factorizer(), [])
+    b = rng.normal(size=ns + nd)
+    r = rng.normal(size=m)
+    x, lam = F.solve(b, r, return_multipliers=True)
+    M = np.zeros((ns + nd, ns + nd))
+    M[:ns, :ns] = H.H_ss.to_scipy_full().toarray()
+    M[:ns, ns:] = H.H_sd
+    M[ns:, :ns] = H.H_sd.T
+    M[ns:, ns:] = H.H_dd
+    V = np.vstack([H.V_s, H.V_d])
+    M = M + V @ V.T
+    K = np.block([[M, C.T], [C, np.zeros((m, m))]])
+    ref = np.linalg.solve(K, np.concatenate([b, r]))
+    assert np.linalg.norm(x - ref[:ns + nd]) <= 1e-9 * np.linalg.norm(ref[:ns + nd])
+    assert np.linalg.norm(lam - ref[ns + nd:]) <= 1e-8 * np.linalg.norm(ref[ns + nd:])
