@@ -455,8 +455,14 @@ void launch_panel(const PanelTask *tasks, int ntasks, int max_nb, T *factor, T *
                   bool round_inv, cudaStream_t st) {
     if (ntasks <= 0) return;
     const size_t smem = panel_smem_bytes(max_nb, sizeof(T) == 8);
+    // the opt-in limit counts static shared memory too
     static PerDeviceOnce once;
-    once([] { cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemOptin); });
+    once([] {
+        cudaFuncAttributes fa{};
+        cudaFuncGetAttributes(&fa, panel_kernel<T>);
+        cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kMaxSmemOptin - int(fa.sharedSizeBytes));
+    });
     ++g_kernel_launches;
     panel_kernel<T><<<ntasks, kPanelThreads, smem, st>>>(tasks, factor, inv_scratch, pv, round_inv);
 }

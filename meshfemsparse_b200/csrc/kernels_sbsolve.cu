@@ -23,8 +23,9 @@
 // proceed. Waits are bounded in time: on expiry the kernel records an error and
 // stops waiting; the host reports MFS_TIMEOUT. Sums run in a fixed order, so
 // results are run-to-run identical. With an FP32 factor (the preconditioner of
-// FP64 refinement) the chunk products are FP32 and chunk results are
-// accumulated in FP64; an FP64 factor keeps FP64 throughout.
+// FP64 refinement) the products with off-diagonal superblocks are FP32 (chunk
+// results accumulated in FP64) and the inverse of the diagonal superblock is
+// applied in FP64; an FP64 factor keeps FP64 throughout.
 #include "device.h"
 
 #include <algorithm>
@@ -118,6 +119,58 @@ struct SbLayout {
 __device__ __forceinline__ int sb_rows(int w, int K) { return min(SB, w - K * SB); }
 __device__ __forceinline__ int sb_pad(int nr) { return (nr + 63) & ~63; }
 
+// Forward chunk product for this thread's row: dst[r * SB] -/+= sum_j tl[j * ldt + tid] v[r * SB + j]
+// (j < ncol), accumulated in Q.
+template <typename Q, typename T>
+__device__ __forceinline__ void fwd_chunk(const T *tl, int ldt, const Q *v, int ncol, int nrhs, double *dst,
+                                          bool sub) {
+    for (int rg = 0; rg < nrhs; rg += kRG) {
+        Q p[kRG];
+#pragma unroll
+        for (int u = 0; u < kRG; ++u) p[u] = Q(0);
+#pragma unroll 8
+        for (int j = 0; j < ncol; ++j) {
+            const Q a = Q(tl[j * ldt + threadIdx.x]);
+#pragma unroll
+            for (int u = 0; u < kRG; ++u)
+                if (rg + u < nrhs) p[u] += a * v[(rg + u) * SB + j];
+        }
+#pragma unroll
+        for (int u = 0; u < kRG; ++u)
+            if (rg + u < nrhs) {
+                if (sub) dst[(rg + u) * SB] -= double(p[u]);
+                else dst[(rg + u) * SB] += double(p[u]);
+            }
+    }
+}
+// Backward chunk product for this thread's column tc (CW rows, rows >= nrow skipped, in
+// skewed order so the lanes of a warp read different banks):
+// dst[r * SB] -/+= sum_i tc[i] v[r * SB + i], accumulated in Q.
+template <typename Q, typename T, int CW>
+__device__ __forceinline__ void bwd_chunk(const T *tc, const Q *v, int nrow, int nrhs, double *dst, bool sub) {
+    for (int rg = 0; rg < nrhs; rg += kRG) {
+        Q p[kRG];
+#pragma unroll
+        for (int u = 0; u < kRG; ++u) p[u] = Q(0);
+#pragma unroll 8
+        for (int w = 0; w < CW; ++w) {
+            const int i = (w + threadIdx.x) & (CW - 1);
+            if (i < nrow) {
+                const Q a = Q(tc[i]);
+#pragma unroll
+                for (int u = 0; u < kRG; ++u)
+                    if (rg + u < nrhs) p[u] += a * v[(rg + u) * SB + i];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kRG; ++u)
+            if (rg + u < nrhs) {
+                if (sub) dst[(rg + u) * SB] -= double(p[u]);
+                else dst[(rg + u) * SB] += double(p[u]);
+            }
+    }
+}
+
 template <typename T, int CW>
 __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
                                                                SnDev sd, const T *__restrict__ factor,
@@ -175,35 +228,16 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__r
                     vec[r * SB + tid] = v;
                     vp[r * SB + tid] = P(v);
                 }
-            } else if (!lpart && c == 0) {
-                // every earlier superblock is in: acc is the right-hand side of y_K = inv(L_KK) acc
-                __syncthreads();
-                for (int r = 0; r < nrhs; ++r) vp[r * SB + tid] = P(acc[r * SB + tid]);
             }
             cpa_wait<1>();
-            __syncthreads();
+            __syncthreads();                             // (also: acc is complete before the inverse)
             const T *tl = ring + (q & 1) * BUF;
             if (tid < nr) {
-                const int ncol = lpart ? CW : min(CW, nrp - c * CW);
                 const int j0 = c * CW;                    // first vector entry of the chunk
-                for (int rg = 0; rg < nrhs; rg += kRG) {
-                    P p[kRG];
-#pragma unroll
-                    for (int u = 0; u < kRG; ++u) p[u] = P(0);
-#pragma unroll 8
-                    for (int j = 0; j < ncol; ++j) {
-                        const P a = P(tl[j * L::FWD_LD + tid]);
-#pragma unroll
-                        for (int u = 0; u < kRG; ++u)
-                            if (rg + u < nrhs) p[u] += a * vp[(rg + u) * SB + j0 + j];
-                    }
-#pragma unroll
-                    for (int u = 0; u < kRG; ++u)
-                        if (rg + u < nrhs) {
-                            if (lpart) acc[(rg + u) * SB + tid] -= double(p[u]);
-                            else out[(rg + u) * SB + tid] += double(p[u]);
-                        }
-                }
+                // off-diagonal superblocks: products of the chunk's precision (FP32 for an
+                // FP32 factor); the inverse of the diagonal superblock: FP64 products
+                if (lpart) fwd_chunk<P>(tl, L::FWD_LD, vp + j0, CW, nrhs, acc + tid, true);
+                else fwd_chunk<double>(tl, L::FWD_LD, acc + j0, min(CW, nrp - j0), nrhs, out + tid, false);
             }
             __syncthreads();                             // the ring slot is refilled at q + 2
         }
@@ -288,38 +322,14 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__r
                     vec[r * SB + tid] = v;
                     vp[r * SB + tid] = P(v);
                 }
-            } else if (!lpart && c == 0) {
-                __syncthreads();
-                for (int r = 0; r < nrhs; ++r) vp[r * SB + tid] = P(acc[r * SB + tid]);
             }
             cpa_wait<1>();
-            __syncthreads();
+            __syncthreads();                             // (also: acc is complete before the inverse)
             const T *tl = ring + (q & 1) * BUF + tid * LDB;   // this thread's column
             if (tid < nr) {
                 const int i0 = c * CW;                        // first vector entry of the chunk
-                const int nrow = lpart ? min(CW, max(0, nrJ - i0)) : min(CW, nrp - i0);
-                for (int rg = 0; rg < nrhs; rg += kRG) {
-                    P p[kRG];
-#pragma unroll
-                    for (int u = 0; u < kRG; ++u) p[u] = P(0);
-                    // rows in skewed order: the lanes of a warp read different banks
-#pragma unroll 8
-                    for (int v = 0; v < CW; ++v) {
-                        const int i = (v + tid) & (CW - 1);
-                        if (i < nrow) {
-                            const P a = P(tl[i]);
-#pragma unroll
-                            for (int u = 0; u < kRG; ++u)
-                                if (rg + u < nrhs) p[u] += a * vp[(rg + u) * SB + i0 + i];
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < kRG; ++u)
-                        if (rg + u < nrhs) {
-                            if (lpart) acc[(rg + u) * SB + tid] -= double(p[u]);
-                            else out[(rg + u) * SB + tid] += double(p[u]);
-                        }
-                }
+                if (lpart) bwd_chunk<P, T, CW>(tl, vp + i0, min(CW, max(0, nrJ - i0)), nrhs, acc + tid, true);
+                else bwd_chunk<double, T, CW>(tl, acc + i0, min(CW, nrp - i0), nrhs, out + tid, false);
             }
             __syncthreads();
         }

@@ -177,13 +177,11 @@ def test_tcgen05_trailing_update_lower(m, n, da, kernel):
 @pytest.mark.parametrize("kernel", TCGEN05)
 def test_tcgen05_several_tasks_one_launch(kernel):
     """Tasks of different shapes in one launch (the tile prefix and the task search)."""
-    ts = [task(0, 0, 0, 512, 512, 400, 300, 250, 64),
-          task(2, 1, 400 * 250, 512, 512, 200, 150, 90, 33, lower=0),
-          task(3, 3, 400 * 250 + 200 * 90, 512, 512, 520, 520, 260, 130, lower=1),
-          task(6, 5, 400 * 250 + 200 * 90 + 520 * 260, 512, 512, 100, 77, 60, 17, lower=0)]
+    ts = [task(0, 0, 0, 528, 528, 400, 300, 250, 64),
+          task(2, 1, 400 * 250, 528, 528, 200, 150, 90, 33, lower=0),
+          task(3, 3, 400 * 250 + 200 * 90, 528, 528, 520, 520, 260, 130, lower=1),
+          task(6, 5, 400 * 250 + 200 * 90 + 520 * 260, 528, 528, 100, 77, 60, 17, lower=0)]
     a_len, b_len, c_len = lens(ts)
-    a_len = max(a_len, 130 * 512 + 600)
-    b_len = max(b_len, 130 * 512 + 600)
     A, B, C0, C = run_case(ts, a_len, b_len, c_len, np.float32, kernel, seed=5)
     check_mode0(ts, A, B, C0, C, 130)
 
