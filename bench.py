@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--tc", type=int, default=0, help="FP32 Schur updates: 0 auto, 1 TF32, 2 split 3xTF32")
     p.add_argument("--maxit", type=int, default=50, help="refinement iteration cap")
+    p.add_argument("--chain", type=int, default=0, help="diagonal solves: 0 superblock inverses, 1 block-pair chains")
     p.add_argument("--cpu-seconds", type=float, default=150.0,
                    help="reference arm: stop timing complete CPU steps once this much is spent")
     p.add_argument("--train-hessians", type=int, default=10, help="config 4: Hessians of the training set")
@@ -156,7 +157,7 @@ def run_b200(args, rank, world, local, dist):
 
     def make(single):
         f = B200Factorizer(single, refine=single, stream=stream.cuda_stream, device=local, tensor_cores=args.tc,
-                           refine_maxit=args.maxit)
+                           refine_maxit=args.maxit, solve_chain=args.chain)
         t = time.time()
         f.factorizeSymbolic(wl.H, wl.pins)
         f.setElements(wl.tets)

@@ -86,7 +86,10 @@ typedef struct {
                                    reuses the previous separator tree, re-dissecting only the subtrees that a
                                    new edge violates (PARTH-style temporal reuse, ParallelNestedDissection/
                                    README.md:86-127); a full dissection every nd_reuse_period analyses */
-    int32_t reserved[5];
+    int32_t solve_chain;        /* diagonal-block solves of the fronts above the subtree cut: 0 through the
+                                   inverses of 256-row superblocks of L11 (one CTA per superblock),
+                                   1 through chains of 64-row blocks (one CTA per pair of blocks) */
+    int32_t reserved[4];
 } mfs_options;
 
 typedef struct mfs_handle mfs_handle;

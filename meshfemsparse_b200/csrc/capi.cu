@@ -739,8 +739,12 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
             const LevelPlan &L = ds.levels[l];
             launch_fwd_asm(ds.sasm_tasks.p + L.sasm_off, L.sasm_n, L.sasm_tiles, ds.sd, Xc, S.n, nr, h->sol.p, st);
             MFS_LAUNCHED();
-            MFS_CUDA(launch_sb_solve<T>(true, ds.fsb_tasks.p + L.fsb_off, L.fsb_n, ds.sd, factor, Xc, S.n, nr,
+            if (h->opt.solve_chain == 1)
+                MFS_CUDA(launch_diag<T>(true, ds.ftri_tasks.p + L.ftri_off, L.ftri_n, ds.sd, factor, Xc, S.n, nr,
                                         ds.flags.p, h->solve_err.p, st));
+            else
+                MFS_CUDA(launch_sb_solve<T>(true, ds.fsb_tasks.p + L.fsb_off, L.fsb_n, ds.sd, factor, Xc, S.n, nr,
+                                            ds.flags.p, h->solve_err.p, st));
             launch_str<T>(true, ds.fstr_tasks.p + L.fstr_off, L.fstr_n, ds.fred.p + L.fred_off, L.fred_n, ds.sd,
                           factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
             MFS_LAUNCHED();
@@ -750,8 +754,12 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
             launch_str<T>(false, ds.bstr_tasks.p + L.bstr_off, L.bstr_n, ds.bred.p + L.bred_off, L.bred_n, ds.sd,
                           factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
             MFS_LAUNCHED();
-            MFS_CUDA(launch_sb_solve<T>(false, ds.bsb_tasks.p + L.bsb_off, L.bsb_n, ds.sd, factor, Xc, S.n, nr,
+            if (h->opt.solve_chain == 1)
+                MFS_CUDA(launch_diag<T>(false, ds.btri_tasks.p + L.btri_off, L.btri_n, ds.sd, factor, Xc, S.n, nr,
                                         ds.flags.p, h->solve_err.p, st));
+            else
+                MFS_CUDA(launch_sb_solve<T>(false, ds.bsb_tasks.p + L.bsb_off, L.bsb_n, ds.sd, factor, Xc, S.n, nr,
+                                            ds.flags.p, h->solve_err.p, st));
         }
         launch_subtree_solve<T>(false, ds.subs.p, ds.nsub, ds.sub_fmax, ds.sd, factor, Xc, S.n, nr, h->sol.p, st);
         MFS_LAUNCHED();

@@ -55,9 +55,11 @@ def test_tiny_fp32_pivot_is_refactored_in_fp64():
     L = pyoracle.panels_to_csc(sn, got, n).toarray()
     Lref = pyoracle.panels_to_csc(sn, ref, n).toarray()
     # the re-factored first column block matches FP64 up to the FP32 rounding of the
-    # block's inputs (about 1e-7 of the diagonal, i.e. a few percent of pivot 5)
+    # block's inputs (about 1e-7 of the diagonal), which the small pivot 5 amplifies
+    # in the columns from 5 on to about 1e-4 of the largest entry
     blk = slice(0, 128)
-    assert np.max(np.abs(L[blk, blk] - Lref[blk, blk])) <= 1e-5 * np.max(np.abs(Lref[blk, blk]))
+    assert np.max(np.abs(L[blk, blk] - Lref[blk, blk])) <= 2e-4 * np.max(np.abs(Lref[blk, blk]))
+    assert np.max(np.abs(L[blk, :5] - Lref[blk, :5])) <= 1e-6 * np.max(np.abs(Lref[blk, blk]))
     assert abs(L[5, 5] - Lref[5, 5]) <= 5e-2 * abs(Lref[5, 5])
     b = np.random.default_rng(1).normal(size=n)
     x = f.solve(b)
