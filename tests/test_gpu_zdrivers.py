@@ -71,6 +71,7 @@ def test_cli_on_gpu(tmp_path):
     assert np.linalg.norm(K @ u - b) <= 1e-12 * np.linalg.norm(b)
 
 
+@pytest.mark.gpu
 @pytest.mark.parametrize("single", [False, True])
 @pytest.mark.parametrize("rank", [0, 2])
 def test_bordered_solve_through_gpu_factorizer(single, rank):
@@ -106,6 +107,7 @@ def test_bordered_solve_through_gpu_factorizer(single, rank):
     assert np.all(got[pins] == 0.0)
 
 
+@pytest.mark.gpu
 def test_bordered_equality_constraints_through_gpu_factorizer():
     """Equality constraints through Lagrange multipliers over the GPU factorization,
     against the dense KKT solve."""
