@@ -12,10 +12,15 @@
 // zeros above the diagonal), built from the 64 x 64 diagonal inverses by block
 // forward substitution. A solve task is one superblock of one front, run by one
 // CTA:
-//   forward   acc = b_K - sum_{J < K} L_KJ y_J   (waiting on superblock J's flag,
-//             L_KJ streamed in 256 x CW chunks), y_K = inv(L_KK) acc, publish;
+//   forward   acc = b_K - sum_{J < K} L_KJ y_J   (waiting on superblock J's flag),
+//             y_K = inv(L_KK) acc, publish (one thread per row);
 //   backward  acc = y_K - sum_{J > K} L_JK^T x_J (J descending),
-//             x_K = inv(L_KK)^T acc, publish.
+//             x_K = inv(L_KK)^T acc, publish (one warp per column, shuffle sums).
+// L and the inverse stream through shared memory in 32 KB chunks of whole columns
+// (256 rows x 32 FP32 / 16 FP64 columns; the inverse's rows above a chunk's first
+// column are zero and skipped) in a ring of up to six chunks in flight, so a CTA
+// keeps enough bytes in flight to stream at a useful fraction of its bandwidth
+// and the chunks of the next dependency are already on chip when its flag comes.
 // The chain thus takes one flag hop, one superblock-wide product and one
 // inverse product per 256 rows. Launches are cooperative (all CTAs co-resident);
 // every CTA walks its tasks in ascending order and a task waits only on
@@ -98,20 +103,25 @@ __device__ __forceinline__ void stage_cols(T *dst, int ldd, const T *src, int64_
     }
 }
 
-// Product type of the chunk sums: FP32 for an FP32 factor, FP64 otherwise.
+// Product type of the off-diagonal chunk sums: FP32 for an FP32 factor, FP64 otherwise.
 template <typename T>
 using PT = std::conditional_t<sizeof(T) == 4, float, double>;
 
-template <typename T, int CW>
+// Chunks of 32 KB: CW columns x SB rows of L (or of the inverse), column-major in
+// shared memory with leading dimension SB, streamed through an NST-deep cp.async ring.
+template <typename T>
+struct SbChunk {
+    static constexpr int CW = 32768 / (SB * int(sizeof(T)));   // 32 columns (FP32), 16 (FP64)
+    static constexpr int BYTES = CW * SB * int(sizeof(T));
+};
+template <typename T, int NST>
 struct SbLayout {
     // doubles: acc[nrhs][SB] | out[nrhs][SB] | vec[nrhs][SB]; PT copy of vec [nrhs][SB]; ring
     static __host__ __device__ constexpr size_t ring_off(int nrhs) {
-        return (size_t(3) * nrhs * SB * sizeof(double) + size_t(nrhs) * SB * sizeof(PT<T>) + 15) & ~size_t(15);
+        return (size_t(3) * nrhs * SB * sizeof(double) + size_t(nrhs) * SB * sizeof(PT<T>) + 127) & ~size_t(127);
     }
-    static constexpr int FWD_LD = SB;                          // forward chunk: (row i, column j) at j * SB + i
-    static constexpr int BWD_LD = CW + 16 / int(sizeof(T));    // backward chunk: (row i, column j) at j * BWD_LD + i
-    static __host__ __device__ constexpr size_t bytes(int nrhs, bool fwd) {
-        return ring_off(nrhs) + 2 * (fwd ? size_t(CW) * FWD_LD : size_t(SB) * BWD_LD) * sizeof(T);
+    static __host__ __device__ constexpr size_t bytes(int nrhs) {
+        return ring_off(nrhs) + size_t(NST) * SbChunk<T>::BYTES;
     }
 };
 
@@ -119,10 +129,10 @@ struct SbLayout {
 __device__ __forceinline__ int sb_rows(int w, int K) { return min(SB, w - K * SB); }
 __device__ __forceinline__ int sb_pad(int nr) { return (nr + 63) & ~63; }
 
-// Forward chunk product for this thread's row: dst[r * SB] -/+= sum_j tl[j * ldt + tid] v[r * SB + j]
-// (j < ncol), accumulated in Q.
+// Row mode (forward): this thread's row t of the chunk (rows offset by row0 in the
+// chunk), dst[r * SB] -/+= sum_j tl[j * SB + t - row0] v[r * SB + j], j < ncol.
 template <typename Q, typename T>
-__device__ __forceinline__ void fwd_chunk(const T *tl, int ldt, const Q *v, int ncol, int nrhs, double *dst,
+__device__ __forceinline__ void row_chunk(const T *tl, int trow, const Q *v, int ncol, int nrhs, double *dst,
                                           bool sub) {
     for (int rg = 0; rg < nrhs; rg += kRG) {
         Q p[kRG];
@@ -130,7 +140,7 @@ __device__ __forceinline__ void fwd_chunk(const T *tl, int ldt, const Q *v, int 
         for (int u = 0; u < kRG; ++u) p[u] = Q(0);
 #pragma unroll 8
         for (int j = 0; j < ncol; ++j) {
-            const Q a = Q(tl[j * ldt + threadIdx.x]);
+            const Q a = Q(tl[j * SB + trow]);
 #pragma unroll
             for (int u = 0; u < kRG; ++u)
                 if (rg + u < nrhs) p[u] += a * v[(rg + u) * SB + j];
@@ -143,48 +153,55 @@ __device__ __forceinline__ void fwd_chunk(const T *tl, int ldt, const Q *v, int 
             }
     }
 }
-// Backward chunk product for this thread's column tc (CW rows, rows >= nrow skipped, in
-// skewed order so the lanes of a warp read different banks):
-// dst[r * SB] -/+= sum_i tc[i] v[r * SB + i], accumulated in Q.
-template <typename Q, typename T, int CW>
-__device__ __forceinline__ void bwd_chunk(const T *tc, const Q *v, int nrow, int nrhs, double *dst, bool sub) {
-    for (int rg = 0; rg < nrhs; rg += kRG) {
-        Q p[kRG];
+// Column mode (backward): one warp per column j of the chunk (columns warp, warp + 8,
+// ...): s_r = sum_{i < nrow} tl[j * SB + i] v[r * SB + i] over the lanes, reduced by
+// shuffles; lane 0 applies dst[r * SB + j] -/+= s_r (or = s_r when set).
+template <typename Q, typename T>
+__device__ __forceinline__ void col_chunk(const T *tl, const Q *v, int nrow, int ncol, int nrhs, double *dst,
+                                          int mode /* 0 subtract, 1 store */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int j = warp; j < ncol; j += nw) {
+        const T *col = tl + j * SB;
+        for (int rg = 0; rg < nrhs; rg += kRG) {
+            Q p[kRG];
 #pragma unroll
-        for (int u = 0; u < kRG; ++u) p[u] = Q(0);
-#pragma unroll 8
-        for (int w = 0; w < CW; ++w) {
-            const int i = (w + threadIdx.x) & (CW - 1);
-            if (i < nrow) {
-                const Q a = Q(tc[i]);
+            for (int u = 0; u < kRG; ++u) p[u] = Q(0);
+            for (int i = lane; i < nrow; i += 32) {
+                const Q a = Q(col[i]);
 #pragma unroll
                 for (int u = 0; u < kRG; ++u)
                     if (rg + u < nrhs) p[u] += a * v[(rg + u) * SB + i];
             }
-        }
 #pragma unroll
-        for (int u = 0; u < kRG; ++u)
-            if (rg + u < nrhs) {
-                if (sub) dst[(rg + u) * SB] -= double(p[u]);
-                else dst[(rg + u) * SB] += double(p[u]);
+            for (int u = 0; u < kRG; ++u) {
+                Q g = p[u];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) g += __shfl_down_sync(0xffffffffu, g, o);
+                if (lane == 0 && rg + u < nrhs) {
+                    if (mode == 0) dst[(rg + u) * SB + j] -= double(g);
+                    else dst[(rg + u) * SB + j] = double(g);
+                }
             }
+        }
     }
 }
 
-template <typename T, int CW>
+template <typename T, int NST>
 __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
                                                                SnDev sd, const T *__restrict__ factor,
                                                                double *__restrict__ X, int64_t ldx, int nrhs,
                                                                int *__restrict__ flags, int *__restrict__ err) {
-    using L = SbLayout<T, CW>;
+    using L = SbLayout<T, NST>;
     using P = PT<T>;
-    extern __shared__ __align__(16) double sb_smem[];
+    constexpr int CW = SbChunk<T>::CW;
+    constexpr int BUF = CW * SB;
+    constexpr int per = SB / CW;                         // chunks per earlier superblock
+    extern __shared__ __align__(128) double sb_smem[];
     double *acc = sb_smem;
     double *out = acc + nrhs * SB;
     double *vec = out + nrhs * SB;
     P *vp = reinterpret_cast<P *>(vec + nrhs * SB);
     T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sb_smem) + L::ring_off(nrhs));
-    constexpr int BUF = CW * L::FWD_LD;
     const int tid = threadIdx.x;
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SbTask tk = tasks[t];
@@ -194,30 +211,33 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__r
         const T *inv = factor + tk.inv;
         const int nr = sb_rows(w, K), nrp = sb_pad(nr);
         const int r0 = K * SB;
-        constexpr int per = SB / CW;                     // chunks per earlier superblock
-        const int ninv = (nrp + CW - 1) / CW;            // chunks of the inverse
+        const int ninv = (nrp + CW - 1) / CW;            // column chunks of the inverse
         const int nq = K * per + ninv;
+        // chunk q: L(K rows, columns of superblock J = q / per), or inverse columns
+        // [c CW, c CW + CW) with the rows from c CW on (the rest is zero)
         auto stage = [&](int q) {
-            T *dst = ring + (q & 1) * BUF;
+            T *dst = ring + (q % NST) * BUF;
             if (q < K * per) {
                 const int J = q / per, c = q - J * per;
-                stage_cols<T>(dst, L::FWD_LD, pan + int64_t(J * SB + c * CW) * ld, ld, r0, nr, nrp, CW);
+                stage_cols<T>(dst, SB, pan + int64_t(J * SB + c * CW) * ld, ld, r0, nr, nrp, CW);
             } else {
                 const int c = q - K * per;
-                const int nc = min(CW, nrp - c * CW);
-                stage_cols<T>(dst, L::FWD_LD, inv + int64_t(c * CW) * nrp, nrp, 0, nrp, nrp, nc);
+                stage_cols<T>(dst, SB, inv + int64_t(c * CW) * nrp, nrp, c * CW, nrp - c * CW, nrp - c * CW,
+                              min(CW, nrp - c * CW));
             }
-            cpa_commit();
         };
         __syncthreads();                                 // the previous task is done with shared memory
-        stage(0);
+        for (int p = 0; p < NST - 1; ++p) {
+            if (p < nq) stage(p);
+            cpa_commit();
+        }
         for (int r = 0; r < nrhs; ++r) {
             acc[r * SB + tid] = tid < nr ? X[c0 + r0 + tid + r * ldx] : 0.0;
             out[r * SB + tid] = 0.0;
         }
         for (int q = 0; q < nq; ++q) {
-            if (q + 1 < nq) stage(q + 1);
-            else cpa_commit();
+            if (q + NST - 1 < nq) stage(q + NST - 1);
+            cpa_commit();
             const bool lpart = q < K * per;
             const int J = lpart ? q / per : K, c = lpart ? q - J * per : q - K * per;
             if (lpart && c == 0) {
@@ -229,17 +249,17 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__r
                     vp[r * SB + tid] = P(v);
                 }
             }
-            cpa_wait<1>();
+            cpa_wait<NST - 1>();
             __syncthreads();                             // (also: acc is complete before the inverse)
-            const T *tl = ring + (q & 1) * BUF;
-            if (tid < nr) {
-                const int j0 = c * CW;                    // first vector entry of the chunk
-                // off-diagonal superblocks: products of the chunk's precision (FP32 for an
-                // FP32 factor); the inverse of the diagonal superblock: FP64 products
-                if (lpart) fwd_chunk<P>(tl, L::FWD_LD, vp + j0, CW, nrhs, acc + tid, true);
-                else fwd_chunk<double>(tl, L::FWD_LD, acc + j0, min(CW, nrp - j0), nrhs, out + tid, false);
+            const T *tl = ring + (q % NST) * BUF;
+            if (lpart) {
+                // off-diagonal superblock: products of the factor's precision
+                if (tid < nr) row_chunk<P>(tl, tid, vp + c * CW, CW, nrhs, acc + tid, true);
+            } else if (tid < nr && tid >= c * CW) {
+                // inverse of the diagonal superblock (rows from c CW): FP64 products
+                row_chunk<double>(tl, tid - c * CW, acc + c * CW, min(CW, nrp - c * CW), nrhs, out + tid, false);
             }
-            __syncthreads();                             // the ring slot is refilled at q + 2
+            __syncthreads();                             // the ring slot is refilled NST - 1 chunks later
         }
         cpa_wait<0>();
         if (tid < nr)
@@ -252,22 +272,22 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__r
     }
 }
 
-template <typename T, int CW>
+template <typename T, int NST>
 __global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
                                                                SnDev sd, const T *__restrict__ factor,
                                                                double *__restrict__ X, int64_t ldx, int nrhs,
                                                                int *__restrict__ flags, int *__restrict__ err) {
-    using L = SbLayout<T, CW>;
+    using L = SbLayout<T, NST>;
     using P = PT<T>;
-    extern __shared__ __align__(16) double sb_smem[];
+    constexpr int CW = SbChunk<T>::CW;
+    constexpr int BUF = CW * SB;
+    constexpr int per = SB / CW;                         // column chunks per later superblock
+    extern __shared__ __align__(128) double sb_smem[];
     double *acc = sb_smem;
     double *out = acc + nrhs * SB;
     double *vec = out + nrhs * SB;
     P *vp = reinterpret_cast<P *>(vec + nrhs * SB);
     T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sb_smem) + L::ring_off(nrhs));
-    constexpr int LDB = L::BWD_LD;
-    constexpr int BUF = SB * LDB;
-    constexpr int per = SB / CW;                         // row chunks per later superblock
     const int tid = threadIdx.x;
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SbTask tk = tasks[t];
@@ -278,43 +298,46 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__r
         const int nr = sb_rows(w, K), nrp = sb_pad(nr);
         const int r0 = K * SB;
         const int nsb = (w + SB - 1) / SB;
-        // chunks: for J = nsb - 1 down to K + 1 the rows of J in chunks of CW, then the
-        // inverse (rows in chunks of CW); chunk (row i, column j) at j * LDB + i
+        // chunk q: for J = nsb - 1 down to K + 1, L(J rows, columns [r0 + c CW, + CW) of K)
+        // (K is not the last superblock then, so its SB columns are whole); then the
+        // inverse's columns [c CW, + CW) with their rows from c CW on
         const int nql = (nsb - 1 - K) * per;
         const int ninv = (nrp + CW - 1) / CW;
         const int nq = nql + ninv;
-        auto jinfo = [&](int q, int &J, int &c, int &nrJ) {
+        auto jinfo = [&](int q, int &J, int &c) {
             const int m = q / per;
             J = nsb - 1 - m;
             c = q - m * per;
-            nrJ = sb_rows(w, J);
         };
         auto stage = [&](int q) {
-            T *dst = ring + (q & 1) * BUF;
+            T *dst = ring + (q % NST) * BUF;
             if (q < nql) {
-                int J, c, nrJ;
-                jinfo(q, J, c, nrJ);
-                // rows [J SB + c CW, + CW) of columns [r0, r0 + nr) (nr = SB: K is not the last)
-                stage_cols<T>(dst, LDB, pan + int64_t(r0) * ld, ld, J * SB + c * CW, max(0, nrJ - c * CW), CW, nr);
+                int J, c;
+                jinfo(q, J, c);
+                const int nrJ = sb_rows(w, J);
+                stage_cols<T>(dst, SB, pan + int64_t(r0 + c * CW) * ld, ld, J * SB, nrJ, sb_pad(nrJ), CW);
             } else {
                 const int c = q - nql;
-                const int nrow = min(CW, nrp - c * CW);
-                stage_cols<T>(dst, LDB, inv, nrp, c * CW, nrow, CW, nrp);
+                stage_cols<T>(dst, SB, inv + int64_t(c * CW) * nrp, nrp, c * CW, nrp - c * CW, nrp - c * CW,
+                              min(CW, nrp - c * CW));
             }
-            cpa_commit();
         };
         __syncthreads();
-        stage(0);
+        for (int p = 0; p < NST - 1; ++p) {
+            if (p < nq) stage(p);
+            cpa_commit();
+        }
         for (int r = 0; r < nrhs; ++r) {
             acc[r * SB + tid] = tid < nr ? X[c0 + r0 + tid + r * ldx] : 0.0;
             out[r * SB + tid] = 0.0;
         }
         for (int q = 0; q < nq; ++q) {
-            if (q + 1 < nq) stage(q + 1);
-            else cpa_commit();
+            if (q + NST - 1 < nq) stage(q + NST - 1);
+            cpa_commit();
             const bool lpart = q < nql;
-            int J = K, c = q - nql, nrJ = 0;
-            if (lpart) jinfo(q, J, c, nrJ);
+            int J = K, c = q - nql;
+            if (lpart) jinfo(q, J, c);
+            const int nrJ = lpart ? sb_rows(w, J) : 0;
             if (lpart && c == 0) {
                 wait_flag(flags + tk.flag0 + J, 2, err);
                 for (int r = 0; r < nrhs; ++r) {
@@ -323,13 +346,15 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__r
                     vp[r * SB + tid] = P(v);
                 }
             }
-            cpa_wait<1>();
+            cpa_wait<NST - 1>();
             __syncthreads();                             // (also: acc is complete before the inverse)
-            const T *tl = ring + (q & 1) * BUF + tid * LDB;   // this thread's column
-            if (tid < nr) {
-                const int i0 = c * CW;                        // first vector entry of the chunk
-                if (lpart) bwd_chunk<P, T, CW>(tl, vp + i0, min(CW, max(0, nrJ - i0)), nrhs, acc + tid, true);
-                else bwd_chunk<double, T, CW>(tl, acc + i0, min(CW, nrp - i0), nrhs, out + tid, false);
+            const T *tl = ring + (q % NST) * BUF;
+            if (lpart) {
+                // acc(columns of the chunk) -= L(J rows, chunk columns)^T x_J
+                col_chunk<P>(tl, vp, nrJ, CW, nrhs, acc + c * CW, 0);
+            } else {
+                // x(chunk columns) = inv(L_KK)(rows from c CW, chunk columns)^T acc: FP64 products
+                col_chunk<double>(tl, acc + c * CW, nrp - c * CW, min(CW, nrp - c * CW), nrhs, out + c * CW, 1);
             }
             __syncthreads();
         }
@@ -447,25 +472,21 @@ int coop_grid(K kernel, size_t smem, int ntasks) {
     return std::min(g, std::max(1, ntasks));
 }
 
-// MAXR: the most right-hand sides this chunk width is launched with
-template <typename T, int CW, int MAXR>
+// MAXR: the most right-hand sides this ring depth is launched with
+template <typename T, int NST, int MAXR>
 cudaError_t launch_sb_impl(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
                            int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st) {
-    using L = SbLayout<T, CW>;
-    static_assert(SbLayout<T, CW>::bytes(MAXR, true) <= size_t(kMaxSmemOptin) &&
-                      SbLayout<T, CW>::bytes(MAXR, false) <= size_t(kMaxSmemOptin),
-                  "superblock solve shared memory");
-    void *kern = forward ? (void *)sb_fwd_kernel<T, CW> : (void *)sb_bwd_kernel<T, CW>;
-    const size_t smem = L::bytes(nrhs, forward);
+    using L = SbLayout<T, NST>;
+    static_assert(L::bytes(MAXR) <= size_t(kMaxSmemOptin), "superblock solve shared memory");
+    void *kern = forward ? (void *)sb_fwd_kernel<T, NST> : (void *)sb_bwd_kernel<T, NST>;
+    const size_t smem = L::bytes(nrhs);
     static PerDeviceOnce once;
     once([] {
-        cudaFuncSetAttribute(sb_fwd_kernel<T, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(L::bytes(MAXR, true)));
-        cudaFuncSetAttribute(sb_bwd_kernel<T, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(L::bytes(MAXR, false)));
+        cudaFuncSetAttribute(sb_fwd_kernel<T, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes(MAXR)));
+        cudaFuncSetAttribute(sb_bwd_kernel<T, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes(MAXR)));
     });
-    const int grid = forward ? coop_grid(sb_fwd_kernel<T, CW>, smem, ntasks)
-                             : coop_grid(sb_bwd_kernel<T, CW>, smem, ntasks);
+    const int grid = forward ? coop_grid(sb_fwd_kernel<T, NST>, smem, ntasks)
+                             : coop_grid(sb_bwd_kernel<T, NST>, smem, ntasks);
     void *args[] = {(void *)&tasks, (void *)&ntasks, (void *)&sd, (void *)&factor, (void *)&X, (void *)&ldx,
                     (void *)&nrhs, (void *)&flags, (void *)&err};
     ++g_kernel_launches;
@@ -479,16 +500,10 @@ cudaError_t launch_sb_solve(bool forward, const SbTask *tasks, int ntasks, SnDev
                             int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st) {
     if (ntasks <= 0) return cudaSuccess;
     if (nrhs > kMaxSolveRhs) return cudaErrorInvalidValue;
-    // chunk width: the widest whose ring fits beside the vectors of nrhs right-hand sides
-    if constexpr (sizeof(T) == 4) {
-        if (nrhs <= 8)
-            return launch_sb_impl<T, 64, 8>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
-        return launch_sb_impl<T, 32, kMaxSolveRhs>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
-    } else {
-        if (nrhs <= 8)
-            return launch_sb_impl<T, 32, 8>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
-        return launch_sb_impl<T, 16, kMaxSolveRhs>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
-    }
+    // ring depth: the deepest that fits beside the vectors of nrhs right-hand sides
+    if (nrhs <= 4) return launch_sb_impl<T, 6, 4>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
+    if (nrhs <= 8) return launch_sb_impl<T, 4, 8>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
+    return launch_sb_impl<T, 2, kMaxSolveRhs>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
 }
 
 template <typename T>
