@@ -18,9 +18,12 @@
 //             x_K = inv(L_KK)^T acc, publish (one warp per column, shuffle sums).
 // L and the inverse stream through shared memory in 32 KB chunks of whole columns
 // (256 rows x 32 FP32 / 16 FP64 columns; the inverse's rows above a chunk's first
-// column are zero and skipped) in a ring of up to six chunks in flight, so a CTA
-// keeps enough bytes in flight to stream at a useful fraction of its bandwidth
-// and the chunks of the next dependency are already on chip when its flag comes.
+// column are zero and skipped): one thread issues a bulk copy per column, the
+// chunk completes on its ring slot's mbarrier, and up to six chunks are in flight,
+// so the chunks of the next dependency are already on chip when its flag comes.
+// Bulk copies of a superblock's rows are rounded up to 64 rows; the extra rows lie
+// inside the factor array (the next rows or column of the panel, or the inverses
+// stored after the panels) and are never used.
 // The chain thus takes one flag hop, one superblock-wide product and one
 // inverse product per 256 rows. Launches are cooperative (all CTAs co-resident);
 // every CTA walks its tasks in ascending order and a task waits only on
@@ -107,8 +110,9 @@ __device__ __forceinline__ void stage_cols(T *dst, int ldd, const T *src, int64_
 template <typename T>
 using PT = std::conditional_t<sizeof(T) == 4, float, double>;
 
-// Chunks of 32 KB: CW columns x SB rows of L (or of the inverse), column-major in
-// shared memory with leading dimension SB, streamed through an NST-deep cp.async ring.
+// Chunks of 32 KB: CW whole columns (SB rows) of L or of the inverse, column-major in
+// shared memory with leading dimension SB, streamed through an NST-deep ring of bulk
+// copies (one per column) that complete on the slot's mbarrier.
 template <typename T>
 struct SbChunk {
     static constexpr int CW = 32768 / (SB * int(sizeof(T)));   // 32 columns (FP32), 16 (FP64)
@@ -129,64 +133,131 @@ struct SbLayout {
 __device__ __forceinline__ int sb_rows(int w, int K) { return min(SB, w - K * SB); }
 __device__ __forceinline__ int sb_pad(int nr) { return (nr + 63) & ~63; }
 
-// Row mode (forward): this thread's row t of the chunk (rows offset by row0 in the
-// chunk), dst[r * SB] -/+= sum_j tl[j * SB + t - row0] v[r * SB + j], j < ncol.
-template <typename Q, typename T>
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Every thread waits for the chunk's copies (bounded; on expiry the error is
+// recorded and the chunk's contents are not trusted).
+__device__ __forceinline__ void mbar_wait_all(uint32_t bar, uint32_t parity, int *err) {
+    if (mbar_try(bar, parity)) return;
+    const unsigned long long t0 = gtimer();
+    for (int it = 1;; ++it) {
+        if (mbar_try(bar, parity)) return;
+        if ((it & 63) == 0) {
+            if (*(volatile int *)err) return;
+            if (gtimer() - t0 > kWaitNs) {
+                atomicExch(err, 1);
+                return;
+            }
+        }
+    }
+}
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+// One thread: ncols columns of a column-major source (leading dimension lds), rows
+// [row0, row0 + nrows) of each (16-byte aligned, a multiple of 16 bytes), to
+// dst + j * SB elements, completing on `bar`.
+template <typename T>
+__device__ __forceinline__ void stage_bulk(T *dst, const T *src, int64_t lds, int row0, int nrows, int ncols,
+                                           uint32_t bar) {
+    const uint32_t bytes = uint32_t(nrows) * sizeof(T);
+    mbar_expect_tx(bar, bytes * uint32_t(ncols));
+    const uint32_t d0 = smem_u32(dst);
+    for (int j = 0; j < ncols; ++j)
+        bulk_copy(d0 + uint32_t(j) * SB * sizeof(T), src + int64_t(j) * lds + row0, bytes, bar);
+}
+
+// After an error (a wait that gave up), the copies a CTA issued may still be in
+// flight: thread 0 waits, again bounded, for the last use of every ring slot, so
+// no copy lands in shared memory after the CTA has exited.
+template <int NST>
+__device__ __forceinline__ void ring_drain(uint64_t *bars, long long issued, const int *err) {
+    if (threadIdx.x != 0 || !*(volatile const int *)err) return;
+    for (int b = 0; b < NST; ++b) {
+        if (issued <= b) continue;
+        const long long last = b + ((issued - 1 - b) / NST) * NST;
+        const uint32_t bar = smem_u32(&bars[b]), par = uint32_t((last / NST) & 1);
+        const unsigned long long t0 = gtimer();
+        while (!mbar_try(bar, par) && gtimer() - t0 < kWaitNs) {
+        }
+    }
+}
+
+// Row mode (forward): this thread's row (chunk row trow), dst[r * SB] -/+=
+// sum_j tl[j * SB + trow] v[r * SB + j], j < ncol, for the NR right-hand sides.
+template <typename Q, int NR, typename T>
 __device__ __forceinline__ void row_chunk(const T *tl, int trow, const Q *v, int ncol, int nrhs, double *dst,
                                           bool sub) {
-    for (int rg = 0; rg < nrhs; rg += kRG) {
-        Q p[kRG];
+    Q p[NR];
 #pragma unroll
-        for (int u = 0; u < kRG; ++u) p[u] = Q(0);
+    for (int u = 0; u < NR; ++u) p[u] = Q(0);
 #pragma unroll 8
-        for (int j = 0; j < ncol; ++j) {
-            const Q a = Q(tl[j * SB + trow]);
+    for (int j = 0; j < ncol; ++j) {
+        const Q a = Q(tl[j * SB + trow]);
 #pragma unroll
-            for (int u = 0; u < kRG; ++u)
-                if (rg + u < nrhs) p[u] += a * v[(rg + u) * SB + j];
-        }
-#pragma unroll
-        for (int u = 0; u < kRG; ++u)
-            if (rg + u < nrhs) {
-                if (sub) dst[(rg + u) * SB] -= double(p[u]);
-                else dst[(rg + u) * SB] += double(p[u]);
-            }
+        for (int u = 0; u < NR; ++u) p[u] += a * v[u * SB + j];
     }
+#pragma unroll
+    for (int u = 0; u < NR; ++u)
+        if (u < nrhs) {
+            if (sub) dst[u * SB] -= double(p[u]);
+            else dst[u * SB] += double(p[u]);
+        }
 }
 // Column mode (backward): one warp per column j of the chunk (columns warp, warp + 8,
 // ...): s_r = sum_{i < nrow} tl[j * SB + i] v[r * SB + i] over the lanes, reduced by
-// shuffles; lane 0 applies dst[r * SB + j] -/+= s_r (or = s_r when set).
-template <typename Q, typename T>
+// shuffles; lane 0 applies dst[r * SB + j] -= s_r (mode 0) or = s_r (mode 1).
+template <typename Q, int NR, typename T>
 __device__ __forceinline__ void col_chunk(const T *tl, const Q *v, int nrow, int ncol, int nrhs, double *dst,
-                                          int mode /* 0 subtract, 1 store */) {
+                                          int mode) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int j = warp; j < ncol; j += nw) {
         const T *col = tl + j * SB;
-        for (int rg = 0; rg < nrhs; rg += kRG) {
-            Q p[kRG];
+        Q p[NR];
 #pragma unroll
-            for (int u = 0; u < kRG; ++u) p[u] = Q(0);
-            for (int i = lane; i < nrow; i += 32) {
-                const Q a = Q(col[i]);
+        for (int u = 0; u < NR; ++u) p[u] = Q(0);
+        for (int i = lane; i < nrow; i += 32) {
+            const Q a = Q(col[i]);
 #pragma unroll
-                for (int u = 0; u < kRG; ++u)
-                    if (rg + u < nrhs) p[u] += a * v[(rg + u) * SB + i];
-            }
+            for (int u = 0; u < NR; ++u) p[u] += a * v[u * SB + i];
+        }
 #pragma unroll
-            for (int u = 0; u < kRG; ++u) {
-                Q g = p[u];
+        for (int u = 0; u < NR; ++u) {
+            Q g = p[u];
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) g += __shfl_down_sync(0xffffffffu, g, o);
-                if (lane == 0 && rg + u < nrhs) {
-                    if (mode == 0) dst[(rg + u) * SB + j] -= double(g);
-                    else dst[(rg + u) * SB + j] = double(g);
-                }
+            for (int o = 16; o > 0; o >>= 1) g += __shfl_down_sync(0xffffffffu, g, o);
+            if (lane == 0 && u < nrhs) {
+                if (mode == 0) dst[u * SB + j] -= double(g);
+                else dst[u * SB + j] = double(g);
             }
         }
     }
 }
 
-template <typename T, int NST>
+// Vectors hold NR right-hand sides (columns >= nrhs are zero), so the products above
+// run without predicates.
+template <typename T, int NST, int NR>
 __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
                                                                SnDev sd, const T *__restrict__ factor,
                                                                double *__restrict__ X, int64_t ldx, int nrhs,
@@ -197,12 +268,19 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__r
     constexpr int BUF = CW * SB;
     constexpr int per = SB / CW;                         // chunks per earlier superblock
     extern __shared__ __align__(128) double sb_smem[];
+    __shared__ __align__(8) uint64_t bars[NST];
     double *acc = sb_smem;
-    double *out = acc + nrhs * SB;
-    double *vec = out + nrhs * SB;
-    P *vp = reinterpret_cast<P *>(vec + nrhs * SB);
-    T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sb_smem) + L::ring_off(nrhs));
+    double *out = acc + NR * SB;
+    double *vec = out + NR * SB;
+    P *vp = reinterpret_cast<P *>(vec + NR * SB);
+    T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sb_smem) + L::ring_off(NR));
     const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int b = 0; b < NST; ++b) mbar_init(smem_u32(&bars[b]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    long long gq = 0;                                    // chunks this CTA has consumed (ring phase)
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SbTask tk = tasks[t];
         const int s = tk.sn, K = tk.K;
@@ -213,55 +291,56 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__r
         const int r0 = K * SB;
         const int ninv = (nrp + CW - 1) / CW;            // column chunks of the inverse
         const int nq = K * per + ninv;
-        // chunk q: L(K rows, columns of superblock J = q / per), or inverse columns
-        // [c CW, c CW + CW) with the rows from c CW on (the rest is zero)
+        // chunk q: L(rows of K, CW columns of superblock J = q / per), or the inverse's
+        // columns [c CW, c CW + CW) with their rows from c CW on (the rest is zero)
         auto stage = [&](int q) {
-            T *dst = ring + (q % NST) * BUF;
+            const int slot = int((gq + q) % NST);
+            T *dst = ring + slot * BUF;
+            const uint32_t bar = smem_u32(&bars[slot]);
             if (q < K * per) {
                 const int J = q / per, c = q - J * per;
-                stage_cols<T>(dst, SB, pan + int64_t(J * SB + c * CW) * ld, ld, r0, nr, nrp, CW);
+                stage_bulk<T>(dst, pan + int64_t(J * SB + c * CW) * ld, ld, r0, nrp, CW, bar);
             } else {
                 const int c = q - K * per;
-                stage_cols<T>(dst, SB, inv + int64_t(c * CW) * nrp, nrp, c * CW, nrp - c * CW, nrp - c * CW,
-                              min(CW, nrp - c * CW));
+                stage_bulk<T>(dst, inv + int64_t(c * CW) * nrp, nrp, c * CW, nrp - c * CW, min(CW, nrp - c * CW),
+                              bar);
             }
         };
         __syncthreads();                                 // the previous task is done with shared memory
-        for (int p = 0; p < NST - 1; ++p) {
-            if (p < nq) stage(p);
-            cpa_commit();
-        }
-        for (int r = 0; r < nrhs; ++r) {
-            acc[r * SB + tid] = tid < nr ? X[c0 + r0 + tid + r * ldx] : 0.0;
+        if (tid == 0)
+            for (int q = 0; q < NST - 1 && q < nq; ++q) stage(q);
+        for (int r = 0; r < NR; ++r) {
+            acc[r * SB + tid] = (r < nrhs && tid < nr) ? X[c0 + r0 + tid + r * ldx] : 0.0;
             out[r * SB + tid] = 0.0;
         }
         for (int q = 0; q < nq; ++q) {
-            if (q + NST - 1 < nq) stage(q + NST - 1);
-            cpa_commit();
+            if (tid == 0 && q + NST - 1 < nq) stage(q + NST - 1);
             const bool lpart = q < K * per;
             const int J = lpart ? q / per : K, c = lpart ? q - J * per : q - K * per;
             if (lpart && c == 0) {
                 // y_J: wait for its superblock, then load it (written by another CTA: through L2)
                 wait_flag(flags + tk.flag0 + J, 1, err);
-                for (int r = 0; r < nrhs; ++r) {
-                    const double v = __ldcg(&X[c0 + J * SB + tid + r * ldx]);
+                for (int r = 0; r < NR; ++r) {
+                    const double v = r < nrhs ? __ldcg(&X[c0 + J * SB + tid + r * ldx]) : 0.0;
                     vec[r * SB + tid] = v;
                     vp[r * SB + tid] = P(v);
                 }
             }
-            cpa_wait<NST - 1>();
-            __syncthreads();                             // (also: acc is complete before the inverse)
-            const T *tl = ring + (q % NST) * BUF;
+            const int slot = int((gq + q) % NST);
+            mbar_wait_all(smem_u32(&bars[slot]), uint32_t(((gq + q) / NST) & 1), err);
+            __syncthreads();                             // (also: vectors and acc are complete)
+            const T *tl = ring + slot * BUF;
             if (lpart) {
                 // off-diagonal superblock: products of the factor's precision
-                if (tid < nr) row_chunk<P>(tl, tid, vp + c * CW, CW, nrhs, acc + tid, true);
+                if (tid < nr) row_chunk<P, NR>(tl, tid, vp + c * CW, CW, nrhs, acc + tid, true);
             } else if (tid < nr && tid >= c * CW) {
                 // inverse of the diagonal superblock (rows from c CW): FP64 products
-                row_chunk<double>(tl, tid - c * CW, acc + c * CW, min(CW, nrp - c * CW), nrhs, out + tid, false);
+                row_chunk<double, NR>(tl, tid - c * CW, acc + c * CW, min(CW, nrp - c * CW), nrhs, out + tid,
+                                      false);
             }
             __syncthreads();                             // the ring slot is refilled NST - 1 chunks later
         }
-        cpa_wait<0>();
+        gq += nq;
         if (tid < nr)
             for (int r = 0; r < nrhs; ++r) X[c0 + r0 + tid + r * ldx] = out[r * SB + tid];
         __syncthreads();
@@ -270,9 +349,10 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__r
             st_release(flags + tk.flag0 + K, 1);
         }
     }
+    ring_drain<NST>(bars, gq, err);
 }
 
-template <typename T, int NST>
+template <typename T, int NST, int NR>
 __global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
                                                                SnDev sd, const T *__restrict__ factor,
                                                                double *__restrict__ X, int64_t ldx, int nrhs,
@@ -283,12 +363,19 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__r
     constexpr int BUF = CW * SB;
     constexpr int per = SB / CW;                         // column chunks per later superblock
     extern __shared__ __align__(128) double sb_smem[];
+    __shared__ __align__(8) uint64_t bars[NST];
     double *acc = sb_smem;
-    double *out = acc + nrhs * SB;
-    double *vec = out + nrhs * SB;
-    P *vp = reinterpret_cast<P *>(vec + nrhs * SB);
-    T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sb_smem) + L::ring_off(nrhs));
+    double *out = acc + NR * SB;
+    double *vec = out + NR * SB;
+    P *vp = reinterpret_cast<P *>(vec + NR * SB);
+    T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sb_smem) + L::ring_off(NR));
     const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int b = 0; b < NST; ++b) mbar_init(smem_u32(&bars[b]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    long long gq = 0;
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SbTask tk = tasks[t];
         const int s = tk.sn, K = tk.K;
@@ -298,9 +385,9 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__r
         const int nr = sb_rows(w, K), nrp = sb_pad(nr);
         const int r0 = K * SB;
         const int nsb = (w + SB - 1) / SB;
-        // chunk q: for J = nsb - 1 down to K + 1, L(J rows, columns [r0 + c CW, + CW) of K)
-        // (K is not the last superblock then, so its SB columns are whole); then the
-        // inverse's columns [c CW, + CW) with their rows from c CW on
+        // chunk q: for J = nsb - 1 down to K + 1, L(rows of J, columns [r0 + c CW, + CW)
+        // of K) (K is not the last superblock then, so its SB columns are whole); then
+        // the inverse's columns [c CW, + CW) with their rows from c CW on
         const int nql = (nsb - 1 - K) * per;
         const int ninv = (nrp + CW - 1) / CW;
         const int nq = nql + ninv;
@@ -310,55 +397,54 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__r
             c = q - m * per;
         };
         auto stage = [&](int q) {
-            T *dst = ring + (q % NST) * BUF;
+            const int slot = int((gq + q) % NST);
+            T *dst = ring + slot * BUF;
+            const uint32_t bar = smem_u32(&bars[slot]);
             if (q < nql) {
                 int J, c;
                 jinfo(q, J, c);
-                const int nrJ = sb_rows(w, J);
-                stage_cols<T>(dst, SB, pan + int64_t(r0 + c * CW) * ld, ld, J * SB, nrJ, sb_pad(nrJ), CW);
+                stage_bulk<T>(dst, pan + int64_t(r0 + c * CW) * ld, ld, J * SB, sb_pad(sb_rows(w, J)), CW, bar);
             } else {
                 const int c = q - nql;
-                stage_cols<T>(dst, SB, inv + int64_t(c * CW) * nrp, nrp, c * CW, nrp - c * CW, nrp - c * CW,
-                              min(CW, nrp - c * CW));
+                stage_bulk<T>(dst, inv + int64_t(c * CW) * nrp, nrp, c * CW, nrp - c * CW, min(CW, nrp - c * CW),
+                              bar);
             }
         };
         __syncthreads();
-        for (int p = 0; p < NST - 1; ++p) {
-            if (p < nq) stage(p);
-            cpa_commit();
-        }
-        for (int r = 0; r < nrhs; ++r) {
-            acc[r * SB + tid] = tid < nr ? X[c0 + r0 + tid + r * ldx] : 0.0;
+        if (tid == 0)
+            for (int q = 0; q < NST - 1 && q < nq; ++q) stage(q);
+        for (int r = 0; r < NR; ++r) {
+            acc[r * SB + tid] = (r < nrhs && tid < nr) ? X[c0 + r0 + tid + r * ldx] : 0.0;
             out[r * SB + tid] = 0.0;
         }
         for (int q = 0; q < nq; ++q) {
-            if (q + NST - 1 < nq) stage(q + NST - 1);
-            cpa_commit();
+            if (tid == 0 && q + NST - 1 < nq) stage(q + NST - 1);
             const bool lpart = q < nql;
             int J = K, c = q - nql;
             if (lpart) jinfo(q, J, c);
             const int nrJ = lpart ? sb_rows(w, J) : 0;
             if (lpart && c == 0) {
                 wait_flag(flags + tk.flag0 + J, 2, err);
-                for (int r = 0; r < nrhs; ++r) {
-                    const double v = tid < nrJ ? __ldcg(&X[c0 + J * SB + tid + r * ldx]) : 0.0;
+                for (int r = 0; r < NR; ++r) {
+                    const double v = (r < nrhs && tid < nrJ) ? __ldcg(&X[c0 + J * SB + tid + r * ldx]) : 0.0;
                     vec[r * SB + tid] = v;
                     vp[r * SB + tid] = P(v);
                 }
             }
-            cpa_wait<NST - 1>();
-            __syncthreads();                             // (also: acc is complete before the inverse)
-            const T *tl = ring + (q % NST) * BUF;
+            const int slot = int((gq + q) % NST);
+            mbar_wait_all(smem_u32(&bars[slot]), uint32_t(((gq + q) / NST) & 1), err);
+            __syncthreads();                             // (also: vectors and acc are complete)
+            const T *tl = ring + slot * BUF;
             if (lpart) {
                 // acc(columns of the chunk) -= L(J rows, chunk columns)^T x_J
-                col_chunk<P>(tl, vp, nrJ, CW, nrhs, acc + c * CW, 0);
+                col_chunk<P, NR>(tl, vp, nrJ, CW, nrhs, acc + c * CW, 0);
             } else {
                 // x(chunk columns) = inv(L_KK)(rows from c CW, chunk columns)^T acc: FP64 products
-                col_chunk<double>(tl, acc + c * CW, nrp - c * CW, min(CW, nrp - c * CW), nrhs, out + c * CW, 1);
+                col_chunk<double, NR>(tl, acc + c * CW, nrp - c * CW, min(CW, nrp - c * CW), nrhs, out + c * CW, 1);
             }
             __syncthreads();
         }
-        cpa_wait<0>();
+        gq += nq;
         if (tid < nr)
             for (int r = 0; r < nrhs; ++r) X[c0 + r0 + tid + r * ldx] = out[r * SB + tid];
         __syncthreads();
@@ -367,6 +453,7 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__r
             st_release(flags + tk.flag0 + K, 2);
         }
     }
+    ring_drain<NST>(bars, gq, err);
 }
 
 // inv(L_KK) of superblock K of front s (nr rows), nrp x nrp column-major at
@@ -472,21 +559,21 @@ int coop_grid(K kernel, size_t smem, int ntasks) {
     return std::min(g, std::max(1, ntasks));
 }
 
-// MAXR: the most right-hand sides this ring depth is launched with
-template <typename T, int NST, int MAXR>
+// NR: the right-hand sides the vectors hold (nrhs <= NR)
+template <typename T, int NST, int NR>
 cudaError_t launch_sb_impl(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
                            int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st) {
     using L = SbLayout<T, NST>;
-    static_assert(L::bytes(MAXR) <= size_t(kMaxSmemOptin), "superblock solve shared memory");
-    void *kern = forward ? (void *)sb_fwd_kernel<T, NST> : (void *)sb_bwd_kernel<T, NST>;
-    const size_t smem = L::bytes(nrhs);
+    static_assert(L::bytes(NR) + 64 <= size_t(kMaxSmemOptin), "superblock solve shared memory");
+    void *kern = forward ? (void *)sb_fwd_kernel<T, NST, NR> : (void *)sb_bwd_kernel<T, NST, NR>;
+    const size_t smem = L::bytes(NR);
     static PerDeviceOnce once;
     once([] {
-        cudaFuncSetAttribute(sb_fwd_kernel<T, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes(MAXR)));
-        cudaFuncSetAttribute(sb_bwd_kernel<T, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes(MAXR)));
+        cudaFuncSetAttribute(sb_fwd_kernel<T, NST, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes(NR)));
+        cudaFuncSetAttribute(sb_bwd_kernel<T, NST, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes(NR)));
     });
-    const int grid = forward ? coop_grid(sb_fwd_kernel<T, NST>, smem, ntasks)
-                             : coop_grid(sb_bwd_kernel<T, NST>, smem, ntasks);
+    const int grid = forward ? coop_grid(sb_fwd_kernel<T, NST, NR>, smem, ntasks)
+                             : coop_grid(sb_bwd_kernel<T, NST, NR>, smem, ntasks);
     void *args[] = {(void *)&tasks, (void *)&ntasks, (void *)&sd, (void *)&factor, (void *)&X, (void *)&ldx,
                     (void *)&nrhs, (void *)&flags, (void *)&err};
     ++g_kernel_launches;
