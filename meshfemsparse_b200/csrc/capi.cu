@@ -317,7 +317,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             const idx s = S.level_list[k];
             const idx nsb = (S.w[s] + SBk - 1) / SBk;
             sb_flag[s] = nsbflags;
-            nsbflags += int(nsb);
+            nsbflags += 2 * int(nsb);
             sb_inv[s] = inv_end;
             for (idx K = 0; K < nsb; ++K) {
                 const idx nr = std::min(SBk, S.w[s] - K * SBk), nrp = (nr + 63) & ~idx(63);
@@ -326,7 +326,10 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             }
         }
     // every superblock before a front's last is full (SB x SB)
-    auto sb_task = [&](idx s, idx K) { return SbTask{int32_t(s), int32_t(K), sb_flag[s], 0, sb_inv[s] + K * SBk * SBk}; };
+    auto sb_task = [&](idx s, idx K, idx part) {
+        return SbTask{int32_t(s), int32_t(K), sb_flag[s], int32_t(part), sb_inv[s] + K * SBk * SBk};
+    };
+    auto sb_parts = [&](idx s, idx K) { return (std::min(SBk, S.w[s] - K * SBk) + 63) / 64; };
     std::vector<SolveAsmTask> sasm;
     std::vector<SolveTask> ftri, btri;
     std::vector<StrTask> fstr, bstr;
@@ -390,8 +393,9 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             }
         L.ftri_n = int(ftri.size()) - L.ftri_off;
         L.btri_n = int(btri.size()) - L.btri_off;
-        // superblock tasks: ascending superblock index across the level's fronts (forward),
-        // descending (backward); every dependency precedes its task
+        // superblock tasks, one per 64-row part: ascending superblock index across the
+        // level's fronts (forward), descending (backward); every dependency precedes
+        // its task and the parts of a superblock are adjacent
         L.fsb_off = int(fsb.size());
         L.bsb_off = int(bsb.size());
         if (l > S.solve_cut) {
@@ -401,13 +405,16 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             for (idx K = 0; K < maxnsb; ++K)
                 for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
                     const idx s = S.level_list[k];
-                    if (K < (S.w[s] + SBk - 1) / SBk) fsb.push_back(sb_task(s, K));
+                    if (K < (S.w[s] + SBk - 1) / SBk)
+                        for (idx part = 0; part < sb_parts(s, K); ++part) fsb.push_back(sb_task(s, K, part));
                 }
             for (idx p = 0; p < maxnsb; ++p)
                 for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
                     const idx s = S.level_list[k];
                     const idx nsb = (S.w[s] + SBk - 1) / SBk;
-                    if (p < nsb) bsb.push_back(sb_task(s, nsb - 1 - p));
+                    if (p < nsb)
+                        for (idx part = 0; part < sb_parts(s, nsb - 1 - p); ++part)
+                            bsb.push_back(sb_task(s, nsb - 1 - p, part));
                 }
         }
         L.fsb_n = int(fsb.size()) - L.fsb_off;
@@ -725,11 +732,14 @@ template <typename T>
 void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) {
     const Symbolic &S = *ds.S;
     cudaStream_t st = h->stream;
-    const int chunk = std::min(nrhs, kMaxSolveRhs);
+    const bool sb = h->opt.solve_chain != 1;
+    const int pass = sb ? kSbMaxRhs : kMaxSolveRhs;
+    const int chunk = std::min(nrhs, pass);
     h->sol.ensure(size_t(std::max<idx>(S.sol_size, 1)) * chunk);
     h->str_partials.ensure(size_t(std::max(ds.max_str_tasks, 1)) * solve_rows_per_task() * chunk);
-    for (int r0 = 0; r0 < nrhs; r0 += kMaxSolveRhs) {
-        const int nr = std::min(kMaxSolveRhs, nrhs - r0);
+    if (sb) h->sb_scratch.ensure(size_t(std::max<idx>(S.n, 1)) * chunk);
+    for (int r0 = 0; r0 < nrhs; r0 += pass) {
+        const int nr = std::min(pass, nrhs - r0);
         double *Xc = X + int64_t(r0) * S.n;
         MFS_CUDA(cudaMemsetAsync(ds.flags.p, 0, ds.flags.bytes(), st));
         // levels <= solve_cut: whole subtrees, one per CTA
@@ -739,12 +749,12 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
             const LevelPlan &L = ds.levels[l];
             launch_fwd_asm(ds.sasm_tasks.p + L.sasm_off, L.sasm_n, L.sasm_tiles, ds.sd, Xc, S.n, nr, h->sol.p, st);
             MFS_LAUNCHED();
-            if (h->opt.solve_chain == 1)
+            if (!sb)
                 MFS_CUDA(launch_diag<T>(true, ds.ftri_tasks.p + L.ftri_off, L.ftri_n, ds.sd, factor, Xc, S.n, nr,
                                         ds.flags.p, h->solve_err.p, st));
             else
                 MFS_CUDA(launch_sb_solve<T>(true, ds.fsb_tasks.p + L.fsb_off, L.fsb_n, ds.sd, factor, Xc, S.n, nr,
-                                            ds.flags.p, h->solve_err.p, st));
+                                            h->sb_scratch.p, ds.flags.p, h->solve_err.p, st));
             launch_str<T>(true, ds.fstr_tasks.p + L.fstr_off, L.fstr_n, ds.fred.p + L.fred_off, L.fred_n, ds.sd,
                           factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
             MFS_LAUNCHED();
@@ -754,12 +764,12 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
             launch_str<T>(false, ds.bstr_tasks.p + L.bstr_off, L.bstr_n, ds.bred.p + L.bred_off, L.bred_n, ds.sd,
                           factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
             MFS_LAUNCHED();
-            if (h->opt.solve_chain == 1)
+            if (!sb)
                 MFS_CUDA(launch_diag<T>(false, ds.btri_tasks.p + L.btri_off, L.btri_n, ds.sd, factor, Xc, S.n, nr,
                                         ds.flags.p, h->solve_err.p, st));
             else
                 MFS_CUDA(launch_sb_solve<T>(false, ds.bsb_tasks.p + L.bsb_off, L.bsb_n, ds.sd, factor, Xc, S.n, nr,
-                                            ds.flags.p, h->solve_err.p, st));
+                                            h->sb_scratch.p, ds.flags.p, h->solve_err.p, st));
         }
         launch_subtree_solve<T>(false, ds.subs.p, ds.nsub, ds.sub_fmax, ds.sd, factor, Xc, S.n, nr, h->sol.p, st);
         MFS_LAUNCHED();

@@ -150,10 +150,11 @@ struct StrTask {
 struct StrReduce {
     int32_t sn, idx, first, nchunks;
 };
-// One superblock of a front's L11 in the diagonal-block solves: a CTA task of the
-// forward / backward chains and of the inverse kernel. inv: factor-array offset of
-// inv(L_KK) (nrp x nrp column-major, nrp = 64 * ceil(rows / 64)); flag0: the front's
-// first superblock flag.
+// One superblock K of a front's L11 in the diagonal-block solves: a CTA task of the
+// inverse kernel (part 0), or of the forward / backward chains for its 64-row part
+// `part`. inv: factor-array offset of inv(L_KK) (nrp x nrp column-major, nrp = 64 *
+// ceil(rows / 64)); flag0: the front's first count (two per superblock: parts
+// solved, parts whose accumulated right-hand side is in the scratch vector).
 struct SbTask {
     int32_t sn, K, flag0, pad;
     int64_t inv;
@@ -162,6 +163,7 @@ constexpr int kSuperBlock = 256;        // rows per superblock
 constexpr int kStrChunk = 512;
 constexpr int kSolveAsmRows = 256;      // front rows per forward extend-add CTA
 constexpr int kMaxSolveRhs = 16;        // right-hand sides per solve pass (more are chunked)
+constexpr int kSbMaxRhs = 8;            // right-hand sides per pass of the superblock solves
 
 constexpr int kAsmCols = 32;            // front columns per assemble CTA
 constexpr int kMaxSmemOptin = 232448;   // opt-in dynamic shared memory per CTA (227 KB)
@@ -225,7 +227,7 @@ void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce 
 // Superblock diagonal solves (cooperative launch) and the superblock inverses they apply.
 template <typename T>
 cudaError_t launch_sb_solve(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
-                            int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st);
+                            int64_t ldx, int nrhs, double *scratch, int *flags, int *err, cudaStream_t st);
 template <typename T>
 void launch_sb_inverse(const SbTask *tasks, int ntasks, SnDev sd, T *factor, cudaStream_t st);
 int solve_rows_per_task();

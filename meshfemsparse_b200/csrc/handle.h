@@ -164,6 +164,7 @@ struct mfs_handle {
     DBuf<double> dscr64;           // inverses of the diagonal blocks of one column-block step
     DBuf<float> dscr32;
     DBuf<double> sol;
+    DBuf<double> sb_scratch;       // accumulated right-hand sides of the superblock solves (n x pass)
     std::shared_ptr<DBuf<double>> asm_ax;   // output of the last mfs_assemble (device resident)
     std::shared_ptr<DBuf<double>> asm_spare;   // an earlier assembly buffer, reused once nothing holds it
     DBuf<double> rhs, work_r, work_z, work_p, work_ap, work_x, work_s, io;

@@ -10,30 +10,36 @@
 // sb_inverse_kernel writes inv(L_KK) of every superblock K of every front above
 // the solve cut (dense, column-major, nrp x nrp with nrp = 64 * ceil(rows / 64),
 // zeros above the diagonal), built from the 64 x 64 diagonal inverses by block
-// forward substitution. A solve task is one superblock of one front, run by one
-// CTA:
-//   forward   acc = b_K - sum_{J < K} L_KJ y_J   (waiting on superblock J's flag),
-//             y_K = inv(L_KK) acc, publish (one thread per row);
-//   backward  acc = y_K - sum_{J > K} L_JK^T x_J (J descending),
-//             x_K = inv(L_KK)^T acc, publish (one warp per column, shuffle sums).
-// L and the inverse stream through shared memory in 32 KB chunks of whole columns
-// (256 rows x 32 FP32 / 16 FP64 columns; the inverse's rows above a chunk's first
-// column are zero and skipped): one thread issues a bulk copy per column, the
-// chunk completes on its ring slot's mbarrier, and up to six chunks are in flight,
-// so the chunks of the next dependency are already on chip when its flag comes.
-// Bulk copies of a superblock's rows are rounded up to 64 rows; the extra rows lie
-// inside the factor array (the next rows or column of the panel, or the inverses
-// stored after the panels) and are never used.
-// The chain thus takes one flag hop, one superblock-wide product and one
-// inverse product per 256 rows. Launches are cooperative (all CTAs co-resident);
-// every CTA walks its tasks in ascending order and a task waits only on
-// lower-numbered tasks of its front, so the lowest unfinished task can always
-// proceed. Waits are bounded in time: on expiry the kernel records an error and
+// forward substitution.
+//
+// A solve task is one 64-row part h of superblock K of one front, run by one CTA;
+// the (up to) four parts of a superblock run side by side:
+//   forward   a_h = b_h - sum_{J < K} L(rows h, superblock J) y_J (J ascending, as
+//             J's count reaches its part count), a_h to a scratch vector, count;
+//             once every part of K has counted, y_h = inv(L_KK)(rows h, :) a_K, count;
+//   backward  a_h = y_h - sum_{J > K} L(superblock J, columns h)^T x_J (J
+//             descending), then x_h = inv(L_KK)(:, columns h)^T a_K the same way.
+// A superblock thus costs two hops between CTAs and two 64 x 256 products on the
+// chain, and what a task reads after its last dependency arrives (64 x 256 of L
+// and at most 64 x 256 of the inverse) is already on chip: L and the inverse
+// stream through shared memory in 32 KB chunks (64 rows x 128 FP32 / 64 FP64
+// columns forward, 128 / 64 rows x 64 columns backward), one bulk copy per
+// column issued by one thread, completing on the ring slot's mbarrier, up to six
+// chunks in flight. Bulk copies of the last superblock's rows are rounded up to
+// 64 rows; the extra rows lie inside the factor array (the next column of the
+// panel) and are masked out of every product.
+//
+// Launches are cooperative (all CTAs co-resident); every CTA walks its tasks in
+// ascending order and a task waits only on lower-numbered tasks and on the other
+// parts of its own superblock (adjacent task numbers, so on other CTAs), hence
+// the lowest unfinished task can always proceed. Counts are zeroed before each
+// solve: forward targets are the superblock's part count, backward ones twice
+// that. Waits are bounded in time: on expiry the kernel records an error and
 // stops waiting; the host reports MFS_TIMEOUT. Sums run in a fixed order, so
 // results are run-to-run identical. With an FP32 factor (the preconditioner of
-// FP64 refinement) the products with off-diagonal superblocks are FP32 (chunk
-// results accumulated in FP64) and the inverse of the diagonal superblock is
-// applied in FP64; an FP64 factor keeps FP64 throughout.
+// FP64 refinement) the products with off-diagonal superblocks are FP32
+// (accumulated per thread over the task, combined in FP64) and the inverse of the
+// diagonal superblock is applied in FP64; an FP64 factor keeps FP64 throughout.
 #include "device.h"
 
 #include <algorithm>
@@ -45,7 +51,6 @@ namespace {
 
 constexpr int SB = kSuperBlock;
 constexpr int kSbThreads = 256;
-constexpr int kRG = 8;                                    // right-hand sides per register group
 constexpr unsigned long long kWaitNs = 2000000000ull;    // 2 s per wait at most
 static_assert(SB == kSbThreads, "one thread per superblock row");
 
@@ -78,55 +83,27 @@ __device__ __forceinline__ void wait_flag(const int *flag, int epoch, int *err) 
     }
     __syncthreads();
 }
-__device__ __forceinline__ void cpa16(void *dst_smem, const void *src, int bytes) {
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cpa_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Stage `ncols` columns of a column-major source (leading dimension lds), rows
-// [row0, row0 + ncopy) of each (ncopy a multiple of 16 bytes), into dst with
-// element (i, j) at dst[j * ldd + i]; rows at or past row0 + nvalid are zero-filled.
-template <typename T>
-__device__ __forceinline__ void stage_cols(T *dst, int ldd, const T *src, int64_t lds, int row0, int nvalid,
-                                           int ncopy, int ncols) {
-    constexpr int E = 16 / int(sizeof(T));
-    const int nch = ncopy / E;
-    const int tot = nch * ncols;
-    for (int q = threadIdx.x; q < tot; q += blockDim.x) {
-        const int j = q / nch, c = q - j * nch;
-        const int i = c * E;
-        const int nv = max(0, min(E, nvalid - i));
-        const T *s = src + int64_t(j) * lds + row0 + i;
-        cpa16(dst + j * ldd + i, nv ? s : src, nv * int(sizeof(T)));
-    }
-}
-
 // Product type of the off-diagonal chunk sums: FP32 for an FP32 factor, FP64 otherwise.
 template <typename T>
 using PT = std::conditional_t<sizeof(T) == 4, float, double>;
 
-// Chunks of 32 KB: CW whole columns (SB rows) of L or of the inverse, column-major in
-// shared memory with leading dimension SB, streamed through an NST-deep ring of bulk
-// copies (one per column) that complete on the slot's mbarrier.
+// Chunks of 32 KB: forward 64 rows x FC columns (column-major, ld 64), backward
+// FC rows x 64 columns (column-major, ld FC).
 template <typename T>
-struct SbChunk {
-    static constexpr int CW = 32768 / (SB * int(sizeof(T)));   // 32 columns (FP32), 16 (FP64)
-    static constexpr int BYTES = CW * SB * int(sizeof(T));
+struct SpChunk {
+    static constexpr int FC = 32768 / (64 * int(sizeof(T)));   // 128 (FP32), 64 (FP64)
+    static constexpr int ELEMS = 64 * FC;
+    static constexpr int BYTES = ELEMS * int(sizeof(T));
 };
-template <typename T, int NST>
-struct SbLayout {
-    // doubles: acc[nrhs][SB] | out[nrhs][SB] | vec[nrhs][SB]; PT copy of vec [nrhs][SB]; ring
-    static __host__ __device__ constexpr size_t ring_off(int nrhs) {
-        return (size_t(3) * nrhs * SB * sizeof(double) + size_t(nrhs) * SB * sizeof(PT<T>) + 127) & ~size_t(127);
-    }
-    static __host__ __device__ constexpr size_t bytes(int nrhs) {
-        return ring_off(nrhs) + size_t(NST) * SbChunk<T>::BYTES;
-    }
+// Shared memory: ring [NST][32 KB] | vec [NR][SB] doubles | vp [NR][SB] products' type
+// | red [4][NR][64] doubles | own [NR][64] doubles.
+template <typename T, int NST, int NR>
+struct SpLayout {
+    static constexpr size_t vec_off = size_t(NST) * SpChunk<T>::BYTES;
+    static constexpr size_t vp_off = vec_off + size_t(NR) * SB * sizeof(double);
+    static constexpr size_t red_off = vp_off + size_t(NR) * SB * sizeof(PT<T>);
+    static constexpr size_t own_off = red_off + size_t(4) * NR * 64 * sizeof(double);
+    static constexpr size_t bytes = own_off + size_t(NR) * 64 * sizeof(double);
 };
 
 // Rows of superblock K of a front with w columns, and its 64-rounded extent.
@@ -177,15 +154,15 @@ __device__ __forceinline__ void bulk_copy(uint32_t dst, const void *src, uint32_
 }
 // One thread: ncols columns of a column-major source (leading dimension lds), rows
 // [row0, row0 + nrows) of each (16-byte aligned, a multiple of 16 bytes), to
-// dst + j * SB elements, completing on `bar`.
+// dst + j * ldd elements, completing on `bar`.
 template <typename T>
-__device__ __forceinline__ void stage_bulk(T *dst, const T *src, int64_t lds, int row0, int nrows, int ncols,
-                                           uint32_t bar) {
+__device__ __forceinline__ void stage_bulk(T *dst, int ldd, const T *src, int64_t lds, int row0, int nrows,
+                                           int ncols, uint32_t bar) {
     const uint32_t bytes = uint32_t(nrows) * sizeof(T);
     mbar_expect_tx(bar, bytes * uint32_t(ncols));
     const uint32_t d0 = smem_u32(dst);
     for (int j = 0; j < ncols; ++j)
-        bulk_copy(d0 + uint32_t(j) * SB * sizeof(T), src + int64_t(j) * lds + row0, bytes, bar);
+        bulk_copy(d0 + uint32_t(j) * uint32_t(ldd) * sizeof(T), src + int64_t(j) * lds + row0, bytes, bar);
 }
 
 // After an error (a wait that gave up), the copies a CTA issued may still be in
@@ -204,77 +181,54 @@ __device__ __forceinline__ void ring_drain(uint64_t *bars, long long issued, con
     }
 }
 
-// Row mode (forward): this thread's row (chunk row trow), dst[r * SB] -/+=
-// sum_j tl[j * SB + trow] v[r * SB + j], j < ncol, for the NR right-hand sides.
-template <typename Q, int NR, typename T>
-__device__ __forceinline__ void row_chunk(const T *tl, int trow, const Q *v, int ncol, int nrhs, double *dst,
-                                          bool sub) {
-    Q p[NR];
-#pragma unroll
-    for (int u = 0; u < NR; ++u) p[u] = Q(0);
-#pragma unroll 8
-    for (int j = 0; j < ncol; ++j) {
-        const Q a = Q(tl[j * SB + trow]);
-#pragma unroll
-        for (int u = 0; u < NR; ++u) p[u] += a * v[u * SB + j];
-    }
-#pragma unroll
-    for (int u = 0; u < NR; ++u)
-        if (u < nrhs) {
-            if (sub) dst[u * SB] -= double(p[u]);
-            else dst[u * SB] += double(p[u]);
-        }
-}
-// Column mode (backward): one warp per column j of the chunk (columns warp, warp + 8,
-// ...): s_r = sum_{i < nrow} tl[j * SB + i] v[r * SB + i] over the lanes, reduced by
-// shuffles; lane 0 applies dst[r * SB + j] -= s_r (mode 0) or = s_r (mode 1).
-template <typename Q, int NR, typename T>
-__device__ __forceinline__ void col_chunk(const T *tl, const Q *v, int nrow, int ncol, int nrhs, double *dst,
-                                          int mode) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int j = warp; j < ncol; j += nw) {
-        const T *col = tl + j * SB;
-        Q p[NR];
-#pragma unroll
-        for (int u = 0; u < NR; ++u) p[u] = Q(0);
-        for (int i = lane; i < nrow; i += 32) {
-            const Q a = Q(col[i]);
-#pragma unroll
-            for (int u = 0; u < NR; ++u) p[u] += a * v[u * SB + i];
-        }
-#pragma unroll
-        for (int u = 0; u < NR; ++u) {
-            Q g = p[u];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) g += __shfl_down_sync(0xffffffffu, g, o);
-            if (lane == 0 && u < nrhs) {
-                if (mode == 0) dst[u * SB + j] -= double(g);
-                else dst[u * SB + j] = double(g);
+// Thread 0 waits until the count at p reaches target (bounded), then the block proceeds.
+__device__ __forceinline__ void wait_count(const int *p, int target, int *err) {
+    if (threadIdx.x == 0) {
+        if (ld_acquire(p) < target) {
+            const unsigned long long t0 = gtimer();
+            while (ld_acquire(p) < target) {
+                if (*(volatile int *)err) break;
+                if (gtimer() - t0 > kWaitNs) {
+                    atomicExch(err, 1);
+                    break;
+                }
             }
         }
     }
+    __syncthreads();
+}
+// After a __syncthreads that follows this block's writes: publish them and count.
+__device__ __forceinline__ void count_up(int *p) {
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(p, 1);
+    }
 }
 
-// Vectors hold NR right-hand sides (columns >= nrhs are zero), so the products above
-// run without predicates.
+// Forward task (s, K, h = tk.pad): rows R0 = K SB + 64 h, nrh of them. Chunks: for
+// J < K, L(rows R0.., columns J SB + c FC ..) (c < SB / FC), then the inverse's
+// rows 64 h.. of columns [c FC, c FC + FC) up to column 64 h + 63 (the rest of
+// the row is zero). Thread (i = tid % 64, part = tid / 64) sums columns
+// [part FC / 4, (part + 1) FC / 4) of every chunk for row i.
 template <typename T, int NST, int NR>
-__global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
+__global__ void __launch_bounds__(kSbThreads, 1) sp_fwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
                                                                SnDev sd, const T *__restrict__ factor,
                                                                double *__restrict__ X, int64_t ldx, int nrhs,
-                                                               int *__restrict__ flags, int *__restrict__ err) {
-    using L = SbLayout<T, NST>;
+                                                               double *__restrict__ scratch, int *__restrict__ flags,
+                                                               int *__restrict__ err) {
+    using Lay = SpLayout<T, NST, NR>;
     using P = PT<T>;
-    constexpr int CW = SbChunk<T>::CW;
-    constexpr int BUF = CW * SB;
-    constexpr int per = SB / CW;                         // chunks per earlier superblock
-    extern __shared__ __align__(128) double sb_smem[];
+    constexpr int FC = SpChunk<T>::FC, CE = SpChunk<T>::ELEMS;
+    constexpr int per = SB / FC;                         // chunks per earlier superblock
+    constexpr int QC = FC / 4;
+    extern __shared__ __align__(128) unsigned char sp_raw[];
     __shared__ __align__(8) uint64_t bars[NST];
-    double *acc = sb_smem;
-    double *out = acc + NR * SB;
-    double *vec = out + NR * SB;
-    P *vp = reinterpret_cast<P *>(vec + NR * SB);
-    T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sb_smem) + L::ring_off(NR));
-    const int tid = threadIdx.x;
+    T *ring = reinterpret_cast<T *>(sp_raw);
+    double *vec = reinterpret_cast<double *>(sp_raw + Lay::vec_off);
+    P *vp = reinterpret_cast<P *>(sp_raw + Lay::vp_off);
+    double *red = reinterpret_cast<double *>(sp_raw + Lay::red_off);
+    double *own = reinterpret_cast<double *>(sp_raw + Lay::own_off);
+    const int tid = threadIdx.x, i = tid & 63, part = tid >> 6;
     if (tid == 0) {
         for (int b = 0; b < NST; ++b) mbar_init(smem_u32(&bars[b]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -283,93 +237,140 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_fwd_kernel(const SbTask *__r
     long long gq = 0;                                    // chunks this CTA has consumed (ring phase)
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SbTask tk = tasks[t];
-        const int s = tk.sn, K = tk.K;
+        const int s = tk.sn, K = tk.K, h = tk.pad;
         const int w = sd.w[s], ld = sd.ld[s], c0 = sd.col0[s];
         const T *pan = factor + sd.pan_off[s];
         const T *inv = factor + tk.inv;
-        const int nr = sb_rows(w, K), nrp = sb_pad(nr);
-        const int r0 = K * SB;
-        const int ninv = (nrp + CW - 1) / CW;            // column chunks of the inverse
-        const int nq = K * per + ninv;
-        // chunk q: L(rows of K, CW columns of superblock J = q / per), or the inverse's
-        // columns [c CW, c CW + CW) with their rows from c CW on (the rest is zero)
+        const int nrK = sb_rows(w, K), nrpK = sb_pad(nrK), nhK = nrpK / 64;
+        const int R0 = K * SB + h * 64, nrh = min(64, w - R0);
+        const int icols = (h + 1) * 64;                  // nonzero columns of the inverse's rows
+        const int ndep = K * per;
+        const int nq = ndep + (icols + FC - 1) / FC;
+        int *ycnt = flags + tk.flag0;                    // [2 J]: parts of J done, [2 J + 1]: a_J parts
         auto stage = [&](int q) {
             const int slot = int((gq + q) % NST);
-            T *dst = ring + slot * BUF;
+            T *dst = ring + slot * CE;
             const uint32_t bar = smem_u32(&bars[slot]);
-            if (q < K * per) {
+            if (q < ndep) {
                 const int J = q / per, c = q - J * per;
-                stage_bulk<T>(dst, pan + int64_t(J * SB + c * CW) * ld, ld, r0, nrp, CW, bar);
+                stage_bulk<T>(dst, 64, pan + int64_t(J * SB + c * FC) * ld, ld, R0, 64, FC, bar);
             } else {
-                const int c = q - K * per;
-                stage_bulk<T>(dst, inv + int64_t(c * CW) * nrp, nrp, c * CW, nrp - c * CW, min(CW, nrp - c * CW),
-                              bar);
+                const int c = q - ndep;
+                stage_bulk<T>(dst, 64, inv + int64_t(c * FC) * nrpK, nrpK, h * 64, 64, min(FC, icols - c * FC), bar);
             }
         };
         __syncthreads();                                 // the previous task is done with shared memory
         if (tid == 0)
             for (int q = 0; q < NST - 1 && q < nq; ++q) stage(q);
+        if (tid < 64)
+            for (int r = 0; r < NR; ++r) own[r * 64 + i] = (r < nrhs && i < nrh) ? X[c0 + R0 + i + r * ldx] : 0.0;
+        P pacc[NR];
+        double dacc[NR];
+#pragma unroll
         for (int r = 0; r < NR; ++r) {
-            acc[r * SB + tid] = (r < nrhs && tid < nr) ? X[c0 + r0 + tid + r * ldx] : 0.0;
-            out[r * SB + tid] = 0.0;
+            pacc[r] = P(0);
+            dacc[r] = 0.0;
         }
-        for (int q = 0; q < nq; ++q) {
+        auto chunk = [&](int q) -> const T * {
+            const int slot = int((gq + q) % NST);
+            mbar_wait_all(smem_u32(&bars[slot]), uint32_t(((gq + q) / NST) & 1), err);
+            __syncthreads();                             // (also: vectors are complete)
+            return ring + slot * CE;
+        };
+        for (int q = 0; q < ndep; ++q) {
             if (tid == 0 && q + NST - 1 < nq) stage(q + NST - 1);
-            const bool lpart = q < K * per;
-            const int J = lpart ? q / per : K, c = lpart ? q - J * per : q - K * per;
-            if (lpart && c == 0) {
-                // y_J: wait for its superblock, then load it (written by another CTA: through L2)
-                wait_flag(flags + tk.flag0 + J, 1, err);
+            const int J = q / per, c = q - J * per;
+            if (c == 0) {
+                // y_J: wait for its parts, then load it (written by other CTAs: through L2)
+                wait_count(ycnt + 2 * J, SB / 64, err);
+#pragma unroll
                 for (int r = 0; r < NR; ++r) {
                     const double v = r < nrhs ? __ldcg(&X[c0 + J * SB + tid + r * ldx]) : 0.0;
                     vec[r * SB + tid] = v;
                     vp[r * SB + tid] = P(v);
                 }
             }
-            const int slot = int((gq + q) % NST);
-            mbar_wait_all(smem_u32(&bars[slot]), uint32_t(((gq + q) / NST) & 1), err);
-            __syncthreads();                             // (also: vectors and acc are complete)
-            const T *tl = ring + slot * BUF;
-            if (lpart) {
-                // off-diagonal superblock: products of the factor's precision
-                if (tid < nr) row_chunk<P, NR>(tl, tid, vp + c * CW, CW, nrhs, acc + tid, true);
-            } else if (tid < nr && tid >= c * CW) {
-                // inverse of the diagonal superblock (rows from c CW): FP64 products
-                row_chunk<double, NR>(tl, tid - c * CW, acc + c * CW, min(CW, nrp - c * CW), nrhs, out + tid,
-                                      false);
+            const T *a = chunk(q) + part * QC * 64 + i;
+            const P *v = vp + c * FC + part * QC;
+#pragma unroll 8
+            for (int j = 0; j < QC; ++j) {
+                const P l = P(a[j * 64]);
+#pragma unroll
+                for (int r = 0; r < NR; ++r) pacc[r] += l * v[r * SB + j];
             }
             __syncthreads();                             // the ring slot is refilled NST - 1 chunks later
         }
-        gq += nq;
-        if (tid < nr)
-            for (int r = 0; r < nrhs; ++r) X[c0 + r0 + tid + r * ldx] = out[r * SB + tid];
+        // every dependency is in: a_h = own - sums, to the scratch vector; count, wait
+        // for the other parts of K, load a_K
+#pragma unroll
+        for (int r = 0; r < NR; ++r) red[(part * NR + r) * 64 + i] = double(pacc[r]);
         __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            st_release(flags + tk.flag0 + K, 1);
+        if (tid < 64)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const int e = r * 64 + i;
+                const double a = own[e] - (((red[e] + red[NR * 64 + e]) + red[2 * NR * 64 + e]) + red[3 * NR * 64 + e]);
+                if (r < nrhs && i < nrh) scratch[c0 + R0 + i + r * ldx] = a;
+            }
+        __syncthreads();
+        count_up(ycnt + 2 * K + 1);
+        wait_count(ycnt + 2 * K + 1, nhK, err);
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            vec[r * SB + tid] = (r < nrhs && tid < nrK) ? __ldcg(&scratch[c0 + K * SB + tid + r * ldx]) : 0.0;
+        for (int q = ndep; q < nq; ++q) {
+            if (tid == 0 && q + NST - 1 < nq) stage(q + NST - 1);
+            const int c = q - ndep;
+            const int j0 = part * QC, j1 = min(QC, min(FC, icols - c * FC) - j0);
+            const T *a = chunk(q) + j0 * 64 + i;
+            const double *v = vec + c * FC + j0;
+            for (int j = 0; j < j1; ++j) {
+                const double l = double(a[j * 64]);
+#pragma unroll
+                for (int r = 0; r < NR; ++r) dacc[r] += l * v[r * SB + j];
+            }
+            __syncthreads();
         }
+        gq += nq;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) red[(part * NR + r) * 64 + i] = dacc[r];
+        __syncthreads();
+        if (tid < 64)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const int e = r * 64 + i;
+                const double y = ((red[e] + red[NR * 64 + e]) + red[2 * NR * 64 + e]) + red[3 * NR * 64 + e];
+                if (r < nrhs && i < nrh) X[c0 + R0 + i + r * ldx] = y;
+            }
+        __syncthreads();
+        count_up(ycnt + 2 * K);
     }
     ring_drain<NST>(bars, gq, err);
 }
 
+// Backward task (s, K, h = tk.pad): columns C0 = K SB + 64 h, nch of them. Chunks:
+// for J = nsb - 1 down to K + 1, L(rows J SB + c FC .., columns C0..) (the last
+// superblock's rows rounded up to 64), then the inverse's columns 64 h.. from row
+// 64 h + c FC on. Warp wp sums columns 8 wp .. 8 wp + 7 of every chunk, its lanes
+// over the chunk's rows.
 template <typename T, int NST, int NR>
-__global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
+__global__ void __launch_bounds__(kSbThreads, 1) sp_bwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
                                                                SnDev sd, const T *__restrict__ factor,
                                                                double *__restrict__ X, int64_t ldx, int nrhs,
-                                                               int *__restrict__ flags, int *__restrict__ err) {
-    using L = SbLayout<T, NST>;
+                                                               double *__restrict__ scratch, int *__restrict__ flags,
+                                                               int *__restrict__ err) {
+    using Lay = SpLayout<T, NST, NR>;
     using P = PT<T>;
-    constexpr int CW = SbChunk<T>::CW;
-    constexpr int BUF = CW * SB;
-    constexpr int per = SB / CW;                         // column chunks per later superblock
-    extern __shared__ __align__(128) double sb_smem[];
+    constexpr int FC = SpChunk<T>::FC, CE = SpChunk<T>::ELEMS;
+    constexpr int per = SB / FC;                         // chunks per full later superblock
+    constexpr int RL = FC / 32;                          // chunk rows per lane
+    extern __shared__ __align__(128) unsigned char sp_raw[];
     __shared__ __align__(8) uint64_t bars[NST];
-    double *acc = sb_smem;
-    double *out = acc + NR * SB;
-    double *vec = out + NR * SB;
-    P *vp = reinterpret_cast<P *>(vec + NR * SB);
-    T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sb_smem) + L::ring_off(NR));
-    const int tid = threadIdx.x;
+    T *ring = reinterpret_cast<T *>(sp_raw);
+    double *vec = reinterpret_cast<double *>(sp_raw + Lay::vec_off);
+    P *vp = reinterpret_cast<P *>(sp_raw + Lay::vp_off);
+    double *own = reinterpret_cast<double *>(sp_raw + Lay::own_off);
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
     if (tid == 0) {
         for (int b = 0; b < NST; ++b) mbar_init(smem_u32(&bars[b]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -378,80 +379,159 @@ __global__ void __launch_bounds__(kSbThreads, 1) sb_bwd_kernel(const SbTask *__r
     long long gq = 0;
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SbTask tk = tasks[t];
-        const int s = tk.sn, K = tk.K;
+        const int s = tk.sn, K = tk.K, h = tk.pad;
         const int w = sd.w[s], ld = sd.ld[s], c0 = sd.col0[s];
         const T *pan = factor + sd.pan_off[s];
         const T *inv = factor + tk.inv;
-        const int nr = sb_rows(w, K), nrp = sb_pad(nr);
-        const int r0 = K * SB;
         const int nsb = (w + SB - 1) / SB;
-        // chunk q: for J = nsb - 1 down to K + 1, L(rows of J, columns [r0 + c CW, + CW)
-        // of K) (K is not the last superblock then, so its SB columns are whole); then
-        // the inverse's columns [c CW, + CW) with their rows from c CW on
-        const int nql = (nsb - 1 - K) * per;
-        const int ninv = (nrp + CW - 1) / CW;
-        const int nq = nql + ninv;
-        auto jinfo = [&](int q, int &J, int &c) {
-            const int m = q / per;
-            J = nsb - 1 - m;
-            c = q - m * per;
+        const int nrK = sb_rows(w, K), nrpK = sb_pad(nrK), nhK = nrpK / 64;
+        const int C0 = K * SB + h * 64, nch = min(64, w - C0);
+        const int nrl = sb_rows(w, nsb - 1), nql = (sb_pad(nrl) + FC - 1) / FC;   // last superblock
+        const int ndep = K < nsb - 1 ? nql + (nsb - 2 - K) * per : 0;
+        const int irows = nrpK - h * 64;                 // the inverse's rows from 64 h
+        const int nq = ndep + (irows + FC - 1) / FC;
+        int *ycnt = flags + tk.flag0;
+        // dependency chunk q: superblock J, chunk c
+        auto dep = [&](int q, int &J, int &c) {
+            if (q < nql) {
+                J = nsb - 1;
+                c = q;
+            } else {
+                const int m = q - nql;
+                J = nsb - 2 - m / per;
+                c = m % per;
+            }
         };
         auto stage = [&](int q) {
             const int slot = int((gq + q) % NST);
-            T *dst = ring + slot * BUF;
+            T *dst = ring + slot * CE;
             const uint32_t bar = smem_u32(&bars[slot]);
-            if (q < nql) {
+            if (q < ndep) {
                 int J, c;
-                jinfo(q, J, c);
-                stage_bulk<T>(dst, pan + int64_t(r0 + c * CW) * ld, ld, J * SB, sb_pad(sb_rows(w, J)), CW, bar);
+                dep(q, J, c);
+                const int rows = min(FC, sb_pad(sb_rows(w, J)) - c * FC);
+                stage_bulk<T>(dst, FC, pan + int64_t(C0) * ld, ld, J * SB + c * FC, rows, 64, bar);
             } else {
-                const int c = q - nql;
-                stage_bulk<T>(dst, inv + int64_t(c * CW) * nrp, nrp, c * CW, nrp - c * CW, min(CW, nrp - c * CW),
-                              bar);
+                const int c = q - ndep;
+                stage_bulk<T>(dst, FC, inv + int64_t(h * 64) * nrpK, nrpK, h * 64 + c * FC, min(FC, irows - c * FC),
+                              64, bar);
             }
         };
         __syncthreads();
         if (tid == 0)
             for (int q = 0; q < NST - 1 && q < nq; ++q) stage(q);
-        for (int r = 0; r < NR; ++r) {
-            acc[r * SB + tid] = (r < nrhs && tid < nr) ? X[c0 + r0 + tid + r * ldx] : 0.0;
-            out[r * SB + tid] = 0.0;
-        }
-        for (int q = 0; q < nq; ++q) {
-            if (tid == 0 && q + NST - 1 < nq) stage(q + NST - 1);
-            const bool lpart = q < nql;
-            int J = K, c = q - nql;
-            if (lpart) jinfo(q, J, c);
-            const int nrJ = lpart ? sb_rows(w, J) : 0;
-            if (lpart && c == 0) {
-                wait_flag(flags + tk.flag0 + J, 2, err);
-                for (int r = 0; r < NR; ++r) {
-                    const double v = (r < nrhs && tid < nrJ) ? __ldcg(&X[c0 + J * SB + tid + r * ldx]) : 0.0;
-                    vec[r * SB + tid] = v;
-                    vp[r * SB + tid] = P(v);
-                }
-            }
+        if (tid < 64)
+            for (int r = 0; r < NR; ++r)
+                own[r * 64 + tid] = (r < nrhs && tid < nch) ? X[c0 + C0 + tid + r * ldx] : 0.0;
+        auto chunk = [&](int q) -> const T * {
             const int slot = int((gq + q) % NST);
             mbar_wait_all(smem_u32(&bars[slot]), uint32_t(((gq + q) / NST) & 1), err);
-            __syncthreads();                             // (also: vectors and acc are complete)
-            const T *tl = ring + slot * BUF;
-            if (lpart) {
-                // acc(columns of the chunk) -= L(J rows, chunk columns)^T x_J
-                col_chunk<P, NR>(tl, vp, nrJ, CW, nrhs, acc + c * CW, 0);
-            } else {
-                // x(chunk columns) = inv(L_KK)(rows from c CW, chunk columns)^T acc: FP64 products
-                col_chunk<double, NR>(tl, acc + c * CW, nrp - c * CW, min(CW, nrp - c * CW), nrhs, out + c * CW, 1);
+            __syncthreads();
+            return ring + slot * CE;
+        };
+        {
+            P pacc[8][NR];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int r = 0; r < NR; ++r) pacc[u][r] = P(0);
+            for (int q = 0; q < ndep; ++q) {
+                if (tid == 0 && q + NST - 1 < nq) stage(q + NST - 1);
+                int J, c;
+                dep(q, J, c);
+                const int nrJ = sb_rows(w, J);
+                if (c == 0) {
+                    wait_count(ycnt + 2 * J, 2 * (sb_pad(nrJ) / 64), err);
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) {
+                        const double v = (r < nrhs && tid < nrJ) ? __ldcg(&X[c0 + J * SB + tid + r * ldx]) : 0.0;
+                        vec[r * SB + tid] = v;
+                        vp[r * SB + tid] = P(v);
+                    }
+                }
+                const T *tl = chunk(q);
+                // rows of the chunk at or past the superblock's end are masked out
+                const int nv = nrJ - c * FC;
+                const P *v = vp + c * FC;
+#pragma unroll
+                for (int k = 0; k < RL; ++k) {
+                    const int row = lane + 32 * k;
+                    const bool ok = row < nv;
+                    P x[NR];
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) x[r] = ok ? v[r * SB + row] : P(0);
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const P l = ok ? P(tl[(wp * 8 + u) * FC + row]) : P(0);
+#pragma unroll
+                        for (int r = 0; r < NR; ++r) pacc[u][r] += l * x[r];
+                    }
+                }
+                __syncthreads();
+            }
+            __syncthreads();                             // own is complete
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    P g = pacc[u][r];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) g += __shfl_down_sync(0xffffffffu, g, o);
+                    if (lane == 0) own[r * 64 + wp * 8 + u] -= double(g);
+                }
+        }
+        __syncthreads();
+        if (tid < 64)
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs && tid < nch) scratch[c0 + C0 + tid + r * ldx] = own[r * 64 + tid];
+        __syncthreads();
+        count_up(ycnt + 2 * K + 1);
+        wait_count(ycnt + 2 * K + 1, 2 * nhK, err);
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            vec[r * SB + tid] = (r < nrhs && tid < nrK) ? __ldcg(&scratch[c0 + K * SB + tid + r * ldx]) : 0.0;
+        double dacc[8][NR];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) dacc[u][r] = 0.0;
+        for (int q = ndep; q < nq; ++q) {
+            if (tid == 0 && q + NST - 1 < nq) stage(q + NST - 1);
+            const int c = q - ndep;
+            const T *tl = chunk(q);
+            const int nv = min(FC, irows - c * FC);
+            const double *v = vec + h * 64 + c * FC;
+#pragma unroll
+            for (int k = 0; k < RL; ++k) {
+                const int row = lane + 32 * k;
+                if (row < nv) {
+                    double x[NR];
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) x[r] = v[r * SB + row];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const double l = double(tl[(wp * 8 + u) * FC + row]);
+#pragma unroll
+                        for (int r = 0; r < NR; ++r) dacc[u][r] += l * x[r];
+                    }
+                }
             }
             __syncthreads();
         }
         gq += nq;
-        if (tid < nr)
-            for (int r = 0; r < nrhs; ++r) X[c0 + r0 + tid + r * ldx] = out[r * SB + tid];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                double g = dacc[u][r];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) g += __shfl_down_sync(0xffffffffu, g, o);
+                const int col = wp * 8 + u;
+                if (lane == 0 && r < nrhs && col < nch) X[c0 + C0 + col + r * ldx] = g;
+            }
         __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            st_release(flags + tk.flag0 + K, 2);
-        }
+        count_up(ycnt + 2 * K);
     }
     ring_drain<NST>(bars, gq, err);
 }
@@ -561,36 +641,37 @@ int coop_grid(K kernel, size_t smem, int ntasks) {
 
 // NR: the right-hand sides the vectors hold (nrhs <= NR)
 template <typename T, int NST, int NR>
-cudaError_t launch_sb_impl(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
-                           int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st) {
-    using L = SbLayout<T, NST>;
-    static_assert(L::bytes(NR) + 64 <= size_t(kMaxSmemOptin), "superblock solve shared memory");
-    void *kern = forward ? (void *)sb_fwd_kernel<T, NST, NR> : (void *)sb_bwd_kernel<T, NST, NR>;
-    const size_t smem = L::bytes(NR);
+cudaError_t launch_sp_impl(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
+                           int64_t ldx, int nrhs, double *scratch, int *flags, int *err, cudaStream_t st) {
+    using L = SpLayout<T, NST, NR>;
+    static_assert(L::bytes + 64 <= size_t(kMaxSmemOptin), "superblock solve shared memory");
+    void *kern = forward ? (void *)sp_fwd_kernel<T, NST, NR> : (void *)sp_bwd_kernel<T, NST, NR>;
     static PerDeviceOnce once;
     once([] {
-        cudaFuncSetAttribute(sb_fwd_kernel<T, NST, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes(NR)));
-        cudaFuncSetAttribute(sb_bwd_kernel<T, NST, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes(NR)));
+        cudaFuncSetAttribute(sp_fwd_kernel<T, NST, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes));
+        cudaFuncSetAttribute(sp_bwd_kernel<T, NST, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes));
     });
-    const int grid = forward ? coop_grid(sb_fwd_kernel<T, NST, NR>, smem, ntasks)
-                             : coop_grid(sb_bwd_kernel<T, NST, NR>, smem, ntasks);
-    void *args[] = {(void *)&tasks, (void *)&ntasks, (void *)&sd, (void *)&factor, (void *)&X, (void *)&ldx,
-                    (void *)&nrhs, (void *)&flags, (void *)&err};
+    const int grid = forward ? coop_grid(sp_fwd_kernel<T, NST, NR>, L::bytes, ntasks)
+                             : coop_grid(sp_bwd_kernel<T, NST, NR>, L::bytes, ntasks);
+    void *args[] = {(void *)&tasks, (void *)&ntasks,  (void *)&sd,    (void *)&factor, (void *)&X, (void *)&ldx,
+                    (void *)&nrhs,  (void *)&scratch, (void *)&flags, (void *)&err};
     ++g_kernel_launches;
-    return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kSbThreads), args, smem, st);
+    return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kSbThreads), args, L::bytes, st);
 }
 
 }  // namespace
 
 template <typename T>
 cudaError_t launch_sb_solve(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
-                            int64_t ldx, int nrhs, int *flags, int *err, cudaStream_t st) {
+                            int64_t ldx, int nrhs, double *scratch, int *flags, int *err, cudaStream_t st) {
     if (ntasks <= 0) return cudaSuccess;
-    if (nrhs > kMaxSolveRhs) return cudaErrorInvalidValue;
+    if (nrhs > kSbMaxRhs) return cudaErrorInvalidValue;
     // ring depth: the deepest that fits beside the vectors of nrhs right-hand sides
-    if (nrhs <= 4) return launch_sb_impl<T, 6, 4>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
-    if (nrhs <= 8) return launch_sb_impl<T, 4, 8>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
-    return launch_sb_impl<T, 2, kMaxSolveRhs>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, flags, err, st);
+    constexpr int D4 = sizeof(T) == 4 ? 6 : 5, D8 = sizeof(T) == 4 ? 5 : 4;
+    if (nrhs <= 4)
+        return launch_sp_impl<T, D4, 4>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, scratch, flags, err, st);
+    return launch_sp_impl<T, D8, kSbMaxRhs>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, scratch, flags, err,
+                                            st);
 }
 
 template <typename T>
@@ -605,9 +686,9 @@ void launch_sb_inverse(const SbTask *tasks, int ntasks, SnDev sd, T *factor, cud
 }
 
 template cudaError_t launch_sb_solve<float>(bool, const SbTask *, int, SnDev, const float *, double *, int64_t, int,
-                                            int *, int *, cudaStream_t);
+                                            double *, int *, int *, cudaStream_t);
 template cudaError_t launch_sb_solve<double>(bool, const SbTask *, int, SnDev, const double *, double *, int64_t,
-                                             int, int *, int *, cudaStream_t);
+                                             int, double *, int *, int *, cudaStream_t);
 template void launch_sb_inverse<float>(const SbTask *, int, SnDev, float *, cudaStream_t);
 template void launch_sb_inverse<double>(const SbTask *, int, SnDev, double *, cudaStream_t);
 
