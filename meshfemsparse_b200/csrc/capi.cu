@@ -310,6 +310,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     std::vector<SbTask> fsb, bsb, isb;
     std::vector<int32_t> sb_flag(nsn, -1);
     std::vector<int64_t> sb_inv(nsn, -1);
+    std::vector<int32_t> sb_first(nsn, -1);
+    ds->sb_fronts.clear();
     int nsbflags = 0;
     const idx SBk = kSuperBlock;
     for (idx l = S.solve_cut + 1; l < S.nlevels; ++l)
@@ -319,15 +321,22 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             sb_flag[s] = nsbflags;
             nsbflags += 2 * int(nsb);
             sb_inv[s] = inv_end;
+            sb_first[s] = int32_t(isb.size());
+            ds->sb_fronts.push_back(int32_t(s));
             for (idx K = 0; K < nsb; ++K) {
                 const idx nr = std::min(SBk, S.w[s] - K * SBk), nrp = (nr + 63) & ~idx(63);
-                isb.push_back({int32_t(s), int32_t(K), sb_flag[s], 0, inv_end});
+                isb.push_back({int32_t(s), int32_t(K), sb_flag[s], 0, inv_end, -1, -1});
                 inv_end += nrp * nrp;
             }
         }
+    // tensor maps of the solves: two per superblock inverse, then two per front
+    const int32_t nsbm = int32_t(isb.size());
+    std::vector<int32_t> sb_fidx(nsn, -1);
+    for (size_t i = 0; i < ds->sb_fronts.size(); ++i) sb_fidx[ds->sb_fronts[i]] = int32_t(i);
     // every superblock before a front's last is full (SB x SB)
     auto sb_task = [&](idx s, idx K, idx part) {
-        return SbTask{int32_t(s), int32_t(K), sb_flag[s], int32_t(part), sb_inv[s] + K * SBk * SBk};
+        return SbTask{int32_t(s),         int32_t(K), sb_flag[s], int32_t(part), sb_inv[s] + K * SBk * SBk,
+                      2 * (nsbm + sb_fidx[s]), 2 * (sb_first[s] + int32_t(K))};
     };
     auto sb_parts = [&](idx s, idx K) { return (std::min(SBk, S.w[s] - K * SBk) + 63) / 64; };
     std::vector<SolveAsmTask> sasm;
@@ -454,6 +463,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     up(ds->bsb_tasks, bsb);
     up(ds->isb_tasks, isb);
     ds->nsb_inv = int(isb.size());
+    ds->isb_host = isb;
     ds->max_str_tasks = max_str;
     {
         std::vector<int2> sv(S.sub_lo.size());
@@ -533,6 +543,44 @@ void ensure_panel_maps(mfs_handle *h, DevSym &ds, const void *base, bool half) {
     MFS_CUDA(cudaStreamSynchronize(h->stream));
     h->tmaps_base = base;
     h->tmaps_sym = &ds;
+}
+
+// Tensor maps of the superblock solves for the factor array `base` (elements of es
+// bytes): per superblock inverse (nrp x nrp) and per front's L11 (w x w, leading
+// dimension ld), a forward box (64 rows x FC columns) and a backward box (FC rows x
+// 64 columns), FC = 32 KB / (64 es).
+void ensure_solve_maps(mfs_handle *h, DevSym &ds, const void *base, int es) {
+    if (h->smaps_base == base && h->smaps_sym == &ds && h->smaps_es == es) return;
+    const Symbolic &S = *ds.S;
+    const uint32_t FC = uint32_t(32768 / (64 * es));
+    const size_t nb = ds.isb_host.size(), nf = ds.sb_fronts.size();
+    std::vector<TensorMapBlob> maps(std::max<size_t>(2 * (nb + nf), 1));
+    std::memset(maps.data(), 0, maps.size() * sizeof(TensorMapBlob));
+    const char *b = static_cast<const char *>(base);
+    bool ok = true;
+    for (size_t i = 0; i < nb && ok; ++i) {
+        const SbTask &t = ds.isb_host[i];
+        const idx nr = std::min<idx>(kSuperBlock, S.w[t.sn] - idx(t.K) * kSuperBlock);
+        const uint64_t nrp = uint64_t((nr + 63) & ~idx(63));
+        const void *p = b + size_t(t.inv) * es;
+        ok = encode_plain_map(&maps[2 * i], p, es, nrp, nrp, nrp, 64, FC) &&
+             encode_plain_map(&maps[2 * i + 1], p, es, nrp, nrp, nrp, FC, 64);
+    }
+    for (size_t i = 0; i < nf && ok; ++i) {
+        const int32_t s = ds.sb_fronts[i];
+        const void *p = b + size_t(ds.dpan[s]) * es;
+        const uint64_t w = uint64_t(S.w[s]), ld = uint64_t(ds.dld[s]);
+        ok = encode_plain_map(&maps[2 * (nb + i)], p, es, w, w, ld, 64, FC) &&
+             encode_plain_map(&maps[2 * (nb + i) + 1], p, es, w, w, ld, FC, 64);
+    }
+    if (!ok) throw StatusError(MFS_INTERNAL, "cuTensorMapEncodeTiled refused a solve tensor map");
+    h->smaps.ensure(maps.size());
+    MFS_CUDA(cudaMemcpyAsync(h->smaps.p, maps.data(), maps.size() * sizeof(TensorMapBlob), cudaMemcpyHostToDevice,
+                             h->stream));
+    MFS_CUDA(cudaStreamSynchronize(h->stream));
+    h->smaps_base = base;
+    h->smaps_sym = &ds;
+    h->smaps_es = es;
 }
 
 template <typename T>
@@ -737,7 +785,10 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
     const int chunk = std::min(nrhs, pass);
     h->sol.ensure(size_t(std::max<idx>(S.sol_size, 1)) * chunk);
     h->str_partials.ensure(size_t(std::max(ds.max_str_tasks, 1)) * solve_rows_per_task() * chunk);
-    if (sb) h->sb_scratch.ensure(size_t(std::max<idx>(S.n, 1)) * chunk);
+    if (sb) {
+        h->sb_scratch.ensure(size_t(std::max<idx>(S.n, 1)) * chunk);
+        ensure_solve_maps(h, ds, factor, int(sizeof(T)));
+    }
     for (int r0 = 0; r0 < nrhs; r0 += pass) {
         const int nr = std::min(pass, nrhs - r0);
         double *Xc = X + int64_t(r0) * S.n;
@@ -753,7 +804,7 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
                 MFS_CUDA(launch_diag<T>(true, ds.ftri_tasks.p + L.ftri_off, L.ftri_n, ds.sd, factor, Xc, S.n, nr,
                                         ds.flags.p, h->solve_err.p, st));
             else
-                MFS_CUDA(launch_sb_solve<T>(true, ds.fsb_tasks.p + L.fsb_off, L.fsb_n, ds.sd, factor, Xc, S.n, nr,
+                MFS_CUDA(launch_sb_solve<T>(true, ds.fsb_tasks.p + L.fsb_off, L.fsb_n, ds.sd, factor, h->smaps.p, Xc, S.n, nr,
                                             h->sb_scratch.p, ds.flags.p, h->solve_err.p, st));
             launch_str<T>(true, ds.fstr_tasks.p + L.fstr_off, L.fstr_n, ds.fred.p + L.fred_off, L.fred_n, ds.sd,
                           factor, Xc, S.n, nr, h->sol.p, h->str_partials.p, st);
@@ -768,7 +819,7 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
                 MFS_CUDA(launch_diag<T>(false, ds.btri_tasks.p + L.btri_off, L.btri_n, ds.sd, factor, Xc, S.n, nr,
                                         ds.flags.p, h->solve_err.p, st));
             else
-                MFS_CUDA(launch_sb_solve<T>(false, ds.bsb_tasks.p + L.bsb_off, L.bsb_n, ds.sd, factor, Xc, S.n, nr,
+                MFS_CUDA(launch_sb_solve<T>(false, ds.bsb_tasks.p + L.bsb_off, L.bsb_n, ds.sd, factor, h->smaps.p, Xc, S.n, nr,
                                             h->sb_scratch.p, ds.flags.p, h->solve_err.p, st));
         }
         launch_subtree_solve<T>(false, ds.subs.p, ds.nsub, ds.sub_fmax, ds.sd, factor, Xc, S.n, nr, h->sol.p, st);

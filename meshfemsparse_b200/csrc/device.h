@@ -152,12 +152,15 @@ struct StrReduce {
 };
 // One superblock K of a front's L11 in the diagonal-block solves: a CTA task of the
 // inverse kernel (part 0), or of the forward / backward chains for its 64-row part
-// `part`. inv: factor-array offset of inv(L_KK) (nrp x nrp column-major, nrp = 64 *
+// `pad`. inv: factor-array offset of inv(L_KK) (nrp x nrp column-major, nrp = 64 *
 // ceil(rows / 64)); flag0: the front's first count (two per superblock: parts
-// solved, parts whose accumulated right-hand side is in the scratch vector).
+// solved, parts whose accumulated right-hand side is in the scratch vector);
+// pmap / imap: the first of the two tensor maps (forward box, backward box) of the
+// front's L11 / of inv(L_KK) in the solve's map array.
 struct SbTask {
     int32_t sn, K, flag0, pad;
     int64_t inv;
+    int32_t pmap, imap;
 };
 constexpr int kSuperBlock = 256;        // rows per superblock
 constexpr int kStrChunk = 512;
@@ -207,6 +210,11 @@ void launch_gemm_tma(bool half, const GemmTask *tasks, int ntasks, int ntiles, c
 // base 16-byte aligned, ld * element size a multiple of 16) in the box and swizzle
 // form of the TMA-fed GEMM; false if the driver refuses it.
 bool encode_operand_map(void *out, const void *base, bool half, uint64_t rows, uint64_t cols, uint64_t ld);
+// Plain (unswizzled) 2D tensor map of a column-major FP32 / FP64 matrix (rows x cols,
+// leading dimension ld elements), box box_rows x box_cols; reads outside the matrix
+// are zero.
+bool encode_plain_map(void *out, const void *base, int esize, uint64_t rows, uint64_t cols, uint64_t ld,
+                      uint32_t box_rows, uint32_t box_cols);
 // Power-of-two scale exponent of each listed front's FP16 operand copy, from the
 // injected diagonal d: sexp[s] = e with max over the front's rows of sqrt(d) < 2^(e + 12),
 // so |L| 2^-e < 2^12 (|L(i, j)| <= sqrt(A(i, i)) for a Cholesky factor).
@@ -226,8 +234,9 @@ void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce 
                 const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st);
 // Superblock diagonal solves (cooperative launch) and the superblock inverses they apply.
 template <typename T>
-cudaError_t launch_sb_solve(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
-                            int64_t ldx, int nrhs, double *scratch, int *flags, int *err, cudaStream_t st);
+cudaError_t launch_sb_solve(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor,
+                            const void *maps, double *X, int64_t ldx, int nrhs, double *scratch, int *flags, int *err,
+                            cudaStream_t st);
 template <typename T>
 void launch_sb_inverse(const SbTask *tasks, int ntasks, SnDev sd, T *factor, cudaStream_t st);
 int solve_rows_per_task();

@@ -109,6 +109,8 @@ struct DevSym {
     DBuf<StrReduce> fred, bred;
     DBuf<SbTask> fsb_tasks, bsb_tasks, isb_tasks;   // superblock solves (forward, backward) and inverses
     int nsb_inv = 0;
+    std::vector<SbTask> isb_host;                   // the superblocks (their inverses' offsets)
+    std::vector<int32_t> sb_fronts;                 // fronts with superblock solves
     int max_str_tasks = 0;
     DBuf<int2> subs;                     // subtree ranges solved one per CTA (levels <= solve_cut)
     int nsub = 0, sub_fmax = 0, solve_cut = -1;
@@ -165,6 +167,12 @@ struct mfs_handle {
     DBuf<float> dscr32;
     DBuf<double> sol;
     DBuf<double> sb_scratch;       // accumulated right-hand sides of the superblock solves (n x pass)
+    // tensor maps of the superblock solves, built for the factor array `smaps_base`
+    // (element size smaps_es) of the symbolic data `smaps_sym`
+    DBuf<TensorMapBlob> smaps;
+    const void *smaps_base = nullptr;
+    const void *smaps_sym = nullptr;
+    int smaps_es = 0;
     std::shared_ptr<DBuf<double>> asm_ax;   // output of the last mfs_assemble (device resident)
     std::shared_ptr<DBuf<double>> asm_spare;   // an earlier assembly buffer, reused once nothing holds it
     DBuf<double> rhs, work_r, work_z, work_p, work_ap, work_x, work_s, io;

@@ -402,6 +402,22 @@ bool encode_operand_map(void *out, const void *base, bool half, uint64_t rows, u
     return r == CUDA_SUCCESS;
 }
 
+bool encode_plain_map(void *out, const void *base, int esize, uint64_t rows, uint64_t cols, uint64_t ld,
+                      uint32_t box_rows, uint32_t box_cols) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn || (esize != 4 && esize != 8)) return false;
+    cuuint64_t dims[2] = {rows, cols};
+    cuuint64_t strides[1] = {ld * uint64_t(esize)};
+    cuuint32_t box[2] = {box_rows, box_cols};
+    cuuint32_t estr[2] = {1, 1};
+    const CUresult r = fn(static_cast<CUtensorMap *>(out),
+                          esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                          const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 void launch_gemm_tma(bool half, const GemmTask *tasks, int ntasks, int ntiles, const void *maps, float *C,
                      const int32_t *sexp, int *err, cudaStream_t st) {
     if (half) launch_tma<__half>(tasks, ntasks, ntiles, maps, C, sexp, err, st);

@@ -23,11 +23,10 @@
 // chain, and what a task reads after its last dependency arrives (64 x 256 of L
 // and at most 64 x 256 of the inverse) is already on chip: L and the inverse
 // stream through shared memory in 32 KB chunks (64 rows x 128 FP32 / 64 FP64
-// columns forward, 128 / 64 rows x 64 columns backward), one bulk copy per
-// column issued by one thread, completing on the ring slot's mbarrier, up to six
-// chunks in flight. Bulk copies of the last superblock's rows are rounded up to
-// 64 rows; the extra rows lie inside the factor array (the next column of the
-// panel) and are masked out of every product.
+// columns forward, 128 / 64 rows x 64 columns backward), one 2D TMA box per chunk
+// issued by one thread through per-front / per-inverse tensor maps, completing on
+// the ring slot's mbarrier, up to six chunks in flight. A box reaching past the
+// front's L11 or past the inverse reads zeros there.
 //
 // Launches are cooperative (all CTAs co-resident); every CTA walks its tasks in
 // ascending order and a task waits only on lower-numbered tasks and on the other
@@ -146,23 +145,14 @@ __device__ __forceinline__ void mbar_wait_all(uint32_t bar, uint32_t parity, int
         }
     }
 }
-__device__ __forceinline__ void bulk_copy(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-// One thread: ncols columns of a column-major source (leading dimension lds), rows
-// [row0, row0 + nrows) of each (16-byte aligned, a multiple of 16 bytes), to
-// dst + j * ldd elements, completing on `bar`.
-template <typename T>
-__device__ __forceinline__ void stage_bulk(T *dst, int ldd, const T *src, int64_t lds, int row0, int nrows,
-                                           int ncols, uint32_t bar) {
-    const uint32_t bytes = uint32_t(nrows) * sizeof(T);
-    mbar_expect_tx(bar, bytes * uint32_t(ncols));
-    const uint32_t d0 = smem_u32(dst);
-    for (int j = 0; j < ncols; ++j)
-        bulk_copy(d0 + uint32_t(j) * uint32_t(ldd) * sizeof(T), src + int64_t(j) * lds + row0, bytes, bar);
+// 2D tiled TMA load of one box of the tensor map at `map` (device memory written
+// before the launch), box origin (x = row, y = column), completing on `bar`.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const char *map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
 }
 
 // After an error (a wait that gave up), the copies a CTA issued may still be in
@@ -213,7 +203,7 @@ __device__ __forceinline__ void count_up(int *p) {
 template <typename T, int NST, int NR>
 __global__ void __launch_bounds__(kSbThreads, 1) sp_fwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
                                                                SnDev sd, const T *__restrict__ factor,
-                                                               double *__restrict__ X, int64_t ldx, int nrhs,
+                                                               const char *__restrict__ maps, double *__restrict__ X, int64_t ldx, int nrhs,
                                                                double *__restrict__ scratch, int *__restrict__ flags,
                                                                int *__restrict__ err) {
     using Lay = SpLayout<T, NST, NR>;
@@ -221,8 +211,10 @@ __global__ void __launch_bounds__(kSbThreads, 1) sp_fwd_kernel(const SbTask *__r
     constexpr int FC = SpChunk<T>::FC, CE = SpChunk<T>::ELEMS;
     constexpr int per = SB / FC;                         // chunks per earlier superblock
     constexpr int QC = FC / 4;
-    extern __shared__ __align__(128) unsigned char sp_raw[];
+    extern __shared__ __align__(128) unsigned char sp_dyn[];
     __shared__ __align__(8) uint64_t bars[NST];
+    // TMA destinations: 128-byte aligned (the launch adds 128 bytes for this)
+    unsigned char *sp_raw = sp_dyn + ((128u - (smem_u32(sp_dyn) & 127u)) & 127u);
     T *ring = reinterpret_cast<T *>(sp_raw);
     double *vec = reinterpret_cast<double *>(sp_raw + Lay::vec_off);
     P *vp = reinterpret_cast<P *>(sp_raw + Lay::vp_off);
@@ -238,9 +230,7 @@ __global__ void __launch_bounds__(kSbThreads, 1) sp_fwd_kernel(const SbTask *__r
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SbTask tk = tasks[t];
         const int s = tk.sn, K = tk.K, h = tk.pad;
-        const int w = sd.w[s], ld = sd.ld[s], c0 = sd.col0[s];
-        const T *pan = factor + sd.pan_off[s];
-        const T *inv = factor + tk.inv;
+        const int w = sd.w[s], c0 = sd.col0[s];
         const int nrK = sb_rows(w, K), nrpK = sb_pad(nrK), nhK = nrpK / 64;
         const int R0 = K * SB + h * 64, nrh = min(64, w - R0);
         const int icols = (h + 1) * 64;                  // nonzero columns of the inverse's rows
@@ -251,12 +241,13 @@ __global__ void __launch_bounds__(kSbThreads, 1) sp_fwd_kernel(const SbTask *__r
             const int slot = int((gq + q) % NST);
             T *dst = ring + slot * CE;
             const uint32_t bar = smem_u32(&bars[slot]);
+            mbar_expect_tx(bar, SpChunk<T>::BYTES);
             if (q < ndep) {
                 const int J = q / per, c = q - J * per;
-                stage_bulk<T>(dst, 64, pan + int64_t(J * SB + c * FC) * ld, ld, R0, 64, FC, bar);
+                tma_load_2d(smem_u32(dst), maps + size_t(tk.pmap) * kTensorMapBytes, R0, J * SB + c * FC, bar);
             } else {
                 const int c = q - ndep;
-                stage_bulk<T>(dst, 64, inv + int64_t(c * FC) * nrpK, nrpK, h * 64, 64, min(FC, icols - c * FC), bar);
+                tma_load_2d(smem_u32(dst), maps + size_t(tk.imap) * kTensorMapBytes, h * 64, c * FC, bar);
             }
         };
         __syncthreads();                                 // the previous task is done with shared memory
@@ -356,7 +347,7 @@ __global__ void __launch_bounds__(kSbThreads, 1) sp_fwd_kernel(const SbTask *__r
 template <typename T, int NST, int NR>
 __global__ void __launch_bounds__(kSbThreads, 1) sp_bwd_kernel(const SbTask *__restrict__ tasks, int ntasks,
                                                                SnDev sd, const T *__restrict__ factor,
-                                                               double *__restrict__ X, int64_t ldx, int nrhs,
+                                                               const char *__restrict__ maps, double *__restrict__ X, int64_t ldx, int nrhs,
                                                                double *__restrict__ scratch, int *__restrict__ flags,
                                                                int *__restrict__ err) {
     using Lay = SpLayout<T, NST, NR>;
@@ -364,8 +355,10 @@ __global__ void __launch_bounds__(kSbThreads, 1) sp_bwd_kernel(const SbTask *__r
     constexpr int FC = SpChunk<T>::FC, CE = SpChunk<T>::ELEMS;
     constexpr int per = SB / FC;                         // chunks per full later superblock
     constexpr int RL = FC / 32;                          // chunk rows per lane
-    extern __shared__ __align__(128) unsigned char sp_raw[];
+    extern __shared__ __align__(128) unsigned char sp_dyn[];
     __shared__ __align__(8) uint64_t bars[NST];
+    // TMA destinations: 128-byte aligned (the launch adds 128 bytes for this)
+    unsigned char *sp_raw = sp_dyn + ((128u - (smem_u32(sp_dyn) & 127u)) & 127u);
     T *ring = reinterpret_cast<T *>(sp_raw);
     double *vec = reinterpret_cast<double *>(sp_raw + Lay::vec_off);
     P *vp = reinterpret_cast<P *>(sp_raw + Lay::vp_off);
@@ -380,9 +373,7 @@ __global__ void __launch_bounds__(kSbThreads, 1) sp_bwd_kernel(const SbTask *__r
     for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const SbTask tk = tasks[t];
         const int s = tk.sn, K = tk.K, h = tk.pad;
-        const int w = sd.w[s], ld = sd.ld[s], c0 = sd.col0[s];
-        const T *pan = factor + sd.pan_off[s];
-        const T *inv = factor + tk.inv;
+        const int w = sd.w[s], c0 = sd.col0[s];
         const int nsb = (w + SB - 1) / SB;
         const int nrK = sb_rows(w, K), nrpK = sb_pad(nrK), nhK = nrpK / 64;
         const int C0 = K * SB + h * 64, nch = min(64, w - C0);
@@ -406,15 +397,15 @@ __global__ void __launch_bounds__(kSbThreads, 1) sp_bwd_kernel(const SbTask *__r
             const int slot = int((gq + q) % NST);
             T *dst = ring + slot * CE;
             const uint32_t bar = smem_u32(&bars[slot]);
+            mbar_expect_tx(bar, SpChunk<T>::BYTES);
             if (q < ndep) {
                 int J, c;
                 dep(q, J, c);
-                const int rows = min(FC, sb_pad(sb_rows(w, J)) - c * FC);
-                stage_bulk<T>(dst, FC, pan + int64_t(C0) * ld, ld, J * SB + c * FC, rows, 64, bar);
+                tma_load_2d(smem_u32(dst), maps + size_t(tk.pmap + 1) * kTensorMapBytes, J * SB + c * FC, C0, bar);
             } else {
                 const int c = q - ndep;
-                stage_bulk<T>(dst, FC, inv + int64_t(h * 64) * nrpK, nrpK, h * 64 + c * FC, min(FC, irows - c * FC),
-                              64, bar);
+                tma_load_2d(smem_u32(dst), maps + size_t(tk.imap + 1) * kTensorMapBytes, h * 64 + c * FC, h * 64,
+                            bar);
             }
         };
         __syncthreads();
@@ -641,36 +632,39 @@ int coop_grid(K kernel, size_t smem, int ntasks) {
 
 // NR: the right-hand sides the vectors hold (nrhs <= NR)
 template <typename T, int NST, int NR>
-cudaError_t launch_sp_impl(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
-                           int64_t ldx, int nrhs, double *scratch, int *flags, int *err, cudaStream_t st) {
+cudaError_t launch_sp_impl(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, const char *maps,
+                           double *X, int64_t ldx, int nrhs, double *scratch, int *flags, int *err, cudaStream_t st) {
     using L = SpLayout<T, NST, NR>;
-    static_assert(L::bytes + 64 <= size_t(kMaxSmemOptin), "superblock solve shared memory");
+    constexpr size_t smem = L::bytes + 128;
+    static_assert(smem + 256 <= size_t(kMaxSmemOptin), "superblock solve shared memory");
     void *kern = forward ? (void *)sp_fwd_kernel<T, NST, NR> : (void *)sp_bwd_kernel<T, NST, NR>;
     static PerDeviceOnce once;
     once([] {
-        cudaFuncSetAttribute(sp_fwd_kernel<T, NST, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes));
-        cudaFuncSetAttribute(sp_bwd_kernel<T, NST, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes));
+        cudaFuncSetAttribute(sp_fwd_kernel<T, NST, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(sp_bwd_kernel<T, NST, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     });
-    const int grid = forward ? coop_grid(sp_fwd_kernel<T, NST, NR>, L::bytes, ntasks)
-                             : coop_grid(sp_bwd_kernel<T, NST, NR>, L::bytes, ntasks);
-    void *args[] = {(void *)&tasks, (void *)&ntasks,  (void *)&sd,    (void *)&factor, (void *)&X, (void *)&ldx,
-                    (void *)&nrhs,  (void *)&scratch, (void *)&flags, (void *)&err};
+    const int grid = forward ? coop_grid(sp_fwd_kernel<T, NST, NR>, smem, ntasks)
+                             : coop_grid(sp_bwd_kernel<T, NST, NR>, smem, ntasks);
+    void *args[] = {(void *)&tasks, (void *)&ntasks, (void *)&sd,      (void *)&factor, (void *)&maps, (void *)&X,
+                    (void *)&ldx,   (void *)&nrhs,   (void *)&scratch, (void *)&flags,  (void *)&err};
     ++g_kernel_launches;
-    return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kSbThreads), args, L::bytes, st);
+    return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kSbThreads), args, smem, st);
 }
 
 }  // namespace
 
 template <typename T>
-cudaError_t launch_sb_solve(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor, double *X,
-                            int64_t ldx, int nrhs, double *scratch, int *flags, int *err, cudaStream_t st) {
+cudaError_t launch_sb_solve(bool forward, const SbTask *tasks, int ntasks, SnDev sd, const T *factor,
+                            const void *maps, double *X, int64_t ldx, int nrhs, double *scratch, int *flags, int *err,
+                            cudaStream_t st) {
+    const char *mp = static_cast<const char *>(maps);
     if (ntasks <= 0) return cudaSuccess;
     if (nrhs > kSbMaxRhs) return cudaErrorInvalidValue;
     // ring depth: the deepest that fits beside the vectors of nrhs right-hand sides
     constexpr int D4 = sizeof(T) == 4 ? 6 : 5, D8 = sizeof(T) == 4 ? 5 : 4;
     if (nrhs <= 4)
-        return launch_sp_impl<T, D4, 4>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, scratch, flags, err, st);
-    return launch_sp_impl<T, D8, kSbMaxRhs>(forward, tasks, ntasks, sd, factor, X, ldx, nrhs, scratch, flags, err,
+        return launch_sp_impl<T, D4, 4>(forward, tasks, ntasks, sd, factor, mp, X, ldx, nrhs, scratch, flags, err, st);
+    return launch_sp_impl<T, D8, kSbMaxRhs>(forward, tasks, ntasks, sd, factor, mp, X, ldx, nrhs, scratch, flags, err,
                                             st);
 }
 
@@ -685,10 +679,10 @@ void launch_sb_inverse(const SbTask *tasks, int ntasks, SnDev sd, T *factor, cud
     sb_inverse_kernel<T><<<ntasks, 256, smem, st>>>(tasks, sd, factor);
 }
 
-template cudaError_t launch_sb_solve<float>(bool, const SbTask *, int, SnDev, const float *, double *, int64_t, int,
-                                            double *, int *, int *, cudaStream_t);
-template cudaError_t launch_sb_solve<double>(bool, const SbTask *, int, SnDev, const double *, double *, int64_t,
-                                             int, double *, int *, int *, cudaStream_t);
+template cudaError_t launch_sb_solve<float>(bool, const SbTask *, int, SnDev, const float *, const void *, double *,
+                                            int64_t, int, double *, int *, int *, cudaStream_t);
+template cudaError_t launch_sb_solve<double>(bool, const SbTask *, int, SnDev, const double *, const void *, double *,
+                                             int64_t, int, double *, int *, int *, cudaStream_t);
 template void launch_sb_inverse<float>(const SbTask *, int, SnDev, float *, cudaStream_t);
 template void launch_sb_inverse<double>(const SbTask *, int, SnDev, double *, cudaStream_t);
 
