@@ -46,7 +46,12 @@ def parse():
     p.add_argument("--k", type=int, default=None, help="override the cube side (smaller runs)")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison arm")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    p.add_argument("--tc", type=int, default=0, help="FP32 Schur updates: 0 auto, 1 TF32, 2 split 3xTF32")
+    p.add_argument("--tc", type=int, default=0,
+                   help="FP32 Schur updates: 0 auto (5 under refinement), 1 TF32, 2 split 3xTF32, 4 TF32 with TMA, "
+                        "5 FP16 operands with TMA")
+    p.add_argument("--profile", action="store_true",
+                   help="build the workload, run one untimed assemble + factorization + refined solve, exit "
+                        "(the command profilers capture)")
     p.add_argument("--maxit", type=int, default=50, help="refinement iteration cap")
     p.add_argument("--chain", type=int, default=0, help="diagonal solves: 0 superblock inverses, 1 block-pair chains")
     p.add_argument("--cpu-seconds", type=float, default=150.0,
@@ -200,6 +205,12 @@ def run_b200(args, rank, world, local, dist):
         return total, launches, clocks
 
     pK, pB, pX = C.c_void_p(Ke_dev.data_ptr()), C.c_void_p(B_dev.data_ptr()), C.c_void_p(X_dev.data_ptr())
+    if args.profile:
+        step(f32, pK, pB, pX, D)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile_step": f32.stats()}), flush=True)
+        return
     tot32, launches, clocks = timed(f32, args.steps, args.warmup, pK, pB, pX, D, sample_clocks=True)
     st32 = f32.stats()
     ms32 = tot32 / args.steps
@@ -254,13 +265,15 @@ def run_b200(args, rank, world, local, dist):
     _lib.check(lib.mfs_set_options(f32._h, C.byref(f32._opts)), f32._h, "options")
     gemm_tf = stk["gemm_flops"] / (stk["gemm_ms"] * 1e-3) / 1e12 if stk["gemm_ms"] > 0 else None
     peak = peaks["bf16_tflops_sustained"]
+    half = args.tc in (0, 5)
     roofline = {"bound": "tensor", "achieved": gemm_tf, "peak": peak, "unit": "TFLOP/s",
                 "frac": (gemm_tf / peak) if gemm_tf else None, "traffic": None,
-                "kernel": "gemm_tc_kernel (tcgen05 kind::tf32)",
+                "kernel": ("gemm_tma_kernel (tcgen05 kind::f16, TMA-fed Schur updates) + gemm_tc_kernel (row solves)"
+                           if half else "gemm_tc_kernel / gemm_tma_kernel (tcgen05 kind::tf32)"),
                 "launches": stk["gemm_launches"], "kernel_ms_per_factorization": stk["gemm_ms"],
                 "kernel_flops_per_factorization": stk["gemm_flops"],
                 "note": f"algorithmic flops of the launches' tasks / CUDA-event time per launch, summed over one "
-                        f"factorization; peak = {peak_kind} sustained dense bf16 (the dense TF32 rate is half of it); "
+                        f"factorization; peak = {peak_kind} sustained dense bf16 (the FP16 rate; TF32 is half of it); "
                         f"whole factorization sequence: {achieved_seq:.1f} TFLOP/s of the symbolic flop count"}
 
     result = {

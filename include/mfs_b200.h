@@ -73,7 +73,7 @@ typedef struct {
     double refine_tol;          /* relative residual target ||b - Hx|| / ||b|| (1e-10) */
     int32_t refine_maxit;       /* iteration cap (50) */
     int32_t use_graphs;         /* capture the factorization / solve launch sequence in CUDA graphs */
-    int32_t tensor_cores;       /* FP32 Schur updates: 0 auto (TF32 with refinement, else split 3xTF32),
+    int32_t tensor_cores;       /* FP32 Schur updates: 0 auto (5 with refinement, else split 3xTF32),
                                    1 TF32 on tcgen05, 2 split 3xTF32 (FP32-level products, mma.sync),
                                    3 TF32 on mma.sync (the pre-Blackwell tensor-core path),
                                    4 TF32 on tcgen05 with TMA-fed operands for the Schur updates,

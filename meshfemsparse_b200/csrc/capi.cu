@@ -516,12 +516,15 @@ void clear_factor_graphs(mfs_handle *h) {
 // with TMA-fed operands for the updates (mode 0) and cp.async for the row solves,
 // 5 = FP16 operands (a per-front power-of-two scaled half copy of the panels, written
 // by the row solves) on tcgen05 kind::f16 with TMA for the updates, 3 = split 3xTF32
-// (mma.sync), 0 = single-pass TF32 on mma.sync. Option values: tensor_cores 0 (auto: 1
+// (mma.sync), 0 = single-pass TF32 on mma.sync. Option values: tensor_cores 0 (auto: 5
 // with refinement, else 3), 1, 2 (-> 3), 3 (-> 0), 4, 5 (with refinement, else 3).
+// FP16 operands are safe under refinement: |L(i, j)| <= sqrt(A(j, j)) for an SPD
+// matrix, so the per-front scale keeps every operand below 2^12 (no overflow), and
+// the refinement needs the same iteration count as with TF32 operands.
 int fp32_split(const mfs_handle *h) {
     const int tc = h->opt.tensor_cores;
-    if (tc == 5) return h->opt.refine ? 5 : 3;
-    return tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : tc == 4 ? 4 : (h->opt.refine ? 1 : 3);
+    if (tc == 5 || tc == 0) return h->opt.refine ? 5 : 3;
+    return tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : 4;
 }
 
 // Tensor maps of the large fronts' panels in `base` (the FP32 factor, or its FP16

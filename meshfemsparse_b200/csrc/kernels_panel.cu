@@ -97,7 +97,7 @@ __device__ __forceinline__ void tile_mma(T (&c)[4][8], const T *A0, int lda, con
     const int rq = lane & 7, cq = lane >> 3;
     const T *a = A0 + 4 * rq;
     const T *b = B0 + 8 * cq * sj;
-#pragma unroll 1
+#pragma unroll 2
     for (int k = 0; k < 32; ++k) {
         T av[4], bv[8];
 #pragma unroll
@@ -149,11 +149,15 @@ __device__ __noinline__ void warp_diag_tile(T *D, T *Iv, T *rdiag, int LDD, int 
     T r[32];
 #pragma unroll
     for (int j = 0; j < 32; ++j) r[j] = (j <= lane) ? Dt[j * LDD + lane] : T(0);
+    // the re-factor test's threshold of this lane's column, loaded once (a global load
+    // per pivot would sit on the pivot chain)
+    const double tiny_lane = (sflag && c0 + lane < nb) ? kRefactorTiny * fabs(dorig[col_base + c0 + lane]) : 0.0;
 #pragma unroll 1
     for (int k = 0; k < 32; ++k) {
         T piv = __shfl_sync(0xffffffffu, r[0], k);
+        const double tiny = __shfl_sync(0xffffffffu, tiny_lane, k);
         const int gcol = c0 + k < nb ? col_base + c0 + k : -1;
-        const bool bad = sflag ? (gcol >= 0 && !(double(piv) > kRefactorTiny * fabs(dorig[gcol]))) : !(piv > T(0));
+        const bool bad = sflag ? (gcol >= 0 && !(double(piv) > tiny)) : !(piv > T(0));
         if (bad) piv = panel_bad_pivot(piv, gcol, pv, sflag);
         const T rs = recip_sqrt(piv);
         const T lik = (lane == k) ? piv * rs : r[0] * rs;

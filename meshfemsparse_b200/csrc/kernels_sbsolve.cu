@@ -528,98 +528,115 @@ __global__ void __launch_bounds__(kSbThreads, 1) sp_bwd_kernel(const SbTask *__r
 }
 
 // inv(L_KK) of superblock K of front s (nr rows), nrp x nrp column-major at
-// factor + tk.inv. The 64 x 64 diagonal inverses D_b come from the panel kernel's
-// stored inverses when the front has them, else by column-wise substitution on
-// L_bb (one thread per column); then X_ab = -D_a sum_{c=b}^{a-1} L_ac X_cb.
+// factor + tk.inv, one CTA per 64-column block b of it (blockIdx.y):
+//   X_bb = D_b, X_ab = -D_a sum_{c=b}^{a-1} L_ac X_cb for a > b, X_ab = 0 for a < b,
+// with D_a = inv(L_aa) the 64 x 64 diagonal inverses: the panel kernel's stored
+// ones when the front has them, else by column-wise substitution on L_aa (one
+// thread per column). The column's blocks X_cb stay in shared memory; each L_ac
+// and D_a is staged there before its 64 x 64 x 64 product (thread = row i, 16
+// columns: the X / T operands are broadcast within a warp).
 template <typename T>
 __global__ void __launch_bounds__(256) sb_inverse_kernel(const SbTask *__restrict__ tasks, SnDev sd, T *factor) {
     constexpr int LD = 65;
-    constexpr int DPAR = sizeof(T) == 4 ? 4 : 2;          // diagonal blocks inverted at once
+    constexpr int TB = 64 * LD;                           // one staged 64 x 64 block
     extern __shared__ __align__(16) double inv_smem[];
-    T *Ls = reinterpret_cast<T *>(inv_smem);              // [DPAR][64 * LD] diagonal blocks of L
-    T *Xs = Ls + DPAR * 64 * LD;                          // [DPAR][64 * LD] their inverses / a product tile
+    T *Xc = reinterpret_cast<T *>(inv_smem);              // [4][TB]: X_cb, c = b .. nbk - 1
+    T *Ls = Xc + 4 * TB;                                  // L_ac, then T = sum L_ac X_cb
+    T *Ds = Ls + TB;                                      // D_a
     const SbTask tk = tasks[blockIdx.x];
-    const int s = tk.sn, K = tk.K;
+    const int s = tk.sn, K = tk.K, b = blockIdx.y;
     const int w = sd.w[s], ld = sd.ld[s];
     const T *pan = factor + sd.pan_off[s];
     T *out = factor + tk.inv;
     const int nr = sb_rows(w, K), nrp = sb_pad(nr), nbk = nrp / 64;
+    if (b >= nbk) return;
     const int r0 = K * SB;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, i = tid & 63, jg = tid >> 6;
     const int64_t dinv = sd.inv_off[s];
-    auto Lv = [&](int i, int j) -> T {                     // superblock-local L(i, j), 0 outside
-        return (i < nr && j < nr) ? pan[int64_t(r0 + j) * ld + r0 + i] : T(0);
+    auto Lv = [&](int gi, int gj) -> T {                   // superblock-local L(gi, gj), 0 outside
+        return (gi < nr && gj < nr) ? pan[int64_t(r0 + gj) * ld + r0 + gi] : T(0);
     };
-    // zero the strict upper block triangle of the output
-    for (int q = tid; q < nrp * nrp; q += blockDim.x) {
-        const int j = q / nrp, i = q - j * nrp;
-        if ((i >> 6) < (j >> 6)) out[q] = T(0);
-    }
-    // 1. diagonal inverses
-    for (int b0 = 0; b0 < nbk; b0 += DPAR) {
-        const int g = tid >> 6, j = tid & 63, b = b0 + g;
+    // D_a into dst (ld LD): stored inverse, or substitution on L_aa (staged in scratch)
+    auto load_diag = [&](int a, T *dst, T *scratch) {
         if (dinv >= 0) {
-            for (int q = tid; q < min(DPAR, nbk - b0) * 4096; q += blockDim.x) {
-                const int bb = b0 + (q >> 12), e = q & 4095, jj = e >> 6, ii = e & 63;
-                const T v = factor[dinv + int64_t(K * (SB / 64) + bb) * 4096 + e];
-                out[int64_t(bb * 64 + jj) * nrp + bb * 64 + ii] = (bb * 64 + ii < nr && bb * 64 + jj < nr) ? v : T(0);
+            const T *src = factor + dinv + int64_t(K * (SB / 64) + a) * 4096;
+            for (int q = tid; q < 4096; q += blockDim.x) {
+                const int jj = q >> 6, ii = q & 63;
+                dst[jj * LD + ii] = (a * 64 + ii < nr && a * 64 + jj < nr) ? src[q] : T(0);
             }
-            continue;
+            __syncthreads();
+            return;
+        }
+        for (int q = tid; q < 4096; q += blockDim.x) {
+            const int jj = q >> 6, ii = q & 63;
+            scratch[jj * LD + ii] = Lv(a * 64 + ii, a * 64 + jj);
         }
         __syncthreads();
-        if (g < DPAR && b < nbk)
-            for (int q = j; q < 64 * 64; q += 64) {
-                const int jj = q >> 6, ii = q & 63;
-                Ls[g * 64 * LD + jj * LD + ii] = Lv(b * 64 + ii, b * 64 + jj);
-            }
-        __syncthreads();
-        if (g < DPAR && b < nbk) {
-            const T *Lb = Ls + g * 64 * LD;
-            T *Xb = Xs + g * 64 * LD;
-            const int nb = min(64, nr - b * 64);
+        if (tid < 64) {
+            const int j = tid, nb = min(64, nr - a * 64);
             for (int k = 0; k < 64; ++k) {
                 T v = T(0);
                 if (k >= j && k < nb && j < nb) {
                     v = k == j ? T(1) : T(0);
-                    for (int m = j; m < k; ++m) v -= Lb[m * LD + k] * Xb[j * LD + m];
-                    v /= Lb[k * LD + k];
+                    for (int m = j; m < k; ++m) v -= scratch[m * LD + k] * dst[j * LD + m];
+                    v /= scratch[k * LD + k];
                 }
-                Xb[j * LD + k] = v;
+                dst[j * LD + k] = v;
             }
-            for (int k = 0; k < 64; ++k) out[int64_t(b * 64 + j) * nrp + b * 64 + k] = Xb[j * LD + k];
+        }
+        __syncthreads();
+    };
+    // the strict upper blocks of this column are zero
+    for (int q = tid; q < b * 64 * 64; q += blockDim.x) {
+        const int jj = q / (b * 64), ii = q - jj * (b * 64);
+        out[int64_t(b * 64 + jj) * nrp + ii] = T(0);
+    }
+    // X_bb = D_b
+    T *Xb = Xc;
+    load_diag(b, Xb, Ls);
+    for (int q = tid; q < 4096; q += blockDim.x) {
+        const int jj = q >> 6, ii = q & 63;
+        out[int64_t(b * 64 + jj) * nrp + b * 64 + ii] = Xb[jj * LD + ii];
+    }
+    for (int a = b + 1; a < nbk; ++a) {
+        T acc[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) acc[u] = T(0);
+        for (int c = b; c < a; ++c) {
+            __syncthreads();                               // Ls is free
+            for (int q = tid; q < 4096; q += blockDim.x) {
+                const int m = q >> 6, ii = q & 63;
+                Ls[m * LD + ii] = Lv(a * 64 + ii, c * 64 + m);
+            }
+            __syncthreads();
+            const T *X = Xc + (c - b) * TB + (jg * 16) * LD;
+#pragma unroll 4
+            for (int m = 0; m < 64; ++m) {
+                const T l = Ls[m * LD + i];
+#pragma unroll
+                for (int u = 0; u < 16; ++u) acc[u] += l * X[u * LD + m];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 16; ++u) Ls[(jg * 16 + u) * LD + i] = acc[u];   // T(i, j)
+        load_diag(a, Ds, Xc + (a - b) * TB);               // (synchronizes; X_ab's slot is free)
+#pragma unroll
+        for (int u = 0; u < 16; ++u) acc[u] = T(0);
+        const T *Tt = Ls + (jg * 16) * LD;
+#pragma unroll 4
+        for (int m = 0; m < 64; ++m) {
+            const T dv = Ds[m * LD + i];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) acc[u] -= dv * Tt[u * LD + m];
+        }
+        T *Xa = Xc + (a - b) * TB;
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            Xa[(jg * 16 + u) * LD + i] = acc[u];
+            out[int64_t(b * 64 + jg * 16 + u) * nrp + a * 64 + i] = acc[u];
         }
     }
-    __syncthreads();
-    // 2. off-diagonal blocks, column block by column block
-    T *Ts = Xs;                                           // 64 x 64 product tile (ld LD)
-    const int i = tid & 63, jg = tid >> 6;                // row, 16-column group
-    for (int b = 0; b + 1 < nbk; ++b)
-        for (int a = b + 1; a < nbk; ++a) {
-            T acc[16];
-#pragma unroll
-            for (int u = 0; u < 16; ++u) acc[u] = T(0);
-            for (int c = b; c < a; ++c)
-                for (int m = 0; m < 64; ++m) {
-                    const T l = Lv(a * 64 + i, c * 64 + m);
-#pragma unroll
-                    for (int u = 0; u < 16; ++u)
-                        acc[u] += l * __ldcg(&out[int64_t(b * 64 + jg * 16 + u) * nrp + c * 64 + m]);
-                }
-            __syncthreads();
-#pragma unroll
-            for (int u = 0; u < 16; ++u) Ts[(jg * 16 + u) * LD + i] = acc[u];
-            __syncthreads();
-#pragma unroll
-            for (int u = 0; u < 16; ++u) acc[u] = T(0);
-            for (int m = 0; m < 64; ++m) {
-                const T dv = __ldcg(&out[int64_t(a * 64 + m) * nrp + a * 64 + i]);
-#pragma unroll
-                for (int u = 0; u < 16; ++u) acc[u] -= dv * Ts[(jg * 16 + u) * LD + m];
-            }
-#pragma unroll
-            for (int u = 0; u < 16; ++u) out[int64_t(b * 64 + jg * 16 + u) * nrp + a * 64 + i] = acc[u];
-            __syncthreads();
-        }
 }
 
 template <typename K>
@@ -671,12 +688,11 @@ cudaError_t launch_sb_solve(bool forward, const SbTask *tasks, int ntasks, SnDev
 template <typename T>
 void launch_sb_inverse(const SbTask *tasks, int ntasks, SnDev sd, T *factor, cudaStream_t st) {
     if (ntasks <= 0) return;
-    constexpr int DPAR = sizeof(T) == 4 ? 4 : 2;
-    const size_t smem = size_t(2) * DPAR * 64 * 65 * sizeof(T);
+    const size_t smem = size_t(6) * 64 * 65 * sizeof(T);
     static PerDeviceOnce once;
     once([smem] { cudaFuncSetAttribute(sb_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); });
     ++g_kernel_launches;
-    sb_inverse_kernel<T><<<ntasks, 256, smem, st>>>(tasks, sd, factor);
+    sb_inverse_kernel<T><<<dim3(ntasks, SB / 64), 256, smem, st>>>(tasks, sd, factor);
 }
 
 template cudaError_t launch_sb_solve<float>(bool, const SbTask *, int, SnDev, const float *, const void *, double *,
