@@ -134,16 +134,22 @@ __device__ __forceinline__ void tile_store(T *M, int ldm, const T (&c)[4][8], T 
 }
 
 // Cholesky of the 32 x 32 tile at (c0, c0) of D by one warp, then its inverse.
-// Both keep a 32-entry vector per lane in registers and rotate it by one entry
-// per step, so the current column (row) is always entry 0: the step loop stays
-// rolled (compact code) while every register index is static.
-//   factor : lane = row i, r[j] = A(i, k + j); pivot from lane k by shuffle,
-//            reciprocal square root, rank-1 update with L(k + j, k) from lane k + j;
-//   inverse: lane = column c, y[i] = Y(k + i, c); y_k = y[0] / L(k, k), then
-//            y[i] -= L(k + i, k) y_k (L read from shared memory, broadcast).
+// Both keep a 32-entry vector per lane in registers, processed four steps at a
+// time and then shifted by four, so the current column (row) of step k0 + t is
+// entry t: the outer step loop stays rolled (compact code) while every register
+// index is static.
+//   factor : lane = row i, r[j] = A(i, k0 + j); pivot from lane k by shuffle,
+//            reciprocal square root; column k of L goes to Lrot[k][.] rotated by k
+//            (Lrot[k][j] = L(k + j, k), zero past the tile) and comes back to every
+//            lane as 16-byte broadcast loads for the rank-1 update;
+//   inverse: lane = column c, y[i] = Y(k0 + i, c); y_k = y[t] / L(k, k), then
+//            y[t + i] -= Lrot[k][i] y_k.
 template <typename T>
-__device__ __noinline__ void warp_diag_tile(T *D, T *Iv, T *rdiag, int LDD, int c0, int nb, int lane, int col_base,
-                                            int *fail_col, int *perturbed, const double *dorig, int *sflag) {
+__device__ __noinline__ void warp_diag_tile(T *D, T *Iv, T *rdiag, T *Lrot, int LDD, int c0, int nb, int lane,
+                                            int col_base, int *fail_col, int *perturbed, const double *dorig,
+                                            int *sflag) {
+    using V = typename Vec16<T>::type;
+    constexpr int E = 16 / int(sizeof(T)), NV = 32 / E;
     const PivotCtl pv{fail_col, perturbed, dorig, nullptr};
     T *Dt = D + c0 * LDD + c0;                       // tile element (i, j) at Dt[j * LDD + i]
     T r[32];
@@ -153,20 +159,30 @@ __device__ __noinline__ void warp_diag_tile(T *D, T *Iv, T *rdiag, int LDD, int 
     // per pivot would sit on the pivot chain)
     const double tiny_lane = (sflag && c0 + lane < nb) ? kRefactorTiny * fabs(dorig[col_base + c0 + lane]) : 0.0;
 #pragma unroll 1
-    for (int k = 0; k < 32; ++k) {
-        T piv = __shfl_sync(0xffffffffu, r[0], k);
-        const double tiny = __shfl_sync(0xffffffffu, tiny_lane, k);
-        const int gcol = c0 + k < nb ? col_base + c0 + k : -1;
-        const bool bad = sflag ? (gcol >= 0 && !(double(piv) > tiny)) : !(piv > T(0));
-        if (bad) piv = panel_bad_pivot(piv, gcol, pv, sflag);
-        const T rs = recip_sqrt(piv);
-        const T lik = (lane == k) ? piv * rs : r[0] * rs;
-        if (lane >= k) Dt[k * LDD + lane] = lik;
-        if (lane == k) rdiag[c0 + k] = rs;
+    for (int k0 = 0; k0 < 32; k0 += 4) {
 #pragma unroll
-        for (int j = 1; j < 32; ++j) r[j] -= lik * __shfl_sync(0xffffffffu, lik, (k + j) & 31);
+        for (int t = 0; t < 4; ++t) {
+            const int k = k0 + t;
+            T piv = __shfl_sync(0xffffffffu, r[t], k);
+            const double tiny = __shfl_sync(0xffffffffu, tiny_lane, k);
+            const int gcol = c0 + k < nb ? col_base + c0 + k : -1;
+            const bool bad = sflag ? (gcol >= 0 && !(double(piv) > tiny)) : !(piv > T(0));
+            if (bad) piv = panel_bad_pivot(piv, gcol, pv, sflag);
+            const T rs = recip_sqrt(piv);
+            const T lik = (lane == k) ? piv * rs : r[t] * rs;
+            if (lane >= k) Dt[k * LDD + lane] = lik;
+            if (lane == k) rdiag[c0 + k] = rs;
+            T *lr = Lrot + k * 32;
+            lr[(lane - k) & 31] = lane >= k ? lik : T(0);
+            __syncwarp();
+            T c[32];
 #pragma unroll
-        for (int j = 0; j < 31; ++j) r[j] = r[j + 1];
+            for (int v = 0; v < NV; ++v) *reinterpret_cast<V *>(&c[v * E]) = reinterpret_cast<const V *>(lr)[v];
+#pragma unroll
+            for (int j = 1; j + t < 32; ++j) r[t + j] -= lik * c[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 28; ++j) r[j] = r[j + 4];
     }
     __syncwarp();
     T *It = Iv + c0 * LDD + c0;
@@ -174,14 +190,21 @@ __device__ __noinline__ void warp_diag_tile(T *D, T *Iv, T *rdiag, int LDD, int 
 #pragma unroll
     for (int i = 0; i < 32; ++i) y[i] = (i == lane) ? T(1) : T(0);
 #pragma unroll 1
-    for (int k = 0; k < 32; ++k) {
-        const T yk = y[0] * rdiag[c0 + k];
-        if (k >= lane) It[lane * LDD + k] = yk;
-        const T *lk = Dt + k * LDD;                  // column k of L
+    for (int k0 = 0; k0 < 32; k0 += 4) {
 #pragma unroll
-        for (int i = 1; i < 32; ++i) y[i] -= lk[(k + i) & 31] * yk;
+        for (int t = 0; t < 4; ++t) {
+            const int k = k0 + t;
+            const T yk = y[t] * rdiag[c0 + k];
+            if (k >= lane) It[lane * LDD + k] = yk;
+            const T *lr = Lrot + k * 32;
+            T c[32];
 #pragma unroll
-        for (int i = 0; i < 31; ++i) y[i] = y[i + 1];
+            for (int v = 0; v < NV; ++v) *reinterpret_cast<V *>(&c[v * E]) = reinterpret_cast<const V *>(lr)[v];
+#pragma unroll
+            for (int i = 1; i + t < 32; ++i) y[t + i] -= c[i] * yk;
+        }
+#pragma unroll
+        for (int i = 0; i < 28; ++i) y[i] = y[i + 4];
     }
     __syncwarp();
 }
@@ -279,6 +302,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask
     T *Iv = D + NBP * LDD;                           // inv(L), column-major, ld LDD
     T *P = Iv + NBP * LDD;                           // 6 x [32][33] partial products
     T *rdiag = P + 6 * 32 * 33;                      // reciprocal diagonal of L
+    T *Lrot = rdiag + NBP;                           // [32][32] rotated columns of a diagonal tile (16-byte aligned)
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     T *blk = factor + tk.off;
     __shared__ int refactor_flag;
@@ -320,7 +344,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask
     }
     __syncthreads();
     if (warp == 0)
-        warp_diag_tile(D, Iv, rdiag, LDD, 0, nb, lane, tk.col, pv.fail_col, pv.perturbed, pv.dorig, sflag);
+        warp_diag_tile(D, Iv, rdiag, Lrot, LDD, 0, nb, lane, tk.col, pv.fail_col, pv.perturbed, pv.dorig, sflag);
     __syncthreads();
     for (int I = 0; I < nblk; ++I) {
         const int c0 = 32 * I;
@@ -365,8 +389,8 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask
                 tile_mma(c, D + c0 * LDD + 32 * R, LDD, D + c0 * LDD + 32 * R, 1, LDD, lane);
                 tile_store(D + (32 * R) * LDD + 32 * R, LDD, c, T(-1), true, lane);
                 __syncwarp();
-                warp_diag_tile(D, Iv, rdiag, LDD, 32 * R, nb, lane, tk.col, pv.fail_col, pv.perturbed, pv.dorig,
-                               sflag);
+                warp_diag_tile(D, Iv, rdiag, Lrot, LDD, 32 * R, nb, lane, tk.col, pv.fail_col, pv.perturbed,
+                               pv.dorig, sflag);
             } else {
                 for (int u = warp; u < ntrail + nterm; u += 7) {
                     T c[4][8];
@@ -451,7 +475,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(const PanelTask
 size_t panel_smem_bytes(int nb, bool fp64) {
     const size_t el = fp64 ? 8 : 4;
     const size_t nbp = size_t((nb + 31) / 32) * 32;
-    return (2 * nbp * (nbp + 1) + 6 * 32 * 33 + nbp) * el;
+    return (2 * nbp * (nbp + 1) + 6 * 32 * 33 + nbp + 32 * 32) * el;
 }
 
 template <typename T>
