@@ -370,20 +370,23 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
                 const int nlk = int((S.w[s] + RB * DG - 1) / (RB * DG));
                 if (b < nlk) ftri.push_back({int32_t(s), b, flag_base[s], 0});
             }
-        // structure slabs: forward 64-row slabs x kStrChunk-column chunks, backward 64-column slabs x row chunks
+        // structure slabs (rows from w rounded down to a multiple of 4): forward kStrRows-row
+        // slabs x kStrCols-column chunks, backward kStrBCols-column slabs x row chunks
         L.fstr_off = int(fstr.size());
         L.fred_off = int(fred.size());
         L.bstr_off = int(bstr.size());
         L.bred_off = int(bred.size());
+        const idx brows = 32 * str_lane_rows(h->opt.precision != MFS_PREC_FP32);
         for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
             const idx s = S.level_list[k];
             if (S.d[s] == 0) continue;
-            const int nrs = int((S.d[s] + RB - 1) / RB), ncs = int((S.w[s] + kStrChunk - 1) / kStrChunk);
+            const idx span = S.f[s] - (S.w[s] & ~idx(3));
+            const int nrs = int((span + kStrRows - 1) / kStrRows), ncs = int((S.w[s] + kStrCols - 1) / kStrCols);
             for (int a = 0; a < nrs; ++a) {
                 fred.push_back({int32_t(s), a, int32_t(fstr.size()) - L.fstr_off, ncs});
                 for (int c = 0; c < ncs; ++c) fstr.push_back({int32_t(s), a, c, 0});
             }
-            const int nws = int((S.w[s] + RB - 1) / RB), nds = int((S.d[s] + kStrChunk - 1) / kStrChunk);
+            const int nws = int((S.w[s] + kStrBCols - 1) / kStrBCols), nds = int((span + brows - 1) / brows);
             for (int a = 0; a < nws; ++a) {
                 bred.push_back({int32_t(s), a, int32_t(bstr.size()) - L.bstr_off, nds});
                 for (int c = 0; c < nds; ++c) bstr.push_back({int32_t(s), a, c, 0});
@@ -433,7 +436,8 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     ds->large_dev.upload(ds->large_fronts, st);
     ds->all_list.upload(all_list, st);
     ds->inv_off.upload(inv_off, st);
-    ds->factor_alloc = std::max<int64_t>(inv_end, 1);
+    // (+64: the solves' 16-byte loads of a panel column may reach 3 elements past its end)
+    ds->factor_alloc = inv_end + 64;
     auto up = [&](auto &buf, const auto &vec) {
         buf.ensure(vec.size());
         if (!vec.empty())
@@ -635,6 +639,7 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         h->gemm_events_used += 2;
     };
     launch_zero<T>(factor, ds.panel_alloc, st);
+    launch_zero<T>(factor + (ds.factor_alloc - 64), 64, st);   // the tail the solves' vector loads may reach
     MFS_LAUNCHED();
     launch_inject<T>(ds.plan.p, int64_t(S.plan.size()), S.vb, S.src_ld, Ax, Bx, Bx ? sigma : 0.0, factor, st);
     MFS_LAUNCHED();
@@ -787,7 +792,7 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
     const int pass = sb ? kSbMaxRhs : kMaxSolveRhs;
     const int chunk = std::min(nrhs, pass);
     h->sol.ensure(size_t(std::max<idx>(S.sol_size, 1)) * chunk);
-    h->str_partials.ensure(size_t(std::max(ds.max_str_tasks, 1)) * solve_rows_per_task() * chunk);
+    h->str_partials.ensure(size_t(std::max(ds.max_str_tasks, 1)) * std::max(kStrRows, kStrBCols) * chunk);
     if (sb) {
         h->sb_scratch.ensure(size_t(std::max<idx>(S.n, 1)) * chunk);
         ensure_solve_maps(h, ds, factor, int(sizeof(T)));

@@ -163,7 +163,12 @@ struct SbTask {
     int32_t pmap, imap;
 };
 constexpr int kSuperBlock = 256;        // rows per superblock
-constexpr int kStrChunk = 512;
+// structure part of the solves: forward tasks are kStrRows rows x kStrCols columns
+// of L21, backward tasks kStrBCols columns x 32 * str_lane_rows rows
+constexpr int kStrRows = 128;
+constexpr int kStrCols = 512;
+constexpr int kStrBCols = 64;
+__host__ __device__ constexpr int str_lane_rows(bool fp64) { return fp64 ? 4 : 8; }
 constexpr int kSolveAsmRows = 256;      // front rows per forward extend-add CTA
 constexpr int kMaxSolveRhs = 16;        // right-hand sides per solve pass (more are chunked)
 constexpr int kSbMaxRhs = 8;            // right-hand sides per pass of the superblock solves

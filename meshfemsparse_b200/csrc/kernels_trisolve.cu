@@ -13,11 +13,11 @@
 //                          pair subtracts L11(rows, k) y_k for every earlier block k
 //                          (waiting on block k's epoch flag) and solves its two
 //                          triangles inside the CTA, publishing each block's flag;
-//             str_partial  P = L21(rows, chunk) y(chunk) for 64-row tiles of L21 and
+//             str_fwd      P = L21(rows, chunk) y(chunk) for 128-row slabs of L21 and
 //                          512-column chunks (independent tasks);
 //             fwd_reduce   u_s(rows) -= sum over chunks of P, in chunk order.
-//   backward  str_partial  P = L21(chunk, cols)^T x_struct for 64-column blocks and
-//                          512-row chunks of L21 (ancestors are final);
+//   backward  str_bwd      P = L21(chunk, cols)^T x_struct for 64-column blocks and
+//                          256-row (FP64: 128-row) chunks of L21 (ancestors are final);
 //             bwd_reduce   x(cols) -= sum over chunks of P, in chunk order;
 //             bwd_diag     L11^T x = y, pairs and blocks descending, waiting on flags.
 // Everything is summed in a fixed order: results are run-to-run identical.
@@ -190,13 +190,6 @@ __device__ __forceinline__ int stage_tile(T *dst, const T *pan, int64_t ld, int 
     return sh;
 }
 
-// shared memory of the structure kernels: out[kRB * nrhs] | vec[2][kRB * nrhs] (double) | tile[2][kRB][TL] |
-// FP32 copy of a vector slice (kRB * 4, FP32 factors)
-template <typename T>
-__host__ __device__ inline size_t str_smem(int nrhs) {
-    return size_t(3) * kRB * nrhs * sizeof(double) + size_t(2) * kRB * TileLd<T>::v * sizeof(T) +
-           size_t(kRB) * 4 * sizeof(double);
-}
 // shared memory of the diag kernels: acc[kDG][kRB * nrhs] | vec[kRB * nrhs] (double) |
 // tile[3][kRB][TL] (ring of two, in-task tile) | dblk[kDG][kRB][kRB + 1] (factor type)
 template <typename T>
@@ -582,189 +575,181 @@ __global__ void __launch_bounds__(kDiagThreads) bwd_diag_kernel(const SolveTask 
 }
 
 // Structure part, forward: P(task) = L21(rows, cols) y(cols); backward:
-// P(task) = L21(rows, cols)^T x(struct rows). One 64 x kStrChunk (or
-// kStrChunk x 64) slab of L21 per CTA, streamed as 64 x 64 tiles with the next
-// tile and its vector slice in flight (cp.async) while the current one is used.
-// P slab layout: P[r * kRB + a].
-template <typename T, bool FWD>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) str_partial_kernel(const StrTask *__restrict__ tasks, SnDev sd,
-                                                          const T *__restrict__ factor,
-                                                          const double *__restrict__ X, int64_t ldx, int nrhs,
-                                                          double *__restrict__ P) {
-    constexpr int TL = TileLd<T>::v;
-    extern __shared__ __align__(16) double smem_d[];
-    double *out = smem_d;                      // [kRB * nrhs]
-    double *vecs = out + kRB * nrhs;           // [2][kRB * nrhs]
-    T *tiles = reinterpret_cast<T *>(vecs + 2 * kRB * nrhs);   // [2][kRB][TL]
+// P(task) = L21(rows, cols)^T x(struct rows). Both stream L21 straight from global
+// memory with 16-byte loads (panel columns are 16-byte aligned; a task's rows start
+// at w rounded down to a multiple of 4), four right-hand sides per pass:
+//   forward   task = kStrRows aligned rows x kStrCols columns; lane = 4 rows of the
+//             slab (one or two loads per column), warp = every 8th column, the
+//             vector slice y(cols) in shared memory (broadcast); the 8 warps' row
+//             sums are added in a fixed order at the end;
+//   backward  task = kStrBCols columns x 32 * RL aligned rows; lane = RL rows whose
+//             x values it holds in registers, warp = every 8th column, one
+//             shuffle reduction per column.
+// Rows of a task outside the front's L21 (rows < w, or >= f) are read but never
+// used: the forward reduction skips them, the backward x values there are zero.
+// With an FP32 factor the products are FP32 (partials combined in FP64); an FP64
+// factor keeps FP64. P slab layout: P[task][r][rows or columns].
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    using type = float4;
+};
+template <>
+struct Vec16<double> {
+    using type = double2;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) str_fwd_kernel(const StrTask *__restrict__ tasks, SnDev sd,
+                                                      const T *__restrict__ factor, const double *__restrict__ X,
+                                                      int64_t ldx, int nrhs, double *__restrict__ P) {
+    using Q = std::conditional_t<sizeof(T) == 4, float, double>;
+    using V = typename Vec16<T>::type;
+    constexpr int E = 16 / int(sizeof(T));
+    constexpr int RPL = kStrRows / 32;                     // rows per lane (4)
+    constexpr int NVL = RPL / E;                           // loads per lane and column
+    extern __shared__ __align__(16) unsigned char str_raw[];
+    Q *ys = reinterpret_cast<Q *>(str_raw);                // [4][kStrCols]
+    Q *red = ys + 4 * kStrCols;                            // [8][4][kStrRows]
     const StrTask tk = tasks[blockIdx.x];
     const int s = tk.sn;
-    const int w = sd.w[s], d = sd.d[s], ld = sd.ld[s];
-    const int c0 = sd.col0[s];
+    const int w = sd.w[s], f = sd.f[s], ld = sd.ld[s], c0 = sd.col0[s];
+    const T *pan = factor + sd.pan_off[s];
+    const int rbase = (w & ~3) + tk.idx * kStrRows;
+    const int jb = tk.chunk * kStrCols, nj = min(w - jb, kStrCols);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int row0[NVL];
+    bool vok[NVL];
+#pragma unroll
+    for (int v = 0; v < NVL; ++v) {
+        row0[v] = rbase + v * 32 * E + E * lane;
+        vok[v] = row0[v] < f;
+    }
+    double *Pt = P + int64_t(blockIdx.x) * kStrRows * nrhs;
+    for (int g = 0; g < nrhs; g += 4) {
+        const int ng = min(4, nrhs - g);
+        __syncthreads();                                   // the previous pass is done with ys / red
+        for (int q = tid; q < 4 * kStrCols; q += 256) {
+            const int r = q / kStrCols, j = q - r * kStrCols;
+            ys[q] = (r < ng && j < nj) ? Q(X[c0 + jb + j + (g + r) * ldx]) : Q(0);
+        }
+        __syncthreads();
+        Q acc[RPL][4];
+#pragma unroll
+        for (int e = 0; e < RPL; ++e)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[e][r] = Q(0);
+#pragma unroll 4
+        for (int j = warp; j < nj; j += 8) {
+            const T *col = pan + int64_t(jb + j) * ld;
+            V lv[NVL];
+#pragma unroll
+            for (int v = 0; v < NVL; ++v) {
+                if (vok[v]) lv[v] = *reinterpret_cast<const V *>(col + row0[v]);
+                else lv[v] = V{};
+            }
+            Q yv[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) yv[r] = ys[r * kStrCols + j];
+#pragma unroll
+            for (int v = 0; v < NVL; ++v) {
+                const T *lp = reinterpret_cast<const T *>(&lv[v]);
+#pragma unroll
+                for (int e = 0; e < E; ++e)
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) acc[v * E + e][r] += Q(lp[e]) * yv[r];
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < NVL; ++v)
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    red[(warp * 4 + r) * kStrRows + v * 32 * E + E * lane + e] = acc[v * E + e][r];
+        __syncthreads();
+        for (int q = tid; q < ng * kStrRows; q += 256) {
+            const int r = q / kStrRows, i = q - r * kStrRows;
+            double sum = 0.0;
+#pragma unroll
+            for (int wi = 0; wi < 8; ++wi) sum += double(red[(wi * 4 + r) * kStrRows + i]);
+            Pt[(g + r) * kStrRows + i] = sum;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) str_bwd_kernel(const StrTask *__restrict__ tasks, SnDev sd,
+                                                      const T *__restrict__ factor, const double *__restrict__ X,
+                                                      int64_t ldx, int nrhs, double *__restrict__ P) {
+    using Q = std::conditional_t<sizeof(T) == 4, float, double>;
+    using V = typename Vec16<T>::type;
+    constexpr int E = 16 / int(sizeof(T));
+    constexpr int RL = str_lane_rows(sizeof(T) == 8);      // rows per lane
+    constexpr int NVL = RL / E;
+    const StrTask tk = tasks[blockIdx.x];
+    const int s = tk.sn;
+    const int w = sd.w[s], f = sd.f[s], ld = sd.ld[s], c0 = sd.col0[s];
     const int vb = sd.vb;
     const T *pan = factor + sd.pan_off[s];
     const int32_t *rows = sd.struct_rows + sd.struct_ptr[s];
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int nq = kRB * nrhs;
-    // FWD: fixed 64 struct rows [a0, a0+na), 64-column blocks of the chunk
-    // BWD: fixed 64 columns [a0, a0+na), 64-row blocks of the chunk
-    const int a0 = tk.idx * kRB;
-    const int na = FWD ? min(kRB, d - a0) : min(kRB, w - a0);
-    const int lim = FWD ? w : d;
-    const int b_begin = tk.chunk * kStrChunk, b_end = min(lim, b_begin + kStrChunk);
-    const int nblk = (b_end - b_begin + kRB - 1) / kRB;
-    int sh = 0;
-    auto stage = [&](int b, int buf) {
-        const int b0 = b_begin + b * kRB, nbk = min(kRB, b_end - b0);
-        double *v = vecs + buf * nq;
-        if (FWD) {
-            sh = stage_tile<T, TL>(tiles + buf * kRB * TL, pan, ld, w + a0, na, b0, nbk, tid, nt);
-            for (int q = tid; q < nq; q += nt) {
-                const int j = q & (kRB - 1), r = q >> 6;
-                if (j < nbk) cpa8(v + q, X + c0 + b0 + j + r * ldx);
-            }
-        } else {
-            sh = stage_tile<T, TL>(tiles + buf * kRB * TL, pan, ld, w + b0, nbk, a0, na, tid, nt);
-            for (int q = tid; q < nq; q += nt) {
-                const int i = q & (kRB - 1), r = q >> 6;
-                const int li = b0 + i;
-                if (i < nbk) cpa8(v + q, X + int64_t(rows[li / vb]) * vb + li % vb + r * ldx);
-            }
-        }
-        cpa_commit();
-    };
-    // Up to 4 right-hand sides (the common case) accumulate in registers:
-    //   FWD: thread = (row pair a, a + 32) x (8-column group of the tile), summed over
-    //        the groups at the end; BWD: lane = (row pair i, i + 32), warp = 8 columns,
-    //        summed over the lanes at the end.
-    // With an FP32 factor (the preconditioner of FP64 refinement) the products and the
-    // chunk's partial sums are FP32: each tile's vector slice is rounded to FP32 once;
-    // chunk partials are reduced in FP64. An FP64 factor keeps FP64 throughout.
-    // More right-hand sides take the generic per-(row, rhs) loop.
-    using Acc = std::conditional_t<sizeof(T) == 4, float, double>;
-    constexpr bool kF32 = sizeof(T) == 4;
-    Acc *vf = reinterpret_cast<Acc *>(tiles + 2 * kRB * TL);   // [kRB * 4] FP32 copy of the slice
-    const bool fast = nrhs <= 4;
-    const int lane = tid & 31, wgrp = tid >> 5;
-    Acc racc[FWD ? 2 : 8][4];
+    const int rbase = (w & ~3) + tk.chunk * 32 * RL;
+    const int j0 = tk.idx * kStrBCols, nj = min(kStrBCols, w - j0);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int row0[NVL];
+    bool vok[NVL];
 #pragma unroll
-    for (int c = 0; c < (FWD ? 2 : 8); ++c)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) racc[c][r] = Acc(0);
-    for (int q = tid; q < nq; q += nt) out[q] = 0.0;
-    stage(0, 0);
-    for (int b = 0; b < nblk; ++b) {
-        const int buf = b & 1;
-        const int nbk = min(kRB, b_end - (b_begin + b * kRB));
-        if (b + 1 < nblk) stage(b + 1, buf ^ 1);
-        else cpa_commit();
-        cpa_wait<1>();
-        __syncthreads();
-        const T *tl = tiles + buf * kRB * TL + sh;
-        const double *v = vecs + buf * nq;
-        if (fast) {
-            const Acc *va;
-            if constexpr (kF32) {
-                for (int q = tid; q < nq; q += nt) vf[q] = Acc(v[q]);
-                __syncthreads();
-                va = vf;
-            } else {
-                va = v;
-            }
-            if (FWD) {
-#pragma unroll
-                for (int jj = 0; jj < 8; ++jj) {
-                    const int j = 8 * wgrp + jj;
-                    if (j < nbk) {
-                        const Acc t0 = Acc(tl[j * TL + lane]), t1 = Acc(tl[j * TL + lane + 32]);
-#pragma unroll
-                        for (int r = 0; r < 4; ++r)
-                            if (r < nrhs) {
-                                const Acc vv = va[r * kRB + j];
-                                racc[0][r] += t0 * vv;
-                                racc[1][r] += t1 * vv;
-                            }
-                    }
-                }
-            } else {
-                Acc x0[4], x1[4];
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    x0[r] = (r < nrhs && lane < nbk) ? va[r * kRB + lane] : Acc(0);
-                    x1[r] = (r < nrhs && lane + 32 < nbk) ? va[r * kRB + lane + 32] : Acc(0);
-                }
-#pragma unroll
-                for (int c = 0; c < (FWD ? 2 : 8); ++c) {
-                    const int a = 8 * wgrp + c;
-                    const Acc t0 = lane < nbk ? Acc(tl[a * TL + lane]) : Acc(0);
-                    const Acc t1 = lane + 32 < nbk ? Acc(tl[a * TL + lane + 32]) : Acc(0);
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) racc[c][r] += t0 * x0[r] + t1 * x1[r];
-                }
-            }
-        } else {
-            for (int q = tid; q < nq; q += nt) {
-                const int a = q & (kRB - 1), r = q >> 6;
-                const double *vr = v + r * kRB;
-                double a0s = 0.0, a1s = 0.0;
-                if (FWD) {
-                    // out(a) += sum_j L(w + a0 + a, b0 + j) y(b0 + j)
-                    int j = 0;
-#pragma unroll 4
-                    for (; j + 1 < nbk; j += 2) {
-                        a0s += double(tl[j * TL + a]) * vr[j];
-                        a1s += double(tl[(j + 1) * TL + a]) * vr[j + 1];
-                    }
-                    if (j < nbk) a0s += double(tl[j * TL + a]) * vr[j];
-                } else {
-                    // out(a) += sum_i L(w + b0 + i, a0 + a) x(struct row b0 + i), rows in skewed order
-#pragma unroll 8
-                    for (int u = 0; u < kRB; u += 2) {
-                        const int i = (u + a) & (kRB - 1), i1 = (u + 1 + a) & (kRB - 1);
-                        a0s += (i < nbk ? double(tl[a * TL + i]) * vr[i] : 0.0);
-                        a1s += (i1 < nbk ? double(tl[a * TL + i1]) * vr[i1] : 0.0);
-                    }
-                }
-                out[q] += a0s + a1s;
-            }
-        }
-        __syncthreads();                       // buffer `buf` is refilled at b + 2
+    for (int v = 0; v < NVL; ++v) {
+        row0[v] = rbase + v * 32 * E + E * lane;
+        vok[v] = row0[v] < f;
     }
-    cpa_wait<0>();
-    if (fast) {
-        if (FWD) {
-            // sum the 8 column groups: red[(group * 4 + r) * kRB + a] in the (now idle) tile buffers
-            double *red = reinterpret_cast<double *>(tiles);
+    double *Pt = P + int64_t(blockIdx.x) * kStrBCols * nrhs;
+    for (int g = 0; g < nrhs; g += 4) {
+        const int ng = min(4, nrhs - g);
+        // this lane's x values (zero outside the front's L21 rows)
+        Q xv[RL][4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
-                if (r < nrhs) {
-                    red[(wgrp * 4 + r) * kRB + lane] = double(racc[0][r]);
-                    red[(wgrp * 4 + r) * kRB + lane + 32] = double(racc[1][r]);
-                }
-            __syncthreads();
-            for (int q = tid; q < nq; q += nt) {
-                const int a = q & (kRB - 1), r = q >> 6;
-                double sacc = 0.0;
-                for (int g = 0; g < 8; ++g) sacc += red[(g * 4 + r) * kRB + a];
-                out[q] = sacc;
+        for (int v = 0; v < NVL; ++v)
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int row = row0[v] + e, li = row - w;
+                const bool ok = row >= w && row < f;
+                const int64_t xr = ok ? int64_t(rows[li / vb]) * vb + li % vb : 0;
+#pragma unroll
+                for (int r = 0; r < 4; ++r) xv[v * E + e][r] = (ok && r < ng) ? Q(X[xr + (g + r) * ldx]) : Q(0);
             }
-        } else {
+#pragma unroll 2
+        for (int jj = warp; jj < nj; jj += 8) {
+            const T *col = pan + int64_t(j0 + jj) * ld;
+            V lv[NVL];
 #pragma unroll
-            for (int c = 0; c < (FWD ? 2 : 8); ++c)
+            for (int v = 0; v < NVL; ++v) {
+                if (vok[v]) lv[v] = *reinterpret_cast<const V *>(col + row0[v]);
+                else lv[v] = V{};
+            }
+            Q a[4] = {Q(0), Q(0), Q(0), Q(0)};
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    double g = double(racc[c][r]);
+            for (int v = 0; v < NVL; ++v) {
+                const T *lp = reinterpret_cast<const T *>(&lv[v]);
 #pragma unroll
-                    for (int off = 16; off > 0; off >>= 1) g += __shfl_down_sync(0xffffffffu, g, off);
-                    if (lane == 0 && r < nrhs) out[r * kRB + 8 * wgrp + c] = g;
-                }
+                for (int e = 0; e < E; ++e)
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) a[r] += Q(lp[e]) * xv[v * E + e][r];
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                Q sum = a[r];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+                if (lane == 0 && r < ng) Pt[(g + r) * kStrBCols + jj] = double(sum);
+            }
         }
     }
-    __syncthreads();
-    double *Pt = P + int64_t(blockIdx.x) * nq;
-    for (int q = tid; q < nq; q += nt) Pt[q] = out[q];
 }
 
-// Subtract the chunk partials of one 64-row (FWD: of u_s) or 64-column (BWD: of x) slab, in chunk order.
+// Subtract the chunk partials of one forward row slab (from u_s) or backward column
+// slab (from x), in chunk order.
 template <bool FWD>
 __global__ void __launch_bounds__(256) str_reduce_kernel(const StrReduce *__restrict__ red, SnDev sd,
                                                          double *__restrict__ X, int64_t ldx, int nrhs,
@@ -772,14 +757,19 @@ __global__ void __launch_bounds__(256) str_reduce_kernel(const StrReduce *__rest
     const StrReduce rd = red[blockIdx.x];
     const int s = rd.sn;
     const int w = sd.w[s], d = sd.d[s];
-    const int a0 = rd.idx * kRB;
-    const int na = FWD ? min(kRB, d - a0) : min(kRB, w - a0);
-    for (int q = threadIdx.x; q < na * nrhs; q += blockDim.x) {
-        const int a = q % na, r = q / na;
+    constexpr int NS = FWD ? kStrRows : kStrBCols;
+    const int64_t stride = int64_t(NS) * nrhs;
+    for (int q = threadIdx.x; q < NS * nrhs; q += blockDim.x) {
+        const int a = q % NS, r = q / NS;
         double acc = 0.0;
-        for (int c = 0; c < rd.nchunks; ++c) acc += P[int64_t(rd.first + c) * kRB * nrhs + r * kRB + a];
-        if (FWD) sol[sd.sol_off[s] * nrhs + (a0 + a) + int64_t(r) * d] -= acc;
-        else X[sd.col0[s] + a0 + a + r * ldx] -= acc;
+        for (int c = 0; c < rd.nchunks; ++c) acc += P[int64_t(rd.first + c) * stride + r * NS + a];
+        if (FWD) {
+            const int drow = (w & ~3) + rd.idx * kStrRows + a - w;
+            if (drow >= 0 && drow < d) sol[sd.sol_off[s] * nrhs + drow + int64_t(r) * d] -= acc;
+        } else {
+            const int col = rd.idx * kStrBCols + a;
+            if (col < w) X[sd.col0[s] + col + r * ldx] -= acc;
+        }
     }
 }
 
@@ -833,19 +823,15 @@ void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce 
                 const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st) {
     if (ntasks <= 0) return;
     g_kernel_launches += 2;
-    const size_t smem = str_smem<T>(nrhs);
+    using Q = std::conditional_t<sizeof(T) == 4, float, double>;
+    const size_t smem = size_t(4) * (kStrCols + 8 * kStrRows) * sizeof(Q);
     static PerDeviceOnce once;
-    once([] {
-        cudaFuncSetAttribute(str_partial_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(str_smem<T>(kMaxSolveRhs)));
-        cudaFuncSetAttribute(str_partial_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(str_smem<T>(kMaxSolveRhs)));
-    });
+    once([smem] { cudaFuncSetAttribute(str_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); });
     if (forward) {
-        str_partial_kernel<T, true><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
+        str_fwd_kernel<T><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
         str_reduce_kernel<true><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
     } else {
-        str_partial_kernel<T, false><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
+        str_bwd_kernel<T><<<ntasks, 256, 0, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
         str_reduce_kernel<false><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
     }
 }
