@@ -343,7 +343,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     std::vector<SolveTask> ftri, btri;
     std::vector<StrTask> fstr, bstr;
     std::vector<StrReduce> fred, bred;
-    int max_str = 0;
+    int64_t max_str = 0;                          // partial-sum entries of one level and one right-hand side
     for (idx l = 0; l < S.nlevels; ++l) {
         LevelPlan &L = ds->levels[l];
         L.sasm_off = int(sasm.size());
@@ -376,7 +376,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         L.fred_off = int(fred.size());
         L.bstr_off = int(bstr.size());
         L.bred_off = int(bred.size());
-        const idx brows = 32 * str_lane_rows(h->opt.precision != MFS_PREC_FP32);
+        const idx brows = str_bwd_rows(h->opt.precision != MFS_PREC_FP32);
         for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
             const idx s = S.level_list[k];
             if (S.d[s] == 0) continue;
@@ -396,7 +396,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
         L.fred_n = int(fred.size()) - L.fred_off;
         L.bstr_n = int(bstr.size()) - L.bstr_off;
         L.bred_n = int(bred.size()) - L.bred_off;
-        max_str = std::max(max_str, std::max(L.fstr_n, L.bstr_n));
+        max_str = std::max<int64_t>(max_str, std::max(int64_t(L.fstr_n) * kStrRows, int64_t(L.bstr_n) * kStrBCols));
         for (int p = 0; p < maxnbw; ++p)
             for (idx k = S.level_ptr[l]; k < S.level_ptr[l + 1]; ++k) {
                 const idx s = S.level_list[k];
@@ -468,7 +468,7 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
     up(ds->isb_tasks, isb);
     ds->nsb_inv = int(isb.size());
     ds->isb_host = isb;
-    ds->max_str_tasks = max_str;
+    ds->max_str_entries = max_str;
     {
         std::vector<int2> sv(S.sub_lo.size());
         for (size_t k = 0; k < sv.size(); ++k) sv[k] = make_int2(int(S.sub_lo[k]), int(S.sub_hi[k]));
@@ -792,7 +792,7 @@ void run_solve(mfs_handle *h, DevSym &ds, const T *factor, double *X, int nrhs) 
     const int pass = sb ? kSbMaxRhs : kMaxSolveRhs;
     const int chunk = std::min(nrhs, pass);
     h->sol.ensure(size_t(std::max<idx>(S.sol_size, 1)) * chunk);
-    h->str_partials.ensure(size_t(std::max(ds.max_str_tasks, 1)) * std::max(kStrRows, kStrBCols) * chunk);
+    h->str_partials.ensure(size_t(std::max<int64_t>(ds.max_str_entries, 1)) * chunk);
     if (sb) {
         h->sb_scratch.ensure(size_t(std::max<idx>(S.n, 1)) * chunk);
         ensure_solve_maps(h, ds, factor, int(sizeof(T)));

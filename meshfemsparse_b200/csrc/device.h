@@ -164,11 +164,11 @@ struct SbTask {
 };
 constexpr int kSuperBlock = 256;        // rows per superblock
 // structure part of the solves: forward tasks are kStrRows rows x kStrCols columns
-// of L21, backward tasks kStrBCols columns x 32 * str_lane_rows rows
-constexpr int kStrRows = 128;
-constexpr int kStrCols = 512;
+// of L21, backward tasks kStrBCols columns x str_bwd_rows rows
+constexpr int kStrRows = 1024;
+constexpr int kStrCols = 256;
 constexpr int kStrBCols = 64;
-__host__ __device__ constexpr int str_lane_rows(bool fp64) { return fp64 ? 4 : 8; }
+__host__ __device__ constexpr int str_bwd_rows(bool fp64) { return fp64 ? 1024 : 2048; }
 constexpr int kSolveAsmRows = 256;      // front rows per forward extend-add CTA
 constexpr int kMaxSolveRhs = 16;        // right-hand sides per solve pass (more are chunked)
 constexpr int kSbMaxRhs = 8;            // right-hand sides per pass of the superblock solves

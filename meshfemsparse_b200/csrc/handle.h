@@ -111,7 +111,7 @@ struct DevSym {
     int nsb_inv = 0;
     std::vector<SbTask> isb_host;                   // the superblocks (their inverses' offsets)
     std::vector<int32_t> sb_fronts;                 // fronts with superblock solves
-    int max_str_tasks = 0;
+    int64_t max_str_entries = 0;       // structure partial sums of one level, per right-hand side
     DBuf<int2> subs;                     // subtree ranges solved one per CTA (levels <= solve_cut)
     int nsub = 0, sub_fmax = 0, solve_cut = -1;
     DBuf<int> flags;                     // one per 64-row diagonal block of every front

@@ -13,11 +13,11 @@
 //                          pair subtracts L11(rows, k) y_k for every earlier block k
 //                          (waiting on block k's epoch flag) and solves its two
 //                          triangles inside the CTA, publishing each block's flag;
-//             str_fwd      P = L21(rows, chunk) y(chunk) for 128-row slabs of L21 and
-//                          512-column chunks (independent tasks);
+//             str_fwd      P = L21(rows, chunk) y(chunk) for 1024-row slabs of L21 and
+//                          256-column chunks (independent tasks);
 //             fwd_reduce   u_s(rows) -= sum over chunks of P, in chunk order.
 //   backward  str_bwd      P = L21(chunk, cols)^T x_struct for 64-column blocks and
-//                          256-row (FP64: 128-row) chunks of L21 (ancestors are final);
+//                          2048-row (FP64: 1024-row) chunks of L21 (ancestors are final);
 //             bwd_reduce   x(cols) -= sum over chunks of P, in chunk order;
 //             bwd_diag     L11^T x = y, pairs and blocks descending, waiting on flags.
 // Everything is summed in a fixed order: results are run-to-run identical.
@@ -578,17 +578,21 @@ __global__ void __launch_bounds__(kDiagThreads) bwd_diag_kernel(const SolveTask 
 // P(task) = L21(rows, cols)^T x(struct rows). Both stream L21 straight from global
 // memory with 16-byte loads (panel columns are 16-byte aligned; a task's rows start
 // at w rounded down to a multiple of 4), four right-hand sides per pass:
-//   forward   task = kStrRows aligned rows x kStrCols columns; lane = 4 rows of the
-//             slab (one or two loads per column), warp = every 8th column, the
-//             vector slice y(cols) in shared memory (broadcast); the 8 warps' row
-//             sums are added in a fixed order at the end;
-//   backward  task = kStrBCols columns x 32 * RL aligned rows; lane = RL rows whose
-//             x values it holds in registers, warp = every 8th column, one
-//             shuffle reduction per column.
+//   forward   task = kStrRows aligned rows x kStrCols columns; warp = 128 of the
+//             rows (lane = 4 of them: one FP32 / two FP64 loads per column) over all
+//             the task's columns, the vector slice y(cols) in shared memory
+//             (broadcast); no sums across warps;
+//   backward  task = kStrBCols columns x kStrBRows aligned rows, the x slice in
+//             shared memory; warp = 8 columns, lane = 4 rows of every 128: per
+//             128-row block the lane's x values go to registers once and serve the
+//             warp's 8 columns (8 independent loads in flight); one shuffle
+//             reduction per column at the end.
 // Rows of a task outside the front's L21 (rows < w, or >= f) are read but never
-// used: the forward reduction skips them, the backward x values there are zero.
-// With an FP32 factor the products are FP32 (partials combined in FP64); an FP64
-// factor keeps FP64. P slab layout: P[task][r][rows or columns].
+// used: the forward reduction skips them, the backward x values there are zero
+// (the values read there are finite: panel entries, zeroed padding, or the zeroed
+// tail of the factor array). With an FP32 factor the products are FP32 (partials
+// combined in FP64); an FP64 factor keeps FP64. P slab layout: P[task][r][rows or
+// columns].
 template <typename T>
 struct Vec16;
 template <>
@@ -607,18 +611,15 @@ __global__ void __launch_bounds__(256) str_fwd_kernel(const StrTask *__restrict_
     using Q = std::conditional_t<sizeof(T) == 4, float, double>;
     using V = typename Vec16<T>::type;
     constexpr int E = 16 / int(sizeof(T));
-    constexpr int RPL = kStrRows / 32;                     // rows per lane (4)
-    constexpr int NVL = RPL / E;                           // loads per lane and column
-    extern __shared__ __align__(16) unsigned char str_raw[];
-    Q *ys = reinterpret_cast<Q *>(str_raw);                // [4][kStrCols]
-    Q *red = ys + 4 * kStrCols;                            // [8][4][kStrRows]
+    constexpr int NVL = 4 / E;                             // loads per lane and column (4 rows)
+    __shared__ __align__(16) Q ys[4][kStrCols];
     const StrTask tk = tasks[blockIdx.x];
     const int s = tk.sn;
     const int w = sd.w[s], f = sd.f[s], ld = sd.ld[s], c0 = sd.col0[s];
     const T *pan = factor + sd.pan_off[s];
-    const int rbase = (w & ~3) + tk.idx * kStrRows;
-    const int jb = tk.chunk * kStrCols, nj = min(w - jb, kStrCols);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int rbase = (w & ~3) + tk.idx * kStrRows + warp * 128;
+    const int jb = tk.chunk * kStrCols, nj = min(w - jb, kStrCols);
     int row0[NVL];
     bool vok[NVL];
 #pragma unroll
@@ -626,23 +627,25 @@ __global__ void __launch_bounds__(256) str_fwd_kernel(const StrTask *__restrict_
         row0[v] = rbase + v * 32 * E + E * lane;
         vok[v] = row0[v] < f;
     }
-    double *Pt = P + int64_t(blockIdx.x) * kStrRows * nrhs;
+    const bool active = rbase < f;
+    double *Pt = P + int64_t(blockIdx.x) * kStrRows * nrhs + warp * 128;
     for (int g = 0; g < nrhs; g += 4) {
         const int ng = min(4, nrhs - g);
-        __syncthreads();                                   // the previous pass is done with ys / red
+        __syncthreads();                                   // the previous pass is done with ys
         for (int q = tid; q < 4 * kStrCols; q += 256) {
             const int r = q / kStrCols, j = q - r * kStrCols;
-            ys[q] = (r < ng && j < nj) ? Q(X[c0 + jb + j + (g + r) * ldx]) : Q(0);
+            ys[r][j] = (r < ng && j < nj) ? Q(X[c0 + jb + j + (g + r) * ldx]) : Q(0);
         }
         __syncthreads();
-        Q acc[RPL][4];
+        if (!active) continue;
+        Q acc[4][4];
 #pragma unroll
-        for (int e = 0; e < RPL; ++e)
+        for (int e = 0; e < 4; ++e)
 #pragma unroll
             for (int r = 0; r < 4; ++r) acc[e][r] = Q(0);
-#pragma unroll 4
-        for (int j = warp; j < nj; j += 8) {
-            const T *col = pan + int64_t(jb + j) * ld;
+        const T *col = pan + int64_t(jb) * ld;
+#pragma unroll 8
+        for (int j = 0; j < nj; ++j, col += ld) {
             V lv[NVL];
 #pragma unroll
             for (int v = 0; v < NVL; ++v) {
@@ -651,7 +654,7 @@ __global__ void __launch_bounds__(256) str_fwd_kernel(const StrTask *__restrict_
             }
             Q yv[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) yv[r] = ys[r * kStrCols + j];
+            for (int r = 0; r < 4; ++r) yv[r] = ys[r][j];
 #pragma unroll
             for (int v = 0; v < NVL; ++v) {
                 const T *lp = reinterpret_cast<const T *>(&lv[v]);
@@ -667,15 +670,7 @@ __global__ void __launch_bounds__(256) str_fwd_kernel(const StrTask *__restrict_
             for (int e = 0; e < E; ++e)
 #pragma unroll
                 for (int r = 0; r < 4; ++r)
-                    red[(warp * 4 + r) * kStrRows + v * 32 * E + E * lane + e] = acc[v * E + e][r];
-        __syncthreads();
-        for (int q = tid; q < ng * kStrRows; q += 256) {
-            const int r = q / kStrRows, i = q - r * kStrRows;
-            double sum = 0.0;
-#pragma unroll
-            for (int wi = 0; wi < 8; ++wi) sum += double(red[(wi * 4 + r) * kStrRows + i]);
-            Pt[(g + r) * kStrRows + i] = sum;
-        }
+                    if (r < ng) Pt[(g + r) * kStrRows + v * 32 * E + E * lane + e] = double(acc[v * E + e][r]);
     }
 }
 
@@ -686,65 +681,85 @@ __global__ void __launch_bounds__(256) str_bwd_kernel(const StrTask *__restrict_
     using Q = std::conditional_t<sizeof(T) == 4, float, double>;
     using V = typename Vec16<T>::type;
     constexpr int E = 16 / int(sizeof(T));
-    constexpr int RL = str_lane_rows(sizeof(T) == 8);      // rows per lane
-    constexpr int NVL = RL / E;
+    constexpr int NVL = 4 / E;                             // loads per lane, column and 128-row block
+    constexpr int BR = str_bwd_rows(sizeof(T) == 8);
+    extern __shared__ __align__(16) unsigned char str_raw[];
+    Q *xs = reinterpret_cast<Q *>(str_raw);                // [4][BR]
     const StrTask tk = tasks[blockIdx.x];
     const int s = tk.sn;
     const int w = sd.w[s], f = sd.f[s], ld = sd.ld[s], c0 = sd.col0[s];
     const int vb = sd.vb;
     const T *pan = factor + sd.pan_off[s];
     const int32_t *rows = sd.struct_rows + sd.struct_ptr[s];
-    const int rbase = (w & ~3) + tk.chunk * 32 * RL;
-    const int j0 = tk.idx * kStrBCols, nj = min(kStrBCols, w - j0);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    int row0[NVL];
-    bool vok[NVL];
-#pragma unroll
-    for (int v = 0; v < NVL; ++v) {
-        row0[v] = rbase + v * 32 * E + E * lane;
-        vok[v] = row0[v] < f;
-    }
-    double *Pt = P + int64_t(blockIdx.x) * kStrBCols * nrhs;
+    const int rbase = (w & ~3) + tk.chunk * BR;
+    const int nrb = min(BR, f - rbase + 127) / 128;        // 128-row blocks reaching row f - 1
+    const int j0 = tk.idx * kStrBCols + (threadIdx.x >> 5) * 8;
+    const int nj = max(0, min(8, w - j0));
+    const int tid = threadIdx.x, lane = tid & 31;
+    double *Pt = P + int64_t(blockIdx.x) * kStrBCols * nrhs + (threadIdx.x >> 5) * 8;
     for (int g = 0; g < nrhs; g += 4) {
         const int ng = min(4, nrhs - g);
-        // this lane's x values (zero outside the front's L21 rows)
-        Q xv[RL][4];
+        __syncthreads();
+        for (int q = tid; q < 4 * BR; q += 256) {
+            const int r = q / BR, i = q - r * BR;
+            const int row = rbase + i, li = row - w;
+            Q v = Q(0);
+            if (r < ng && row >= w && row < f) v = Q(X[int64_t(rows[li / vb]) * vb + li % vb + (g + r) * ldx]);
+            xs[q] = v;
+        }
+        __syncthreads();
+        Q acc[8][4];
 #pragma unroll
-        for (int v = 0; v < NVL; ++v)
+        for (int u = 0; u < 8; ++u)
 #pragma unroll
-            for (int e = 0; e < E; ++e) {
-                const int row = row0[v] + e, li = row - w;
-                const bool ok = row >= w && row < f;
-                const int64_t xr = ok ? int64_t(rows[li / vb]) * vb + li % vb : 0;
-#pragma unroll
-                for (int r = 0; r < 4; ++r) xv[v * E + e][r] = (ok && r < ng) ? Q(X[xr + (g + r) * ldx]) : Q(0);
-            }
-#pragma unroll 2
-        for (int jj = warp; jj < nj; jj += 8) {
-            const T *col = pan + int64_t(j0 + jj) * ld;
-            V lv[NVL];
-#pragma unroll
-            for (int v = 0; v < NVL; ++v) {
-                if (vok[v]) lv[v] = *reinterpret_cast<const V *>(col + row0[v]);
-                else lv[v] = V{};
-            }
-            Q a[4] = {Q(0), Q(0), Q(0), Q(0)};
+            for (int r = 0; r < 4; ++r) acc[u][r] = Q(0);
+        for (int b = 0; b < nrb; ++b) {
+            int row0[NVL];
+            bool vok[NVL];
+            Q xv[4][4];
 #pragma unroll
             for (int v = 0; v < NVL; ++v) {
-                const T *lp = reinterpret_cast<const T *>(&lv[v]);
+                const int i0 = b * 128 + v * 32 * E + E * lane;
+                row0[v] = rbase + i0;
+                vok[v] = row0[v] < f;
 #pragma unroll
-                for (int e = 0; e < E; ++e)
+                for (int r = 0; r < 4; ++r) {
+                    const V xv4 = *reinterpret_cast<const V *>(xs + r * BR + i0);
+                    const Q *xp = reinterpret_cast<const Q *>(&xv4);
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) a[r] += Q(lp[e]) * xv[v * E + e][r];
+                    for (int e = 0; e < E; ++e) xv[v * E + e][r] = xp[e];
+                }
             }
+            V lv[8][NVL];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const T *col = pan + int64_t(j0 + min(u, nj - 1)) * ld;
+#pragma unroll
+                for (int v = 0; v < NVL; ++v) {
+                    if (vok[v] && u < nj) lv[u][v] = *reinterpret_cast<const V *>(col + row0[v]);
+                    else lv[u][v] = V{};
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int v = 0; v < NVL; ++v) {
+                    const T *lp = reinterpret_cast<const T *>(&lv[u][v]);
+#pragma unroll
+                    for (int e = 0; e < E; ++e)
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) acc[u][r] += Q(lp[e]) * xv[v * E + e][r];
+                }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                Q sum = a[r];
+                Q sum = acc[u][r];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
-                if (lane == 0 && r < ng) Pt[(g + r) * kStrBCols + jj] = double(sum);
+                if (lane == 0 && r < ng && u < nj) Pt[(g + r) * kStrBCols + u] = double(sum);
             }
-        }
     }
 }
 
@@ -824,14 +839,14 @@ void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce 
     if (ntasks <= 0) return;
     g_kernel_launches += 2;
     using Q = std::conditional_t<sizeof(T) == 4, float, double>;
-    const size_t smem = size_t(4) * (kStrCols + 8 * kStrRows) * sizeof(Q);
+    const size_t smem = size_t(4) * str_bwd_rows(sizeof(T) == 8) * sizeof(Q);
     static PerDeviceOnce once;
-    once([smem] { cudaFuncSetAttribute(str_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); });
+    once([smem] { cudaFuncSetAttribute(str_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); });
     if (forward) {
-        str_fwd_kernel<T><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
+        str_fwd_kernel<T><<<ntasks, 256, 0, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
         str_reduce_kernel<true><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
     } else {
-        str_bwd_kernel<T><<<ntasks, 256, 0, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
+        str_bwd_kernel<T><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
         str_reduce_kernel<false><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
     }
 }
