@@ -236,20 +236,6 @@ def run_b200(args, rank, world, local, dist):
                           C.c_void_p(X_h.data_ptr()), 0)
     e2e_ms = tot_e2e / K_e2e
 
-    out64 = {}
-    if not args.no_fp64:
-        f64, _ = make(False)
-        X64 = torch.empty_like(B_dev)
-        K64 = max(1, min(args.steps, 3))
-        tot64, _, _ = timed(f64, K64, 1, pK, pB, C.c_void_p(X64.data_ptr()), D)
-        ms64 = tot64 / K64
-        st64 = f64.stats()
-        out64 = {"fp64_plain_solves_per_s": world * 1000.0 / ms64, "fp64_plain_ms_per_step": ms64,
-                 "fp64_factor_ms": st64["factor_ms"], "fp64_solve_ms": st64["solve_ms"],
-                 "fp64_residual": residual(f64, X64),
-                 "speedup_fp32_refine_vs_fp64_plain": ms64 / ms32}
-        del f64
-
     peaks, peak_kind = measured_peaks()
     flops = f32.getFlopEstimate()
     achieved_seq = flops / (st32["factor_ms"] * 1e-3) / 1e12
@@ -264,6 +250,29 @@ def run_b200(args, rank, world, local, dist):
     f32._opts.time_kernels = 0
     _lib.check(lib.mfs_set_options(f32._h, C.byref(f32._opts)), f32._h, "options")
     gemm_tf = stk["gemm_flops"] / (stk["gemm_ms"] * 1e-3) / 1e12 if stk["gemm_ms"] > 0 else None
+    flops_est, nnz32, nred = flops, f32.getFactorNNZ(), f32.n_reduced()
+    sym = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sym = (f32.supernodes(), f32.conversionPlan(), f32._row_maps()[1])
+    # the FP32 handle is released before the FP64 arm (the largest workloads do not
+    # hold both factorizations at once)
+    del f32
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    out64 = {}
+    if not args.no_fp64:
+        f64, _ = make(False)
+        X64 = torch.empty_like(B_dev)
+        K64 = max(1, min(args.steps, 3))
+        tot64, _, _ = timed(f64, K64, 1, pK, pB, C.c_void_p(X64.data_ptr()), D)
+        ms64 = tot64 / K64
+        st64 = f64.stats()
+        out64 = {"fp64_plain_solves_per_s": world * 1000.0 / ms64, "fp64_plain_ms_per_step": ms64,
+                 "fp64_factor_ms": st64["factor_ms"], "fp64_solve_ms": st64["solve_ms"],
+                 "fp64_residual": residual(f64, X64),
+                 "speedup_fp32_refine_vs_fp64_plain": ms64 / ms32}
+        del f64
+
     peak = peaks["bf16_tflops_sustained"]
     half = args.tc in (0, 5)
     roofline = {"bound": "tensor", "achieved": gemm_tf, "peak": peak, "unit": "TFLOP/s",
@@ -280,7 +289,7 @@ def run_b200(args, rank, world, local, dist):
         "metric": METRIC, "value": world * 1000.0 * 1.0 / ms32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 factor / f64 refine", "data": "synthetic",
-        "config": {"workload": f"config{args.config}:{wl.name}", "n_free_dofs": f32.n_reduced(),
+        "config": {"workload": f"config{args.config}:{wl.name}", "n_free_dofs": nred,
                    "tets": int(wl.tets.shape[0]), "nrhs": nrhs, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (element Hessians %.2f GB)" % (wl.Ke.nbytes / 1e9),
                    **wl.info},
@@ -291,12 +300,13 @@ def run_b200(args, rank, world, local, dist):
         "roofline": roofline,
         "residual": res32,
         "refine_iterations": st32["refine_iterations"], "perturbed_pivots": st32["perturbed_pivots"],
+        "refactored_blocks": st32["refactored_blocks"],
         "factor_ms": st32["factor_ms"], "solve_ms": st32["solve_ms"], "assemble_ms": st32["assemble_ms"],
-        "factor_nnz": f32.getFactorNNZ(), "flops": flops, "symbolic_s": t_sym, "input_gen_s": t_gen,
+        "factor_nnz": nnz32, "flops": flops_est, "symbolic_s": t_sym, "input_gen_s": t_gen,
         **out64,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        result["cpu_baseline"] = cpu_baseline(wl, f32, args)
+        result["cpu_baseline"] = cpu_baseline(wl, sym, args)
     if rank == 0:
         print(json.dumps(result), flush=True)
 
@@ -468,7 +478,7 @@ def run_newton_sequence(args, rank, world, local, dist):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         wl.Ke = Ke2[-1].numpy().reshape(-1, 12, 12)
-        result["cpu_baseline"] = cpu_baseline(wl, f32, args)
+        result["cpu_baseline"] = cpu_baseline(wl, (f32.supernodes(), f32.conversionPlan(), f32._row_maps()[1]), args)
     if rank == 0:
         print(json.dumps(result), flush=True)
 
@@ -504,13 +514,14 @@ def cpu_step(wl, sn, plan, prr, threads):
             "solve": t_sol, "pivot_failure": int(fail)}
 
 
-def cpu_baseline(wl, f, args):
+def cpu_baseline(wl, sym, args):
     """The oracle port timed on one complete step of the same workload (no sampling,
-    no extrapolation) on all host threads."""
+    no extrapolation) on all host threads. sym: (supernodes, conversion plan, row map)
+    of the factorizer's symbolic analysis."""
     from oracle import pyoracle
     pyoracle.load_blas()
     threads = int(pyoracle.load().orc_max_threads())
-    r = cpu_step(wl, f.supernodes(), f.conversionPlan(), f._row_maps()[1], threads)
+    r = cpu_step(wl, sym[0], sym[1], sym[2], threads)
     return {"value": 1.0 / r["total"], "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"one complete step of the same workload (nrhs={wl.nrhs}): CPU assembly, injection, "
                       f"FP64 multifrontal factorization of the whole tree and supernodal solve with OpenBLAS; "
