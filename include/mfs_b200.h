@@ -264,7 +264,11 @@ typedef struct {
     int32_t refactored_blocks;   /* FP32 factor under refinement: large-front diagonal blocks whose FP32
                                     factorization met a pivot <= 1e-5 x the injected diagonal and were
                                     factored again in FP64 (last numeric) */
-    int32_t reserved_stats;
+    int32_t split_escalations;   /* FP32 under refinement: times a single-pass TF32 / FP16 factorization was
+                                    redone with split 3xTF32 (FP32-level) products because it perturbed a
+                                    pivot or its refinement stalled; the handle then keeps the split
+                                    products until the next symbolic analysis or mfs_set_options
+                                    (cumulative) */
 } mfs_stats;
 mfs_status mfs_get_stats(const mfs_handle *h, mfs_stats *st);
 

@@ -51,7 +51,7 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_int64), ("perturbed_pivots", C.c_int32), ("pcg_iterations", C.c_int32),
         ("pcg_fallback", C.c_int32), ("nd_reused", C.c_int32), ("pcg_ms", C.c_double),
         ("gemm_ms", C.c_double), ("gemm_flops", C.c_double), ("gemm_launches", C.c_int64),
-        ("nd_rebuilt_vertices", C.c_int64), ("refactored_blocks", C.c_int32), ("reserved_stats", C.c_int32),
+        ("nd_rebuilt_vertices", C.c_int64), ("refactored_blocks", C.c_int32), ("split_escalations", C.c_int32),
     ]
 
 

@@ -526,6 +526,7 @@ void clear_factor_graphs(mfs_handle *h) {
 // matrix, so the per-front scale keeps every operand below 2^12 (no overflow), and
 // the refinement needs the same iteration count as with TF32 operands.
 int fp32_split(const mfs_handle *h) {
+    if (h->split_escalated) return 3;
     const int tc = h->opt.tensor_cores;
     if (tc == 5 || tc == 0) return h->opt.refine ? 5 : 3;
     return tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : 4;
@@ -1063,6 +1064,7 @@ mfs_status mfs_set_options(mfs_handle *h, const mfs_options *opt) {
     if (opt->precision != h->opt.precision || opt->device != h->opt.device)
         return MFS_INVALID_ARG;   // fixed for the lifetime of a handle
     void *stream = h->opt.stream;
+    if (opt->tensor_cores != h->opt.tensor_cores || opt->refine != h->opt.refine) h->split_escalated = false;
     h->opt = *opt;
     h->opt.stream = stream;
     return MFS_OK;
@@ -1172,6 +1174,7 @@ mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, cons
             ds->S = Sp;
             ds->ax_len = Ap[n_blocks] * int64_t(block_size) * block_size;
             h->cur.sym = ds;
+            h->split_escalated = false;
             h->cur.type = 1;
             h->stats.num_levels = int(Sp->nlevels);
             return;
@@ -1185,10 +1188,77 @@ mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, cons
         if (h->opt.precision == MFS_PREC_FP32) h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
         else h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
         h->cur.sym = ds;
+        h->split_escalated = false;
         h->cur.type = 1;
         h->stats.num_levels = int(S.nlevels);
         h->stats.num_large = ds->num_large;
     });
+}
+
+// The numeric factorization of the current values (h->cur.ax / bx, h->cur.sigma);
+// counters to mfs_stats, errors thrown. An FP32 factorization under refinement with
+// single-pass TF32 / FP16 products that had to perturb a pivot is redone once with
+// split 3xTF32 (FP32-level) products, which the handle then keeps: on high-contrast
+// inputs the low-precision Schur updates lose definiteness and refinement stalls.
+void numeric_core(mfs_handle *h) {
+    DevSym &ds = *h->cur.sym;
+    const Symbolic &S = *ds.S;
+    cudaStream_t st = h->stream;
+    const double *dBx = h->cur.bx ? h->cur.bx->p : nullptr;
+    const double sigma = h->cur.sigma;
+    const int big = INT_MAX;
+    MFS_CUDA(cudaMemcpyAsync(h->fail.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+    MFS_CUDA(cudaMemsetAsync(h->perturbed.p, 0, sizeof(int), st));
+    MFS_CUDA(cudaMemsetAsync(h->refactored.p, 0, sizeof(int), st));
+    MFS_CUDA(cudaEventRecord(h->ev0, st));
+    if (h->opt.precision == MFS_PREC_FP32) {
+        if (!h->cur.f32 || h->cur.f32.use_count() > 1) h->cur.f32 = std::make_shared<DBuf<float>>();
+        h->cur.f32->ensure(size_t(ds.factor_alloc));
+        h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
+        h->dscr32.ensure(size_t(std::max<int64_t>(ds.inv_scratch, 1)));
+        factor_sequence<float>(h, ds, h->cur.f32->p, h->upd32.p, h->dscr32.p, h->cur.ax->p, dBx, sigma);
+    } else {
+        if (!h->cur.f64 || h->cur.f64.use_count() > 1) h->cur.f64 = std::make_shared<DBuf<double>>();
+        h->cur.f64->ensure(size_t(ds.factor_alloc));
+        h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
+        h->dscr64.ensure(size_t(std::max<int64_t>(ds.inv_scratch, 1)));
+        factor_sequence<double>(h, ds, h->cur.f64->p, h->upd64.p, h->dscr64.p, h->cur.ax->p, dBx, sigma);
+    }
+    MFS_CUDA(cudaEventRecord(h->ev1, st));
+    MFS_CUDA(cudaMemcpyAsync(h->fail_host, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MFS_CUDA(cudaMemcpyAsync(h->fail_host + 1, h->perturbed.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MFS_CUDA(cudaMemcpyAsync(h->fail_host + 2, h->gemm_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MFS_CUDA(cudaMemcpyAsync(h->fail_host + 3, h->refactored.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MFS_CUDA(cudaStreamSynchronize(st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->stats.factor_ms = ms;
+    h->stats.perturbed_pivots = h->fail_host[1];
+    h->stats.refactored_blocks = h->fail_host[3];
+    h->stats.gemm_ms = 0.0;
+    h->stats.gemm_flops = h->gemm_flops_timed;
+    h->stats.gemm_launches = int64_t(h->gemm_events_used / 2);
+    for (size_t e = 0; e + 1 < h->gemm_events_used; e += 2) {
+        float g = 0;
+        MFS_CUDA(cudaEventElapsedTime(&g, h->gemm_events[e], h->gemm_events[e + 1]));
+        h->stats.gemm_ms += g;
+    }
+    if (h->fail_host[2]) {
+        MFS_CUDA(cudaMemset(h->gemm_err.p, 0, sizeof(int)));
+        throw StatusError(MFS_TIMEOUT, "Schur update: a tensor-core pipeline wait timed out");
+    }
+    if (*h->fail_host != INT_MAX) {
+        h->stats.failed_column = *h->fail_host;
+        throw StatusError(MFS_NOT_POSDEF, std::to_string(*h->fail_host) + "/" + std::to_string(S.n) +
+                                              "  pivots successful in numeric factorization (non-positive definite?)");
+    }
+    const int sp = h->opt.precision == MFS_PREC_FP32 ? fp32_split(h) : 3;
+    if (h->opt.precision == MFS_PREC_FP32 && h->opt.refine && sp != 3 && h->stats.perturbed_pivots > 0 &&
+        !h->split_escalated) {
+        h->split_escalated = true;
+        ++h->stats.split_escalations;
+        numeric_core(h);
+    }
 }
 
 mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double sigma, int32_t flags) {
@@ -1197,7 +1267,6 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
         require_symbolic(h);
         set_device(h);
         DevSym &ds = *h->cur.sym;
-        const Symbolic &S = *ds.S;
         const bool dev = (flags & MFS_DEVICE_POINTERS) != 0;
         cudaStream_t st = h->stream;
         // The numeric factor becomes invalid from here until success.
@@ -1218,54 +1287,8 @@ mfs_status mfs_numeric(mfs_handle *h, const double *Ax, const double *Bx, double
         }
         if (Bx) take_values(h->cur.bx, Bx);
         else h->cur.bx.reset();
-        const double *dBx = h->cur.bx ? h->cur.bx->p : nullptr;
-        const int big = INT_MAX;
-        MFS_CUDA(cudaMemcpyAsync(h->fail.p, &big, sizeof(int), cudaMemcpyHostToDevice, st));
-        MFS_CUDA(cudaMemsetAsync(h->perturbed.p, 0, sizeof(int), st));
-        MFS_CUDA(cudaMemsetAsync(h->refactored.p, 0, sizeof(int), st));
-        MFS_CUDA(cudaEventRecord(h->ev0, st));
-        if (h->opt.precision == MFS_PREC_FP32) {
-            if (!h->cur.f32 || h->cur.f32.use_count() > 1) h->cur.f32 = std::make_shared<DBuf<float>>();
-            h->cur.f32->ensure(size_t(ds.factor_alloc));
-            h->upd32.ensure(size_t(std::max<idx>(S.upd_size, 1)));
-            h->dscr32.ensure(size_t(std::max<int64_t>(ds.inv_scratch, 1)));
-            factor_sequence<float>(h, ds, h->cur.f32->p, h->upd32.p, h->dscr32.p, h->cur.ax->p, dBx, sigma);
-        } else {
-            if (!h->cur.f64 || h->cur.f64.use_count() > 1) h->cur.f64 = std::make_shared<DBuf<double>>();
-            h->cur.f64->ensure(size_t(ds.factor_alloc));
-            h->upd64.ensure(size_t(std::max<idx>(S.upd_size, 1)));
-            h->dscr64.ensure(size_t(std::max<int64_t>(ds.inv_scratch, 1)));
-            factor_sequence<double>(h, ds, h->cur.f64->p, h->upd64.p, h->dscr64.p, h->cur.ax->p, dBx, sigma);
-        }
-        MFS_CUDA(cudaEventRecord(h->ev1, st));
-        MFS_CUDA(cudaMemcpyAsync(h->fail_host, h->fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-        MFS_CUDA(cudaMemcpyAsync(h->fail_host + 1, h->perturbed.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-        MFS_CUDA(cudaMemcpyAsync(h->fail_host + 2, h->gemm_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-        MFS_CUDA(cudaMemcpyAsync(h->fail_host + 3, h->refactored.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-        MFS_CUDA(cudaStreamSynchronize(st));
-        float ms = 0;
-        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-        h->stats.factor_ms = ms;
-        h->stats.perturbed_pivots = h->fail_host[1];
-        h->stats.refactored_blocks = h->fail_host[3];
-        h->stats.gemm_ms = 0.0;
-        h->stats.gemm_flops = h->gemm_flops_timed;
-        h->stats.gemm_launches = int64_t(h->gemm_events_used / 2);
-        for (size_t e = 0; e + 1 < h->gemm_events_used; e += 2) {
-            float g = 0;
-            MFS_CUDA(cudaEventElapsedTime(&g, h->gemm_events[e], h->gemm_events[e + 1]));
-            h->stats.gemm_ms += g;
-        }
         h->cur.sigma = sigma;
-        if (h->fail_host[2]) {
-            MFS_CUDA(cudaMemset(h->gemm_err.p, 0, sizeof(int)));
-            throw StatusError(MFS_TIMEOUT, "Schur update: a tensor-core pipeline wait timed out");
-        }
-        if (*h->fail_host != INT_MAX) {
-            h->stats.failed_column = *h->fail_host;
-            throw StatusError(MFS_NOT_POSDEF, std::to_string(*h->fail_host) + "/" + std::to_string(S.n) +
-                                                  "  pivots successful in numeric factorization (non-positive definite?)");
-        }
+        numeric_core(h);
         h->stats.failed_column = -1;
         h->cur.type = 2;
     });
@@ -1304,7 +1327,17 @@ mfs_status mfs_solve(mfs_handle *h, const double *B, double *X, int64_t nrhs, in
         const bool refine = h->opt.refine && h->opt.precision == MFS_PREC_FP32;
         if (refine) {
             h->work_x.ensure(sz);
-            refine_solve(h, h->rhs.p, h->work_x.p, int(nrhs));
+            try {
+                refine_solve(h, h->rhs.p, h->work_x.p, int(nrhs));
+            } catch (const StatusError &e) {
+                // refinement stalled on a low-precision factor: factor the same values again
+                // with FP32-level products (kept for the handle) and solve once more
+                if (e.status != MFS_NOT_POSDEF || fp32_split(h) == 3) throw;
+                h->split_escalated = true;
+                ++h->stats.split_escalations;
+                numeric_core(h);
+                refine_solve(h, h->rhs.p, h->work_x.p, int(nrhs));
+            }
             result = h->work_x.p;
         } else {
             solve_current(h, h->rhs.p, int(nrhs));

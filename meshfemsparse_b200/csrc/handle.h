@@ -161,6 +161,10 @@ struct mfs_handle {
     bool own_stream = false;
     State cur, stash;
     bool has_stash = false;
+    // FP32 factorizations under refinement use FP32-level (split 3xTF32) products from
+    // now on: a low-precision one perturbed a pivot or its refinement stalled. Cleared
+    // by a new symbolic analysis and by mfs_set_options.
+    bool split_escalated = false;
     DBuf<double> upd64;            // update arena (multifrontal Schur complements)
     DBuf<float> upd32;
     DBuf<double> dscr64;           // inverses of the diagonal blocks of one column-block step

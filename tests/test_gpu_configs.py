@@ -84,6 +84,23 @@ def test_two_material_contrast_32_rhs(tc):
     assert residual(wl, X64) <= 1e-10
 
 
+def test_contrast_escalates_low_precision_factor():
+    """At 1e3 contrast and k=32 the single-pass FP16 factorization perturbs pivots and
+    its refinement stalls (measured: residual 3e-5 after 50 iterations); the handle
+    redoes it with split 3xTF32 products, reaches 1e-10 and keeps the split products
+    for the next factorization of the same pattern."""
+    wl = workloads.config5(k=32, seed=5)
+    f32 = assembled(wl, single=True, refine=True, tc=0)
+    X = f32.solveMultiRHS(wl.rhs)
+    st = f32.stats()
+    assert st["split_escalations"] >= 1
+    assert st["perturbed_pivots"] == 0
+    assert residual(wl, X) <= 1e-10
+    f32.factorizeAssembled()
+    assert f32.stats()["split_escalations"] == st["split_escalations"]
+    assert f32.stats()["perturbed_pivots"] == 0
+
+
 def test_newton_ramp_with_learned_pcg():
     seq = workloads.newton_sequence(k=6, final_hessians=False)
     wl = seq.wl
