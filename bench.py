@@ -45,6 +45,9 @@ def parse():
     p.add_argument("--config", type=int, default=2)
     p.add_argument("--k", type=int, default=None, help="override the cube side (smaller runs)")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison arm")
+    p.add_argument("--no-config4", action="store_true",
+                   help="default workload: skip the short learned-PCG Newton-sequence arm (config 4) whose summary "
+                        "the line carries under \"config4\"")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--tc", type=int, default=0,
                    help="FP32 Schur updates: 0 auto (5 under refinement), 1 TF32, 2 split 3xTF32, 4 TF32 with TMA, "
@@ -312,7 +315,8 @@ def run_b200(args, rank, world, local, dist):
     if rank == 0 and world == 1 and not args.no_cpu:
         result["cpu_baseline"] = cpu_baseline(wl, sym, args)
     if rank == 0:
-        print(json.dumps(result), flush=True)
+        return result
+    return None
 
 
 # ------------------------------------------------- config 4: learned PCG on a Newton sequence
@@ -483,8 +487,7 @@ def run_newton_sequence(args, rank, world, local, dist):
     if rank == 0 and world == 1 and not args.no_cpu:
         wl.Ke = Ke2[-1].numpy().reshape(-1, 12, 12)
         result["cpu_baseline"] = cpu_baseline(wl, (f32.supernodes(), f32.conversionPlan(), f32._row_maps()[1]), args)
-    if rank == 0:
-        print(json.dumps(result), flush=True)
+    return result if rank == 0 else None
 
 
 # -------------------------------------------------------------- CPU legs
@@ -573,6 +576,26 @@ def run_reference(args, rank, world, dist):
     print(json.dumps(out), flush=True)
 
 
+def config4_summary(args, rank, world, local, dist):
+    """A short run of the config-4 arm (learned PCG on the Newton load ramp, beside
+    FP32+refine and FP64 plain on the same steps), summarized for the default line."""
+    import copy
+    a = copy.copy(args)
+    a.config, a.k, a.steps, a.warmup, a.no_cpu = 4, None, 3, 3, True
+    a.train_hessians = min(args.train_hessians, 4)
+    r = run_newton_sequence(a, rank, world, local, dist)
+    if r is None:
+        return None
+    keep = ("value", "ms_per_step", "residual", "learned_pcg", "jacobi_pcg", "fp32_refine", "fp64_plain_solves_per_s",
+            "fp64_plain_ms_per_step", "fp64_residual", "speedup_learned_pcg_vs_fp64_plain",
+            "speedup_fp32_refine_vs_fp64_plain", "training", "steps", "warmup", "e2e")
+    out = {k: r[k] for k in keep if k in r}
+    out["workload"] = r["config"]["workload"]
+    out["n_free_dofs"] = r["config"]["n_free_dofs"]
+    out["unit"] = UNIT
+    return out
+
+
 def main():
     args = parse()
     rank, world, local, dist = dist_setup(args)
@@ -580,9 +603,18 @@ def main():
         if args.impl == "reference":
             run_reference(args, rank, world, dist)
         elif args.config == 4:
-            run_newton_sequence(args, rank, world, local, dist)
+            result = run_newton_sequence(args, rank, world, local, dist)
+            if result is not None:
+                print(json.dumps(result), flush=True)
         else:
-            run_b200(args, rank, world, local, dist)
+            result = run_b200(args, rank, world, local, dist)
+            if (result is not None and args.config == 2 and world == 1 and not args.no_config4
+                    and not args.profile and args.k is None):
+                import torch
+                torch.cuda.empty_cache()
+                result["config4"] = config4_summary(args, rank, world, local, dist)
+            if result is not None:
+                print(json.dumps(result), flush=True)
     finally:
         if dist:
             dist.destroy_process_group()
