@@ -56,6 +56,7 @@ def parse():
                    help="build the workload, run one untimed assemble + factorization + refined solve, exit "
                         "(the command profilers capture)")
     p.add_argument("--maxit", type=int, default=50, help="refinement iteration cap")
+    p.add_argument("--group", type=int, default=0, help="column blocks per factorization group (0: default)")
     p.add_argument("--chain", type=int, default=0, help="diagonal solves: 0 superblock inverses, 1 block-pair chains")
     p.add_argument("--cpu-seconds", type=float, default=150.0,
                    help="reference arm: stop timing complete CPU steps once this much is spent")
@@ -165,7 +166,7 @@ def run_b200(args, rank, world, local, dist):
 
     def make(single):
         f = B200Factorizer(single, refine=single, stream=stream.cuda_stream, device=local, tensor_cores=args.tc,
-                           refine_maxit=args.maxit, solve_chain=args.chain)
+                           refine_maxit=args.maxit, solve_chain=args.chain, factor_group=args.group)
         t = time.time()
         f.factorizeSymbolic(wl.H, wl.pins)
         f.setElements(wl.tets)

@@ -89,7 +89,10 @@ typedef struct {
     int32_t solve_chain;        /* diagonal-block solves of the fronts above the subtree cut: 0 through the
                                    inverses of 256-row superblocks of L11 (one CTA per superblock),
                                    1 through chains of 64-row blocks (one CTA per pair of blocks) */
-    int32_t reserved[4];
+    int32_t factor_group;       /* large fronts: column blocks per group of the blocked factorization (inside a
+                                   group left-looking, after it one update of the rest of the front);
+                                   0: default (4); read at the symbolic analysis */
+    int32_t reserved[3];
 } mfs_options;
 
 typedef struct mfs_handle mfs_handle;

@@ -199,12 +199,12 @@ std::shared_ptr<DevSym> upload_symbolic(mfs_handle *h, std::shared_ptr<Symbolic>
             base += g.tiles_m * g.tiles_n;
             gemm_tasks.push_back(g);
         };
-        // Column blocks of NB are grouped by GB = 4 NB: inside a group the block
+        // Column blocks of NB are grouped by GB = factor_group NB (default 4): inside a group the block
         // columns are brought up to date left-looking (one GEMM with k = kb - group
         // start), after a group the rest of the front gets one rank-GB update. The
         // Schur updates so run with k up to GB instead of NB, reading and writing
         // the trailing columns GB / NB times less often.
-        const idx GB = 4 * NB;
+        const idx GB = idx(h->opt.factor_group > 0 ? h->opt.factor_group : 4) * NB;
         for (idx kb = 0; kb < maxw; kb += NB) {
             LevelPlan::Step sp{};
             const idx ko = kb - kb % GB;                // start of the block's group
