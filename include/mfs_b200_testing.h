@@ -28,8 +28,13 @@ extern "C" {
  * float arrays, `kernel` 1 = single-pass TF32 on the 5th-generation tensor cores
  * (tcgen05), 4 = the same with TMA-fed operands (mode 0 only; arrays 16-byte
  * aligned), 5 = FP16 A and B (IEEE half arrays, leading dimensions multiples of 8)
- * with FP32 C on tcgen05 with TMA (mode 0 only; scale_exp is used by this kernel
- * only), 3 = split 3xTF32 (mma.sync), 0 = single-pass TF32 (mma.sync);
+ * with FP32 C on tcgen05 with TMA (mode 0 only; scale_exp is used by kernels 5 and
+ * 6 only), 6 = split FP16: A and B each hold an FP16 hi array of a_len / 2 (b_len / 2)
+ * elements followed by the lo array (A ~ hi + 2^-11 lo), offsets index either half;
+ * three MMAs per k slice (mode 0 only), 7 = split TF32 on tcgen05 (float arrays, hi /
+ * lo split in shared memory, the row-solve kernel of tensor_cores 6; mode 1 writes
+ * its half copies to scratch), 3 = split 3xTF32 (mma.sync), 0 = single-pass TF32
+ * (mma.sync);
  * MFS_PREC_FP64: double arrays on the FP64 tensor cores (kernel ignored).
  * FP32 leading dimensions must be multiples of 4 (16-byte aligned columns, as
  * the factor's panels are). Every access is checked against the array lengths

@@ -526,8 +526,9 @@ void clear_factor_graphs(mfs_handle *h) {
 // matrix, so the per-front scale keeps every operand below 2^12 (no overflow), and
 // the refinement needs the same iteration count as with TF32 operands.
 int fp32_split(const mfs_handle *h) {
-    if (h->split_escalated) return 3;
+    if (h->split_escalated) return 6;
     const int tc = h->opt.tensor_cores;
+    if (tc == 6) return 6;
     if (tc == 5 || tc == 0) return h->opt.refine ? 5 : 3;
     return tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : 4;
 }
@@ -535,22 +536,28 @@ int fp32_split(const mfs_handle *h) {
 // Tensor maps of the large fronts' panels in `base` (the FP32 factor, or its FP16
 // copy) for the TMA-fed GEMM (built on the host once per symbolic analysis and
 // array; not during graph capture).
-void ensure_panel_maps(mfs_handle *h, DevSym &ds, const void *base, bool half) {
-    if (h->tmaps_base == base && h->tmaps_sym == &ds) return;
+void ensure_panel_maps(mfs_handle *h, DevSym &ds, const void *base, bool half, const void *lo = nullptr) {
+    if (h->tmaps_base == base && h->tmaps_sym == &ds && h->tmaps_lo == lo) return;
     const Symbolic &S = *ds.S;
     const size_t es = half ? 2 : 4;
-    std::vector<TensorMapBlob> maps(size_t(std::max<idx>(S.nsn, 1)));
+    const size_t nsn = size_t(std::max<idx>(S.nsn, 1));
+    // [0, nsn): the copy at base; [nsn, 2 nsn): the lo copy (split FP16)
+    std::vector<TensorMapBlob> maps(lo ? 2 * nsn : nsn);
     std::memset(maps.data(), 0, maps.size() * sizeof(TensorMapBlob));
-    for (int32_t s : ds.large_fronts)
-        if (!encode_operand_map(&maps[size_t(s)], static_cast<const char *>(base) + size_t(ds.dpan[s]) * es, half,
-                                uint64_t(S.f[s]), uint64_t(S.w[s]), uint64_t(ds.dld[s])))
-            throw StatusError(MFS_INTERNAL, "cuTensorMapEncodeTiled refused a panel tensor map");
+    for (int c = 0; c < (lo ? 2 : 1); ++c) {
+        const char *b = static_cast<const char *>(c ? lo : base);
+        for (int32_t s : ds.large_fronts)
+            if (!encode_operand_map(&maps[c * nsn + size_t(s)], b + size_t(ds.dpan[s]) * es, half, uint64_t(S.f[s]),
+                                    uint64_t(S.w[s]), uint64_t(ds.dld[s])))
+                throw StatusError(MFS_INTERNAL, "cuTensorMapEncodeTiled refused a panel tensor map");
+    }
     h->tmaps.ensure(maps.size());
     MFS_CUDA(cudaMemcpyAsync(h->tmaps.p, maps.data(), maps.size() * sizeof(TensorMapBlob), cudaMemcpyHostToDevice,
                              h->stream));
     MFS_CUDA(cudaStreamSynchronize(h->stream));
     h->tmaps_base = base;
     h->tmaps_sym = &ds;
+    h->tmaps_lo = lo;
 }
 
 // Tensor maps of the superblock solves for the factor array `base` (elements of es
@@ -607,12 +614,14 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
     auto launch = [&](const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int sp, int *err,
                       cudaStream_t s, bool mode0) {
         if constexpr (std::is_same<T, float>::value) {
-            if ((sp == 4 || sp == 5) && mode0) {
-                launch_gemm_tma(sp == 5, tasks, ntasks, ntiles, h->tmaps.p, C, sp == 5 ? h->sexp.p : nullptr, err, s);
+            if ((sp == 4 || sp == 5 || sp == 6) && mode0) {
+                launch_gemm_tma(sp == 6 ? 2 : sp == 5 ? 1 : 0, tasks, ntasks, ntiles, h->tmaps.p, C,
+                                sp >= 5 ? h->sexp.p : nullptr, err, s, int(std::max<idx>(ds.S->nsn, 1)));
                 return;
             }
-            if (sp == 5) {
-                launch_gemm_tc(tasks, ntasks, ntiles, A, B, C, err, s, h->h16.p, h->sexp.p);
+            if (sp == 5 || sp == 6) {
+                launch_gemm_tc(tasks, ntasks, ntiles, A, B, C, err, s, h->h16.p, h->sexp.p,
+                               sp == 6 ? h->h16lo.p : nullptr);
                 return;
             }
         }
@@ -658,7 +667,7 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         h->dorig.ensure(size_t(std::max<idx>(S.n, 1)));
         pv.refactored = h->refactored.p;
         launch_extract_diag<T>(ds.diag_off.p, S.n, factor, h->dorig.p, st);
-        if (split == 5)
+        if (split == 5 || split == 6)
             launch_front_scale(ds.large_dev.p, int(ds.large_fronts.size()), ds.sd, h->dorig.p, h->sexp.p, st);
         MFS_LAUNCHED();
         pv.dorig = h->dorig.p;
@@ -685,7 +694,7 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
             tgemm(ds.gemm_tasks.p + sp.left_off, sp.left_n, sp.left_tiles, factor, factor, factor, split,
                            h->gemm_err.p, hs);
             MFS_LAUNCHED();
-            launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, dscr, pv, split == 1 || split >= 4,
+            launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, dscr, pv, split == 1 || split == 4 || split == 5,
                             hs);
             MFS_LAUNCHED();
             tgemm(ds.gemm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, factor, dscr, factor, split,
@@ -733,10 +742,11 @@ void factor_sequence(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, cons
     const int split = fp32_split(h);
     if constexpr (std::is_same<T, float>::value) {
         if (split == 4) ensure_panel_maps(h, ds, factor, false);
-        if (split == 5) {
+        if (split == 5 || split == 6) {
             h->h16.ensure(size_t(std::max<int64_t>(ds.panel_alloc, 1)));
             h->sexp.ensure(size_t(std::max<idx>(ds.S->nsn, 1)));
-            ensure_panel_maps(h, ds, h->h16.p, true);
+            if (split == 6) h->h16lo.ensure(size_t(std::max<int64_t>(ds.panel_alloc, 1)));
+            ensure_panel_maps(h, ds, h->h16.p, true, split == 6 ? h->h16lo.p : nullptr);
         }
     }
     // (the legacy default stream cannot be captured: graphs need a handle or caller stream)
@@ -745,10 +755,11 @@ void factor_sequence(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, cons
         return;
     }
     const void *dorig = h->dorig.p;
-    mfs_handle::FactorGraph key{&ds, factor, upd, dscr, Ax, Bx, dorig, h->h16.p, h->tmaps.p, sigma, split, nullptr};
+    mfs_handle::FactorGraph key{&ds,      factor,      upd,         dscr,  Ax,    Bx,     dorig,
+                                h->h16.p, h->h16lo.p, h->tmaps.p, sigma, split, nullptr};
     auto same = [&](const mfs_handle::FactorGraph &g) {
         return g.ds == key.ds && g.factor == key.factor && g.upd == key.upd && g.dscr == key.dscr &&
-               g.ax == key.ax && g.bx == key.bx && g.dorig == key.dorig && g.h16 == key.h16 &&
+               g.ax == key.ax && g.bx == key.bx && g.dorig == key.dorig && g.h16 == key.h16 && g.h16lo == key.h16lo &&
                g.tmaps == key.tmaps && g.sigma == key.sigma &&
                g.split == key.split;
     };
@@ -1253,7 +1264,7 @@ void numeric_core(mfs_handle *h) {
                                               "  pivots successful in numeric factorization (non-positive definite?)");
     }
     const int sp = h->opt.precision == MFS_PREC_FP32 ? fp32_split(h) : 3;
-    if (h->opt.precision == MFS_PREC_FP32 && h->opt.refine && sp != 3 && h->stats.perturbed_pivots > 0 &&
+    if (h->opt.precision == MFS_PREC_FP32 && h->opt.refine && sp != 3 && sp != 6 && h->stats.perturbed_pivots > 0 &&
         !h->split_escalated) {
         h->split_escalated = true;
         ++h->stats.split_escalations;
@@ -1332,7 +1343,7 @@ mfs_status mfs_solve(mfs_handle *h, const double *B, double *X, int64_t nrhs, in
             } catch (const StatusError &e) {
                 // refinement stalled on a low-precision factor: factor the same values again
                 // with FP32-level products (kept for the handle) and solve once more
-                if (e.status != MFS_NOT_POSDEF || fp32_split(h) == 3) throw;
+                if (e.status != MFS_NOT_POSDEF || fp32_split(h) == 3 || fp32_split(h) == 6) throw;
                 h->split_escalated = true;
                 ++h->stats.split_escalations;
                 numeric_core(h);

@@ -37,12 +37,20 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
         put_error(err_buf, err_len, "empty task list or null array");
         return MFS_INVALID_ARG;
     }
-    if (!f64 && kernel != 0 && kernel != 1 && kernel != 3 && kernel != 4 && kernel != 5) {
-        put_error(err_buf, err_len, "kernel must be 0, 1, 3, 4 or 5");
+    if (!f64 && (kernel < 0 || kernel > 7 || kernel == 2)) {
+        put_error(err_buf, err_len, "kernel must be 0, 1, 3, 4, 5, 6 or 7");
         return MFS_INVALID_ARG;
     }
-    const bool tma = !f64 && (kernel == 4 || kernel == 5);
-    const bool half = !f64 && kernel == 5;              // A and B are FP16
+    const bool tma = !f64 && (kernel == 4 || kernel == 5 || kernel == 6);
+    const bool split16 = !f64 && kernel == 6;           // A and B: FP16 hi array, then FP16 lo array
+    const bool half = !f64 && (kernel == 5 || kernel == 6);   // A and B are FP16
+    const bool split32 = !f64 && kernel == 7;           // tcgen05 split TF32 (FP32 operands)
+    if (split16 && ((a_len & 1) || (b_len & 1))) {
+        put_error(err_buf, err_len, "kernel 6: A and B hold two equal halves (hi, lo)");
+        return MFS_INVALID_ARG;
+    }
+    // element count of one operand copy (kernel 6: each half)
+    const int64_t a_ext = split16 ? a_len / 2 : a_len, b_ext = split16 ? b_len / 2 : b_len;
     std::vector<TensorMapBlob> maps;
     const int TM = gemm_tile_m(f64), TN = gemm_tile_n(f64);
     std::vector<GemmTask> gt(static_cast<size_t>(ntasks));
@@ -82,8 +90,8 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
         }
         // the kernels read A rows [a_off - da, a_off + m) of columns 0..k-1, B likewise,
         // and write C rows [0, m) of columns 0..n-1
-        if (a_off - da < 0 || b_off - db < 0 || c_off < 0 || a_off + (k - 1) * lda + m > a_len ||
-            b_off + (k - 1) * ldb + n > b_len || c_off + (n - 1) * ldc + m > c_len) {
+        if (a_off - da < 0 || b_off - db < 0 || c_off < 0 || a_off + (k - 1) * lda + m > a_ext ||
+            b_off + (k - 1) * ldb + n > b_ext || c_off + (n - 1) * ldc + m > c_len) {
             put_error(err_buf, err_len, id + "an access falls outside the arrays");
             return MFS_INVALID_ARG;
         }
@@ -100,7 +108,7 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
         g.amap = g.bmap = -1;
         g.ax = g.ay = g.bx = g.by = 0;
         g.scale_exp = int32_t(scale_exp);
-        g.sn = -1;
+        g.sn = split32 ? 0 : -1;
         if (tma) {
             // one tensor map per operand, starting at the shifted (16-byte aligned) operand
             if (mode != 0) {
@@ -124,20 +132,48 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
             g.amap = int32_t(maps.size() - 2);
             g.bmap = int32_t(maps.size() - 1);
         }
+        if (split32 && lower && mode == 1) {
+            put_error(err_buf, err_len, id + "row solves (mode 1) are not lower");
+            return MFS_INVALID_ARG;
+        }
         if (int64_t(base) + int64_t(g.tiles_m) * g.tiles_n > INT32_MAX / 2) {
             put_error(err_buf, err_len, "too many tiles");
             return MFS_INVALID_ARG;
         }
         base += g.tiles_m * g.tiles_n;
     }
+    if (split16) {
+        // the lo copies' maps, in the same order, 2 ntasks entries after the hi ones
+        const size_t nh = maps.size();
+        maps.resize(2 * nh);
+        for (int64_t t = 0; t < ntasks; ++t) {
+            const GemmTask &g = gt[size_t(t)];
+            const int da = g.shift & 255, db = g.shift >> 8;
+            const char *Al = static_cast<const char *>(A) + size_t(a_ext + g.a_off - da) * 2;
+            const char *Bl = static_cast<const char *>(B) + size_t(b_ext + g.b_off - db) * 2;
+            if ((reinterpret_cast<uintptr_t>(Al) & 15) || (reinterpret_cast<uintptr_t>(Bl) & 15) ||
+                !encode_operand_map(&maps[nh + size_t(g.amap)], Al, true, uint64_t(g.m + da), uint64_t(g.k),
+                                    uint64_t(g.lda)) ||
+                !encode_operand_map(&maps[nh + size_t(g.bmap)], Bl, true, uint64_t(g.n + db), uint64_t(g.k),
+                                    uint64_t(g.ldb))) {
+                put_error(err_buf, err_len, "kernel 6: lo tensor map refused (alignment or driver)");
+                return MFS_INVALID_ARG;
+            }
+        }
+    }
     GemmTask *dt = nullptr;
     int *derr = nullptr;
     TensorMapBlob *dmaps = nullptr;
+    void *h16s = nullptr, *h16l = nullptr;
+    int32_t *dsexp = nullptr;
     auto fail = [&](cudaError_t e) {
         put_error(err_buf, err_len, cudaGetErrorString(e));
         if (dt) cudaFree(dt);
         if (derr) cudaFree(derr);
         if (dmaps) cudaFree(dmaps);
+        if (h16s) cudaFree(h16s);
+        if (h16l) cudaFree(h16l);
+        if (dsexp) cudaFree(dsexp);
         return MFS_CUDA_ERROR;
     };
     cudaError_t e = cudaSetDevice(device);
@@ -152,7 +188,16 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
         if ((e = cudaMemcpy(dmaps, maps.data(), maps.size() * sizeof(TensorMapBlob), cudaMemcpyHostToDevice)) !=
             cudaSuccess)
             return fail(e);
-        launch_gemm_tma(half, dt, int(ntasks), base, dmaps, static_cast<float *>(C), nullptr, derr, nullptr);
+        launch_gemm_tma(split16 ? 2 : half ? 1 : 0, dt, int(ntasks), base, dmaps, static_cast<float *>(C), nullptr,
+                        derr, nullptr, int(maps.size() / 2));
+    } else if (split32) {
+        // the row solves' half-copy outputs go to scratch (scale exponent 0)
+        if ((e = cudaMalloc(&h16s, size_t(c_len) * 2)) != cudaSuccess) return fail(e);
+        if ((e = cudaMalloc(&h16l, size_t(c_len) * 2)) != cudaSuccess) return fail(e);
+        if ((e = cudaMalloc(&dsexp, sizeof(int32_t))) != cudaSuccess) return fail(e);
+        if ((e = cudaMemset(dsexp, 0, sizeof(int32_t))) != cudaSuccess) return fail(e);
+        launch_gemm_tc(dt, int(ntasks), base, static_cast<const float *>(A), static_cast<const float *>(B),
+                       static_cast<float *>(C), derr, nullptr, h16s, dsexp, h16l);
     } else if (f64)
         launch_gemm<double>(dt, int(ntasks), base, static_cast<const double *>(A), static_cast<const double *>(B),
                             static_cast<double *>(C), 0, derr, nullptr);
@@ -166,6 +211,9 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
     cudaFree(dt);
     cudaFree(derr);
     if (dmaps) cudaFree(dmaps);
+    if (h16s) cudaFree(h16s);
+    if (h16l) cudaFree(h16l);
+    if (dsexp) cudaFree(dsexp);
     if (herr) {
         put_error(err_buf, err_len, "a tensor-core pipeline wait timed out");
         return MFS_TIMEOUT;

@@ -204,13 +204,18 @@ void launch_gemm(const GemmTask *tasks, int ntasks, int ntiles, const T *A, cons
 // h16 (row solves, mode 1): also store each result as FP16 scaled by 2^-sexp[task.sn]
 // at the same offset of the half-precision copy, and store the FP32 result as that
 // FP16 value scaled back (nullptr: the result is stored rounded to TF32).
+// With h16lo as well (split-FP16 mode, mode-1 tasks): A and B are split into TF32 hi
+// + lo in shared memory (FP32-level products), the FP32 result is stored as is, and
+// the half copies get hi = rn16(2^-e v) and lo = rn16(2^11 (2^-e v - hi)).
 void launch_gemm_tc(const GemmTask *tasks, int ntasks, int ntiles, const float *A, const float *B, float *C, int *err,
-                    cudaStream_t st, void *h16 = nullptr, const int32_t *sexp = nullptr);
-// TMA-fed tcgen05 GEMM (mode 0 tasks only): FP32 operands as TF32, or FP16 operands
-// (kind::f16). C -= 2^e A B^T with e = 2 sexp[task.amap] when sexp is given (the
-// operands of a front's panel carry the front's scale), else e = task.scale_exp.
-void launch_gemm_tma(bool half, const GemmTask *tasks, int ntasks, int ntiles, const void *maps, float *C,
-                     const int32_t *sexp, int *err, cudaStream_t st);
+                    cudaStream_t st, void *h16 = nullptr, const int32_t *sexp = nullptr, void *h16lo = nullptr);
+// TMA-fed tcgen05 GEMM (mode 0 tasks only). operands: 0 FP32 read as TF32, 1 FP16
+// (kind::f16), 2 split FP16 (hi + 2^-11 lo, three MMAs per k slice into two TMEM
+// accumulators; the lo operands' tensor maps are lo_maps entries after the hi ones).
+// C -= 2^e A B^T with e = 2 sexp[task.amap] when sexp is given (the operands of a
+// front's panel carry the front's scale), else e = task.scale_exp.
+void launch_gemm_tma(int operands, const GemmTask *tasks, int ntasks, int ntiles, const void *maps, float *C,
+                     const int32_t *sexp, int *err, cudaStream_t st, int lo_maps = 0);
 // Tensor map of a column-major operand (rows x cols, leading dimension ld elements,
 // base 16-byte aligned, ld * element size a multiple of 16) in the box and swizzle
 // form of the TMA-fed GEMM; false if the driver refuses it.

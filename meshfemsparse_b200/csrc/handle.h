@@ -161,9 +161,9 @@ struct mfs_handle {
     bool own_stream = false;
     State cur, stash;
     bool has_stash = false;
-    // FP32 factorizations under refinement use FP32-level (split 3xTF32) products from
-    // now on: a low-precision one perturbed a pivot or its refinement stalled. Cleared
-    // by a new symbolic analysis and by mfs_set_options.
+    // FP32 factorizations under refinement use FP32-level (split FP16 / TF32 on tcgen05)
+    // products from now on: a low-precision one perturbed a pivot or its refinement
+    // stalled. Cleared by a new symbolic analysis and by a change of tensor_cores / refine.
     bool split_escalated = false;
     DBuf<double> upd64;            // update arena (multifrontal Schur complements)
     DBuf<float> upd32;
@@ -204,7 +204,7 @@ struct mfs_handle {
     // use_graphs: instantiated graphs of the factorization's launch sequence, keyed by
     // everything the launches bake in (symbolic data, buffers, values, shift)
     struct FactorGraph {
-        const void *ds, *factor, *upd, *dscr, *ax, *bx, *dorig, *h16, *tmaps;
+        const void *ds, *factor, *upd, *dscr, *ax, *bx, *dorig, *h16, *h16lo, *tmaps;
         double sigma;
         int split;
         cudaGraphExec_t exec;
@@ -218,7 +218,9 @@ struct mfs_handle {
     DBuf<TensorMapBlob> tmaps;
     const void *tmaps_base = nullptr;
     const void *tmaps_sym = nullptr;
-    DBuf<uint16_t> h16;                      // FP16 operand copy of the panels (tensor_cores 5)
+    const void *tmaps_lo = nullptr;          // the lo copy the maps after the first nsn cover (split FP16)
+    DBuf<uint16_t> h16;                      // FP16 operand copy of the panels (tensor_cores 5, 6)
+    DBuf<uint16_t> h16lo;                    // split FP16 (tensor_cores 6): 2^11 x the remainder of h16
     DBuf<int32_t> sexp;                      // per front: power-of-two scale exponent of that copy
     std::vector<cudaEvent_t> gemm_events;    // time_kernels: (start, end) per GEMM launch
     size_t gemm_events_used = 0;

@@ -176,6 +176,18 @@ __device__ __forceinline__ void round_tf32_16b(uint32_t addr) {
                  : "memory");
 }
 
+// hi = rn_tf32(x) in place, lo = x - hi (exact in FP32) at addr + lo_off.
+__device__ __forceinline__ void split_tf32_16b(uint32_t addr, uint32_t lo_off) {
+    float a, b, c, d;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(a), "=f"(b), "=f"(c), "=f"(d) : "r"(addr) : "memory");
+    const float ha = tf32_round(a), hb = tf32_round(b), hc = tf32_round(c), hd = tf32_round(d);
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(ha), "f"(hb), "f"(hc), "f"(hd)
+                 : "memory");
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr + lo_off), "f"(a - ha), "f"(b - hb),
+                 "f"(c - hc), "f"(d - hd)
+                 : "memory");
+}
+
 // Byte offset of operand element (row x of the M or N extent, depth k < 32)
 // inside one stage buffer.
 __device__ __forceinline__ uint32_t swz_off(int x, int k) {
@@ -193,11 +205,16 @@ __device__ __forceinline__ int find_gemm_task(const GemmTask *tasks, int ntasks,
     return lo;
 }
 
-template <int STAGES>
+// SPLIT (row solves of the split-FP16 mode): A and B are split in shared memory into
+// TF32 hi = rn(x) and lo = x - hi (stored one stage-size further on); the MMA adds
+// hi x hi + hi x lo + lo x hi, FP32-level products. The result is stored in FP32 as
+// is, and into the half copies as hi = rn16(2^-e v) and lo = rn16(2^11 (2^-e v - hi)).
+template <int STAGES, bool SPLIT>
 __global__ void __launch_bounds__(kUThreads, 1) gemm_tc_kernel(const GemmTask *__restrict__ tasks, int ntasks,
                                                                const float *Abase, const float *__restrict__ Bbase,
-                                                               float *Cbase, int *err, __half *h16,
+                                                               float *Cbase, int *err, __half *h16, __half *h16lo,
                                                                const int32_t *__restrict__ sexp) {
+    constexpr uint32_t kSlot = SPLIT ? 2u * kUStage : uint32_t(kUStage);   // ring slot bytes
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
     __shared__ __align__(8) uint64_t bars[2 * STAGES + 1];
     __shared__ uint32_t tmem_holder;
@@ -261,7 +278,7 @@ __global__ void __launch_bounds__(kUThreads, 1) gemm_tc_kernel(const GemmTask *_
                 if (kb >= STAGES && !aborted && !mbar_wait(empty0 + 8 * s, uint32_t((kb / STAGES) - 1) & 1u, err))
                     aborted = true;
                 if (!aborted) {
-                    const uint32_t sa = sbase + uint32_t(s) * kUStage;
+                    const uint32_t sa = sbase + uint32_t(s) * kSlot;
                     const uint32_t sb = sa + kUStageA;
                     const int k0 = kb * UBK;
 #pragma unroll
@@ -282,7 +299,23 @@ __global__ void __launch_bounds__(kUThreads, 1) gemm_tc_kernel(const GemmTask *_
             if (kb >= STAGES - 1) {
                 const int j = kb - (STAGES - 1);
                 cp_wait_group<STAGES - 1>();
-                if (tk.mode == 1 && !aborted) {
+                if constexpr (SPLIT) {
+                    // split this thread's chunks of k-block j (A and B) into hi / lo
+                    if (!aborted) {
+                        const uint32_t sa = sbase + uint32_t(j % STAGES) * kSlot;
+                        const uint32_t sb = sa + kUStageA;
+#pragma unroll
+                        for (int p = warp; p < (UBM / 32) * (UBK / 4); p += 8) {
+                            const int x = (p & 3) * 32 + c8 * 4, k = (p >> 2) * 4 + kr;
+                            split_tf32_16b(sa + swz_off(x, k), uint32_t(kUStage));
+                        }
+#pragma unroll 4
+                        for (int p = warp; p < batoms; p += 8) {
+                            const int x = (p % (bn / 32)) * 32 + c8 * 4, k = (p / (bn / 32)) * 4 + kr;
+                            split_tf32_16b(sb + swz_off(x, k), uint32_t(kUStage));
+                        }
+                    }
+                } else if (tk.mode == 1 && !aborted) {
                     // Row solve: its A operand (assembled / updated panel rows) is
                     // FP32; round this thread's chunks of k-block j to TF32 (nearest)
                     // in place, as the tensor cores would otherwise truncate them.
@@ -327,6 +360,22 @@ __global__ void __launch_bounds__(kUThreads, 1) gemm_tc_kernel(const GemmTask *_
 #pragma unroll
                         for (int e = 0; e < 32; ++e)
                             if (e >= e_lo && e < e_hi) p[int64_t(e) * tk.ldc] = cv[e] - v[e];
+                    } else if (SPLIT) {
+                        // FP32-level result: the factor keeps it as is; the half copies
+                        // get its scaled FP16 hi part and the 2^11-scaled remainder
+                        const int se = sexp[tk.sn];
+                        const float down = ldexpf(1.0f, -se);
+                        __half *ph = h16 + tk.c_off + int64_t(jb) * tk.ldc + row;
+                        __half *pl = h16lo + tk.c_off + int64_t(jb) * tk.ldc + row;
+#pragma unroll
+                        for (int e = 0; e < 32; ++e)
+                            if (e >= e_lo && e < e_hi) {
+                                const float sv = fminf(fmaxf(v[e] * down, -65504.0f), 65504.0f);
+                                const __half hv = __float2half_rn(sv);
+                                ph[int64_t(e) * tk.ldc] = hv;
+                                pl[int64_t(e) * tk.ldc] = __float2half_rn((sv - __half2float(hv)) * 2048.0f);
+                                p[int64_t(e) * tk.ldc] = v[e];
+                            }
                     } else if (!h16) {
                         // the solved rows become Schur-update operands: store them
                         // TF32-exact (rounded to nearest)
@@ -363,13 +412,19 @@ __global__ void __launch_bounds__(kUThreads, 1) gemm_tc_kernel(const GemmTask *_
                 break;
             }
             tc_fence_after();
-            const uint32_t sa = sbase + uint32_t(s) * kUStage;
+            const uint32_t sa = sbase + uint32_t(s) * kSlot;
             const uint32_t sb = sa + kUStageA;
 #pragma unroll
             for (int g = 0; g < UBK / 8; ++g) {
                 const uint64_t ad = umma_desc(sa + uint32_t(g) * 1024u, 4096u, 512u);
                 const uint64_t bd = umma_desc(sb + uint32_t(g) * 1024u, 4096u, 512u);
                 umma_tf32(tmem, ad, bd, idesc, (kb > 0 || g > 0) ? 1u : 0u);
+                if constexpr (SPLIT) {
+                    const uint64_t adl = umma_desc(sa + kUStage + uint32_t(g) * 1024u, 4096u, 512u);
+                    const uint64_t bdl = umma_desc(sb + kUStage + uint32_t(g) * 1024u, 4096u, 512u);
+                    umma_tf32(tmem, ad, bdl, idesc, 1u);
+                    umma_tf32(tmem, adl, bd, idesc, 1u);
+                }
             }
             umma_commit(empty0 + 8 * s);
         }
@@ -386,17 +441,27 @@ __global__ void __launch_bounds__(kUThreads, 1) gemm_tc_kernel(const GemmTask *_
 }
 
 constexpr int kTcSmem = kTcStages * kUStage + 1024;
+constexpr int kTcSplitStages = 2;
+constexpr int kTcSplitSmem = kTcSplitStages * 2 * kUStage + 1024;
 
 }  // namespace
 
 void launch_gemm_tc(const GemmTask *tasks, int ntasks, int ntiles, const float *A, const float *B, float *C, int *err,
-                    cudaStream_t st, void *h16, const int32_t *sexp) {
+                    cudaStream_t st, void *h16, const int32_t *sexp, void *h16lo) {
     if (ntiles <= 0) return;
     static PerDeviceOnce once;
-    once([] { cudaFuncSetAttribute(gemm_tc_kernel<kTcStages>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem); });
+    once([] {
+        cudaFuncSetAttribute(gemm_tc_kernel<kTcStages, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        cudaFuncSetAttribute(gemm_tc_kernel<kTcSplitStages, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kTcSplitSmem);
+    });
     ++g_kernel_launches;
-    gemm_tc_kernel<kTcStages><<<ntiles, kUThreads, kTcSmem, st>>>(tasks, ntasks, A, B, C, err,
-                                                                    static_cast<__half *>(h16), sexp);
+    if (h16lo)
+        gemm_tc_kernel<kTcSplitStages, true><<<ntiles, kUThreads, kTcSplitSmem, st>>>(
+            tasks, ntasks, A, B, C, err, static_cast<__half *>(h16), static_cast<__half *>(h16lo), sexp);
+    else
+        gemm_tc_kernel<kTcStages, false><<<ntiles, kUThreads, kTcSmem, st>>>(
+            tasks, ntasks, A, B, C, err, static_cast<__half *>(h16), nullptr, sexp);
 }
 
 }  // namespace mfs

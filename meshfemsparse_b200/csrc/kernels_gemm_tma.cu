@@ -38,6 +38,7 @@
 
 #include <cstdint>
 #include <mutex>
+#include <type_traits>
 
 namespace mfs {
 
@@ -71,12 +72,27 @@ struct OpTraits<__half> {
     static constexpr uint32_t IDESC_AB = 0u; // F16 A and B
 };
 
+// Split FP16 operands (hi + 2^-11 lo, each FP16): same atoms as __half, 32 k rows
+// per stage so that the four boxes of a stage (A hi / lo, B hi / lo) fit a 4-deep ring.
+struct HalfSplit {};
+template <>
+struct OpTraits<HalfSplit> {
+    static constexpr int ATOM = 64;
+    static constexpr int TBK = 32;
+    static constexpr int MMA_K = 16;
+    static constexpr uint32_t SBO = 1024;
+    static constexpr uint32_t LAYOUT = 2;
+    static constexpr uint32_t IDESC_AB = 0u;
+};
+
 template <typename E>
 struct StageShape {
     static constexpr int BOX = 128 * OpTraits<E>::TBK;          // bytes of one box (one 128-byte group)
     static constexpr int A = (TBM / OpTraits<E>::ATOM) * BOX;   // 16 KB
     static constexpr int B = (TBN / OpTraits<E>::ATOM) * BOX;   // 32 KB
-    static constexpr int BYTES = A + B;
+    static constexpr bool SPLIT = std::is_same<E, HalfSplit>::value;
+    // ring slot: A hi, B hi (, A lo, B lo)
+    static constexpr int BYTES = SPLIT ? 2 * (A + B) : A + B;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -172,6 +188,11 @@ __device__ __forceinline__ void umma<__half>(uint32_t tmem, uint64_t ad, uint64_
         "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
         : "memory");
 }
+template <>
+__device__ __forceinline__ void umma<HalfSplit>(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc,
+                                                uint32_t acc) {
+    umma<__half>(tmem, ad, bd, idesc, acc);
+}
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
@@ -205,9 +226,12 @@ __device__ __forceinline__ int find_task(const GemmTask *tasks, int ntasks, int 
 template <typename E, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1) gemm_tma_kernel(const GemmTask *__restrict__ tasks, int ntasks,
                                                                const CUtensorMap *__restrict__ maps, float *Cbase,
-                                                               const int32_t *__restrict__ sexp, int *err) {
+                                                               const int32_t *__restrict__ sexp, int *err,
+                                                               int lo_maps) {
     using Tr = OpTraits<E>;
     using SS = StageShape<E>;
+    constexpr bool SPLIT = SS::SPLIT;
+    constexpr int TMEM_COLS = SPLIT ? 2 * kTmemCols : kTmemCols;
     extern __shared__ __align__(1024) unsigned char tma_smem_raw[];
     __shared__ __align__(8) uint64_t bars[2 * STAGES + 1];
     __shared__ uint32_t tmem_holder;
@@ -244,7 +268,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tma_kernel(const GemmTask *_
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_addr(&tmem_holder)),
-                     "r"(kTmemCols)
+                     "r"(TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -260,7 +284,13 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tma_kernel(const GemmTask *_
             const CUtensorMap *bm = maps + tk.bmap;
             tmap_acquire(am);
             if (tk.bmap != tk.amap) tmap_acquire(bm);
-            const uint32_t bytes = uint32_t(SS::A + (bn / Tr::ATOM) * SS::BOX);
+            const CUtensorMap *aml = maps + (SPLIT ? tk.amap + lo_maps : tk.amap);
+            const CUtensorMap *bml = maps + (SPLIT ? tk.bmap + lo_maps : tk.bmap);
+            if (SPLIT) {
+                tmap_acquire(aml);
+                if (tk.bmap != tk.amap) tmap_acquire(bml);
+            }
+            const uint32_t bytes = uint32_t(SS::A + (bn / Tr::ATOM) * SS::BOX) * (SPLIT ? 2u : 1u);
             int issued = 0;
             for (int kb = 0; kb < nk; ++kb) {
                 const int s = kb % STAGES;
@@ -275,6 +305,14 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tma_kernel(const GemmTask *_
                     tma_load_2d(sa + uint32_t(g) * SS::BOX, am, tk.ax + i0 + g * Tr::ATOM, tk.ay + ky, fb);
                 for (int g = 0; g < bn / Tr::ATOM; ++g)
                     tma_load_2d(sb + uint32_t(g) * SS::BOX, bm, tk.bx + j0 + g * Tr::ATOM, tk.by + ky, fb);
+                if constexpr (SPLIT) {
+                    const uint32_t sal = sa + SS::A + SS::B, sbl = sal + SS::A;
+#pragma unroll
+                    for (int g = 0; g < TBM / Tr::ATOM; ++g)
+                        tma_load_2d(sal + uint32_t(g) * SS::BOX, aml, tk.ax + i0 + g * Tr::ATOM, tk.ay + ky, fb);
+                    for (int g = 0; g < bn / Tr::ATOM; ++g)
+                        tma_load_2d(sbl + uint32_t(g) * SS::BOX, bml, tk.bx + j0 + g * Tr::ATOM, tk.by + ky, fb);
+                }
                 issued = kb + 1;
             }
             // the copies this thread issued land before the CTA can exit
@@ -300,7 +338,16 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tma_kernel(const GemmTask *_
                     const uint32_t off = uint32_t(g) * 128u * Tr::MMA_K;
                     const uint64_t ad = umma_desc(sa + off, SS::BOX, Tr::SBO, Tr::LAYOUT);
                     const uint64_t bd = umma_desc(sb + off, SS::BOX, Tr::SBO, Tr::LAYOUT);
-                    umma<E>(tmem, ad, bd, idesc, (kb > 0 || g > 0) ? 1u : 0u);
+                    const uint32_t first = (kb > 0 || g > 0) ? 1u : 0u;
+                    umma<E>(tmem, ad, bd, idesc, first);
+                    if constexpr (SPLIT) {
+                        // cross terms hi x lo + lo x hi into the second accumulator
+                        const uint32_t sal = sa + SS::A + SS::B, sbl = sal + SS::A;
+                        const uint64_t adl = umma_desc(sal + off, SS::BOX, Tr::SBO, Tr::LAYOUT);
+                        const uint64_t bdl = umma_desc(sbl + off, SS::BOX, Tr::SBO, Tr::LAYOUT);
+                        umma<E>(tmem + kTmemCols, ad, bdl, idesc, first);
+                        umma<E>(tmem + kTmemCols, adl, bd, idesc, 1u);
+                    }
                 }
                 umma_commit(empty0 + 8 * s);
             }
@@ -324,6 +371,13 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tma_kernel(const GemmTask *_
             for (int c0 = half * cw; c0 < (half + 1) * cw; c0 += 32) {
                 float v[32];
                 tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(c0), v);
+                if constexpr (SPLIT) {
+                    // hi x hi + 2^-11 (hi x lo + lo x hi)
+                    float x[32];
+                    tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(kTmemCols + c0), x);
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) v[e] = fmaf(x[e], 0x1p-11f, v[e]);
+                }
                 if (row >= 0 && row < tk.m) {
                     const int jb = j0 + c0 - db;
                     const int e_lo = max(0, -jb);
@@ -344,7 +398,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tma_kernel(const GemmTask *_
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
                      : "memory");
     }
 }
@@ -370,7 +424,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 template <typename E>
 void launch_tma(const GemmTask *tasks, int ntasks, int ntiles, const void *maps, float *C, const int32_t *sexp,
-                int *err, cudaStream_t st) {
+                int *err, cudaStream_t st, int lo_maps) {
     if (ntiles <= 0) return;
     static PerDeviceOnce once;
     once([] {
@@ -379,7 +433,7 @@ void launch_tma(const GemmTask *tasks, int ntasks, int ntiles, const void *maps,
     });
     ++g_kernel_launches;
     gemm_tma_kernel<E, kTmaStages><<<ntiles, kThreads, tma_smem<E>(), st>>>(
-        tasks, ntasks, static_cast<const CUtensorMap *>(maps), C, sexp, err);
+        tasks, ntasks, static_cast<const CUtensorMap *>(maps), C, sexp, err, lo_maps);
 }
 
 }  // namespace
@@ -418,10 +472,11 @@ bool encode_plain_map(void *out, const void *base, int esize, uint64_t rows, uin
     return r == CUDA_SUCCESS;
 }
 
-void launch_gemm_tma(bool half, const GemmTask *tasks, int ntasks, int ntiles, const void *maps, float *C,
-                     const int32_t *sexp, int *err, cudaStream_t st) {
-    if (half) launch_tma<__half>(tasks, ntasks, ntiles, maps, C, sexp, err, st);
-    else launch_tma<float>(tasks, ntasks, ntiles, maps, C, sexp, err, st);
+void launch_gemm_tma(int operands, const GemmTask *tasks, int ntasks, int ntiles, const void *maps, float *C,
+                     const int32_t *sexp, int *err, cudaStream_t st, int lo_maps) {
+    if (operands == 2) launch_tma<HalfSplit>(tasks, ntasks, ntiles, maps, C, sexp, err, st, lo_maps);
+    else if (operands == 1) launch_tma<__half>(tasks, ntasks, ntiles, maps, C, sexp, err, st, 0);
+    else launch_tma<float>(tasks, ntasks, ntiles, maps, C, sexp, err, st, 0);
 }
 
 }  // namespace mfs

@@ -250,3 +250,71 @@ def test_tcgen05_fp16_operands(m, n, k, da, db, e, lower):
     a_len, b_len, c_len = lens(t)
     A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float32, 5, seed=m + n + k + lower)
     check_mode0(t, A, B, C0, C, k)
+
+
+def split_fp16(x: np.ndarray):
+    """hi = rn16(x), lo = rn16(2^11 (x - hi)): the split-FP16 operand pair."""
+    hi = x.astype(np.float16)
+    lo = ((x.astype(np.float64) - hi.astype(np.float64)) * 2048.0).astype(np.float16)
+    return hi, lo
+
+
+@pytest.mark.parametrize("lower", [0, 1])
+@pytest.mark.parametrize("m,n,k,da,db,e", [(300, 200, 77, 3, 5, 0), (520, 256, 512, 7, 7, 6), (129, 100, 64, 0, 2, -9)])
+def test_tcgen05_split_fp16_operands(m, n, k, da, db, e, lower):
+    """Split FP16 with TMA (kernel 6): A = hi + 2^-11 lo, B likewise (each FP16), three
+    MMAs per k slice (hi hi into one accumulator, hi lo + lo hi into another), C -=
+    2^e (hi hi + 2^-11 (hi lo + lo hi)). Against the FP64 product of the operands'
+    exact values the only errors are the dropped lo lo term (2^-22 relative) and FP32
+    accumulation: normwise within 4e-6 of ||S||, FP32-level."""
+    if lower:
+        n = min(n, m)
+        db = da
+    lda = (m + da + 7) // 8 * 8 + 8
+    ldb = (n + db + 7) // 8 * 8
+    t = [task(8 + da, 16 + db, 5, lda, ldb, m + 3, m, n, k, lower=lower, scale_exp=e)]
+    a_len, b_len, c_len = lens(t)
+    a_len = (a_len + 7) // 8 * 8                # the lo halves start 16-byte aligned
+    b_len = (b_len + 7) // 8 * 8
+    rng = np.random.default_rng(m + n + k + lower + 99)
+    Ax = rng.uniform(-1, 1, a_len)
+    Bx = rng.uniform(-1, 1, b_len)
+    Ah, Al = split_fp16(Ax)
+    Bh, Bl = split_fp16(Bx)
+    A_val = Ah.astype(np.float64) + Al.astype(np.float64) / 2048.0
+    B_val = Bh.astype(np.float64) + Bl.astype(np.float64) / 2048.0
+    C0 = rng.uniform(-1, 1, c_len).astype(np.float32)
+    dev = "cuda:0"
+    tA = torch.from_numpy(np.concatenate([Ah, Al])).to(dev)
+    tB = torch.from_numpy(np.concatenate([Bh, Bl])).to(dev)
+    tC = torch.from_numpy(C0.copy()).to(dev)
+    tk = np.array([[t[0][f] for f in FIELDS]], dtype=np.int64)
+    _lib.debug_gemm(0, _lib.MFS_PREC_FP32, 6, tk, tA.data_ptr(), 2 * a_len, tB.data_ptr(), 2 * b_len,
+                    tC.data_ptr(), c_len)
+    C = tC.cpu().numpy()
+    ref, scale, written = expected(t, A_val, B_val, C0)
+    err = np.abs(C.astype(np.float64) - ref)
+    assert np.linalg.norm(err[written]) <= 4e-6 * np.linalg.norm(scale[written])
+    # the split is far more accurate than the hi operands alone
+    ref_hi, _, _ = expected(t, Ah.astype(np.float64), Bh.astype(np.float64), C0)
+    assert np.linalg.norm(err[written]) < 0.05 * np.linalg.norm((ref_hi - ref)[written])
+    assert np.array_equal(C[~written], C0[~written])
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("m,n,da,db", [(500, 128, 0, 0), (333, 128, 3, 0), (61, 72, 2, 1), (1024, 200, 1, 3)])
+def test_tcgen05_split_tf32(m, n, da, db, mode):
+    """Split TF32 on tcgen05 (kernel 7, the row solves of tensor_cores 6): arbitrary FP32
+    operands split in shared memory into TF32 hi + lo, three MMAs; FP32-level accuracy
+    (normwise 1e-5 of the product), for updates (mode 0) and row solves (mode 1, whose
+    FP32 result is stored unrounded)."""
+    k = n
+    lda = (m + da + 7) // 8 * 8
+    ldb = (n + db + 7) // 8 * 8
+    t = [task(da, db, 7, lda, ldb, m + 9, m, n, k, mode=mode)]
+    a_len, b_len, c_len = lens(t)
+    A, B, C0, C = run_case(t, a_len, b_len, c_len, np.float32, 7, seed=m + n + mode, tf32_exact=False)
+    ref, scale, written = expected(t, A, B, C0)
+    prod = (ref - (C0.astype(np.float64) if mode == 0 else 0.0))[written]
+    assert np.linalg.norm((C.astype(np.float64) - ref)[written]) <= 1e-5 * np.linalg.norm(prod)
+    assert np.array_equal(C[~written], C0[~written])
