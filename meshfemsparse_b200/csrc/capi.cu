@@ -519,16 +519,18 @@ void clear_factor_graphs(mfs_handle *h) {
 // FP32 Schur updates: 1 = single-pass TF32 on tcgen05 (cp.async operands), 4 = the same
 // with TMA-fed operands for the updates (mode 0) and cp.async for the row solves,
 // 5 = FP16 operands (a per-front power-of-two scaled half copy of the panels, written
-// by the row solves) on tcgen05 kind::f16 with TMA for the updates, 3 = split 3xTF32
-// (mma.sync), 0 = single-pass TF32 on mma.sync. Option values: tensor_cores 0 (auto: 5
-// with refinement, else 3), 1, 2 (-> 3), 3 (-> 0), 4, 5 (with refinement, else 3).
+// by the row solves) on tcgen05 kind::f16 with TMA for the updates, 6 = split FP16
+// (hi and 2^11-scaled lo half copies, three MMAs per k slice; row solves in split
+// TF32 on tcgen05): FP32-level products, 3 = split 3xTF32 (mma.sync), 0 = single-pass
+// TF32 on mma.sync. Option values: tensor_cores 0 (auto: 5 with refinement, else 3),
+// 1, 2 (-> 3), 3 (-> 0), 4, 5 and 6 (with refinement, else 3).
 // FP16 operands are safe under refinement: |L(i, j)| <= sqrt(A(j, j)) for an SPD
 // matrix, so the per-front scale keeps every operand below 2^12 (no overflow), and
 // the refinement needs the same iteration count as with TF32 operands.
 int fp32_split(const mfs_handle *h) {
     if (h->split_escalated) return 6;
     const int tc = h->opt.tensor_cores;
-    if (tc == 6) return 6;
+    if (tc == 6) return h->opt.refine ? 6 : 3;
     if (tc == 5 || tc == 0) return h->opt.refine ? 5 : 3;
     return tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : 4;
 }
@@ -1209,7 +1211,7 @@ mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, cons
 // The numeric factorization of the current values (h->cur.ax / bx, h->cur.sigma);
 // counters to mfs_stats, errors thrown. An FP32 factorization under refinement with
 // single-pass TF32 / FP16 products that had to perturb a pivot is redone once with
-// split 3xTF32 (FP32-level) products, which the handle then keeps: on high-contrast
+// split FP16 (FP32-level) products, which the handle then keeps: on high-contrast
 // inputs the low-precision Schur updates lose definiteness and refinement stalls.
 void numeric_core(mfs_handle *h) {
     DevSym &ds = *h->cur.sym;
