@@ -549,7 +549,8 @@ void ensure_panel_maps(mfs_handle *h, DevSym &ds, const void *base, bool half, c
     for (int c = 0; c < (lo ? 2 : 1); ++c) {
         const char *b = static_cast<const char *>(c ? lo : base);
         for (int32_t s : ds.large_fronts)
-            if (!encode_operand_map(&maps[c * nsn + size_t(s)], b + size_t(ds.dpan[s]) * es, half, uint64_t(S.f[s]),
+            if (!encode_operand_map(&maps[c * nsn + size_t(s)], b + size_t(ds.dpan[s]) * es, lo ? 2 : half ? 1 : 0,
+                                    uint64_t(S.f[s]),
                                     uint64_t(S.w[s]), uint64_t(ds.dld[s])))
                 throw StatusError(MFS_INTERNAL, "cuTensorMapEncodeTiled refused a panel tensor map");
     }

@@ -124,8 +124,9 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
                 put_error(err_buf, err_len, id + "arrays must be 16-byte aligned");
                 return MFS_INVALID_ARG;
             }
-            if (!encode_operand_map(ma, Af, half, uint64_t(m + da), uint64_t(k), uint64_t(lda)) ||
-                !encode_operand_map(mb, Bf, half, uint64_t(n + db), uint64_t(k), uint64_t(ldb))) {
+            const int ops = split16 ? 2 : half ? 1 : 0;
+            if (!encode_operand_map(ma, Af, ops, uint64_t(m + da), uint64_t(k), uint64_t(lda)) ||
+                !encode_operand_map(mb, Bf, ops, uint64_t(n + db), uint64_t(k), uint64_t(ldb))) {
                 put_error(err_buf, err_len, id + "tensor map refused by the driver");
                 return MFS_INVALID_ARG;
             }
@@ -152,9 +153,9 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
             const char *Al = static_cast<const char *>(A) + size_t(a_ext + g.a_off - da) * 2;
             const char *Bl = static_cast<const char *>(B) + size_t(b_ext + g.b_off - db) * 2;
             if ((reinterpret_cast<uintptr_t>(Al) & 15) || (reinterpret_cast<uintptr_t>(Bl) & 15) ||
-                !encode_operand_map(&maps[nh + size_t(g.amap)], Al, true, uint64_t(g.m + da), uint64_t(g.k),
+                !encode_operand_map(&maps[nh + size_t(g.amap)], Al, 2, uint64_t(g.m + da), uint64_t(g.k),
                                     uint64_t(g.lda)) ||
-                !encode_operand_map(&maps[nh + size_t(g.bmap)], Bl, true, uint64_t(g.n + db), uint64_t(g.k),
+                !encode_operand_map(&maps[nh + size_t(g.bmap)], Bl, 2, uint64_t(g.n + db), uint64_t(g.k),
                                     uint64_t(g.ldb))) {
                 put_error(err_buf, err_len, "kernel 6: lo tensor map refused (alignment or driver)");
                 return MFS_INVALID_ARG;

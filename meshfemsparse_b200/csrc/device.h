@@ -218,8 +218,9 @@ void launch_gemm_tma(int operands, const GemmTask *tasks, int ntasks, int ntiles
                      const int32_t *sexp, int *err, cudaStream_t st, int lo_maps = 0);
 // Tensor map of a column-major operand (rows x cols, leading dimension ld elements,
 // base 16-byte aligned, ld * element size a multiple of 16) in the box and swizzle
-// form of the TMA-fed GEMM; false if the driver refuses it.
-bool encode_operand_map(void *out, const void *base, bool half, uint64_t rows, uint64_t cols, uint64_t ld);
+// form that launch_gemm_tma's `operands` variant (0, 1 or 2; both the hi and the lo
+// maps for 2) stages; false if the driver refuses it.
+bool encode_operand_map(void *out, const void *base, int operands, uint64_t rows, uint64_t cols, uint64_t ld);
 // Plain (unswizzled) 2D tensor map of a column-major FP32 / FP64 matrix (rows x cols,
 // leading dimension ld elements), box box_rows x box_cols; reads outside the matrix
 // are zero.

@@ -440,13 +440,19 @@ void launch_tma(const GemmTask *tasks, int ntasks, int ntiles, const void *maps,
 
 static_assert(sizeof(CUtensorMap) == kTensorMapBytes, "tensor map size");
 
-bool encode_operand_map(void *out, const void *base, bool half, uint64_t rows, uint64_t cols, uint64_t ld) {
+bool encode_operand_map(void *out, const void *base, int operands, uint64_t rows, uint64_t cols, uint64_t ld) {
     PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
-    if (!fn) return false;
+    if (!fn || operands < 0 || operands > 2) return false;
+    const bool half = operands != 0;
     const uint32_t es = half ? 2 : 4;
+    // the box is one 128-byte group of rows by the k rows of one ring stage
+    const uint32_t box_k = operands == 2 ? uint32_t(OpTraits<HalfSplit>::TBK)
+                           : half        ? uint32_t(OpTraits<__half>::TBK)
+                                         : uint32_t(OpTraits<float>::TBK);
+    static_assert(StageShape<HalfSplit>::BOX == 128 * OpTraits<HalfSplit>::TBK, "split box");
     cuuint64_t dims[2] = {rows, cols};
     cuuint64_t strides[1] = {ld * es};
-    cuuint32_t box[2] = {128u / es, half ? uint32_t(OpTraits<__half>::TBK) : uint32_t(OpTraits<float>::TBK)};
+    cuuint32_t box[2] = {128u / es, box_k};
     cuuint32_t estr[2] = {1, 1};
     const CUresult r =
         fn(static_cast<CUtensorMap *>(out), half ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
