@@ -34,6 +34,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Newton solves/s at 1e-10 residual: FP32+refine & learned PCG vs FP64 plain"
 UNIT = "solves/s"
+# DRAM bytes of the split-FP16 GEMM launches over one config-2 factorization (ncu
+# capture; None until captured)
+GEMM_TRAFFIC_SPLIT16_CONFIG2 = None
 
 
 def parse():
@@ -50,8 +53,8 @@ def parse():
                         "the line carries under \"config4\"")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--tc", type=int, default=0,
-                   help="FP32 Schur updates: 0 auto (5 under refinement), 1 TF32, 2 split 3xTF32, 4 TF32 with TMA, "
-                        "5 FP16 operands with TMA")
+                   help="FP32 Schur updates: 0 auto (6 under refinement), 1 TF32, 2 split 3xTF32, 4 TF32 with TMA, "
+                        "5 FP16 operands with TMA, 6 split FP16 (hi/lo) operands with TMA")
     p.add_argument("--profile", action="store_true",
                    help="build the workload, run one untimed assemble + factorization + refined solve, exit "
                         "(the command profilers capture)")
@@ -282,14 +285,19 @@ def run_b200(args, rank, world, local, dist):
             out64 = {"fp64_plain": f"unavailable: {str(e)[:160]}"}
 
     peak = peaks["bf16_tflops_sustained"]
-    half = args.tc in (0, 5)
+    half = args.tc == 5
+    split16 = args.tc in (0, 6)
     # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) over the GEMM launches
-    # of one factorization of the full-size workload, FP16-operand mode, group width 4
-    gemm_traffic = {2: 89.9e9}.get(args.config) if (half and args.k is None and args.group in (0, 4)) else None
+    # of one factorization of the full-size workload (per operand mode, group width 4)
+    traffic_by_mode = {(2, True): GEMM_TRAFFIC_SPLIT16_CONFIG2, (2, False): 89.9e9}
+    gemm_traffic = (traffic_by_mode.get((args.config, split16)) if ((half or split16) and args.k is None
+                                                                   and args.group in (0, 4)) else None)
     roofline = {"bound": "tensor", "achieved": gemm_tf, "peak": peak, "unit": "TFLOP/s",
                 "frac": (gemm_tf / peak) if gemm_tf else None, "traffic": gemm_traffic,
                 "traffic_unit": "DRAM bytes per factorization over the same GEMM launches (ncu capture of this workload)",
-                "kernel": ("gemm_tma_kernel (tcgen05 kind::f16, TMA-fed Schur updates) + gemm_tc_kernel (row solves)"
+                "kernel": ("gemm_tma_kernel (tcgen05 kind::f16, split hi/lo FP16 operands: three MMAs per k slice, "
+                           "TMA-fed Schur updates) + gemm_tc_kernel (split-TF32 row solves)" if split16 else
+                           "gemm_tma_kernel (tcgen05 kind::f16, TMA-fed Schur updates) + gemm_tc_kernel (row solves)"
                            if half else "gemm_tc_kernel / gemm_tma_kernel (tcgen05 kind::tf32)"),
                 "launches": stk["gemm_launches"], "kernel_ms_per_factorization": stk["gemm_ms"],
                 "kernel_flops_per_factorization": stk["gemm_flops"],

@@ -73,13 +73,16 @@ typedef struct {
     double refine_tol;          /* relative residual target ||b - Hx|| / ||b|| (1e-10) */
     int32_t refine_maxit;       /* iteration cap (50) */
     int32_t use_graphs;         /* capture the factorization / solve launch sequence in CUDA graphs */
-    int32_t tensor_cores;       /* FP32 Schur updates: 0 auto (5 with refinement, else split 3xTF32),
+    int32_t tensor_cores;       /* FP32 Schur updates: 0 auto (6 with refinement, else split 3xTF32),
                                    1 TF32 on tcgen05, 2 split 3xTF32 (FP32-level products, mma.sync),
                                    3 TF32 on mma.sync (the pre-Blackwell tensor-core path),
                                    4 TF32 on tcgen05 with TMA-fed operands for the Schur updates,
                                    5 FP16 operands on tcgen05 (kind::f16, TMA-fed): the row solves
                                      write a copy of the panels scaled by a power of two per front;
-                                     needs refine = 1 (without it: as 2) */
+                                     needs refine = 1 (without it: as 2),
+                                   6 split FP16 on tcgen05: hi and 2^11-scaled lo half copies, three
+                                     MMAs per k slice into two TMEM accumulators (FP32-level products),
+                                     split-TF32 row solves; needs refine = 1 (without it: as 2) */
     int32_t time_kernels;       /* 1: mfs_numeric times each tensor-core GEMM launch with CUDA events on its
                                    stream (mfs_stats.gemm_ms / gemm_flops); adds event records, off by default */
     int32_t nd_reuse_period;    /* > 0: a nested-dissection analysis of a changed pattern on the same variables
@@ -268,7 +271,7 @@ typedef struct {
                                     factorization met a pivot <= 1e-5 x the injected diagonal and were
                                     factored again in FP64 (last numeric) */
     int32_t split_escalations;   /* FP32 under refinement: times a single-pass TF32 / FP16 factorization was
-                                    redone with split 3xTF32 (FP32-level) products because it perturbed a
+                                    redone with split FP16 (FP32-level, tensor_cores 6) products because it perturbed a
                                     pivot or its refinement stalled; the handle then keeps the split
                                     products until the next symbolic analysis or mfs_set_options
                                     (cumulative) */

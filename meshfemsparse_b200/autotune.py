@@ -90,7 +90,7 @@ def tune(H, pins, tets, Ke, rhs, single: bool = True, refine: bool = True, devic
     if cutoffs is None:
         cutoffs = CUTOFFS_FP32 if single else CUTOFFS_FP64
     if tensor_modes is None:
-        tensor_modes = (1, 2) if (single and refine) else (0,)
+        tensor_modes = (5, 6) if (single and refine) else (0,)
     if measure is None:
         def measure(cut, tc):
             return measure_step(H, pins, tets, Ke, rhs, single, refine, device, cut, tc, repeats)

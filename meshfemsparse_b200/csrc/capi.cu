@@ -522,16 +522,19 @@ void clear_factor_graphs(mfs_handle *h) {
 // by the row solves) on tcgen05 kind::f16 with TMA for the updates, 6 = split FP16
 // (hi and 2^11-scaled lo half copies, three MMAs per k slice; row solves in split
 // TF32 on tcgen05): FP32-level products, 3 = split 3xTF32 (mma.sync), 0 = single-pass
-// TF32 on mma.sync. Option values: tensor_cores 0 (auto: 5 with refinement, else 3),
-// 1, 2 (-> 3), 3 (-> 0), 4, 5 and 6 (with refinement, else 3).
+// TF32 on mma.sync. Option values: tensor_cores 0 (auto: 6 with refinement, else 3),
+// 1, 2 (-> 3), 3 (-> 0), 4, 5 and 6 (with refinement, else 3). The automatic choice
+// is split FP16: its FP32-level factor needs 3-4 refinement iterations where the
+// single-pass modes need 6-7, which outweighs its dearer Schur updates as soon as the
+// solves carry several right-hand sides, and it never needs escalating.
 // FP16 operands are safe under refinement: |L(i, j)| <= sqrt(A(j, j)) for an SPD
 // matrix, so the per-front scale keeps every operand below 2^12 (no overflow), and
 // the refinement needs the same iteration count as with TF32 operands.
 int fp32_split(const mfs_handle *h) {
     if (h->split_escalated) return 6;
     const int tc = h->opt.tensor_cores;
-    if (tc == 6) return h->opt.refine ? 6 : 3;
-    if (tc == 5 || tc == 0) return h->opt.refine ? 5 : 3;
+    if (tc == 6 || tc == 0) return h->opt.refine ? 6 : 3;
+    if (tc == 5) return h->opt.refine ? 5 : 3;
     return tc == 1 ? 1 : tc == 2 ? 3 : tc == 3 ? 0 : 4;
 }
 

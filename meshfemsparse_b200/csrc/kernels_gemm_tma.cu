@@ -5,7 +5,8 @@
 // Operands are FP32 read as TF32 (kind::tf32) or FP16 (kind::f16, the scaled
 // half-precision copy of the factor's panels); C and the accumulation are FP32.
 // Same task lists and 128 x 256 task tiles as the cp.async kernel
-// (kernels_gemm_tc.cu): one CTA per task tile, 320 threads.
+// (kernels_gemm_tc.cu): one CTA per task tile, 320 threads, two CTAs per SM for
+// FP32 and FP16 operands (see Occupancy).
 //   warp 0     lane 0 issues the TMA loads of a STAGES-deep ring: per k-block one
 //              box of 128 bytes x TBK k rows per 128-byte group of M (N) rows;
 //              A and B are 2D tensor maps (rows x k columns, column-major) built
@@ -14,8 +15,8 @@
 //   warp 1     allocates 256 TMEM columns (the 128 x 256 FP32 accumulator); lane 0
 //              issues tcgen05.mma (M = 128, N = 256 or 128) from shared-memory
 //              descriptors and frees ring slots with tcgen05.commit.
-//   warps 2-9  epilogue: TMEM -> registers -> C (two warps per 32-lane quarter of
-//              TMEM, one per column half).
+//   warps 2-9  epilogue: TMEM -> registers -> C in 16-column chunks (two warps per
+//              32-lane quarter of TMEM, one per column half).
 // Shared-memory operand layout: MN-major, 128-byte swizzle; FP32 with 32-byte
 // atoms (a 512-byte atom holds 4 k rows of 32 elements, the 32-byte chunk index
 // XOR-ed with the k row), FP16 with 16-byte atoms (1024-byte atoms of 8 k rows of
@@ -197,21 +198,18 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
 }
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr)
         : "memory");
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int e = 0; e < 32; ++e) v[e] = __uint_as_float(r[e]);
+    for (int e = 0; e < 16; ++e) v[e] = __uint_as_float(r[e]);
 }
 
 __device__ __forceinline__ int find_task(const GemmTask *tasks, int ntasks, int t) {
@@ -223,8 +221,8 @@ __device__ __forceinline__ int find_task(const GemmTask *tasks, int ntasks, int 
     return lo;
 }
 
-template <typename E, int STAGES>
-__global__ void __launch_bounds__(kThreads, 1) gemm_tma_kernel(const GemmTask *__restrict__ tasks, int ntasks,
+template <typename E, int STAGES, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) gemm_tma_kernel(const GemmTask *__restrict__ tasks, int ntasks,
                                                                const CUtensorMap *__restrict__ maps, float *Cbase,
                                                                const int32_t *__restrict__ sexp, int *err,
                                                                int lo_maps) {
@@ -368,27 +366,27 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tma_kernel(const GemmTask *_
             const int se = sexp ? 2 * sexp[tk.amap] : tk.scale_exp;
             const float scale = se ? ldexpf(1.0f, se) : 1.0f;
             float *C = Cbase + tk.c_off;
-            for (int c0 = half * cw; c0 < (half + 1) * cw; c0 += 32) {
-                float v[32];
-                tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(c0), v);
+            for (int c0 = half * cw; c0 < (half + 1) * cw; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(c0), v);
                 if constexpr (SPLIT) {
                     // hi x hi + 2^-11 (hi x lo + lo x hi)
-                    float x[32];
-                    tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(kTmemCols + c0), x);
+                    float x[16];
+                    tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(kTmemCols + c0), x);
 #pragma unroll
-                    for (int e = 0; e < 32; ++e) v[e] = fmaf(x[e], 0x1p-11f, v[e]);
+                    for (int e = 0; e < 16; ++e) v[e] = fmaf(x[e], 0x1p-11f, v[e]);
                 }
                 if (row >= 0 && row < tk.m) {
                     const int jb = j0 + c0 - db;
                     const int e_lo = max(0, -jb);
-                    const int e_hi = min(32, (tk.lower ? min(tk.n, row + 1) : tk.n) - jb);
+                    const int e_hi = min(16, (tk.lower ? min(tk.n, row + 1) : tk.n) - jb);
                     float *p = C + int64_t(jb) * tk.ldc + row;
-                    float cv[32];
+                    float cv[16];
 #pragma unroll
-                    for (int e = 0; e < 32; ++e)
+                    for (int e = 0; e < 16; ++e)
                         if (e >= e_lo && e < e_hi) cv[e] = p[int64_t(e) * tk.ldc];
 #pragma unroll
-                    for (int e = 0; e < 32; ++e)
+                    for (int e = 0; e < 16; ++e)
                         if (e >= e_lo && e < e_hi) p[int64_t(e) * tk.ldc] = fmaf(-scale, v[e], cv[e]);
                 }
             }
@@ -403,11 +401,24 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tma_kernel(const GemmTask *_
     }
 }
 
-constexpr int kTmaStages = 4;
+// Ring depth and CTAs per SM: the single-operand forms run two CTAs per SM (two
+// 48 KB stages each, 256 TMEM columns each), so that one CTA's epilogue (the C
+// read-modify-write) overlaps the other's main loop; split FP16 holds two 256-column
+// accumulators (all 512 TMEM columns), one CTA per SM with a 4-deep ring.
+template <typename E>
+struct Occupancy {
+    static constexpr int STAGES = 2, MINB = 2;
+};
+template <>
+struct Occupancy<HalfSplit> {
+    static constexpr int STAGES = 4, MINB = 1;
+};
 template <typename E>
 constexpr int tma_smem() {
-    return kTmaStages * StageShape<E>::BYTES + 1024;
+    return Occupancy<E>::STAGES * StageShape<E>::BYTES + 1024;
 }
+static_assert(2 * (Occupancy<float>::STAGES * StageShape<float>::BYTES + 1024 + 1024) <= 228 * 1024, "2 CTAs / SM");
+static_assert(2 * (Occupancy<__half>::STAGES * StageShape<__half>::BYTES + 1024 + 1024) <= 228 * 1024, "2 CTAs / SM");
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -428,11 +439,11 @@ void launch_tma(const GemmTask *tasks, int ntasks, int ntiles, const void *maps,
     if (ntiles <= 0) return;
     static PerDeviceOnce once;
     once([] {
-        cudaFuncSetAttribute(gemm_tma_kernel<E, kTmaStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             tma_smem<E>());
+        cudaFuncSetAttribute(gemm_tma_kernel<E, Occupancy<E>::STAGES, Occupancy<E>::MINB>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem<E>());
     });
     ++g_kernel_launches;
-    gemm_tma_kernel<E, kTmaStages><<<ntiles, kThreads, tma_smem<E>(), st>>>(
+    gemm_tma_kernel<E, Occupancy<E>::STAGES, Occupancy<E>::MINB><<<ntiles, kThreads, tma_smem<E>(), st>>>(
         tasks, ntasks, static_cast<const CUtensorMap *>(maps), C, sexp, err, lo_maps);
 }
 

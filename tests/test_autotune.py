@@ -11,11 +11,11 @@ def test_picks_fastest_and_caches(tmp_path):
 
     def fake(cut, tc):
         calls.append((cut, tc))
-        return abs(cut - 128) + (0.5 if tc == 2 else 0.0)
+        return abs(cut - 128) + (0.5 if tc == 6 else 0.0)
 
     cache = tmp_path / "tune.json"
     r = autotune.tune(H, pins, None, None, None, single=True, refine=True, cache=cache, measure=fake)
-    assert (r["small_front_max"], r["tensor_cores"]) == (128, 1) and not r["cached"]
+    assert (r["small_front_max"], r["tensor_cores"]) == (128, 5) and not r["cached"]
     assert len(calls) == len(autotune.CUTOFFS_FP32) * 2
     r2 = autotune.tune(H, pins, None, None, None, single=True, refine=True, cache=cache, measure=fake)
     assert r2["cached"] and r2["small_front_max"] == 128 and len(calls) == len(autotune.CUTOFFS_FP32) * 2
@@ -31,6 +31,6 @@ def test_choose_form_keeps_the_faster_precision(tmp_path):
     fast64 = lambda single, cut, tc: (10.0 if single else 5.0) + cut / 1000.0
     r = autotune.choose_form(H, [0], None, None, None, cache=tmp_path / "a.json", measure=fast64)
     assert not r["singlePrecision"] and not r["refine"] and r["small_front_max"] == 64
-    fast32 = lambda single, cut, tc: (3.0 if single else 5.0) + tc
+    fast32 = lambda single, cut, tc: (3.0 if single else 5.0) + tc / 10.0
     r = autotune.choose_form(H, [1], None, None, None, cache=tmp_path / "b.json", measure=fast32)
-    assert r["singlePrecision"] and r["refine"] and r["tensor_cores"] == 1
+    assert r["singlePrecision"] and r["refine"] and r["tensor_cores"] == 5
