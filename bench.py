@@ -59,6 +59,9 @@ def parse():
                    help="build the workload, run one untimed assemble + factorization + refined solve, exit "
                         "(the command profilers capture)")
     p.add_argument("--maxit", type=int, default=50, help="refinement iteration cap")
+    p.add_argument("--gemm-table", default=None,
+                   help="write the per-launch GEMM record (ms, flops, tiles, tasks, kind) of the kernel-timed "
+                        "factorization to this file")
     p.add_argument("--group", type=int, default=0, help="column blocks per factorization group (0: default)")
     p.add_argument("--chain", type=int, default=0, help="diagonal solves: 0 superblock inverses, 1 block-pair chains")
     p.add_argument("--cpu-seconds", type=float, default=150.0,
@@ -254,6 +257,9 @@ def run_b200(args, rank, world, local, dist):
     step(f32, pK, pB, pX, D)
     torch.cuda.synchronize()
     stk = f32.stats()
+    if args.gemm_table:
+        np.savetxt(args.gemm_table, _lib.debug_gemm_launches(f32._h), fmt="%.6g",
+                   header="ms flops tiles tasks kind(0 left,1 rowsolve,2 next-group,3 trailing,4 syrk)")
     f32._opts.time_kernels = 0
     _lib.check(lib.mfs_set_options(f32._h, C.byref(f32._opts)), f32._h, "options")
     gemm_tf = stk["gemm_flops"] / (stk["gemm_ms"] * 1e-3) / 1e12 if stk["gemm_ms"] > 0 else None

@@ -43,6 +43,14 @@ mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t kernel, int
                           const int64_t *tasks, const void *A, int64_t a_len, const void *B, int64_t b_len,
                           void *C, int64_t c_len, char *err_buf, size_t err_len);
 
+/* Per-launch record of the last numeric factorization run with time_kernels = 1:
+ * for each tensor-core GEMM launch (in launch order) out[5 i .. 5 i + 4] = {CUDA-event
+ * ms, algorithmic flops, CTA tiles, tasks, kind}; kind 0 = left-looking update inside
+ * a column-block group, 1 = row solve, 2 = update of the next group's columns, 3 =
+ * trailing update of the columns after it, 4 = the level's Schur-complement SYRK.
+ * *count receives the number of launches; at most max_launches are written. */
+mfs_status mfs_debug_gemm_launches(const mfs_handle *h, int64_t max_launches, double *out, int64_t *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,7 +27,7 @@ EXPORTED = [
     "mfs_stash", "mfs_swap_stash", "mfs_clear_stash", "mfs_has_stash", "mfs_clear_factors", "mfs_get_stats",
     "mfs_set_options", "mfs_apply_noalloc", "mfs_lpc_param_count", "mfs_lpc_create", "mfs_lpc_destroy",
     "mfs_lpc_get_weights", "mfs_lpc_set_weights", "mfs_lpc_loss_grad", "mfs_lpc_train_step", "mfs_pcg_solve",
-    "mfs_debug_gemm", "mfs_build_pattern_device", "mfs_conversion_plan_device",
+    "mfs_debug_gemm", "mfs_build_pattern_device", "mfs_conversion_plan_device", "mfs_debug_gemm_launches",
 ]
 GEMM_TASK_FIELDS = 12
 
@@ -106,6 +106,7 @@ def load() -> C.CDLL:
                                   C.POINTER(C.c_int32)]
     lib.mfs_debug_gemm.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, i64p, P, C.c_int64, P, C.c_int64,
                                    P, C.c_int64, C.c_char_p, C.c_size_t]
+    lib.mfs_debug_gemm_launches.argtypes = [P, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -198,3 +199,16 @@ def build_pattern_device(nvars: int, conn_ptr: int, nelem: int, npe: int, Ap_ptr
 
 def library_present() -> bool:
     return LIB_PATH.exists() and os.access(LIB_PATH, os.R_OK)
+
+
+def debug_gemm_launches(handle) -> np.ndarray:
+    """Per tensor-core GEMM launch of the handle's last numeric factorization run with
+    time_kernels on: rows of (ms, flops, tiles, tasks, kind); kind 0 left-looking group
+    update, 1 row solve, 2 next-group update, 3 trailing update, 4 level SYRK."""
+    lib = load()
+    cnt = C.c_int64(0)
+    check(lib.mfs_debug_gemm_launches(handle, 0, None, C.byref(cnt)), None, "mfs_debug_gemm_launches")
+    out = np.zeros((max(cnt.value, 1), 5), dtype=np.float64)
+    check(lib.mfs_debug_gemm_launches(handle, cnt.value, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(cnt)),
+          None, "mfs_debug_gemm_launches")
+    return out[:cnt.value]

@@ -3,6 +3,7 @@
 // assembly and the factor stash. Host logic only; kernels live in
 // kernels_factor.cu / kernels_solve.cu.
 #include "../../include/mfs_b200.h"
+#include "../../include/mfs_b200_testing.h"
 #include "device.h"
 #include "handle.h"
 #include "host_symbolic.h"
@@ -617,6 +618,7 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
     const bool timing = h->opt.time_kernels != 0;
     h->gemm_events_used = 0;
     h->gemm_flops_timed = 0.0;
+    h->gemm_launch_info.clear();
     auto launch = [&](const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int sp, int *err,
                       cudaStream_t s, bool mode0) {
         if constexpr (std::is_same<T, float>::value) {
@@ -634,7 +636,7 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         launch_gemm<T>(tasks, ntasks, ntiles, A, B, C, sp >= 4 ? 1 : sp, err, s);
     };
     auto tgemm = [&](const GemmTask *tasks, int ntasks, int ntiles, const T *A, const T *B, T *C, int sp, int *err,
-                     cudaStream_t s, bool mode0 = true) {
+                     cudaStream_t s, int kind, bool mode0 = true) {
         if (ntasks <= 0) return;
         if (!timing) {
             launch(tasks, ntasks, ntiles, A, B, C, sp, err, s, mode0);
@@ -648,7 +650,9 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
             h->gemm_events.push_back(e1);
         }
         const size_t t0 = size_t(tasks - ds.gemm_tasks.p);
-        h->gemm_flops_timed += ds.gemm_flops_prefix[t0 + ntasks] - ds.gemm_flops_prefix[t0];
+        const double fl = ds.gemm_flops_prefix[t0 + ntasks] - ds.gemm_flops_prefix[t0];
+        h->gemm_flops_timed += fl;
+        h->gemm_launch_info.insert(h->gemm_launch_info.end(), {fl, double(ntiles), double(ntasks), double(kind)});
         MFS_CUDA(cudaEventRecord(h->gemm_events[h->gemm_events_used], s));
         launch(tasks, ntasks, ntiles, A, B, C, sp, err, s, mode0);
         MFS_CUDA(cudaEventRecord(h->gemm_events[h->gemm_events_used + 1], s));
@@ -698,13 +702,13 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         bool rest_pending = false;
         for (const auto &sp : L.steps) {
             tgemm(ds.gemm_tasks.p + sp.left_off, sp.left_n, sp.left_tiles, factor, factor, factor, split,
-                           h->gemm_err.p, hs);
+                           h->gemm_err.p, hs, 0);
             MFS_LAUNCHED();
             launch_panel<T>(ds.potrf_tasks.p + sp.potrf_off, sp.potrf_n, sp.potrf_maxnb, factor, dscr, pv, split == 1 || split == 4 || split == 5,
                             hs);
             MFS_LAUNCHED();
             tgemm(ds.gemm_tasks.p + sp.trsm_off, sp.trsm_n, sp.trsm_tiles, factor, dscr, factor, split,
-                           h->gemm_err.p, hs, false);
+                           h->gemm_err.p, hs, 1, false);
             MFS_LAUNCHED();
             if (sp.gemm_n == 0) continue;
             if (sp.rest_n > 0) MFS_CUDA(cudaEventRecord(h->ev_ready, hs));
@@ -713,12 +717,12 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
                 rest_pending = false;
             }
             tgemm(ds.gemm_tasks.p + sp.gemm_off, sp.gemm_n, sp.gemm_tiles, factor, factor, factor, split,
-                           h->gemm_err.p, hs);
+                           h->gemm_err.p, hs, 2);
             MFS_LAUNCHED();
             if (sp.rest_n > 0) {
                 MFS_CUDA(cudaStreamWaitEvent(st, h->ev_ready, 0));
                 tgemm(ds.gemm_tasks.p + sp.rest_off, sp.rest_n, sp.rest_tiles, factor, factor, factor, split,
-                               h->gemm_err.p, st);
+                               h->gemm_err.p, st, 3);
                 MFS_LAUNCHED();
                 MFS_CUDA(cudaEventRecord(h->ev_rest, st));
                 rest_pending = true;
@@ -727,7 +731,8 @@ void run_factor(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, const dou
         MFS_CUDA(cudaEventRecord(h->ev_join, hs));
         MFS_CUDA(cudaStreamWaitEvent(st, h->ev_join, 0));
         if (L.syrk_n > 0) {
-            tgemm(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, factor, upd, split, h->gemm_err.p, st);
+            tgemm(ds.gemm_tasks.p + L.syrk_off, L.syrk_n, L.syrk_tiles, factor, factor, upd, split, h->gemm_err.p, st,
+                  4);
             MFS_LAUNCHED();
         }
     }
@@ -1255,10 +1260,12 @@ void numeric_core(mfs_handle *h) {
     h->stats.gemm_ms = 0.0;
     h->stats.gemm_flops = h->gemm_flops_timed;
     h->stats.gemm_launches = int64_t(h->gemm_events_used / 2);
+    h->gemm_launch_ms.clear();
     for (size_t e = 0; e + 1 < h->gemm_events_used; e += 2) {
         float g = 0;
         MFS_CUDA(cudaEventElapsedTime(&g, h->gemm_events[e], h->gemm_events[e + 1]));
         h->stats.gemm_ms += g;
+        h->gemm_launch_ms.push_back(g);
     }
     if (h->fail_host[2]) {
         MFS_CUDA(cudaMemset(h->gemm_err.p, 0, sizeof(int)));
@@ -1706,6 +1713,17 @@ mfs_status mfs_apply_noalloc(mfs_handle *h, const double *x, double *y, int64_t 
         MFS_LAUNCHED();
         MFS_CUDA(cudaStreamSynchronize(st));
     });
+}
+
+mfs_status mfs_debug_gemm_launches(const mfs_handle *h, int64_t max_launches, double *out, int64_t *count) {
+    if (!h || !count || (max_launches > 0 && !out)) return MFS_INVALID_ARG;
+    const size_t n = std::min(h->gemm_launch_ms.size(), h->gemm_launch_info.size() / 4);
+    *count = int64_t(n);
+    for (size_t i = 0; i < n && int64_t(i) < max_launches; ++i) {
+        out[5 * i] = double(h->gemm_launch_ms[i]);
+        for (int c = 0; c < 4; ++c) out[5 * i + 1 + c] = h->gemm_launch_info[4 * i + c];
+    }
+    return MFS_OK;
 }
 
 mfs_status mfs_get_stats(const mfs_handle *h, mfs_stats *st) {

@@ -225,6 +225,10 @@ struct mfs_handle {
     std::vector<cudaEvent_t> gemm_events;    // time_kernels: (start, end) per GEMM launch
     size_t gemm_events_used = 0;
     double gemm_flops_timed = 0.0;
+    // time_kernels: per timed GEMM launch {flops, tiles, tasks, kind} (kind: 0 left-looking
+    // group update, 1 row solve, 2 next-group update, 3 trailing update, 4 level SYRK)
+    std::vector<double> gemm_launch_info;
+    std::vector<float> gemm_launch_ms;
 };
 
 namespace mfs {

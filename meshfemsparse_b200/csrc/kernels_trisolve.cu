@@ -604,7 +604,7 @@ struct Vec16<double> {
     using type = double2;
 };
 
-template <typename T>
+template <typename T, int NG>
 __global__ void __launch_bounds__(256) str_fwd_kernel(const StrTask *__restrict__ tasks, SnDev sd,
                                                       const T *__restrict__ factor, const double *__restrict__ X,
                                                       int64_t ldx, int nrhs, double *__restrict__ P) {
@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(256) str_fwd_kernel(const StrTask *__restrict_
     using V = typename Vec16<T>::type;
     constexpr int E = 16 / int(sizeof(T));
     constexpr int NVL = 4 / E;                             // loads per lane and column (4 rows)
-    __shared__ __align__(16) Q ys[4][kStrCols];
+    __shared__ __align__(16) Q ys[NG][kStrCols];
     const StrTask tk = tasks[blockIdx.x];
     const int s = tk.sn;
     const int w = sd.w[s], f = sd.f[s], ld = sd.ld[s], c0 = sd.col0[s];
@@ -629,20 +629,20 @@ __global__ void __launch_bounds__(256) str_fwd_kernel(const StrTask *__restrict_
     }
     const bool active = rbase < f;
     double *Pt = P + int64_t(blockIdx.x) * kStrRows * nrhs + warp * 128;
-    for (int g = 0; g < nrhs; g += 4) {
-        const int ng = min(4, nrhs - g);
+    for (int g = 0; g < nrhs; g += NG) {
+        const int ng = min(NG, nrhs - g);
         __syncthreads();                                   // the previous pass is done with ys
-        for (int q = tid; q < 4 * kStrCols; q += 256) {
+        for (int q = tid; q < NG * kStrCols; q += 256) {
             const int r = q / kStrCols, j = q - r * kStrCols;
             ys[r][j] = (r < ng && j < nj) ? Q(X[c0 + jb + j + (g + r) * ldx]) : Q(0);
         }
         __syncthreads();
         if (!active) continue;
-        Q acc[4][4];
+        Q acc[4][NG];
 #pragma unroll
         for (int e = 0; e < 4; ++e)
 #pragma unroll
-            for (int r = 0; r < 4; ++r) acc[e][r] = Q(0);
+            for (int r = 0; r < NG; ++r) acc[e][r] = Q(0);
         const T *col = pan + int64_t(jb) * ld;
 #pragma unroll 8
         for (int j = 0; j < nj; ++j, col += ld) {
@@ -652,16 +652,16 @@ __global__ void __launch_bounds__(256) str_fwd_kernel(const StrTask *__restrict_
                 if (vok[v]) lv[v] = *reinterpret_cast<const V *>(col + row0[v]);
                 else lv[v] = V{};
             }
-            Q yv[4];
+            Q yv[NG];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) yv[r] = ys[r][j];
+            for (int r = 0; r < NG; ++r) yv[r] = ys[r][j];
 #pragma unroll
             for (int v = 0; v < NVL; ++v) {
                 const T *lp = reinterpret_cast<const T *>(&lv[v]);
 #pragma unroll
                 for (int e = 0; e < E; ++e)
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) acc[v * E + e][r] += Q(lp[e]) * yv[r];
+                    for (int r = 0; r < NG; ++r) acc[v * E + e][r] += Q(lp[e]) * yv[r];
             }
         }
 #pragma unroll
@@ -669,12 +669,12 @@ __global__ void __launch_bounds__(256) str_fwd_kernel(const StrTask *__restrict_
 #pragma unroll
             for (int e = 0; e < E; ++e)
 #pragma unroll
-                for (int r = 0; r < 4; ++r)
+                for (int r = 0; r < NG; ++r)
                     if (r < ng) Pt[(g + r) * kStrRows + v * 32 * E + E * lane + e] = double(acc[v * E + e][r]);
     }
 }
 
-template <typename T>
+template <typename T, int NG>
 __global__ void __launch_bounds__(256) str_bwd_kernel(const StrTask *__restrict__ tasks, SnDev sd,
                                                       const T *__restrict__ factor, const double *__restrict__ X,
                                                       int64_t ldx, int nrhs, double *__restrict__ P) {
@@ -684,7 +684,7 @@ __global__ void __launch_bounds__(256) str_bwd_kernel(const StrTask *__restrict_
     constexpr int NVL = 4 / E;                             // loads per lane, column and 128-row block
     constexpr int BR = str_bwd_rows(sizeof(T) == 8);
     extern __shared__ __align__(16) unsigned char str_raw[];
-    Q *xs = reinterpret_cast<Q *>(str_raw);                // [4][BR]
+    Q *xs = reinterpret_cast<Q *>(str_raw);                // [NG][BR]
     const StrTask tk = tasks[blockIdx.x];
     const int s = tk.sn;
     const int w = sd.w[s], f = sd.f[s], ld = sd.ld[s], c0 = sd.col0[s];
@@ -697,10 +697,10 @@ __global__ void __launch_bounds__(256) str_bwd_kernel(const StrTask *__restrict_
     const int nj = max(0, min(8, w - j0));
     const int tid = threadIdx.x, lane = tid & 31;
     double *Pt = P + int64_t(blockIdx.x) * kStrBCols * nrhs + (threadIdx.x >> 5) * 8;
-    for (int g = 0; g < nrhs; g += 4) {
-        const int ng = min(4, nrhs - g);
+    for (int g = 0; g < nrhs; g += NG) {
+        const int ng = min(NG, nrhs - g);
         __syncthreads();
-        for (int q = tid; q < 4 * BR; q += 256) {
+        for (int q = tid; q < NG * BR; q += 256) {
             const int r = q / BR, i = q - r * BR;
             const int row = rbase + i, li = row - w;
             Q v = Q(0);
@@ -708,22 +708,22 @@ __global__ void __launch_bounds__(256) str_bwd_kernel(const StrTask *__restrict_
             xs[q] = v;
         }
         __syncthreads();
-        Q acc[8][4];
+        Q acc[8][NG];
 #pragma unroll
         for (int u = 0; u < 8; ++u)
 #pragma unroll
-            for (int r = 0; r < 4; ++r) acc[u][r] = Q(0);
+            for (int r = 0; r < NG; ++r) acc[u][r] = Q(0);
         for (int b = 0; b < nrb; ++b) {
             int row0[NVL];
             bool vok[NVL];
-            Q xv[4][4];
+            Q xv[4][NG];
 #pragma unroll
             for (int v = 0; v < NVL; ++v) {
                 const int i0 = b * 128 + v * 32 * E + E * lane;
                 row0[v] = rbase + i0;
                 vok[v] = row0[v] < f;
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
+                for (int r = 0; r < NG; ++r) {
                     const V xv4 = *reinterpret_cast<const V *>(xs + r * BR + i0);
                     const Q *xp = reinterpret_cast<const Q *>(&xv4);
 #pragma unroll
@@ -748,13 +748,13 @@ __global__ void __launch_bounds__(256) str_bwd_kernel(const StrTask *__restrict_
 #pragma unroll
                     for (int e = 0; e < E; ++e)
 #pragma unroll
-                        for (int r = 0; r < 4; ++r) acc[u][r] += Q(lp[e]) * xv[v * E + e][r];
+                        for (int r = 0; r < NG; ++r) acc[u][r] += Q(lp[e]) * xv[v * E + e][r];
                 }
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u)
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
+            for (int r = 0; r < NG; ++r) {
                 Q sum = acc[u][r];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
@@ -833,22 +833,36 @@ cudaError_t launch_diag(bool forward, const SolveTask *tasks, int ntasks, SnDev 
     return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kDiagThreads), args, smem, st);
 }
 
+template <typename T, int NG>
+void launch_str_ng(bool forward, const StrTask *tasks, int ntasks, const StrReduce *red, int nred, SnDev sd,
+                   const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st) {
+    using Q = std::conditional_t<sizeof(T) == 4, float, double>;
+    const size_t smem = size_t(NG) * str_bwd_rows(sizeof(T) == 8) * sizeof(Q);
+    static PerDeviceOnce once;
+    once([smem] { cudaFuncSetAttribute(str_bwd_kernel<T, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); });
+    if (forward) {
+        str_fwd_kernel<T, NG><<<ntasks, 256, 0, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
+        str_reduce_kernel<true><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
+    } else {
+        str_bwd_kernel<T, NG><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
+        str_reduce_kernel<false><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
+    }
+}
+
+// Right-hand sides per sweep over L21: 4, or 8 for an FP32 factor with more than
+// four (each sweep streams the task's L21 once; FP64 keeps 4 for its registers).
 template <typename T>
 void launch_str(bool forward, const StrTask *tasks, int ntasks, const StrReduce *red, int nred, SnDev sd,
                 const T *factor, double *X, int64_t ldx, int nrhs, double *sol, double *P, cudaStream_t st) {
     if (ntasks <= 0) return;
     g_kernel_launches += 2;
-    using Q = std::conditional_t<sizeof(T) == 4, float, double>;
-    const size_t smem = size_t(4) * str_bwd_rows(sizeof(T) == 8) * sizeof(Q);
-    static PerDeviceOnce once;
-    once([smem] { cudaFuncSetAttribute(str_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); });
-    if (forward) {
-        str_fwd_kernel<T><<<ntasks, 256, 0, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
-        str_reduce_kernel<true><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
-    } else {
-        str_bwd_kernel<T><<<ntasks, 256, smem, st>>>(tasks, sd, factor, X, ldx, nrhs, P);
-        str_reduce_kernel<false><<<nred, 256, 0, st>>>(red, sd, X, ldx, nrhs, sol, P);
+    if constexpr (sizeof(T) == 4) {
+        if (nrhs > 4) {
+            launch_str_ng<T, 8>(forward, tasks, ntasks, red, nred, sd, factor, X, ldx, nrhs, sol, P, st);
+            return;
+        }
     }
+    launch_str_ng<T, 4>(forward, tasks, ntasks, red, nred, sd, factor, X, ldx, nrhs, sol, P, st);
 }
 
 #define MFS_TRI_INSTANTIATE(T)                                                                                    \

@@ -71,8 +71,9 @@ def test_batch_instances_are_independent():
 
 @pytest.mark.parametrize("tc", [0, 5])
 def test_two_material_contrast_32_rhs(tc):
-    """1e3 stiffness contrast, 32 right-hand sides: FP32 + refinement with TF32 Schur
-    updates (tc 0) and with FP16 operands scaled per front (tc 5) reach 1e-10."""
+    """1e3 stiffness contrast, 32 right-hand sides (the solves sweep L21 with eight of
+    them at a time): FP32 + refinement with split FP16 Schur updates (tc 0, automatic)
+    and with single FP16 operands scaled per front (tc 5) reach 1e-10."""
     wl = workloads.config5(k=10, seed=5)
     assert wl.nrhs == 32
     f32 = assembled(wl, single=True, refine=True, tc=tc)
@@ -85,12 +86,17 @@ def test_two_material_contrast_32_rhs(tc):
 
 
 def test_contrast_escalates_low_precision_factor():
-    """At 1e3 contrast and k=32 the single-pass FP16 factorization perturbs pivots and
-    its refinement stalls (measured: residual 3e-5 after 50 iterations); the handle
-    redoes it with split 3xTF32 products, reaches 1e-10 and keeps the split products
-    for the next factorization of the same pattern."""
+    """At 1e3 contrast and k=32 the single-pass FP16 factorization (tc 5) perturbs
+    pivots and its refinement stalls (measured: residual 3e-5 after 50 iterations); the
+    handle redoes it with split FP16 products (tc 6), reaches 1e-10 and keeps the split
+    products for the next factorization of the same pattern. The automatic mode starts
+    with the split products and never escalates."""
     wl = workloads.config5(k=32, seed=5)
-    f32 = assembled(wl, single=True, refine=True, tc=0)
+    auto = assembled(wl, single=True, refine=True, tc=0)
+    assert residual(wl, auto.solveMultiRHS(wl.rhs)) <= 1e-10
+    assert auto.stats()["split_escalations"] == 0 and auto.stats()["perturbed_pivots"] == 0
+    del auto
+    f32 = assembled(wl, single=True, refine=True, tc=5)
     X = f32.solveMultiRHS(wl.rhs)
     st = f32.stats()
     assert st["split_escalations"] >= 1
