@@ -565,7 +565,14 @@ NDResult nested_dissection_reuse(idx n, const std::vector<idx> &xadj, const std:
             idx a = prev.cmember[u], b = prev.cmember[adj[e]];
             if (a == b || is_anc(a, b) || is_anc(b, a)) continue;
             idx c = a;                            // lowest common ancestor: climb until it covers b
-            while (!is_anc(c, b)) c = prev.cparent[c];
+            while (c >= 0 && !is_anc(c, b)) c = prev.cparent[c];
+            if (c < 0) {
+                // the edge joins two trees of the previous forest (e.g. new contact between
+                // bodies): no separator of the old tree is left to keep, dissect afresh
+                // (persistent_separator_tree.hh:97-99 rebuilds fully in this case)
+                if (rebuilt_vertices) *rebuilt_vertices = n;
+                return nested_dissection(n, xadj, adj, opt);
+            }
             rebuild[c] = 1;
         }
     NDState st(xadj, adj, opt, n);

@@ -152,6 +152,29 @@ class BlockCSCHessian:
     def trace(self) -> float:
         return float(sum(self.Ax[self.locForScalar(i, i)] for i in range(self.n)))
 
+    def addWithSubSparsity(self, b: "BlockCSCHessian", alpha: float = 1.0) -> "BlockCSCHessian":
+        """self += alpha * b where b's block pattern is contained in self's (the
+        numeric matrix enlarged into a cached pattern; reference
+        BlockCSCHessian::addWithSubSparsityFast, BlockCSCHessian.hh:1222-1262).
+        Raises ValueError on incompatible blocks or a block of b outside self."""
+        if b.bs != self.bs or b.numBlocks != self.numBlocks:
+            raise ValueError("addWithSubSparsity: incompatible variable block structure")
+        if b.isSparsityOnly():
+            return self
+        if self.isSparsityOnly():
+            self.setZero()
+        bcols = np.repeat(np.arange(b.numBlocks, dtype=np.int64), np.diff(b.Ap))
+        # position of each of b's blocks in self: search its row among self's column
+        key_self = np.repeat(np.arange(self.numBlocks, dtype=np.int64), np.diff(self.Ap)) * self.numBlocks + self.Ai
+        key_b = bcols * b.numBlocks + b.Ai
+        pos = np.searchsorted(key_self, key_b)
+        if key_b.size and (np.any(pos >= key_self.size) or np.any(key_self[np.minimum(pos, key_self.size - 1)] != key_b)):
+            raise ValueError("addWithSubSparsity: the added matrix has a block outside this pattern")
+        bb = self.bs * self.bs
+        dst = self.Ax.reshape(-1, bb)
+        dst[pos] += alpha * b.Ax.reshape(-1, bb)
+        return self
+
     # -------------------------------------------------- scalar conversions
     def dataOffsetsForScalarCSCDataOffsets(self) -> np.ndarray:
         """For every entry of the scalar upper CSC (toScalar order), its offset in Ax."""

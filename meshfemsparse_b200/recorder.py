@@ -116,30 +116,55 @@ def recorded_sequence(directory) -> list[tuple[str, int, Path]]:
     return sorted(events, key=lambda e: e[1])
 
 
-def replay(directory, factorizer, solve: bool = True, seed: int = 0, shift_ratio: float | None = None) -> list[dict]:
+def replay(directory, factorizer, solve: bool = True, seed: int = 0, shift_ratio: float | None = None,
+           sparsity_cache: float | None = None) -> list[dict]:
     """Run a recorded sequence through `factorizer` (a B200Factorizer). Each numeric
     step returns its relative residual when `solve` is set (a seeded N(0,1) RHS, pins
     zero). With `shift_ratio`, each numeric step factors H + (shift_ratio * trace(H) / n) I,
     as the reference's benchmark driver does with 1e-8 (benchmark_linear_systems.cc:298-302);
-    the residual is then against H + shift I."""
+    the residual is then against H + shift I.
+
+    With `sparsity_cache` (the entry budget ratio), patterns pass through a SparsityLRU
+    as in the reference's contact-sequence driver (benchmark_sparsity_lru.cc:100-150): a
+    symbolic file whose entries the cache already holds reuses the last symbolic
+    factorization (its record has "symbolic_factorization": False), otherwise the
+    factorizer analyses the cache's enlarged pattern; every numeric matrix is added into
+    the cached pattern before it is factored."""
+    from .sparsity_lru import SparsityLRU
+
     out = []
     pins = np.zeros(0, dtype=np.int64)
     rng = np.random.default_rng(seed)
+    lru = None
     for kind, i, path in recorded_sequence(directory):
         H = BlockCSCHessian.constructFromBinaryFile(path)
         if kind == "symbolic":
             pv = Path(directory) / MatrixRecorder.pinnedVarsFileName(i)
             pins = np.loadtxt(pv, dtype=np.int64, ndmin=1) if pv.exists() and pv.stat().st_size else \
                 np.zeros(0, dtype=np.int64)
-            factorizer.factorizeSymbolic(H, pins)
-            out.append({"id": i, "kind": kind, "n": H.n, "blocks": H.nz})
+            rec = {"id": i, "kind": kind, "n": H.n, "blocks": H.nz}
+            if sparsity_cache is None:
+                factorizer.factorizeSymbolic(H, pins)
+            else:
+                if lru is None:
+                    lru = SparsityLRU(H.numBlocks, H.Ap, H.Ai, budget_ratio=float(sparsity_cache))
+                    needs = True
+                else:
+                    needs = lru.update(H.numBlocks, H.Ap, H.Ai) != 0
+                if needs:
+                    factorizer.factorizeSymbolic(BlockCSCHessian(H.numBlocks, lru.Ap, lru.Ai, H.bs), pins)
+                rec.update(symbolic_factorization=bool(needs), cached_blocks=int(lru.Ap[-1]))
+            out.append(rec)
             continue
+        Hf = H
+        if lru is not None:
+            Hf = BlockCSCHessian(H.numBlocks, lru.Ap, lru.Ai, H.bs).setZero().addWithSubSparsity(H)
         sigma = 0.0
         if shift_ratio is not None:
             sigma = float(shift_ratio) * H.trace() / H.n
-            factorizer.factorizeNumericWithShift(H, sigma)
+            factorizer.factorizeNumericWithShift(Hf, sigma)
         else:
-            factorizer.factorizeNumeric(H)
+            factorizer.factorizeNumeric(Hf)
         rec = {"id": i, "kind": kind, "n": H.n, "shift": sigma}
         if solve:
             b = rng.normal(size=H.n)
