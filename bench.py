@@ -34,9 +34,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Newton solves/s at 1e-10 residual: FP32+refine & learned PCG vs FP64 plain"
 UNIT = "solves/s"
-# DRAM bytes of the split-FP16 GEMM launches over one config-2 factorization (ncu
-# capture; None until captured)
-GEMM_TRAFFIC_SPLIT16_CONFIG2 = None
+# DRAM bytes (read + write) of the split-FP16 GEMM launches over one config-2
+# factorization: ncu capture of `bench.py --profile`, gemm_tma 72.73 + 29.0 GB,
+# gemm_tc 6.78 + 3.5 GB
+GEMM_TRAFFIC_SPLIT16_CONFIG2 = 112.0e9
 
 
 def parse():
