@@ -64,6 +64,8 @@ def parse():
                    help="write the per-launch GEMM record (ms, flops, tiles, tasks, kind) of the kernel-timed "
                         "factorization to this file")
     p.add_argument("--group", type=int, default=0, help="column blocks per factorization group (0: default)")
+    p.add_argument("--subtrees", type=int, default=0,
+                   help="subtree count the solve cut aims for (0: default)")
     p.add_argument("--chain", type=int, default=0, help="diagonal solves: 0 superblock inverses, 1 block-pair chains")
     p.add_argument("--cpu-seconds", type=float, default=150.0,
                    help="reference arm: stop timing complete CPU steps once this much is spent")
@@ -173,7 +175,8 @@ def run_b200(args, rank, world, local, dist):
 
     def make(single):
         f = B200Factorizer(single, refine=single, stream=stream.cuda_stream, device=local, tensor_cores=args.tc,
-                           refine_maxit=args.maxit, solve_chain=args.chain, factor_group=args.group)
+                           refine_maxit=args.maxit, solve_chain=args.chain, factor_group=args.group,
+                           solve_subtrees=args.subtrees)
         t = time.time()
         f.factorizeSymbolic(wl.H, wl.pins)
         f.setElements(wl.tets)

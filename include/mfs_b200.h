@@ -95,7 +95,11 @@ typedef struct {
     int32_t factor_group;       /* large fronts: column blocks per group of the blocked factorization (inside a
                                    group left-looking, after it one update of the rest of the front);
                                    0: default (4); read at the symbolic analysis */
-    int32_t reserved[3];
+    int32_t solve_subtrees;     /* solves: the levels below the highest level with at least this many subtrees
+                                   (fronts of at most 2048 rows) are solved one subtree per CTA, the levels above
+                                   by level kernels; 0: default (the larger of 2368 and 48 per tree of the
+                                   assembly forest); read at the symbolic analysis */
+    int32_t reserved[2];
 } mfs_options;
 
 typedef struct mfs_handle mfs_handle;

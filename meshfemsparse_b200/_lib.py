@@ -39,7 +39,8 @@ class Options(C.Structure):
         ("seed", C.c_uint64), ("stream", C.c_void_p), ("small_front_max", C.c_int32), ("refine", C.c_int32),
         ("refine_tol", C.c_double), ("refine_maxit", C.c_int32), ("use_graphs", C.c_int32),
         ("tensor_cores", C.c_int32), ("time_kernels", C.c_int32), ("nd_reuse_period", C.c_int32),
-        ("solve_chain", C.c_int32), ("factor_group", C.c_int32), ("reserved", C.c_int32 * 3),
+        ("solve_chain", C.c_int32), ("factor_group", C.c_int32),
+        ("solve_subtrees", C.c_int32), ("reserved", C.c_int32 * 2),
     ]
 
 

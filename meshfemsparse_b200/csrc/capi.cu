@@ -1173,6 +1173,7 @@ mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, cons
         so.relax_ratio = h->opt.relax_ratio;
         so.nd.leaf_size = h->opt.nd_leaf_size > 0 ? h->opt.nd_leaf_size : 120;
         so.nd.seed = h->opt.seed;
+        so.solve_subtrees = h->opt.solve_subtrees;
         const bool reuse = h->opt.nd_reuse_period > 0 && h->nd_prev && h->nd_reuse_count < h->opt.nd_reuse_period;
         if (reuse) so.nd_prev = h->nd_prev.get();
         std::string e = analyze(n_blocks, Ap, Ai, block_size, pinned, n_pinned, so, user_perm, *Sp, supernode_sizes,

@@ -75,6 +75,7 @@ struct SymbolicOptions {
     double relax_ratio = 0.01;       // alternative allowance: zeros / stored entries
     OrderingOptions nd;
     const NDResult *nd_prev = nullptr;   // reuse this dissection's separator tree (same vertices)
+    idx solve_subtrees = 0;          // subtree count the solve cut aims for (0: max(2368, 48 per tree))
 };
 
 // One conversion-plan entry: copy a vb x vb block of the user's value array

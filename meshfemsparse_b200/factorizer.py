@@ -91,7 +91,7 @@ class B200Factorizer:
                  refine_maxit: int = 50, small_front_max: int = 0, tensor_cores: int = 0, relax: bool = True,
                  use_graphs: bool = False, nd_reuse_period: int = 0,
                  relax_zeros: int = 128, relax_ratio: float = 0.01, nd_leaf_size: int = 120, seed: int = 12345,
-                 stream: int | None = None, solve_chain: int = 0, factor_group: int = 0):
+                 stream: int | None = None, solve_chain: int = 0, factor_group: int = 0, solve_subtrees: int = 0):
         self._lib = _lib.load()
         self.singlePrecision = bool(singlePrecision)
         self.orderingMethod = OrderingMethod(orderingMethod)
@@ -100,7 +100,8 @@ class B200Factorizer:
             refine=int(refine), refine_tol=refine_tol, refine_maxit=refine_maxit, small_front_max=small_front_max,
             use_graphs=int(use_graphs), nd_reuse_period=int(nd_reuse_period),
             tensor_cores=tensor_cores, relax=int(relax), relax_zeros=relax_zeros, relax_ratio=relax_ratio,
-            nd_leaf_size=nd_leaf_size, seed=seed, solve_chain=solve_chain, factor_group=factor_group)
+            nd_leaf_size=nd_leaf_size, seed=seed, solve_chain=solve_chain, factor_group=factor_group,
+            solve_subtrees=solve_subtrees)
         opts = _lib.default_options(**self._base_opts)
         opts.ordering = int(self.orderingMethod)
         if stream is not None:
