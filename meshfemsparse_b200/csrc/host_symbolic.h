@@ -56,6 +56,24 @@ NDResult nested_dissection(idx n, const std::vector<idx> &xadj, const std::vecto
 NDResult nested_dissection_reuse(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
                                  const NDResult &prev, const OrderingOptions &opt, idx *rebuilt_vertices);
 
+// Final order of a dissection (hierarchical_camd.cc:165-333): constrained minimum
+// degree with the separator forest's components as constraint sets (descendants
+// first, each component contiguous), one independent problem per subtree rooted at
+// `cut_depth` (clamped to the forest's depth) and one for the separators above,
+// which receive every subtree's boundary clique as an initial element. Returns the
+// new iperm (nd.iperm unchanged when cut_depth < 0 or the forest does not fit).
+struct HierarchicalMDStats {
+    int cut_depth = -1;
+    idx tasks = 0, upper_vertices = 0, upper_elements = 0;
+};
+std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
+                                             const NDResult &nd, int cut_depth, HierarchicalMDStats *stats = nullptr);
+// Cut depth of that final order: MFS_ND_CAMD_CUT_DEPTH from the environment (the
+// reference reads CHOLMOD_NESDIS_CAMD_CUT_DEPTH), default 4; negative values keep
+// the dissection's own order (separators in vertex order, leaves by halo minimum
+// degree).
+int camd_cut_depth_from_env();
+
 // Minimum-degree order of the whole graph (used for the AMD-style mode and for
 // nested-dissection leaves).
 std::vector<idx> minimum_degree(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj);

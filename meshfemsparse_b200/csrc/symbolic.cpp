@@ -274,6 +274,8 @@ std::string analyze(idx nblocks, const idx *Ap, const idx *Ai, int bs, const idx
         idx rebuilt = -1;
         NDResult nd = opt.nd_prev ? nested_dissection_reuse(nv, gx, ga, *opt.nd_prev, opt.nd, &rebuilt)
                                   : nested_dissection(nv, gx, ga, opt.nd);
+        const int cut = camd_cut_depth_from_env();
+        if (cut >= 0) nd.iperm = hierarchical_constrained_md(nv, gx, ga, nd, cut);
         iperm = nd.iperm;
         S.nd_cparent = nd.cparent;
         S.nd_cmember = nd.cmember;
