@@ -543,7 +543,7 @@ int fp32_split(const mfs_handle *h) {
 // copy) for the TMA-fed GEMM (built on the host once per symbolic analysis and
 // array; not during graph capture).
 void ensure_panel_maps(mfs_handle *h, DevSym &ds, const void *base, bool half, const void *lo = nullptr) {
-    if (h->tmaps_base == base && h->tmaps_sym == &ds && h->tmaps_lo == lo) return;
+    if (h->tmaps_base == base && h->tmaps_sym == ds.id && h->tmaps_lo == lo) return;
     const Symbolic &S = *ds.S;
     const size_t es = half ? 2 : 4;
     const size_t nsn = size_t(std::max<idx>(S.nsn, 1));
@@ -563,7 +563,7 @@ void ensure_panel_maps(mfs_handle *h, DevSym &ds, const void *base, bool half, c
                              h->stream));
     MFS_CUDA(cudaStreamSynchronize(h->stream));
     h->tmaps_base = base;
-    h->tmaps_sym = &ds;
+    h->tmaps_sym = ds.id;
     h->tmaps_lo = lo;
 }
 
@@ -572,7 +572,7 @@ void ensure_panel_maps(mfs_handle *h, DevSym &ds, const void *base, bool half, c
 // dimension ld), a forward box (64 rows x FC columns) and a backward box (FC rows x
 // 64 columns), FC = 32 KB / (64 es).
 void ensure_solve_maps(mfs_handle *h, DevSym &ds, const void *base, int es) {
-    if (h->smaps_base == base && h->smaps_sym == &ds && h->smaps_es == es) return;
+    if (h->smaps_base == base && h->smaps_sym == ds.id && h->smaps_es == es) return;
     const Symbolic &S = *ds.S;
     const uint32_t FC = uint32_t(32768 / (64 * es));
     const size_t nb = ds.isb_host.size(), nf = ds.sb_fronts.size();
@@ -601,7 +601,7 @@ void ensure_solve_maps(mfs_handle *h, DevSym &ds, const void *base, int es) {
                              h->stream));
     MFS_CUDA(cudaStreamSynchronize(h->stream));
     h->smaps_base = base;
-    h->smaps_sym = &ds;
+    h->smaps_sym = ds.id;
     h->smaps_es = es;
 }
 
@@ -766,7 +766,7 @@ void factor_sequence(mfs_handle *h, DevSym &ds, T *factor, T *upd, T *dscr, cons
         return;
     }
     const void *dorig = h->dorig.p;
-    mfs_handle::FactorGraph key{&ds,      factor,      upd,         dscr,  Ax,    Bx,     dorig,
+    mfs_handle::FactorGraph key{ds.id,    factor,      upd,         dscr,  Ax,    Bx,     dorig,
                                 h->h16.p, h->h16lo.p, h->tmaps.p, sigma, split, nullptr};
     auto same = [&](const mfs_handle::FactorGraph &g) {
         return g.ds == key.ds && g.factor == key.factor && g.upd == key.upd && g.dscr == key.dscr &&

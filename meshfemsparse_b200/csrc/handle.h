@@ -7,6 +7,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <memory>
 #include <new>
 #include <stdexcept>
@@ -93,6 +94,13 @@ struct LevelPlan {
 };
 
 struct DevSym {
+    // unique per upload (never reused, unlike the object's address once it is freed):
+    // the key of the caches built from this symbolic data
+    uint64_t id = next_id();
+    static uint64_t next_id() {
+        static std::atomic<uint64_t> counter{0};
+        return ++counter;
+    }
     std::shared_ptr<Symbolic> S;
     DBuf<int32_t> w, d, f, ld, col0, child_ptr, child_list, struct_rows, rel, small_list, all_list;
     DBuf<int64_t> pan_off, upd_off, sol_off, struct_ptr, diag_off;
@@ -175,7 +183,7 @@ struct mfs_handle {
     // (element size smaps_es) of the symbolic data `smaps_sym`
     DBuf<TensorMapBlob> smaps;
     const void *smaps_base = nullptr;
-    const void *smaps_sym = nullptr;
+    uint64_t smaps_sym = 0;
     int smaps_es = 0;
     std::shared_ptr<DBuf<double>> asm_ax;   // output of the last mfs_assemble (device resident)
     std::shared_ptr<DBuf<double>> asm_spare;   // an earlier assembly buffer, reused once nothing holds it
@@ -204,7 +212,8 @@ struct mfs_handle {
     // use_graphs: instantiated graphs of the factorization's launch sequence, keyed by
     // everything the launches bake in (symbolic data, buffers, values, shift)
     struct FactorGraph {
-        const void *ds, *factor, *upd, *dscr, *ax, *bx, *dorig, *h16, *h16lo, *tmaps;
+        uint64_t ds;                       // DevSym::id
+        const void *factor, *upd, *dscr, *ax, *bx, *dorig, *h16, *h16lo, *tmaps;
         double sigma;
         int split;
         cudaGraphExec_t exec;
@@ -217,7 +226,7 @@ struct mfs_handle {
     // symbolic data `tmaps_sym`
     DBuf<TensorMapBlob> tmaps;
     const void *tmaps_base = nullptr;
-    const void *tmaps_sym = nullptr;
+    uint64_t tmaps_sym = 0;
     const void *tmaps_lo = nullptr;          // the lo copy the maps after the first nsn cover (split FP16)
     DBuf<uint16_t> h16;                      // FP16 operand copy of the panels (tensor_cores 5, 6)
     DBuf<uint16_t> h16lo;                    // split FP16 (tensor_cores 6): 2^11 x the remainder of h16
