@@ -12,9 +12,11 @@
 //              A and B are 2D tensor maps (rows x k columns, column-major) built
 //              on the host, one per factor panel (or per task for the test hook);
 //              rows or columns outside a map arrive as zeros.
-//   warp 1     allocates 256 TMEM columns (the 128 x 256 FP32 accumulator); lane 0
-//              issues tcgen05.mma (M = 128, N = 256 or 128) from shared-memory
-//              descriptors and frees ring slots with tcgen05.commit.
+//   warp 1     allocates 256 TMEM columns (the 128 x 256 FP32 accumulator, or with
+//              split FP16 operands two 128 x 128 ones: a 256-column task tile then
+//              runs as two CTAs of 128 columns); lane 0 issues tcgen05.mma (M = 128,
+//              N = 256 or 128) from shared-memory descriptors and frees ring slots
+//              with tcgen05.commit.
 //   warps 2-9  epilogue: TMEM -> registers -> C in 16-column chunks (two warps per
 //              32-lane quarter of TMEM, one per column half).
 // Shared-memory operand layout: MN-major, 128-byte swizzle; FP32 with 32-byte
@@ -48,7 +50,6 @@ namespace {
 constexpr int TBM = 128, TBN = 256;
 constexpr int kEpiWarps = 8;
 constexpr int kThreads = (2 + kEpiWarps) * 32;
-constexpr int kTmemCols = 256;
 constexpr unsigned long long kWaitNs = 1000000000ull;   // 1 s per wait at most
 constexpr int kGroupM = 8;
 
@@ -86,11 +87,13 @@ struct OpTraits<HalfSplit> {
     static constexpr uint32_t IDESC_AB = 0u;
 };
 
-template <typename E>
+// TN: the columns one CTA computes (256, or 128 when a 256-column task tile is split
+// between two CTAs)
+template <typename E, int TN>
 struct StageShape {
     static constexpr int BOX = 128 * OpTraits<E>::TBK;          // bytes of one box (one 128-byte group)
     static constexpr int A = (TBM / OpTraits<E>::ATOM) * BOX;   // 16 KB
-    static constexpr int B = (TBN / OpTraits<E>::ATOM) * BOX;   // 32 KB
+    static constexpr int B = (TN / OpTraits<E>::ATOM) * BOX;    // 32 KB for TN = 256
     static constexpr bool SPLIT = std::is_same<E, HalfSplit>::value;
     // ring slot: A hi, B hi (, A lo, B lo)
     static constexpr int BYTES = SPLIT ? 2 * (A + B) : A + B;
@@ -221,20 +224,21 @@ __device__ __forceinline__ int find_task(const GemmTask *tasks, int ntasks, int 
     return lo;
 }
 
-template <typename E, int STAGES, int MINB>
+template <typename E, int STAGES, int MINB, int CTA_N>
 __global__ void __launch_bounds__(kThreads, MINB) gemm_tma_kernel(const GemmTask *__restrict__ tasks, int ntasks,
                                                                const CUtensorMap *__restrict__ maps, float *Cbase,
                                                                const int32_t *__restrict__ sexp, int *err,
                                                                int lo_maps) {
     using Tr = OpTraits<E>;
-    using SS = StageShape<E>;
+    using SS = StageShape<E, CTA_N>;
     constexpr bool SPLIT = SS::SPLIT;
-    constexpr int TMEM_COLS = SPLIT ? 2 * kTmemCols : kTmemCols;
+    constexpr int HALVES = TBN / CTA_N;                 // CTAs per 256-column task tile
+    constexpr int TMEM_COLS = SPLIT ? 2 * CTA_N : CTA_N;   // split: second accumulator at column CTA_N
     extern __shared__ __align__(1024) unsigned char tma_smem_raw[];
     __shared__ __align__(8) uint64_t bars[2 * STAGES + 1];
     __shared__ uint32_t tmem_holder;
 
-    const int t = blockIdx.x;
+    const int t = blockIdx.x / HALVES, hj = blockIdx.x % HALVES;
     const GemmTask tk = tasks[find_task(tasks, ntasks, t)];
     // groups of kGroupM row tiles sweep the columns (co-resident CTAs share panels in L2)
     const int local = t - tk.tile_base;
@@ -242,10 +246,10 @@ __global__ void __launch_bounds__(kThreads, MINB) gemm_tma_kernel(const GemmTask
     const int first = (local / per_group) * kGroupM;
     const int gs = min(kGroupM, tk.tiles_m - first);
     const int ti = first + (local % per_group) % gs, tj = (local % per_group) / gs;
-    const int i0 = ti * TBM, j0 = tj * TBN;            // tile origin in shifted coordinates
+    const int i0 = ti * TBM, j0 = tj * TBN + hj * CTA_N;   // CTA tile origin in shifted coordinates
     const int da = tk.shift & 255, db = tk.shift >> 8;  // shifted row x is operand row x - d
     if ((tk.lower && i0 + TBM - 1 - da < j0 - db) || tk.k <= 0 || j0 >= tk.n + db) return;   // CTA-uniform
-    const int bn = (tk.n + db - j0 <= 128) ? 128 : TBN;
+    const int bn = (tk.n + db - j0 <= 128) ? 128 : CTA_N;
     const int nk = (tk.k + Tr::TBK - 1) / Tr::TBK;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -343,8 +347,8 @@ __global__ void __launch_bounds__(kThreads, MINB) gemm_tma_kernel(const GemmTask
                         const uint32_t sal = sa + SS::A + SS::B, sbl = sal + SS::A;
                         const uint64_t adl = umma_desc(sal + off, SS::BOX, Tr::SBO, Tr::LAYOUT);
                         const uint64_t bdl = umma_desc(sbl + off, SS::BOX, Tr::SBO, Tr::LAYOUT);
-                        umma<E>(tmem + kTmemCols, ad, bdl, idesc, first);
-                        umma<E>(tmem + kTmemCols, adl, bd, idesc, 1u);
+                        umma<E>(tmem + CTA_N, ad, bdl, idesc, first);
+                        umma<E>(tmem + CTA_N, adl, bd, idesc, 1u);
                     }
                 }
                 umma_commit(empty0 + 8 * s);
@@ -372,7 +376,7 @@ __global__ void __launch_bounds__(kThreads, MINB) gemm_tma_kernel(const GemmTask
                 if constexpr (SPLIT) {
                     // hi x hi + 2^-11 (hi x lo + lo x hi)
                     float x[16];
-                    tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(kTmemCols + c0), x);
+                    tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(CTA_N + c0), x);
 #pragma unroll
                     for (int e = 0; e < 16; ++e) v[e] = fmaf(x[e], 0x1p-11f, v[e]);
                 }
@@ -401,24 +405,27 @@ __global__ void __launch_bounds__(kThreads, MINB) gemm_tma_kernel(const GemmTask
     }
 }
 
-// Ring depth and CTAs per SM: the single-operand forms run two CTAs per SM (two
-// 48 KB stages each, 256 TMEM columns each), so that one CTA's epilogue (the C
-// read-modify-write) overlaps the other's main loop; split FP16 holds two 256-column
-// accumulators (all 512 TMEM columns), one CTA per SM with a 4-deep ring.
+// Ring depth, CTAs per SM and columns per CTA. The single-operand forms run two CTAs
+// per SM (two 48 KB stages each, 256 TMEM columns each), so that one CTA's epilogue
+// (the C read-modify-write) overlaps the other's main loop. Split FP16 holds two
+// accumulators; it splits every 256-column task tile between two CTAs of 128 columns
+// (two 128-column accumulators, 256 TMEM columns; three 32 KB stages) for the same
+// two-CTA overlap (one 256-column CTA would hold all 512 TMEM columns alone).
 template <typename E>
 struct Occupancy {
-    static constexpr int STAGES = 2, MINB = 2;
+    static constexpr int STAGES = 2, MINB = 2, CTA_N = TBN;
 };
 template <>
 struct Occupancy<HalfSplit> {
-    static constexpr int STAGES = 4, MINB = 1;
+    static constexpr int STAGES = 3, MINB = 2, CTA_N = 128;
 };
 template <typename E>
 constexpr int tma_smem() {
-    return Occupancy<E>::STAGES * StageShape<E>::BYTES + 1024;
+    return Occupancy<E>::STAGES * StageShape<E, Occupancy<E>::CTA_N>::BYTES + 1024;
 }
-static_assert(2 * (Occupancy<float>::STAGES * StageShape<float>::BYTES + 1024 + 1024) <= 228 * 1024, "2 CTAs / SM");
-static_assert(2 * (Occupancy<__half>::STAGES * StageShape<__half>::BYTES + 1024 + 1024) <= 228 * 1024, "2 CTAs / SM");
+static_assert(2 * (tma_smem<float>() + 1024) <= 228 * 1024, "2 CTAs / SM");
+static_assert(2 * (tma_smem<__half>() + 1024) <= 228 * 1024, "2 CTAs / SM");
+static_assert(2 * (tma_smem<HalfSplit>() + 1024) <= 228 * 1024, "2 CTAs / SM");
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -439,11 +446,13 @@ void launch_tma(const GemmTask *tasks, int ntasks, int ntiles, const void *maps,
     if (ntiles <= 0) return;
     static PerDeviceOnce once;
     once([] {
-        cudaFuncSetAttribute(gemm_tma_kernel<E, Occupancy<E>::STAGES, Occupancy<E>::MINB>,
+        cudaFuncSetAttribute(gemm_tma_kernel<E, Occupancy<E>::STAGES, Occupancy<E>::MINB, Occupancy<E>::CTA_N>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem<E>());
     });
     ++g_kernel_launches;
-    gemm_tma_kernel<E, Occupancy<E>::STAGES, Occupancy<E>::MINB><<<ntiles, kThreads, tma_smem<E>(), st>>>(
+    constexpr int halves = TBN / Occupancy<E>::CTA_N;
+    gemm_tma_kernel<E, Occupancy<E>::STAGES, Occupancy<E>::MINB, Occupancy<E>::CTA_N>
+        <<<ntiles * halves, kThreads, tma_smem<E>(), st>>>(
         tasks, ntasks, static_cast<const CUtensorMap *>(maps), C, sexp, err, lo_maps);
 }
 
@@ -460,7 +469,7 @@ bool encode_operand_map(void *out, const void *base, int operands, uint64_t rows
     const uint32_t box_k = operands == 2 ? uint32_t(OpTraits<HalfSplit>::TBK)
                            : half        ? uint32_t(OpTraits<__half>::TBK)
                                          : uint32_t(OpTraits<float>::TBK);
-    static_assert(StageShape<HalfSplit>::BOX == 128 * OpTraits<HalfSplit>::TBK, "split box");
+    static_assert(StageShape<HalfSplit, 128>::BOX == 128 * OpTraits<HalfSplit>::TBK, "split box");
     cuuint64_t dims[2] = {rows, cols};
     cuuint64_t strides[1] = {ld * es};
     cuuint32_t box[2] = {128u / es, box_k};
