@@ -36,7 +36,9 @@ METRIC = "Newton solves/s at 1e-10 residual: FP32+refine & learned PCG vs FP64 p
 UNIT = "solves/s"
 # DRAM bytes (read + write) of the split-FP16 GEMM launches over one config-2
 # factorization: ncu capture of `bench.py --profile`, gemm_tma 72.73 + 29.0 GB,
-# gemm_tc 6.78 + 3.5 GB
+# gemm_tc 6.78 + 3.5 GB (captured with one 256-column CTA per split tile; the two
+# 128-column CTAs that now share a tile read its A operand twice, the second time
+# mostly from L2)
 GEMM_TRAFFIC_SPLIT16_CONFIG2 = 112.0e9
 
 
