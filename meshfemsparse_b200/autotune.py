@@ -3,9 +3,10 @@
 Two choices have no single best value: the small/large front cutoff (fronts up
 to it are factored whole in one CTA's shared memory, larger ones by 128-column
 panels and tensor-core tiles) and, for an FP32 factor under FP64 refinement,
-the tensor-core mode (single-pass TF32 on tcgen05: a faster factor, more
-refinement iterations; split 3xTF32: a slower, FP32-accurate factor, fewer
-iterations). `tune` times every candidate on the caller's own matrix and
+the tensor-core mode (5, single FP16 operands: a faster factor, more refinement
+iterations; 6, split hi/lo FP16 operands: a slower, FP32-accurate factor, fewer
+iterations, which wins as the right-hand sides per solve grow). `tune` times every
+candidate on the caller's own matrix and
 right-hand sides (device times of the library's CUDA events: factorization plus
 refined solve), keeps the fastest, and caches the choice on disk keyed by the
 pattern, the pins, the precision and the GPU name, so a pattern that is
