@@ -51,6 +51,18 @@ mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t kernel, int
  * *count receives the number of launches; at most max_launches are written. */
 mfs_status mfs_debug_gemm_launches(const mfs_handle *h, int64_t max_launches, double *out, int64_t *count);
 
+/* The temporal nested-dissection reuse rule on its own (host only, no device): for a
+ * previous separator forest (ncomp components, cparent postordered with -1 for roots,
+ * cmember[v] the component of vertex v) and a new symmetric graph on the same n
+ * vertices (CSR xadj / adj, self loops allowed), *full_rebuild = 1 when a full
+ * dissection is needed, else the violated subtree roots go to roots[0 .. *nroots)
+ * (ascending; roots holds ncomp entries). Replaces no reference entry point: it
+ * exposes PersistentSeparatorTree::dirty_subtrees
+ * (ParallelNestedDissection/persistent_separator_tree.hh:81-118) for its tests. */
+mfs_status mfs_debug_dirty_subtrees(int64_t n, const int64_t *xadj, const int64_t *adj, int64_t ncomp,
+                                    const int64_t *cparent, const int64_t *cmember, int32_t *full_rebuild,
+                                    int64_t *roots, int64_t *nroots);
+
 #ifdef __cplusplus
 }
 #endif

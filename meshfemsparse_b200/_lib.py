@@ -28,6 +28,7 @@ EXPORTED = [
     "mfs_set_options", "mfs_apply_noalloc", "mfs_lpc_param_count", "mfs_lpc_create", "mfs_lpc_destroy",
     "mfs_lpc_get_weights", "mfs_lpc_set_weights", "mfs_lpc_loss_grad", "mfs_lpc_train_step", "mfs_pcg_solve",
     "mfs_debug_gemm", "mfs_build_pattern_device", "mfs_conversion_plan_device", "mfs_debug_gemm_launches",
+    "mfs_debug_dirty_subtrees",
 ]
 GEMM_TASK_FIELDS = 12
 
@@ -108,6 +109,8 @@ def load() -> C.CDLL:
     lib.mfs_debug_gemm.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, i64p, P, C.c_int64, P, C.c_int64,
                                    P, C.c_int64, C.c_char_p, C.c_size_t]
     lib.mfs_debug_gemm_launches.argtypes = [P, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    lib.mfs_debug_dirty_subtrees.argtypes = [C.c_int64, i64p, i64p, C.c_int64, i64p, i64p, C.POINTER(C.c_int32),
+                                             i64p, C.POINTER(C.c_int64)]
     for name in EXPORTED:
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -213,3 +216,18 @@ def debug_gemm_launches(handle) -> np.ndarray:
     check(lib.mfs_debug_gemm_launches(handle, cnt.value, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(cnt)),
           None, "mfs_debug_gemm_launches")
     return out[:cnt.value]
+
+
+def debug_dirty_subtrees(xadj: np.ndarray, adj: np.ndarray, cparent: np.ndarray, cmember: np.ndarray):
+    """(full_rebuild, roots) of the temporal nested-dissection reuse rule for a previous
+    separator forest and a new graph in CSR form (host only)."""
+    xadj = np.ascontiguousarray(xadj, dtype=np.int64)
+    adj = np.ascontiguousarray(adj, dtype=np.int64)
+    cparent = np.ascontiguousarray(cparent, dtype=np.int64)
+    cmember = np.ascontiguousarray(cmember, dtype=np.int64)
+    roots = np.zeros(max(cparent.size, 1), dtype=np.int64)
+    full, nroots = C.c_int32(0), C.c_int64(0)
+    check(load().mfs_debug_dirty_subtrees(xadj.size - 1, i64ptr(xadj), i64ptr(adj if adj.size else np.zeros(1, np.int64)),
+                                          cparent.size, i64ptr(cparent), i64ptr(cmember), C.byref(full),
+                                          i64ptr(roots), C.byref(nroots)), None, "mfs_debug_dirty_subtrees")
+    return bool(full.value), roots[:nroots.value].tolist()

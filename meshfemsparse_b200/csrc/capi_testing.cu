@@ -3,6 +3,7 @@
 // host before the launch.
 #include "../../include/mfs_b200_testing.h"
 #include "device.h"
+#include "host_symbolic.h"
 
 #include <cuda_runtime.h>
 
@@ -220,4 +221,31 @@ extern "C" mfs_status mfs_debug_gemm(int32_t device, int32_t precision, int32_t 
         return MFS_TIMEOUT;
     }
     return MFS_OK;
+}
+
+extern "C" mfs_status mfs_debug_dirty_subtrees(int64_t n, const int64_t *xadj, const int64_t *adj, int64_t ncomp,
+                                               const int64_t *cparent, const int64_t *cmember,
+                                               int32_t *full_rebuild, int64_t *roots, int64_t *nroots) {
+    if (n < 0 || ncomp < 0 || !xadj || !full_rebuild || !nroots || (ncomp > 0 && (!cparent || !roots)) ||
+        (n > 0 && !cmember))
+        return MFS_INVALID_ARG;
+    const int64_t ne = xadj[n];
+    if (ne < 0 || (ne > 0 && !adj)) return MFS_INVALID_ARG;
+    for (int64_t v = 0; v < n; ++v)
+        if (xadj[v] > xadj[v + 1] || cmember[v] < 0 || cmember[v] >= ncomp) return MFS_INVALID_ARG;
+    for (int64_t k = 0; k < ne; ++k)
+        if (adj[k] < 0 || adj[k] >= n) return MFS_INVALID_ARG;
+    for (int64_t c = 0; c < ncomp; ++c)
+        if (cparent[c] != -1 && (cparent[c] <= c || cparent[c] >= ncomp)) return MFS_INVALID_ARG;
+    try {
+        const std::vector<idx> x(xadj, xadj + n + 1), a(adj, adj + ne), p(cparent, cparent + ncomp),
+            m(cmember, cmember + n);
+        const DirtySubtrees d = dirty_subtrees(n, x, a, p, m);
+        *full_rebuild = d.full ? 1 : 0;
+        *nroots = int64_t(d.roots.size());
+        for (size_t r = 0; r < d.roots.size(); ++r) roots[r] = d.roots[r];
+        return MFS_OK;
+    } catch (const std::bad_alloc &) {
+        return MFS_OOM;
+    }
 }

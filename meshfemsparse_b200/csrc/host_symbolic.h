@@ -56,6 +56,19 @@ NDResult nested_dissection(idx n, const std::vector<idx> &xadj, const std::vecto
 NDResult nested_dissection_reuse(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
                                  const NDResult &prev, const OrderingOptions &opt, idx *rebuilt_vertices);
 
+// The subtrees of a previous separator forest (cparent postordered, cmember per
+// vertex) that a graph on the same vertices violates (persistent_separator_tree.hh:
+// 81-118): an edge whose two components are not ancestor and descendant marks their
+// lowest common ancestor; `roots` are the marked components without a marked
+// ancestor, ascending. An edge between two trees, or one whose ancestor is the root
+// of a single-tree forest, asks for a full dissection (`full`, roots empty).
+struct DirtySubtrees {
+    bool full = false;
+    std::vector<idx> roots;
+};
+DirtySubtrees dirty_subtrees(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
+                             const std::vector<idx> &cparent, const std::vector<idx> &cmember);
+
 // Final order of a dissection (hierarchical_camd.cc:165-333): constrained minimum
 // degree with the separator forest's components as constraint sets (descendants
 // first, each component contiguous), one independent problem per subtree rooted at

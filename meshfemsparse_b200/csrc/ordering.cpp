@@ -545,9 +545,56 @@ NDResult finish_result(NDState &st, idx n) {
 
 }  // namespace
 
+DirtySubtrees dirty_subtrees(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
+                             const std::vector<idx> &cparent, const std::vector<idx> &cmember) {
+    const idx nc = idx(cparent.size());
+    DirtySubtrees out;
+    std::vector<idx> depth(nc, 0);
+    idx nroots = 0;
+    for (idx c = nc - 1; c >= 0; --c) {              // parents follow children
+        if (cparent[c] >= 0) depth[c] = depth[cparent[c]] + 1;
+        else ++nroots;
+    }
+    auto lca = [&](idx a, idx b) {
+        while (depth[a] > depth[b]) a = cparent[a];
+        while (depth[b] > depth[a]) b = cparent[b];
+        while (a != b && a >= 0 && b >= 0) { a = cparent[a]; b = cparent[b]; }
+        return a == b ? a : idx(-1);
+    };
+    std::vector<char> dirty(nc, 0);
+    for (idx v = 0; v < n; ++v)
+        for (idx k = xadj[v]; k < xadj[v + 1]; ++k) {
+            const idx u = adj[k];
+            if (u >= v) continue;                        // each undirected edge once
+            const idx a = cmember[v], b = cmember[u];
+            const idx r = lca(a, b);
+            if (r == a || r == b) continue;              // one component below the other
+            if (r < 0 || (cparent[r] < 0 && nroots == 1)) {
+                out.full = true;
+                out.roots.clear();
+                return out;
+            }
+            dirty[r] = 1;
+        }
+    for (idx c = 0; c < nc; ++c) {
+        if (!dirty[c]) continue;
+        idx p = cparent[c];
+        while (p >= 0 && !dirty[p]) p = cparent[p];
+        if (p < 0) out.roots.push_back(c);
+    }
+    return out;
+}
+
 NDResult nested_dissection_reuse(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
                                  const NDResult &prev, const OrderingOptions &opt, idx *rebuilt_vertices) {
     if (idx(prev.cmember.size()) != n || prev.ncomp <= 0) return nested_dissection(n, xadj, adj, opt);
+    const DirtySubtrees dirty = dirty_subtrees(n, xadj, adj, prev.cparent, prev.cmember);
+    if (dirty.full) {
+        // no separator of the old forest is left to keep (an edge joins two trees, e.g.
+        // new contact between bodies, or crosses the only root): dissect afresh
+        if (rebuilt_vertices) *rebuilt_vertices = n;
+        return nested_dissection(n, xadj, adj, opt);
+    }
     const idx nc = prev.ncomp;
     std::vector<std::vector<idx>> children(nc), members(nc);
     std::vector<idx> first(nc);
@@ -558,23 +605,8 @@ NDResult nested_dissection_reuse(idx n, const std::vector<idx> &xadj, const std:
             first[prev.cparent[c]] = std::min(first[prev.cparent[c]], first[c]);
         }
     for (idx v = 0; v < n; ++v) members[prev.cmember[v]].push_back(v);
-    auto is_anc = [&](idx a, idx d) { return first[a] <= d && d <= a; };
     std::vector<char> rebuild(nc, 0);
-    for (idx u = 0; u < n; ++u)
-        for (idx e = xadj[u]; e < xadj[u + 1]; ++e) {
-            idx a = prev.cmember[u], b = prev.cmember[adj[e]];
-            if (a == b || is_anc(a, b) || is_anc(b, a)) continue;
-            idx c = a;                            // lowest common ancestor: climb until it covers b
-            while (c >= 0 && !is_anc(c, b)) c = prev.cparent[c];
-            if (c < 0) {
-                // the edge joins two trees of the previous forest (e.g. new contact between
-                // bodies): no separator of the old tree is left to keep, dissect afresh
-                // (persistent_separator_tree.hh:97-99 rebuilds fully in this case)
-                if (rebuilt_vertices) *rebuilt_vertices = n;
-                return nested_dissection(n, xadj, adj, opt);
-            }
-            rebuild[c] = 1;
-        }
+    for (idx c : dirty.roots) rebuild[c] = 1;
     NDState st(xadj, adj, opt, n);
     st.iperm.reserve(n);
     idx rebuilt = 0;
