@@ -63,6 +63,19 @@ mfs_status mfs_debug_dirty_subtrees(int64_t n, const int64_t *xadj, const int64_
                                     const int64_t *cparent, const int64_t *cmember, int32_t *full_rebuild,
                                     int64_t *roots, int64_t *nroots);
 
+/* The hierarchical constrained-minimum-degree final order on its own (host only): for a
+ * symmetric graph (CSR, n vertices) and a separator forest (ncomp components, cparent
+ * postordered, cmember per vertex), the order at cut_depth (clamped to the forest's
+ * depth) into perm[0 .. n) (new -> old) and stats[4] = {effective cut depth, subtree
+ * problems, vertices above the cut, boundary cliques passed to the upper problem}.
+ * MFS_INVALID_ARG when the forest does not fit the graph (an edge between two subtrees
+ * of the cut, or between components that are not ancestor and descendant). Replaces no
+ * reference entry point: it exposes the stage hierarchical_camd
+ * (ParallelNestedDissection/hierarchical_camd.cc:165-333) stands for, for its tests. */
+mfs_status mfs_debug_hierarchical_order(int64_t n, const int64_t *xadj, const int64_t *adj, int64_t ncomp,
+                                        const int64_t *cparent, const int64_t *cmember, int32_t cut_depth,
+                                        int64_t *perm, int64_t *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,7 +28,7 @@ EXPORTED = [
     "mfs_set_options", "mfs_apply_noalloc", "mfs_lpc_param_count", "mfs_lpc_create", "mfs_lpc_destroy",
     "mfs_lpc_get_weights", "mfs_lpc_set_weights", "mfs_lpc_loss_grad", "mfs_lpc_train_step", "mfs_pcg_solve",
     "mfs_debug_gemm", "mfs_build_pattern_device", "mfs_conversion_plan_device", "mfs_debug_gemm_launches",
-    "mfs_debug_dirty_subtrees",
+    "mfs_debug_dirty_subtrees", "mfs_debug_hierarchical_order",
 ]
 GEMM_TASK_FIELDS = 12
 
@@ -109,6 +109,8 @@ def load() -> C.CDLL:
     lib.mfs_debug_gemm.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, i64p, P, C.c_int64, P, C.c_int64,
                                    P, C.c_int64, C.c_char_p, C.c_size_t]
     lib.mfs_debug_gemm_launches.argtypes = [P, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    lib.mfs_debug_hierarchical_order.argtypes = [C.c_int64, i64p, i64p, C.c_int64, i64p, i64p, C.c_int32, i64p,
+                                                 i64p]
     lib.mfs_debug_dirty_subtrees.argtypes = [C.c_int64, i64p, i64p, C.c_int64, i64p, i64p, C.POINTER(C.c_int32),
                                              i64p, C.POINTER(C.c_int64)]
     for name in EXPORTED:
@@ -231,3 +233,23 @@ def debug_dirty_subtrees(xadj: np.ndarray, adj: np.ndarray, cparent: np.ndarray,
                                           cparent.size, i64ptr(cparent), i64ptr(cmember), C.byref(full),
                                           i64ptr(roots), C.byref(nroots)), None, "mfs_debug_dirty_subtrees")
     return bool(full.value), roots[:nroots.value].tolist()
+
+
+def debug_hierarchical_order(xadj: np.ndarray, adj: np.ndarray, cparent: np.ndarray, cmember: np.ndarray,
+                             cut_depth: int):
+    """(perm new -> old, stats {cut, tasks, upper vertices, upper elements}) of the
+    hierarchical constrained-minimum-degree final order (host only)."""
+    xadj = np.ascontiguousarray(xadj, dtype=np.int64)
+    adj = np.ascontiguousarray(adj, dtype=np.int64)
+    cparent = np.ascontiguousarray(cparent, dtype=np.int64)
+    cmember = np.ascontiguousarray(cmember, dtype=np.int64)
+    n = xadj.size - 1
+    perm = np.zeros(max(n, 1), dtype=np.int64)
+    stats = np.zeros(4, dtype=np.int64)
+    one = np.zeros(1, dtype=np.int64)
+    check(load().mfs_debug_hierarchical_order(n, i64ptr(xadj), i64ptr(adj if adj.size else one), cparent.size,
+                                              i64ptr(cparent if cparent.size else one),
+                                              i64ptr(cmember if cmember.size else one), int(cut_depth),
+                                              i64ptr(perm), i64ptr(stats)), None, "mfs_debug_hierarchical_order")
+    return perm[:n], dict(cut=int(stats[0]), tasks=int(stats[1]), upper_vertices=int(stats[2]),
+                          upper_elements=int(stats[3]))

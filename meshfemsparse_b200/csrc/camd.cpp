@@ -353,6 +353,7 @@ std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj
     for (idx a : uord) iperm.push_back(upper[a]);
     if (idx(iperm.size()) != n) return nd.iperm;
     if (stats) {
+        stats->applied = true;
         stats->cut_depth = cut;
         stats->tasks = nt;
         stats->upper_vertices = nu;

@@ -249,3 +249,50 @@ extern "C" mfs_status mfs_debug_dirty_subtrees(int64_t n, const int64_t *xadj, c
         return MFS_OOM;
     }
 }
+
+extern "C" mfs_status mfs_debug_hierarchical_order(int64_t n, const int64_t *xadj, const int64_t *adj,
+                                                   int64_t ncomp, const int64_t *cparent, const int64_t *cmember,
+                                                   int32_t cut_depth, int64_t *perm, int64_t *stats) {
+    if (n < 0 || ncomp < 0 || !xadj || !stats || cut_depth < 0 || (n > 0 && (!cmember || !perm)) ||
+        (ncomp > 0 && !cparent))
+        return MFS_INVALID_ARG;
+    const int64_t ne = xadj[n];
+    if (ne < 0 || (ne > 0 && !adj)) return MFS_INVALID_ARG;
+    for (int64_t v = 0; v < n; ++v)
+        if (xadj[v] > xadj[v + 1] || cmember[v] < 0 || cmember[v] >= ncomp) return MFS_INVALID_ARG;
+    for (int64_t k = 0; k < ne; ++k)
+        if (adj[k] < 0 || adj[k] >= n) return MFS_INVALID_ARG;
+    for (int64_t c = 0; c < ncomp; ++c)
+        if (cparent[c] != -1 && (cparent[c] <= c || cparent[c] >= ncomp)) return MFS_INVALID_ARG;
+    try {
+        NDResult nd;
+        nd.ncomp = ncomp;
+        nd.cparent.assign(cparent, cparent + ncomp);
+        nd.cmember.assign(cmember, cmember + n);
+        nd.iperm.resize(size_t(n));
+        for (int64_t v = 0; v < n; ++v) nd.iperm[size_t(v)] = v;
+        // every edge joins a component to itself or to an ancestor or descendant
+        std::vector<int64_t> depth(size_t(ncomp), 0);
+        for (int64_t c = ncomp - 1; c >= 0; --c)
+            if (cparent[c] >= 0) depth[size_t(c)] = depth[size_t(cparent[c])] + 1;
+        for (int64_t v = 0; v < n; ++v)
+            for (int64_t k = xadj[v]; k < xadj[v + 1]; ++k) {
+                int64_t a = cmember[v], b = cmember[adj[k]];
+                if (depth[size_t(a)] < depth[size_t(b)]) std::swap(a, b);
+                while (depth[size_t(a)] > depth[size_t(b)]) a = cparent[a];
+                if (a != b) return MFS_INVALID_ARG;
+            }
+        const std::vector<idx> x(xadj, xadj + n + 1), a(adj, adj + ne);
+        HierarchicalMDStats st;
+        const std::vector<idx> p = hierarchical_constrained_md(n, x, a, nd, cut_depth, &st);
+        if (!st.applied && n > 0) return MFS_INVALID_ARG;
+        for (int64_t k = 0; k < n; ++k) perm[k] = p[size_t(k)];
+        stats[0] = st.cut_depth;
+        stats[1] = st.tasks;
+        stats[2] = st.upper_vertices;
+        stats[3] = st.upper_elements;
+        return MFS_OK;
+    } catch (const std::bad_alloc &) {
+        return MFS_OOM;
+    }
+}

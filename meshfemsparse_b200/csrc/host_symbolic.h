@@ -76,6 +76,7 @@ DirtySubtrees dirty_subtrees(idx n, const std::vector<idx> &xadj, const std::vec
 // which receive every subtree's boundary clique as an initial element. Returns the
 // new iperm (nd.iperm unchanged when cut_depth < 0 or the forest does not fit).
 struct HierarchicalMDStats {
+    bool applied = false;           // false: nd.iperm returned (cut < 0, or the forest does not fit the graph)
     int cut_depth = -1;
     idx tasks = 0, upper_vertices = 0, upper_elements = 0;
 };
