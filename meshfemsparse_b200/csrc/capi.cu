@@ -1174,7 +1174,18 @@ mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, cons
         so.nd.leaf_size = h->opt.nd_leaf_size > 0 ? h->opt.nd_leaf_size : 120;
         so.nd.seed = h->opt.seed;
         so.solve_subtrees = h->opt.solve_subtrees;
-        const bool reuse = h->opt.nd_reuse_period > 0 && h->nd_prev && h->nd_reuse_count < h->opt.nd_reuse_period;
+        // the history belongs to one variable set: the same block size, block count and
+        // pins (a pin change or the scalar fallback starts afresh, as the reference's
+        // temporal reuse state does)
+        std::vector<int64_t> key{int64_t(block_size), n_blocks};
+        {
+            std::vector<int64_t> pins(pinned, pinned + std::max<int64_t>(n_pinned, 0));
+            std::sort(pins.begin(), pins.end());
+            pins.erase(std::unique(pins.begin(), pins.end()), pins.end());
+            key.insert(key.end(), pins.begin(), pins.end());
+        }
+        const bool reuse = h->opt.nd_reuse_period > 0 && h->nd_prev && h->nd_prev_key == key &&
+                           h->nd_reuse_count < h->opt.nd_reuse_period;
         if (reuse) so.nd_prev = h->nd_prev.get();
         std::string e = analyze(n_blocks, Ap, Ai, block_size, pinned, n_pinned, so, user_perm, *Sp, supernode_sizes,
                                 supernode_sizes ? num_supernodes : 0);
@@ -1190,6 +1201,7 @@ mfs_status mfs_symbolic(mfs_handle *h, int64_t n_blocks, const int64_t *Ap, cons
             nd->cmember = Sp->nd_cmember;
             nd->ncomp = Sp->nd_ncomp;
             h->nd_prev = nd;
+            h->nd_prev_key = key;
             h->nd_reuse_count = Sp->nd_rebuilt >= 0 ? h->nd_reuse_count + 1 : 0;
         }
         if (host_only) {

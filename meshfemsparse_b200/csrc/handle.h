@@ -220,6 +220,7 @@ struct mfs_handle {
     };
     std::vector<FactorGraph> factor_graphs;
     std::shared_ptr<NDResult> nd_prev;       // last nested dissection (temporal reuse)
+    std::vector<int64_t> nd_prev_key;        // its block size, block count and sorted pins: reuse needs the same
     int nd_reuse_count = 0;                  // analyses since the last full dissection
     // TMA-fed GEMM: one tensor map per large front's panel (indexed by supernode),
     // built for the array `tmaps_base` (the FP32 factor or its FP16 copy) of the

@@ -51,8 +51,8 @@ NDResult nested_dissection(idx n, const std::vector<idx> &xadj, const std::vecto
 // PARTH idea): the previous separator tree is kept, and only the subtrees whose
 // components an edge of the new graph joins (their lowest common ancestor) are
 // dissected afresh; leaves are reordered by minimum degree as usual. Falls back to
-// a full dissection when `prev` does not match. *rebuilt_vertices = vertices
-// re-dissected.
+// a full dissection when `prev` does not match or the new edges leave no subtree to
+// keep (*rebuilt_vertices = -1 then), else *rebuilt_vertices = vertices re-dissected.
 NDResult nested_dissection_reuse(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj,
                                  const NDResult &prev, const OrderingOptions &opt, idx *rebuilt_vertices);
 

@@ -591,8 +591,9 @@ NDResult nested_dissection_reuse(idx n, const std::vector<idx> &xadj, const std:
     const DirtySubtrees dirty = dirty_subtrees(n, xadj, adj, prev.cparent, prev.cmember);
     if (dirty.full) {
         // no separator of the old forest is left to keep (an edge joins two trees, e.g.
-        // new contact between bodies, or crosses the only root): dissect afresh
-        if (rebuilt_vertices) *rebuilt_vertices = n;
+        // new contact between bodies, or crosses the only root): dissect afresh, which
+        // counts as a full dissection (-1)
+        if (rebuilt_vertices) *rebuilt_vertices = -1;
         return nested_dissection(n, xadj, adj, opt);
     }
     const idx nc = prev.ncomp;

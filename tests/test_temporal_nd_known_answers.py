@@ -1,4 +1,4 @@
-"""The temporal nested-dissection reuse rule against the reference's known answers
+"""The temporal nested-dissection reuse rule and its history against the reference's known answers
 (tests/test_hierarchical_camd.cc:670-725, "temporal ND detects minimal disjoint invalid
 subtrees", and :1178-1230, "temporal ND repairs forest roots independently"): the same
 15-component tree (two vertices per component), the same base graph, the same added
@@ -6,7 +6,8 @@ edges, the same expected dirty roots and full-rebuild decisions. Host only."""
 import numpy as np
 import pytest
 
-from meshfemsparse_b200 import _lib
+from meshfemsparse_b200 import B200Factorizer, ScalarCSC, SystemAssembler, _lib
+from meshfemsparse_b200.hessian import BlockCSCHessian
 
 # the reference's test tree: parent of each of the 15 components, member[v] = v / 2
 TREE_PARENT = [2, 2, 6, 5, 5, 6, 14, 9, 9, 13, 12, 12, 13, 14, -1]
@@ -105,3 +106,71 @@ def test_invalid_forest_is_rejected():
     bad[3] = 1                      # a parent numbered before its child
     with pytest.raises(ValueError):
         _lib.debug_dirty_subtrees(xadj, adj, bad, member)
+
+
+# ----------------------------------------------------------------- reuse history
+
+
+def scalar_matrix(n, edges, diag):
+    cols = [[] for _ in range(n)]
+    for a, b in edges:
+        a, b = min(a, b), max(a, b)
+        cols[b].append(a)
+    Ap, Ai = [0], []
+    for j in range(n):
+        Ai += sorted(set(cols[j])) + [j]
+        Ap.append(len(Ai))
+    Ax = np.where(np.array(Ai) == np.repeat(np.arange(n), np.diff(Ap)), diag, -1.0)
+    S = ScalarCSC(n, np.array(Ap), np.array(Ai), Ax)
+    return BlockCSCHessian(n, S.Ap, S.Ai, 1, S.Ax)
+
+
+def analyse(f, A, pins):
+    f.factorizeSymbolic(A, pins)
+    st = f.stats()
+    return st["nd_reused"] == 0, st["nd_rebuilt_vertices"]
+
+
+def test_reuse_period_counts_incremental_analyses():
+    """tests/test_catamari_factorizer.cc:232-258: period 32 on an unchanged 16-vertex path:
+    analyses 0 and 33 are full, 1-32 incremental with nothing re-dissected."""
+    A = scalar_matrix(16, [(v, v + 1) for v in range(15)], 4.0)
+    f = B200Factorizer(device=-1, nd_reuse_period=32)
+    for call in range(34):
+        full, rebuilt = analyse(f, A, [])
+        assert full == (call in (0, 33))
+        assert rebuilt == (16 if full else 0)
+
+
+def test_reuse_history_resets_for_pin_changes():
+    """tests/test_hierarchical_camd.cc:1024-1061: period 2 on a 16 x 16 grid; a new edge at
+    step 4; pins {0} from step 5 and {1} from step 7. Full at steps 0, 3, 5 and 7 (the
+    first, the period, and each pin change); incremental with nothing re-dissected at 1, 2,
+    6 and 8."""
+    n, side = 256, 16
+    edges = [(v, v + 1) for v in range(n) if v % side + 1 < side] + [(v, v + side) for v in range(n - side)]
+    f = B200Factorizer(device=-1, nd_reuse_period=2)
+    for step in range(9):
+        if step == 4:
+            edges.append((0, n - 1))
+        pins = [] if step < 5 else [0 if step <= 6 else 1]
+        full, rebuilt = analyse(f, scalar_matrix(n, edges, 10.0), pins)
+        if step in (0, 3, 5, 7):
+            assert full
+        if step in (1, 2, 6, 8):
+            assert not full and rebuilt == 0
+
+
+def test_reuse_history_follows_the_scalar_fallback():
+    """tests/test_catamari_factorizer.cc:270-297: a 32-node chain of 3 x 3 blocks; a
+    partial-block pin analyses 95 scalar variables, whole-block pins 31 blocks, and each
+    switch starts a new history (full first, then incremental)."""
+    H = SystemAssembler(32).blockSparsityPattern(np.array([[i, i + 1] for i in range(31)]))
+    f = B200Factorizer(device=-1, nd_reuse_period=2)
+    for pins, nv in (([1], 95), ([0, 1, 2], 31)):
+        for repeat in range(2):
+            full, rebuilt = analyse(f, H, pins)
+            assert full == (repeat == 0)
+            assert f.ndOrdering().CMember.size == nv
+            if repeat:
+                assert rebuilt == 0
