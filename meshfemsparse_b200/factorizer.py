@@ -20,11 +20,13 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import time
 from dataclasses import dataclass
 
 import numpy as np
 
 from . import _lib
+from .adaptive_ordering import AdaptiveOrderingSelection
 from .hessian import BlockCSCHessian, ScalarCSC
 
 
@@ -60,6 +62,9 @@ class OrderingMethod(enum.IntEnum):
     Native = _lib.MFS_ORDER_NATIVE
     AMD = _lib.MFS_ORDER_MD
     User = _lib.MFS_ORDER_USER
+    # nested dissection or minimum degree, chosen per analysis from the timing history
+    # (CatamariFactorizer::OrderingMethod::Adaptive); host-side only
+    Adaptive = 100
 
 
 class FactorizationType(enum.IntEnum):
@@ -103,7 +108,10 @@ class B200Factorizer:
             nd_leaf_size=nd_leaf_size, seed=seed, solve_chain=solve_chain, factor_group=factor_group,
             solve_subtrees=solve_subtrees)
         opts = _lib.default_options(**self._base_opts)
-        opts.ordering = int(self.orderingMethod)
+        # nested dissection, or minimum degree when the adaptive choice switches to it
+        self.adaptiveOrdering = AdaptiveOrderingSelection(OrderingMethod.CholmodNesdisParallel, OrderingMethod.AMD)
+        opts.ordering = int(OrderingMethod.CholmodNesdisParallel if self.orderingMethod == OrderingMethod.Adaptive
+                            else self.orderingMethod)
         if stream is not None:
             opts.stream = C.c_void_p(stream)
         self._h = C.c_void_p()
@@ -168,7 +176,23 @@ class B200Factorizer:
         return [int(v) for v in self._fixed]
 
     def provider(self) -> CholeskyProvider:
+        if self.orderingMethod == OrderingMethod.Adaptive:
+            return CholeskyProvider.CatamariAdaptive
         return CholeskyProvider.B200Native if self.orderingMethod == OrderingMethod.Native else CholeskyProvider.B200
+
+    def wantsSymbolicFactorizationRecompute(self) -> bool:
+        """Adaptive ordering: whether to redo the analysis now with the other method
+        (CatamariFactorizer.hh:114-117)."""
+        return self.orderingMethod == OrderingMethod.Adaptive and self.adaptiveOrdering.should_trigger_recompute()
+
+    def _adaptive_record(self, what: str) -> None:
+        if self.orderingMethod != OrderingMethod.Adaptive:
+            return
+        st = self.stats()
+        if what == "numeric":
+            self.adaptiveOrdering.record_numeric(st["factor_ms"] * 1e-3)
+        else:
+            self.adaptiveOrdering.record_solve(st["solve_ms"] * 1e-3)
 
     def preferInPlaceSolve(self) -> bool:
         return True
@@ -189,11 +213,16 @@ class B200Factorizer:
             up = np.ascontiguousarray(np.asarray(user_perm, dtype=np.int64))
         sns = None if supernode_sizes is None else np.ascontiguousarray(np.asarray(supernode_sizes, dtype=np.int64))
         # the ordering choice takes effect here, at symbolic analysis
-        self._opts.ordering = int(self.orderingMethod)
+        adaptive = self.orderingMethod == OrderingMethod.Adaptive
+        method = self.adaptiveOrdering.update_selection() if adaptive else self.orderingMethod
+        self._opts.ordering = int(method)
         _lib.check(self._lib.mfs_set_options(self._h, C.byref(self._opts)), self._h, "set options")
+        t0 = time.perf_counter()
         st = self._lib.mfs_symbolic(self._h, H.numBlocks, _lib.i64ptr(H.Ap), _lib.i64ptr(H.Ai), H.bs,
                                     _lib.i64ptr(pins) if pins.size else None, int(pins.size), _lib.i64ptr(up),
                                     _lib.i64ptr(sns), 0 if sns is None else int(sns.size))
+        if adaptive and st == _lib.MFS_OK:
+            self.adaptiveOrdering.record_symbolic(time.perf_counter() - t0, self.getFactorNNZ())
         if st != _lib.MFS_OK:
             self._fixed = np.zeros(0, dtype=np.int64)
             _lib.check(st, self._h, "symbolic factorization failed")
@@ -216,6 +245,7 @@ class B200Factorizer:
         self._assert(FactorizationType.Symbolic)
         Ax = self._values(mat)
         _lib.check(self._lib.mfs_numeric(self._h, _lib.dptr(Ax), None, 0.0, 0), self._h, "numeric failed")
+        self._adaptive_record("numeric")
 
     def factorizeNumericWithShift(self, A, sigma: float, B=None, isInTryCatch: bool = False):
         self._assert(FactorizationType.Symbolic)
@@ -229,6 +259,7 @@ class B200Factorizer:
             Bx = self._values(B)
         _lib.check(self._lib.mfs_numeric(self._h, _lib.dptr(Ax), _lib.dptr(Bx), float(sigma), 0), self._h,
                    "numeric failed")
+        self._adaptive_record("numeric")
 
     def factorize(self, mat, fixedVars=(), isInTryCatch: bool = False):
         self.factorizeSymbolic(mat, fixedVars)
@@ -251,6 +282,7 @@ class B200Factorizer:
 
     def factorizeAssembled(self, sigma: float = 0.0):
         _lib.check(self._lib.mfs_numeric(self._h, None, None, float(sigma), 0), self._h, "numeric failed")
+        self._adaptive_record("numeric")
 
     def _ax_len(self) -> int:
         return self._axlen
@@ -302,6 +334,7 @@ class B200Factorizer:
         nrhs = X.shape[1]
         _lib.check(self._lib.mfs_solve(self._h, _lib.dptr(X), _lib.dptr(X), nrhs, X.shape[0], mode), self._h,
                    "solve failed")
+        self._adaptive_record("solve")
         return X[:, 0].copy() if vec else np.ascontiguousarray(X)
 
     def solve(self, b: np.ndarray, sys: CholeskySys = CholeskySys.A) -> np.ndarray:
@@ -448,6 +481,8 @@ def make_cholesky_factorizer(provider: CholeskyProvider = CholeskyProvider.B200,
         kw.setdefault("orderingMethod", OrderingMethod.Native)
     elif provider in (CholeskyProvider.CatamariAMD,):
         kw.setdefault("orderingMethod", OrderingMethod.AMD)
+    elif provider in (CholeskyProvider.CatamariAdaptive,):
+        kw.setdefault("orderingMethod", OrderingMethod.Adaptive)
     elif provider in (CholeskyProvider.B200, CholeskyProvider.CatamariNesdisParallel, CholeskyProvider.Catamari,
                       CholeskyProvider.CatamariNesdis):
         kw.setdefault("orderingMethod", OrderingMethod.CholmodNesdisParallel)
