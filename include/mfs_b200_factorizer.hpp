@@ -15,8 +15,10 @@
 
 #include "mfs_b200.h"
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
+#include <optional>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -26,6 +28,14 @@ namespace mfs {
 
 enum class CholeskySys { A, L, Lt, P, Pt };
 enum class FactorizationType { None = 0, Symbolic = 1, Numeric = 2 };
+
+// Separator forest of the last nested-dissection analysis (CholeskyFactorizerBase.hh:55-59):
+// CParent per component (postordered, -1 for roots), CMember per analysis variable of the
+// reduced ordering graph, at the block size the analysis ran at.
+struct NDOrdering {
+    std::vector<int64_t> CParent, CMember;
+    int blockSize = 1;
+};
 
 // Borrowed view of an upper block-CSC Hessian.
 struct BlockCSCView {
@@ -63,12 +73,18 @@ public:
     // ---- factorization
     void factorizeSymbolic(const BlockCSCView &A, const std::vector<size_t> &pinnedVars = {}) {
         std::vector<int64_t> pins(pinnedVars.begin(), pinnedVars.end());
+        m_fixed.clear();
+        m_rr.clear();
+        m_prr.clear();
         check(mfs_symbolic(m_h, A.numBlocks, A.Ap, A.Ai, A.blockSize, pins.empty() ? nullptr : pins.data(),
                            int64_t(pins.size()), nullptr, nullptr, 0));
         int64_t nf = 0, nr = 0;
         check(mfs_info(m_h, &nf, &nr, nullptr, nullptr, nullptr, nullptr));
         m_n = size_t(nf);
         m_nr = size_t(nr);
+        m_fixed.assign(pinnedVars.begin(), pinnedVars.end());
+        std::sort(m_fixed.begin(), m_fixed.end());
+        m_fixed.erase(std::unique(m_fixed.begin(), m_fixed.end()), m_fixed.end());
     }
     void factorizeNumeric(const BlockCSCView &A, bool /* isInTryCatch */ = false) {
         check(mfs_numeric(m_h, values(A), nullptr, 0.0, 0));
@@ -144,9 +160,48 @@ public:
     }
     bool preferInPlaceSolve() const { return true; }
     bool supportsPrePermutation() const { return true; }
+    bool checkPosDef() const { return factorizationType() == FactorizationType::Numeric; }
+    // this provider never asks for an early symbolic analysis
+    bool wantsSymbolicFactorizationRecompute() const { return false; }
+    bool hasFixedVars() const { return !m_fixed.empty(); }
+    const std::vector<size_t> &getFixedVars() const { return m_fixed; }
+
+    // Separator forest of the last analysis; empty for orderings other than nested
+    // dissection and without a symbolic factorization.
+    std::optional<NDOrdering> ndOrdering() const {
+        if (factorizationType() < FactorizationType::Symbolic) return std::nullopt;
+        int64_t nc = 0, nm = 0;
+        if (mfs_nd_ordering(m_h, &nc, &nm, nullptr, nullptr) != MFS_OK || nc == 0) return std::nullopt;
+        NDOrdering out;
+        out.CParent.resize(size_t(nc));
+        out.CMember.resize(size_t(nm));
+        check(mfs_nd_ordering(m_h, &nc, &nm, out.CParent.data(), out.CMember.data()));
+        int64_t nsn = 0, nst = 0;
+        int32_t vb = 1;
+        check(mfs_supernodes(m_h, &nsn, &nst, &vb, nullptr, nullptr, nullptr, nullptr, nullptr));
+        out.blockSize = vb;
+        return out;
+    }
+
+    // x (n entries) -> its free entries (n_reduced), in the original order or in the
+    // factorization's order (CholeskyFactorizerBase.hh:299-330)
+    void removeFixedEntries(const double *x, double *xr, bool permute = false) const {
+        const std::vector<int64_t> &map = rowMap(permute);
+        for (size_t i = 0; i < m_n; ++i)
+            if (map[i] >= 0) xr[map[i]] = x[i];
+    }
+    // free entries (n_reduced) -> a full vector with zeros on the pinned entries
+    // (CholeskyFactorizerBase.hh:331-363)
+    void extractFullSolution(const double *xr, double *x, bool permute = false) const {
+        const std::vector<int64_t> &map = rowMap(permute);
+        for (size_t i = 0; i < m_n; ++i) x[i] = map[i] >= 0 ? xr[map[i]] : 0.0;
+    }
 
     // ---- stash (CatamariFactorizer.cc:925-948)
-    void stashFactorization() { check(mfs_stash(m_h)); }
+    void stashFactorization() {
+        check(mfs_stash(m_h));
+        m_stash_fixed = m_fixed;
+    }
     bool hasStashedFactorization() const {
         int32_t v = 0;
         check(mfs_has_stash(m_h, &v));
@@ -154,18 +209,27 @@ public:
     }
     void swapStashedFactorization() {
         check(mfs_swap_stash(m_h));
+        std::swap(m_fixed, m_stash_fixed);
+        m_rr.clear();
+        m_prr.clear();
         int64_t nf = 0, nr = 0;
         check(mfs_info(m_h, &nf, &nr, nullptr, nullptr, nullptr, nullptr));
         m_n = size_t(nf);
         m_nr = size_t(nr);
     }
-    void clearStashedFactorization() { check(mfs_clear_stash(m_h)); }
+    void clearStashedFactorization() {
+        check(mfs_clear_stash(m_h));
+        m_stash_fixed.clear();
+    }
     // The sizes follow the factorization state, as in the reference: after
     // clearFactors() a solve fails its size check until the next factorizeSymbolic.
     void clearFactors() {
         check(mfs_clear_factors(m_h));
         m_n = 0;
         m_nr = 0;
+        m_fixed.clear();
+        m_rr.clear();
+        m_prr.clear();
     }
 
     mfs_handle *handle() const { return m_h; }
@@ -186,8 +250,32 @@ private:
         throw std::runtime_error(msg);
     }
 
+    // full row -> reduced row (-1 when pinned), plain or in the factorization's order
+    const std::vector<int64_t> &rowMap(bool permute) const {
+        if (m_rr.size() != m_n) {
+            if (m_n == 0 || factorizationType() < FactorizationType::Symbolic)
+                throw std::runtime_error("no symbolic factorization");
+            m_rr.assign(m_n, -1);
+            size_t next = 0, f = 0;
+            for (size_t i = 0; i < m_n; ++i) {
+                while (f < m_fixed.size() && m_fixed[f] < i) ++f;
+                if (f < m_fixed.size() && m_fixed[f] == i) continue;
+                m_rr[i] = int64_t(next++);
+            }
+            std::vector<int64_t> iperm(m_nr), perm(m_nr);
+            check(mfs_inverse_permutation(m_h, iperm.data()));
+            for (size_t k = 0; k < m_nr; ++k) perm[size_t(iperm[k])] = int64_t(k);
+            m_prr.assign(m_n, -1);
+            for (size_t i = 0; i < m_n; ++i)
+                if (m_rr[i] >= 0) m_prr[i] = perm[size_t(m_rr[i])];
+        }
+        return permute ? m_prr : m_rr;
+    }
+
     mfs_handle *m_h = nullptr;
     size_t m_n = 0, m_nr = 0;
+    std::vector<size_t> m_fixed, m_stash_fixed;    // sorted pinned scalar variables (current, stashed)
+    mutable std::vector<int64_t> m_rr, m_prr;      // row maps (built on first use)
 };
 
 }  // namespace mfs

@@ -52,5 +52,24 @@ int main() {
         caught |= 4;
     }
     std::printf("caught %d\n", caught);
+    // pins, row maps and the separator forest (a fresh analysis: the failed one above
+    // left the handle without a symbolic factorization)
+    f.factorizeSymbolic(A, {0, 1, 2, 7});
+    std::printf("fixed %d %zu posdef %d\n", int(f.hasFixedVars()), f.getFixedVars().size(), int(f.checkPosDef()));
+    std::vector<double> x(f.n()), xr(f.n_reduced()), back(f.n());
+    for (size_t i = 0; i < x.size(); ++i) x[i] = double(i) + 0.5;
+    for (int permute = 0; permute < 2; ++permute) {
+        f.removeFixedEntries(x.data(), xr.data(), permute != 0);
+        std::printf("reduced%d", permute);
+        for (double v : xr) std::printf(" %g", v);
+        std::printf("\n");
+        f.extractFullSolution(xr.data(), back.data(), permute != 0);
+        std::printf("full%d", permute);
+        for (double v : back) std::printf(" %g", v);
+        std::printf("\n");
+    }
+    const auto nd = f.ndOrdering();
+    std::printf("nd %d %zu %zu %d\n", int(nd.has_value()), nd ? nd->CParent.size() : 0, nd ? nd->CMember.size() : 0,
+                nd ? nd->blockSize : 0);
     return 0;
 }

@@ -36,3 +36,14 @@ def test_cpp_adapter_matches_python(tmp_path):
     # solve without a factor -> runtime_error; numeric on an analysis-only handle and a
     # non-upper pattern -> invalid_argument
     assert out[2] == "caught 7"
+    # pins (one partial block: scalar analysis), row maps and the forest against the Python binding
+    f.factorizeSymbolic(H, [0, 1, 2, 7])
+    assert out[3] == "fixed 1 4 posdef 0"
+    x = np.arange(60) + 0.5
+    for permute in (0, 1):
+        xr = np.array([float(v) for v in out[4 + 2 * permute].split()[1:]])
+        assert np.array_equal(xr, f.removeFixedEntries(x, permute=bool(permute)))
+        full = np.array([float(v) for v in out[5 + 2 * permute].split()[1:]])
+        assert np.array_equal(full, f.extractFullSolution(xr, permute=bool(permute)))
+    nd = f.ndOrdering()
+    assert out[8].split() == ["nd", "1", str(nd.CParent.size), str(nd.CMember.size), str(nd.blockSize)]
