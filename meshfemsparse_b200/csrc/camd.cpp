@@ -31,6 +31,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <exception>
 #include <limits>
 #include <numeric>
 #include <queue>
@@ -324,12 +325,21 @@ std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj
     if (nthreads <= 1) {
         for (idx t = 0; t < nt; ++t) run_task(t);
     } else {
+        // an exception must not leave a worker thread (that would terminate the
+        // process): the first one is kept and rethrown on this thread after the join
+        std::vector<std::exception_ptr> errors(size_t(nthreads));
         std::vector<std::thread> pool;
         for (idx th = 0; th < nthreads; ++th)
             pool.emplace_back([&, th] {
-                for (idx t = th; t < nt; t += nthreads) run_task(t);
+                try {
+                    for (idx t = th; t < nt; t += nthreads) run_task(t);
+                } catch (...) {
+                    errors[size_t(th)] = std::current_exception();
+                }
             });
         for (auto &th : pool) th.join();
+        for (auto &e : errors)
+            if (e) std::rethrow_exception(e);
     }
 
     // the separators above the cut, with the subtrees' cliques as initial elements
