@@ -327,7 +327,7 @@ std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj
     } else {
         // an exception must not leave a worker thread (that would terminate the
         // process): the first one is kept and rethrown on this thread after the join
-        std::vector<std::exception_ptr> errors(size_t(nthreads));
+        std::vector<std::exception_ptr> errors(static_cast<size_t>(nthreads));
         std::vector<std::thread> pool;
         for (idx th = 0; th < nthreads; ++th)
             pool.emplace_back([&, th] {
