@@ -255,13 +255,23 @@ std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj
 
     std::vector<std::vector<idx>> perms(nt);
     std::vector<std::vector<std::vector<idx>>> bounds(nt);
-    auto run_task = [&](idx t) {
+    // per-worker maps over the upper vertices, set up once and reset after each task
+    // (a forest of many trees has thousands of subtrees at the cut)
+    struct Scratch {
+        std::vector<idx> hid, umark;
+        idx stamp = 0;
+    };
+    auto run_task = [&](idx t, Scratch &sc) {
+        if (sc.hid.size() != upper.size()) {
+            sc.hid.assign(upper.size(), -1);
+            sc.umark.assign(upper.size(), 0);
+        }
         const auto &vs = verts[t];
         const idx m = idx(vs.size());
         // local graph: the subtree's vertices, then its halo (the upper vertices next to
         // it, labelled after every component and never eliminated: they count in the
         // degrees, as the separators above will be eliminated later)
-        std::vector<idx> hid(upper.size(), -1), halo;
+        std::vector<idx> &hid = sc.hid, halo;
         std::vector<std::vector<idx>> hadj;
         std::vector<idx> lx(m + 1, 0), la, lab(m);
         for (idx a = 0; a < m; ++a) {
@@ -287,6 +297,7 @@ std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj
             la.insert(la.end(), hadj[h].begin(), hadj[h].end());
             lx[m + h + 1] = idx(la.size());
         }
+        for (idx u : halo) hid[local[u]] = -1;
         lab.resize(m + nh, nc);
         std::vector<idx> ord = constrained_md(m + nh, lx, la, {}, lab, nc);
         for (idx &a : ord) a = vs[a];
@@ -294,10 +305,11 @@ std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj
         // every connected part of the subtree leaves its upper neighbours one clique
         std::vector<char> seen(m, 0);
         std::vector<idx> stack, b;
-        std::vector<idx> umark(upper.size(), -1);
+        std::vector<idx> &umark = sc.umark;
         for (idx s0 = 0; s0 < m; ++s0) {
             if (seen[s0]) continue;
             seen[s0] = 1;
+            const idx part = ++sc.stamp;             // marks this connected part's boundary
             stack.assign(1, s0);
             b.clear();
             while (!stack.empty()) {
@@ -307,7 +319,7 @@ std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj
                 for (idx k = xadj[v]; k < xadj[v + 1]; ++k) {
                     const idx u = adj[k];
                     if (owner[u] < 0) {
-                        if (umark[local[u]] != s0) { umark[local[u]] = s0; b.push_back(local[u]); }
+                        if (umark[local[u]] != part) { umark[local[u]] = part; b.push_back(local[u]); }
                     } else if (!seen[local[u]]) {
                         seen[local[u]] = 1;
                         stack.push_back(local[u]);
@@ -323,7 +335,8 @@ std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const idx nthreads = std::min<idx>(idx(hw), nt);
     if (nthreads <= 1) {
-        for (idx t = 0; t < nt; ++t) run_task(t);
+        Scratch sc;
+        for (idx t = 0; t < nt; ++t) run_task(t, sc);
     } else {
         // an exception must not leave a worker thread (that would terminate the
         // process): the first one is kept and rethrown on this thread after the join
@@ -332,7 +345,8 @@ std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj
         for (idx th = 0; th < nthreads; ++th)
             pool.emplace_back([&, th] {
                 try {
-                    for (idx t = th; t < nt; t += nthreads) run_task(t);
+                    Scratch sc;
+                    for (idx t = th; t < nt; t += nthreads) run_task(t, sc);
                 } catch (...) {
                     errors[size_t(th)] = std::current_exception();
                 }
