@@ -54,10 +54,10 @@ def _device_name(device: int) -> str:
 
 
 def measure_step(H, pins, tets, Ke, rhs, single: bool, refine: bool, device: int, small_front_max: int,
-                 tensor_cores: int, repeats: int) -> float:
+                 tensor_cores: int, repeats: int, factor_group: int = 0, solve_subtrees: int = 0) -> float:
     """Best device time (ms) of assemble -> factorize -> solve with these options."""
     f = B200Factorizer(single, refine=refine, device=device, small_front_max=small_front_max,
-                       tensor_cores=tensor_cores)
+                       tensor_cores=tensor_cores, factor_group=factor_group, solve_subtrees=solve_subtrees)
     f.factorizeSymbolic(H, pins)
     f.setElements(tets)
     best = float("inf")
@@ -72,14 +72,22 @@ def measure_step(H, pins, tets, Ke, rhs, single: bool, refine: bool, device: int
 
 def tune(H, pins, tets, Ke, rhs, single: bool = True, refine: bool = True, device: int = 0,
          cutoffs=None, tensor_modes=None, repeats: int = 2, cache: Path | str | None = None,
-         measure: Callable | None = None) -> dict:
-    """Pick small_front_max (and tensor_cores for FP32 + refinement) for this pattern.
+         measure: Callable | None = None, factor_groups=(0,), solve_subtrees=(0,)) -> dict:
+    """Pick small_front_max (and tensor_cores for FP32 + refinement) for this pattern, and,
+    when more than one value is given, the schedule shapes: factor_group (128-column blocks
+    per group of the blocked large-front factorization; 0 = its default) and solve_subtrees
+    (the subtree count the solve cut aims for; 0 = its default).
 
-    Returns {"small_front_max", "tensor_cores", "ms", "candidates", "cached"}; pass the
-    first two to B200Factorizer. `measure(small_front_max, tensor_cores) -> ms` replaces
-    the GPU timing (tests)."""
+    Returns {"small_front_max", "tensor_cores", "factor_group", "solve_subtrees", "ms",
+    "candidates", "cached"}; pass the first four to B200Factorizer.
+    `measure(small_front_max, tensor_cores) -> ms` (or, when groups or subtree counts are
+    tuned, `measure(small_front_max, tensor_cores, factor_group, solve_subtrees)`)
+    replaces the GPU timing (tests)."""
     cache = Path(cache) if cache is not None else default_cache()
+    shapes = len(factor_groups) > 1 or len(solve_subtrees) > 1
     key = pattern_key(H, pins, single, refine, _device_name(device))
+    if shapes:          # a choice among schedule shapes is another entry
+        key += f"|groups={tuple(int(g) for g in factor_groups)}|subtrees={tuple(int(s) for s in solve_subtrees)}"
     store = {}
     if cache.exists():
         try:
@@ -87,20 +95,26 @@ def tune(H, pins, tets, Ke, rhs, single: bool = True, refine: bool = True, devic
         except (OSError, ValueError):
             store = {}
     if key in store:
-        return {**store[key], "cached": True}
+        return {"factor_group": 0, "solve_subtrees": 0, **store[key], "cached": True}
     if cutoffs is None:
         cutoffs = CUTOFFS_FP32 if single else CUTOFFS_FP64
     if tensor_modes is None:
         tensor_modes = (5, 6) if (single and refine) else (0,)
     if measure is None:
-        def measure(cut, tc):
-            return measure_step(H, pins, tets, Ke, rhs, single, refine, device, cut, tc, repeats)
+        def measure(cut, tc, group=0, subtrees=0):
+            return measure_step(H, pins, tets, Ke, rhs, single, refine, device, cut, tc, repeats, group, subtrees)
     cands = []
     for cut in cutoffs:
         for tc in tensor_modes:
-            cands.append({"small_front_max": int(cut), "tensor_cores": int(tc), "ms": float(measure(cut, tc))})
-    best = min(cands, key=lambda c: (c["ms"], c["small_front_max"], c["tensor_cores"]))
-    choice = {"small_front_max": best["small_front_max"], "tensor_cores": best["tensor_cores"], "ms": best["ms"],
+            for group in factor_groups:
+                for sub in solve_subtrees:
+                    ms = measure(cut, tc, group, sub) if shapes else measure(cut, tc)
+                    cands.append({"small_front_max": int(cut), "tensor_cores": int(tc), "factor_group": int(group),
+                                  "solve_subtrees": int(sub), "ms": float(ms)})
+    best = min(cands, key=lambda c: (c["ms"], c["small_front_max"], c["tensor_cores"], c["factor_group"],
+                                     c["solve_subtrees"]))
+    choice = {"small_front_max": best["small_front_max"], "tensor_cores": best["tensor_cores"],
+              "factor_group": best["factor_group"], "solve_subtrees": best["solve_subtrees"], "ms": best["ms"],
               "candidates": cands}
     store[key] = choice
     cache.parent.mkdir(parents=True, exist_ok=True)
