@@ -205,6 +205,10 @@ std::vector<idx> constrained_md(idx nv, const std::vector<idx> &xadj, const std:
 
 }  // namespace
 
+std::vector<idx> quotient_minimum_degree(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj) {
+    return constrained_md(n, xadj, adj, {}, std::vector<idx>(size_t(n), 0));
+}
+
 int camd_cut_depth_from_env() {
     const char *e = std::getenv("MFS_ND_CAMD_CUT_DEPTH");
     if (!e || !*e) return 4;

@@ -88,8 +88,12 @@ std::vector<idx> hierarchical_constrained_md(idx n, const std::vector<idx> &xadj
 // degree).
 int camd_cut_depth_from_env();
 
-// Minimum-degree order of the whole graph (used for the AMD-style mode and for
-// nested-dissection leaves).
+// Minimum degree on a quotient graph (approximate external degrees, element
+// absorption, simplicial mass elimination; ties to the lower vertex): the
+// constrained engine above with a single constraint set.
+std::vector<idx> quotient_minimum_degree(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj);
+
+// Minimum-degree order of the whole graph (the AMD-style mode).
 std::vector<idx> minimum_degree(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj);
 
 // ---------------------------------------------------------------- symbolic --

@@ -628,11 +628,9 @@ NDResult nested_dissection(idx n, const std::vector<idx> &xadj, const std::vecto
 }
 
 std::vector<idx> minimum_degree(idx n, const std::vector<idx> &xadj, const std::vector<idx> &adj) {
-    std::vector<std::vector<idx>> a(n);
-    for (idx v = 0; v < n; ++v)
-        for (idx e = xadj[v]; e < xadj[v + 1]; ++e) if (adj[e] != v) a[v].push_back(adj[e]);
-    std::vector<char> elim(n, 1);
-    return md_local(n, a, elim);
+    // on a quotient graph: an explicit elimination graph (md_local, kept for the small
+    // nested-dissection leaves) grows with the fill and is quadratic on whole meshes
+    return quotient_minimum_degree(n, xadj, adj);
 }
 
 }  // namespace mfs
