@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <functional>
 #include <numeric>
 #include <queue>
 #include <stdexcept>
@@ -134,19 +135,29 @@ void fm_refine(const WGraph &g, std::vector<int8_t> &where, int passes, double i
         return ext - in;
     };
     struct HE { idx gain, v, st; bool operator<(const HE &o) const { return gain < o.gain || (gain == o.gain && v > o.v); } };
+    // max-heaps of (gain, lower vertex first) kept in vectors whose capacity survives
+    // the passes (the same push / pop order as a std::priority_queue)
+    std::vector<HE> heap[2];
+    const std::less<HE> cmp;
+    auto push = [&](int side, HE h) {
+        heap[side].push_back(h);
+        std::push_heap(heap[side].begin(), heap[side].end(), cmp);
+    };
+    std::vector<idx> moves;
     for (int pass = 0; pass < passes; ++pass) {
-        std::priority_queue<HE> heap[2];
+        heap[0].clear();
+        heap[1].clear();
         std::fill(locked.begin(), locked.end(), 0);
         for (idx v = 0; v < n; ++v) {
             gain[v] = compute_gain(v);
             bool boundary = false;
             for (idx e = g.xadj[v]; e < g.xadj[v + 1]; ++e) if (where[g.adj[e]] != where[v]) { boundary = true; break; }
-            if (boundary) heap[where[v]].push({gain[v], v, ++stamp[v]});
+            if (boundary) push(where[v], {gain[v], v, ++stamp[v]});
         }
         idx cut = cut_of(g, where);
         idx best_cut = cut;
         idx best_bal = std::max(pw[0], pw[1]);
-        std::vector<idx> moves;
+        moves.clear();
         idx best_len = 0;
         idx since_best = 0;
         const idx limit = std::max<idx>(25, n / 50);
@@ -157,11 +168,15 @@ void fm_refine(const WGraph &g, std::vector<int8_t> &where, int passes, double i
             for (int attempt = 0; attempt < 2 && v < 0; ++attempt) {
                 int side = attempt == 0 ? from : 1 - from;
                 auto &h = heap[side];
+                auto pop = [&] {
+                    std::pop_heap(h.begin(), h.end(), cmp);
+                    h.pop_back();
+                };
                 while (!h.empty()) {
-                    HE top = h.top();
-                    if (locked[top.v] || top.st != stamp[top.v] || where[top.v] != side) { h.pop(); continue; }
+                    const HE top = h.front();
+                    if (locked[top.v] || top.st != stamp[top.v] || where[top.v] != side) { pop(); continue; }
                     if (pw[1 - side] + g.vw[top.v] > maxside) break;
-                    v = top.v; h.pop();
+                    v = top.v; pop();
                     break;
                 }
             }
@@ -176,7 +191,7 @@ void fm_refine(const WGraph &g, std::vector<int8_t> &where, int passes, double i
                 idx u = g.adj[e];
                 if (locked[u]) continue;
                 gain[u] = compute_gain(u);
-                heap[where[u]].push({gain[u], u, ++stamp[u]});
+                push(where[u], {gain[u], u, ++stamp[u]});
             }
             idx bal = std::max(pw[0], pw[1]);
             bool feasible = bal <= maxside;
