@@ -361,9 +361,60 @@ std::vector<char> cut_vertex_cover(const WGraph &g, const std::vector<int8_t> &w
     return sep;
 }
 
+// The same elimination on bit rows (graphs of up to kBitsetMdMax vertices, the
+// nested-dissection leaves with their halos): a row's popcount is the vertex's
+// degree and the neighbour update is a word-wise OR, so pivots and order are those
+// of the list form below.
+constexpr idx kBitsetMdMax = 4096;
+std::vector<idx> md_local_bits(idx n, const std::vector<std::vector<idx>> &adj0, const std::vector<char> &elim) {
+    const idx W = (n + 63) / 64;
+    std::vector<uint64_t> rows(size_t(n * W), 0);
+    auto row = [&](idx v) { return rows.data() + v * W; };
+    for (idx v = 0; v < n; ++v)
+        for (idx u : adj0[v])
+            if (u != v) row(v)[u >> 6] |= uint64_t(1) << (u & 63);
+    std::vector<idx> deg(n, 0);
+    for (idx v = 0; v < n; ++v)
+        for (idx w = 0; w < W; ++w) deg[v] += idx(__builtin_popcountll(row(v)[w]));
+    std::vector<char> gone(n, 0);
+    idx todo = 0;
+    for (idx v = 0; v < n; ++v) todo += elim[v] ? 1 : 0;
+    std::vector<idx> order;
+    order.reserve(todo);
+    std::vector<uint64_t> nb(static_cast<size_t>(W));
+    while (idx(order.size()) < todo) {
+        idx best = -1, bd = 0;
+        for (idx v = 0; v < n; ++v) {
+            if (!elim[v] || gone[v]) continue;
+            if (best < 0 || deg[v] < bd) { best = v; bd = deg[v]; }
+        }
+        const idx p = best;
+        order.push_back(p);
+        gone[p] = 1;
+        std::copy(row(p), row(p) + W, nb.begin());
+        for (idx w = 0; w < W; ++w)
+            for (uint64_t bits = nb[size_t(w)]; bits; bits &= bits - 1) {
+                const idx u = w * 64 + idx(__builtin_ctzll(bits));
+                uint64_t *ru = row(u);
+                idx d = 0;
+                for (idx x = 0; x < W; ++x) {
+                    ru[x] |= nb[size_t(x)];
+                    if (x == (u >> 6)) ru[x] &= ~(uint64_t(1) << (u & 63));
+                    if (x == (p >> 6)) ru[x] &= ~(uint64_t(1) << (p & 63));
+                    d += idx(__builtin_popcountll(ru[x]));
+                }
+                deg[u] = d;
+            }
+        std::fill(row(p), row(p) + W, 0);
+        deg[p] = 0;
+    }
+    return order;
+}
+
 // Minimum degree on an explicit elimination graph. `elim` marks the vertices
 // to order (the others are halo vertices that stay in the graph).
 std::vector<idx> md_local(idx n, const std::vector<std::vector<idx>> &adj0, const std::vector<char> &elim) {
+    if (n <= kBitsetMdMax) return md_local_bits(n, adj0, elim);
     std::vector<std::vector<idx>> adj = adj0;
     for (auto &a : adj) std::sort(a.begin(), a.end());
     std::vector<char> gone(n, 0);
