@@ -187,10 +187,12 @@ void fm_refine(const WGraph &g, std::vector<int8_t> &where, int passes, double i
             pw[s] -= g.vw[v]; pw[1 - s] += g.vw[v];
             locked[v] = 1;
             moves.push_back(v);
+            // v left side s: for a neighbour on s the edge turns external (+2w), for one on
+            // the other side internal (-2w); the exact gains of the unlocked neighbours
             for (idx e = g.xadj[v]; e < g.xadj[v + 1]; ++e) {
                 idx u = g.adj[e];
                 if (locked[u]) continue;
-                gain[u] = compute_gain(u);
+                gain[u] += where[u] == s ? 2 * g.ew[e] : -2 * g.ew[e];
                 push(where[u], {gain[u], u, ++stamp[u]});
             }
             idx bal = std::max(pw[0], pw[1]);
